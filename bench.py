@@ -1,0 +1,385 @@
+"""Benchmark of the B200 snapshot imager (one JSON line on stdout).
+
+Workload: the W-projection snapshot of the reference's headline
+configuration -- 4096 x 4096 image, 1 arcsec cells, 1,000,000 visibilities
+with uvw uniform in a uv disk and w ~ U[-2000, 2000] lambda, 20 point sources
+(log-uniform 0.1-10 Jy) plus 0.05 Jy noise, Gaussian-Sinc AA kernel S=3,
+32 w-planes, W-kernel support <= 16 (1 % truncation), oversampling 8.
+Synthetic, seeded data (no dataset exists for it).
+
+A step = one full imaging pass of one snapshot through the library (prepass,
+W-planes and FP64 W-kernels, binning, gridding, cuFFT c2r, gcf/normalise).
+value = visibilities imaged per second (Mvis/s), compensated FP32 (FP32C),
+inputs resident in HBM, L2 flushed (256 MB write) before every timed step.
+The FP64 plain form is timed the same way and reported beside it together
+with the FP32C image's error against it.  e2e = the same metric through the
+host-buffer C-ABI call (stpgpu_image_visibilities_ex with host pointers) from
+pinned memory, host->device copies and the image read-back inside the timed
+region.
+
+--impl reference times the reference's algorithm on the host cores (the CPU
+oracle port compiled with the reference's release flags, OpenMP threads in
+place of TBB, scipy FFT with all threads) on a bounded sample of the workload.
+Multi-GPU (torchrun): independent snapshots per rank (replicas; no collective
+on the data path), barrier + max-over-ranks timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mvis/s imaged, comp-FP32 vs FP64 GPU at ≤1e-5 peak-rel err; p50/p99 snapshot ms"
+WORKLOAD = ("W-projection snapshot imager: 4096^2 image, 1 arcsec cells, 1M visibilities, uv disk, "
+            "w~U[-2000,2000] lambda, 32 w-planes, W-kernel support<=16 (1% truncation), GaussianSinc S=3, os=8")
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def _peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for k, nm in enumerate(names):
+                    if f[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+
+    from fastimaging_b200 import capi
+    from fastimaging_b200.synthetic import CONFIG2_IMAGER, config2
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    ctx = capi.Context(local)
+    snap = config2(seed=2 + rank)
+    N = snap.image_size
+    n = snap.vis.size
+    kw = dict(CONFIG2_IMAGER)
+    dev = torch.device("cuda", local)
+    dv = torch.from_numpy(snap.vis).to(dev)
+    dw = torch.from_numpy(snap.weights).to(dev)
+    duvw = torch.from_numpy(np.ascontiguousarray(snap.uvw.T)).to(dev)  # (3, n): column-major n x 3
+    out32 = torch.empty(N * N, dtype=torch.float32, device=dev)
+    out64 = torch.empty(N * N, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    st = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    def step(prec):
+        out = out64 if prec == capi.FP64 else out32
+        odt = capi.F64 if prec == capi.FP64 else capi.F32
+        return ctx.image_visibilities(dv, dw, duvw, N, snap.cell_size, precision=prec, out_dtype=odt,
+                                      device_ptrs=True, image_out=out, **kw)[2]
+
+    def timed(prec, steps, warmup, phases=False):
+        ctx.set_timing(phases)
+        for _ in range(warmup):
+            step(prec)
+        torch.cuda.synchronize(dev)
+        if ws > 1:
+            torch.distributed.barrier()
+        times, grid_ms, launches, info = [], [], 0, None
+        with torch.cuda.stream(st):
+            for _ in range(steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                info = step(prec)
+                e1.record(st)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                grid_ms.append(list(info.phase_ms))
+                launches += info.n_launches
+        torch.cuda.synchronize(dev)
+        if ws > 1:
+            torch.distributed.barrier()
+        ctx.set_timing(False)
+        return times, grid_ms, launches, info
+
+    # parity of the two arms (FP32C against the FP64 plain form)
+    step(capi.FP64)
+    torch.cuda.synchronize(dev)
+    ref64 = out64.double().clone()
+    step(capi.FP32C)
+    torch.cuda.synchronize(dev)
+    d = out32.double() - ref64
+    peak = float(ref64.abs().max())
+    peak_rel = float(d.abs().max()) / peak
+    rms_rel = float(torch.linalg.vector_norm(d) / torch.linalg.vector_norm(ref64))
+
+    t64, ph64, l64, info64 = timed(capi.FP64, args.steps, args.warmup)
+    with Clocks(local) as clk:
+        t32, ph32, l32, info32 = timed(capi.FP32C, args.steps, args.warmup)
+    clocks = clk.summary()
+    _, ph, _, _ = timed(capi.FP32C, max(3, min(args.steps, 10)), 1, phases=True)
+
+    tot32 = sum(t32)
+    tot64 = sum(t64)
+    if ws > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([tot32, tot64], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        tot32, tot64 = float(tt[0]), float(tt[1])
+    value = ws * n * args.steps / (tot32 / 1e3) / 1e6
+    value64 = ws * n * args.steps / (tot64 / 1e3) / 1e6
+
+    # ---- e2e: host buffers (pinned), H2D + image D2H inside the timed region
+    pv = torch.from_numpy(snap.vis).pin_memory()
+    pw = torch.from_numpy(snap.weights).pin_memory()
+    puvw = torch.from_numpy(np.ascontiguousarray(snap.uvw.T).reshape(-1)).pin_memory()  # u[], v[], w[]
+    pimg = torch.empty(N * N, dtype=torch.float32).pin_memory()
+    from fastimaging_b200.capi import AProjPars, ImagerInfo, ImagerPars, WProjPars
+    import ctypes
+
+    ip = ImagerPars(N, 0, snap.cell_size, 1.0, kw["kernel_func"], kw["kernel_support"], 0, kw["oversampling"], 0, 1,
+                    0, 0)
+    wp = WProjPars(kw["num_wplanes"], kw["max_wpconv_support"], kw["undersampling_opt"], kw["kernel_trunc_perc"], 0,
+                   0, 0, 0)
+    ap = AProjPars(0, 0.0, 0.0, 0, 0.0)
+    einfo = ImagerInfo()
+
+    def e2e_step():
+        r = ctx.L.stpgpu_image_visibilities_ex(ctx.h, ctypes.c_void_p(pv.data_ptr()), capi.C128,
+                                               ctypes.c_void_p(pw.data_ptr()), ctypes.c_void_p(puvw.data_ptr()), n,
+                                               ctypes.byref(ip), ctypes.byref(wp), ctypes.byref(ap), capi.FP32C,
+                                               ctypes.c_void_p(pimg.data_ptr()), None, capi.F32, 0,
+                                               ctypes.byref(einfo))
+        if r != 0:
+            raise RuntimeError(ctx.L.stpgpu_last_error(ctx.h).decode())
+        return einfo.device_ms
+
+    for _ in range(args.warmup):
+        e2e_step()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        e2e_ms.append(e2e_step())  # device events around H2D .. D2H on the library stream
+    e2e_tot = sum(e2e_ms)
+    if ws > 1:
+        import torch.distributed as dist
+
+        tt = torch.tensor([e2e_tot], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_tot = float(tt[0])
+    e2e_value = ws * n * args.steps / (e2e_tot / 1e3) / 1e6
+    h2d = snap.vis.nbytes + snap.weights.nbytes + snap.uvw.nbytes
+    d2h = N * N * 4
+    assert abs(float(pimg.double().max()) - float(out32.double().max())) <= 1e-6 * peak
+
+    # ---- roofline of the dominant phase (phase timers over the timed FP32C steps)
+    ph = np.array(ph)  # steps x [grid init, grid loop, FFT, normalise]
+    mean_ph = ph.mean(axis=0)
+    names = ["grid_init", "grid_loop", "fft_c2r", "normalise"]
+    hbm, peak_kind = _peaks()
+    rows = N // 2 + 1
+    items = info32.n_grid_items
+    # algorithmic bytes per launch of each phase
+    alg = {
+        # grid loop: item records (28 B each, FP32) + list entries (4 B) read once, grid written once (FP32 complex)
+        "grid_loop": items * (28 + 4) + rows * N * 8,
+        # c2r FFT: read the half-plane grid, write the N x N image (FP32)
+        "fft_c2r": rows * N * 8 + N * N * 4,
+        # normalise: read image, write image (FP32)
+        "normalise": N * N * 4 * 2,
+        # prepass + W-planes + binning: read vis/uvw/weights, write items, lists
+        "grid_init": n * (16 + 24 + 8) + n * 28 + items * 4 * 2,
+    }
+    dom = int(np.argmax(mean_ph))
+    dom_name = names[dom]
+    achieved = alg[dom_name] / (mean_ph[dom] / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        try:
+            traffic = json.load(open(tfile)).get(dom_name)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
+                "phase_ms": {k: round(float(v), 4) for k, v in zip(names, mean_ph)},
+                "algorithmic_bytes": alg[dom_name]}
+
+    p50 = float(np.percentile(t32, 50))
+    p99 = float(np.percentile(t32, 99))
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": "Mvis/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(tot32 / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (two-sum compensated), FP64 W-kernels/uvw/normalise",
+        "data": "synthetic (seeded point sources + noise, config-2 shapes)",
+        "config": {"workload": WORKLOAD, "n_vis": n, "image_size": N, "precision": "fp32c",
+                   "l2": "flushed (256 MB write) before each timed step", "inputs": "resident in HBM",
+                   "parallelism": f"replicas x{ws}"},
+        "fp64": {"value": round(value64, 2), "ms_per_step": round(tot64 / args.steps, 4)},
+        "fp32c_over_fp64": round(value / value64, 3),
+        "error_vs_fp64": {"peak_rel": peak_rel, "rms_rel": rms_rel, "tolerance": 1e-5},
+        "latency_ms": {"p50": round(p50, 4), "p99": round(p99, 4)},
+        "roofline": roofline,
+        "e2e": {"value": round(e2e_value, 2), "unit": "Mvis/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(l32),
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, snap)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _cpu_one(snap, threads, fast=True):
+    from fastimaging_b200.synthetic import CONFIG2_IMAGER
+    from oracle import stp_oracle as orc
+
+    kw = {k: v for k, v in CONFIG2_IMAGER.items()}
+    t0 = time.perf_counter()
+    orc.image_visibilities(snap.vis, snap.weights, snap.uvw, snap.image_size, snap.cell_size, threads=threads,
+                           fast=fast, **kw)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(args, snap, budget_s=20.0):
+    threads = len(os.sched_getaffinity(0))
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    times = []
+    t_start = time.perf_counter()
+    while True:
+        times.append(_cpu_one(snap, threads))
+        if time.perf_counter() - t_start > budget_s or len(times) >= 3:
+            break
+    n = snap.vis.size
+    v = n * len(times) / sum(times) / 1e6
+    return {"value": round(v, 3), "unit": "Mvis/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} full config-2 snapshot(s) ({n} vis, 4096^2) through the CPU oracle port "
+                      f"(-O3 -ffast-math, OpenMP residue-partitioned gridder, scipy FFT workers={threads})"}
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    from fastimaging_b200.synthetic import config2
+
+    snap = config2(seed=2)
+    threads = len(os.sched_getaffinity(0))
+    for _ in range(max(0, min(args.warmup, 1))):
+        _cpu_one(snap, threads)
+    times = [_cpu_one(snap, threads) for _ in range(max(1, min(args.steps, 3)))]
+    n = snap.vis.size
+    v = n * len(times) / sum(times) / 1e6
+    line = {
+        "metric": METRIC, "value": round(v, 3), "unit": "Mvis/s", "n_gpus": ws, "steps": len(times),
+        "warmup": min(args.warmup, 1), "ms_per_step": round(1e3 * sum(times) / len(times), 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded point sources + noise, config-2 shapes)",
+        "config": {"workload": WORKLOAD, "n_vis": n, "image_size": snap.image_size, "precision": "fp64"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(v, 3), "unit": "Mvis/s", "cores": threads, "kind": "port",
+                         "sample": f"{len(times)} full config-2 snapshot(s) through the CPU oracle port of the "
+                                   f"reference algorithm (reference C++ needs Armadillo/TBB, absent)"},
+        "e2e": {"value": round(v, 3), "unit": "Mvis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl != "reference":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,276 @@
+"""ctypes binding of the C ABI in include/stpgpu.h (libstpgpu.so).
+
+This is the boundary every Python caller goes through; there is no CPU
+fallback: if the library or a CUDA device is missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libstpgpu.so")
+
+# enums (src/stp/types.h:32-89)
+TopHat, Triangle, Sinc, Gaussian, GaussianSinc, PSWF = range(6)
+ZEROMEDIAN, BINMEDIAN, BINAPPROX, NTHELEMENT = range(4)
+FP64, FP32, FP32C = 0, 1, 2
+C128, C64 = 0, 1
+F64, F32 = 0, 1
+
+STATUS = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED", 3: "CUDA", 4: "CUFFT", 5: "OOM", 6: "CAPACITY", 7: "DEVICE",
+          8: "TIMEOUT", 9: "NO_DEVICE"}
+
+
+class StpGpuError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"stpgpu {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class ImagerPars(ctypes.Structure):
+    _fields_ = [("image_size", ctypes.c_int32), ("padded_image_size", ctypes.c_int32), ("cell_size", ctypes.c_double),
+                ("padding_factor", ctypes.c_double), ("kernel_function", ctypes.c_int32),
+                ("kernel_support", ctypes.c_int32), ("kernel_exact", ctypes.c_int32), ("oversampling", ctypes.c_int32),
+                ("generate_beam", ctypes.c_int32), ("gridding_correction", ctypes.c_int32),
+                ("analytic_gcf", ctypes.c_int32), ("r_fft", ctypes.c_int32)]
+
+
+class WProjPars(ctypes.Structure):
+    _fields_ = [("num_wplanes", ctypes.c_int32), ("max_wpconv_support", ctypes.c_int32),
+                ("undersampling_opt", ctypes.c_int32), ("kernel_trunc_perc", ctypes.c_double),
+                ("hankel_opt", ctypes.c_int32), ("hankel_proj_slice", ctypes.c_int32), ("interp_type", ctypes.c_int32),
+                ("wplanes_median", ctypes.c_int32)]
+
+
+class AProjPars(ctypes.Structure):
+    _fields_ = [("num_timesteps", ctypes.c_int32), ("obs_dec", ctypes.c_double), ("obs_ra", ctypes.c_double),
+                ("aproj_opt", ctypes.c_int32), ("aproj_mask_perc", ctypes.c_double)]
+
+
+class ImagerInfo(ctypes.Structure):
+    _fields_ = [("sample_grid_total", ctypes.c_double), ("n_good_vis", ctypes.c_int64),
+                ("n_grid_items", ctypes.c_int64), ("padded_image_size", ctypes.c_int32),
+                ("image_size", ctypes.c_int32), ("num_wplanes", ctypes.c_int32),
+                ("max_plane_support", ctypes.c_int32), ("device_ms", ctypes.c_double),
+                ("phase_ms", ctypes.c_double * 4), ("n_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class Island(ctypes.Structure):
+    _fields_ = [("label_idx", ctypes.c_int32), ("sign", ctypes.c_int32), ("extremum_val", ctypes.c_double),
+                ("extremum_y_idx", ctypes.c_int32), ("extremum_x_idx", ctypes.c_int32),
+                ("num_samples", ctypes.c_int32), ("bbox_top", ctypes.c_int32), ("bbox_bottom", ctypes.c_int32),
+                ("bbox_left", ctypes.c_int32), ("bbox_right", ctypes.c_int32),
+                ("moments_fit", ctypes.c_double * 6), ("leastsq_fit", ctypes.c_double * 6)]
+
+
+class SfPars(ctypes.Structure):
+    _fields_ = [("detection_n_sigma", ctypes.c_double), ("analysis_n_sigma", ctypes.c_double),
+                ("rms_est", ctypes.c_double), ("find_negative_sources", ctypes.c_int32),
+                ("sigma_clip_iters", ctypes.c_int32), ("median_method", ctypes.c_int32),
+                ("gaussian_fitting", ctypes.c_int32), ("ccl_4connectivity", ctypes.c_int32),
+                ("generate_labelmap", ctypes.c_int32), ("source_min_area", ctypes.c_int32),
+                ("ccl_slice_cols", ctypes.c_int32)]
+
+
+class SfInfo(ctypes.Structure):
+    _fields_ = [("bg_level", ctypes.c_double), ("rms_est", ctypes.c_double), ("mean", ctypes.c_double),
+                ("sigma", ctypes.c_double), ("n_labels_pos", ctypes.c_int32), ("n_labels_neg", ctypes.c_int32),
+                ("n_valid_labels", ctypes.c_int32), ("n_islands", ctypes.c_int32), ("device_ms", ctypes.c_double)]
+
+
+EXPORTED = ["stpgpu_abi_version", "stpgpu_create", "stpgpu_destroy", "stpgpu_last_error", "stpgpu_stream",
+            "stpgpu_set_timing", "stpgpu_trim", "stpgpu_image_visibilities", "stpgpu_image_visibilities_ex", "stpgpu_convolve_to_grid",
+            "stpgpu_source_find", "stpgpu_source_find_ex"]
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load libstpgpu.so (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built; run `python -m fastimaging_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        L.stpgpu_abi_version.restype = ctypes.c_int
+        L.stpgpu_create.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.stpgpu_destroy.argtypes = [vp]
+        L.stpgpu_last_error.argtypes = [vp]
+        L.stpgpu_last_error.restype = ctypes.c_char_p
+        L.stpgpu_stream.argtypes = [vp]
+        L.stpgpu_stream.restype = vp
+        L.stpgpu_trim.argtypes = [vp]
+        L.stpgpu_set_timing.argtypes = [vp, ctypes.c_int]
+        L.stpgpu_image_visibilities.argtypes = [vp, vp, vp, vp, ctypes.c_int64, ctypes.POINTER(ImagerPars),
+                                                ctypes.POINTER(WProjPars), ctypes.POINTER(AProjPars), vp, vp,
+                                                ctypes.POINTER(ImagerInfo)]
+        L.stpgpu_image_visibilities_ex.argtypes = [vp, vp, ctypes.c_int, vp, vp, ctypes.c_int64,
+                                                   ctypes.POINTER(ImagerPars), ctypes.POINTER(WProjPars),
+                                                   ctypes.POINTER(AProjPars), ctypes.c_int, vp, vp, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.POINTER(ImagerInfo)]
+        L.stpgpu_convolve_to_grid.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp, vp, vp,
+                                              ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.POINTER(WProjPars), vp, ctypes.c_double,
+                                              ctypes.c_int, vp, vp, ctypes.POINTER(ctypes.c_double)]
+        L.stpgpu_source_find.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(SfPars), vp, vp,
+                                         ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(SfInfo)]
+        L.stpgpu_source_find_ex.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.POINTER(SfPars), vp, ctypes.c_int, vp, ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(SfInfo)]
+        _lib = L
+        return L
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):  # torch tensor
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Context:
+    """One device + stream + cached buffers/plans (stpgpu_context)."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.h = ctypes.c_void_p()
+        st = self.L.stpgpu_create(int(device), ctypes.byref(self.h))
+        if st != 0:
+            raise StpGpuError(st, "stpgpu_create failed")
+
+    def close(self):
+        if self.h:
+            self.L.stpgpu_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise StpGpuError(st, self.L.stpgpu_last_error(self.h).decode())
+
+    def set_timing(self, enable=True):
+        self._check(self.L.stpgpu_set_timing(self.h, int(bool(enable))))
+
+    @property
+    def stream(self):
+        return self.L.stpgpu_stream(self.h)
+
+    # ------------------------------------------------------------ imager
+    def image_visibilities(self, vis, weights, uvw, image_size, cell_size, padding_factor=1.0, kernel_func=PSWF,
+                           kernel_support=3, kernel_exact=True, oversampling=8, generate_beam=False,
+                           gridding_correction=True, analytic_gcf=False, num_wplanes=0, wplanes_median=False,
+                           max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, hankel_opt=False,
+                           aproj_numtimesteps=0, precision=FP64, out_dtype=F64, padded_image_size=0,
+                           device_ptrs=False, image_out=None, beam_out=None):
+        """stp::image_visibilities semantics (sizes used as given).
+
+        Host mode: numpy inputs (vis complex128/complex64 (n,), weights (n,),
+        uvw (n, 3)); returns (image, beam, info) as F-ordered arrays.
+        Device mode: torch CUDA tensors; uvw must be (3, n) contiguous (the
+        column-major n x 3 layout); outputs written into image_out/beam_out.
+        """
+        ip = ImagerPars(int(image_size), int(padded_image_size), float(cell_size), float(padding_factor),
+                        int(kernel_func), int(kernel_support), int(bool(kernel_exact)), int(oversampling),
+                        int(bool(generate_beam)), int(bool(gridding_correction)), int(bool(analytic_gcf)), 0)
+        wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc),
+                       int(bool(hankel_opt)), 0, 0, int(bool(wplanes_median)))
+        ap = AProjPars(int(aproj_numtimesteps), 0.0, 0.0, 0, 0.0)
+        info = ImagerInfo()
+        if device_ptrs:
+            n = int(weights.numel())
+            vdt = C64 if str(vis.dtype).endswith("complex64") else C128
+            self._check(self.L.stpgpu_image_visibilities_ex(self.h, _ptr(vis), vdt, _ptr(weights), _ptr(uvw), n,
+                                                            ctypes.byref(ip), ctypes.byref(wp), ctypes.byref(ap),
+                                                            int(precision), _ptr(image_out), _ptr(beam_out),
+                                                            int(out_dtype), 1, ctypes.byref(info)))
+            return image_out, beam_out, info
+        vis = np.ascontiguousarray(vis)
+        if vis.dtype not in (np.complex128, np.complex64):
+            vis = vis.astype(np.complex128)
+        vdt = C64 if vis.dtype == np.complex64 else C128
+        n = vis.size
+        w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
+        uvwF = np.asfortranarray(np.asarray(uvw, dtype=np.float64).reshape(n, 3))
+        odt = np.float32 if out_dtype == F32 else np.float64
+        img = np.empty((image_size, image_size), dtype=odt, order="F")
+        beam = np.empty((image_size, image_size), dtype=odt, order="F") if generate_beam else None
+        self._check(self.L.stpgpu_image_visibilities_ex(self.h, _ptr(vis), vdt, _ptr(w), _ptr(uvwF), n,
+                                                        ctypes.byref(ip), ctypes.byref(wp), ctypes.byref(ap),
+                                                        int(precision), _ptr(img), _ptr(beam), int(out_dtype), 0,
+                                                        ctypes.byref(info)))
+        if info.image_size == 0:
+            return np.zeros((0, 0)), np.zeros((0, 0)), info
+        return img, (beam if beam is not None else np.zeros((0, 0))), info
+
+    def convolve_to_grid(self, kernel_func, kernel_trunc, support, image_size, uv, vis, weights, kernel_exact=True,
+                         oversampling=1, shift_uv=True, halfplane=True, generate_beam=True, num_wplanes=0,
+                         max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, wplanes_median=False,
+                         w=None, cell_size=0.0, analytic_gcf=True):
+        vis = np.ascontiguousarray(vis, dtype=np.complex128).reshape(-1)
+        n = vis.size
+        uvF = np.asfortranarray(np.asarray(uv, dtype=np.float64).reshape(n, 2))
+        wts = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
+        ww = None if w is None else np.ascontiguousarray(w, dtype=np.float64).reshape(-1)
+        rows = image_size // 2 + 1 if halfplane else image_size
+        vg = np.empty((rows, image_size), dtype=np.complex128, order="F")
+        sg = np.empty((rows, image_size), dtype=np.complex128, order="F") if generate_beam else None
+        wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc), 0,
+                       0, 0, int(bool(wplanes_median)))
+        tot = ctypes.c_double()
+        self._check(self.L.stpgpu_convolve_to_grid(self.h, int(kernel_func), float(kernel_trunc), int(support),
+                                                   int(image_size), _ptr(uvF), _ptr(vis), _ptr(wts), n,
+                                                   int(bool(kernel_exact)), int(oversampling), int(bool(shift_uv)),
+                                                   int(bool(halfplane)), int(bool(generate_beam)), ctypes.byref(wp),
+                                                   _ptr(ww), float(cell_size), int(bool(analytic_gcf)), _ptr(vg),
+                                                   _ptr(sg), ctypes.byref(tot)))
+        return vg, (sg if sg is not None else np.zeros((0, 0), np.complex128)), tot.value
+
+    # ------------------------------------------------------------ source finder
+    def source_find(self, image, detection_n_sigma, analysis_n_sigma, rms_est=0.0, find_negative_sources=True,
+                    sigma_clip_iters=5, median_method=BINAPPROX, gaussian_fitting=False, ccl_4connectivity=False,
+                    generate_labelmap=True, source_min_area=5, ccl_slice_cols=0, want_labels=True,
+                    device_ptrs=False, rows=None, cols=None, label_out=None, capacity=4096):
+        p = SfPars(float(detection_n_sigma), float(analysis_n_sigma), float(rms_est), int(bool(find_negative_sources)),
+                   int(sigma_clip_iters), int(median_method), int(bool(gaussian_fitting)),
+                   int(bool(ccl_4connectivity)), int(bool(generate_labelmap)), int(source_min_area),
+                   int(ccl_slice_cols))
+        info = SfInfo()
+        nis = ctypes.c_int32()
+        if device_ptrs:
+            dt = F32 if str(image.dtype).endswith("float32") else F64
+            r, c = int(rows), int(cols)
+            labels = label_out
+        else:
+            img = np.asfortranarray(image)
+            if img.dtype not in (np.float64, np.float32):
+                img = img.astype(np.float64)
+            dt = F32 if img.dtype == np.float32 else F64
+            r, c = img.shape
+            labels = np.empty((r, c), dtype=np.int32, order="F") if want_labels else None
+        while True:
+            buf = (Island * max(1, capacity))()
+            st = self.L.stpgpu_source_find_ex(self.h, _ptr(image) if device_ptrs else _ptr(img), dt, r, c,
+                                              ctypes.byref(p), _ptr(labels), int(bool(device_ptrs)), buf,
+                                              int(capacity), ctypes.byref(nis), ctypes.byref(info))
+            if st == 6:
+                capacity = nis.value
+                continue
+            self._check(st)
+            break
+        islands = [buf[i] for i in range(nis.value)]
+        return islands, labels, info

@@ -1,0 +1,1373 @@
+// Host orchestration and the extern "C" layer (include/stpgpu.h).
+//
+// One stpgpu_context = one device + one stream + cached scratch buffers and
+// cuFFT plans.  An entry point enqueues its whole pipeline on the context
+// stream and synchronises once at the end to read back the few scalars the
+// caller needs.
+#include <cub/cub.cuh>
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <vector>
+
+#include "common.cuh"
+#include "imager_kernels.cuh"
+#include "sourcefind_kernels.cuh"
+
+using namespace stpgpu;
+
+namespace {
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+} // namespace
+
+struct stpgpu_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timing = false;
+    cudaEvent_t pev[5] = { nullptr, nullptr, nullptr, nullptr, nullptr };
+    std::string err;
+
+    void mark(int k)
+    {
+        if (timing && pev[k])
+            STPGPU_CUDA_TRY(cudaEventRecord(pev[k], stream));
+    }
+    std::map<std::string, DevBuf> bufs;
+    std::map<std::tuple<int, int>, cufftHandle> plans; // (N, cufftType)
+    void* pinned = nullptr;
+    size_t pinned_cap = 0;
+    std::map<std::string, std::string> memo_keys; // buffer name -> key of its current contents
+
+    // True when buffer `name` already holds the data described by `key`
+    // (static tables: gcf, kernel tables, cos tables); records `key`.
+    bool memo(const std::string& name, const std::string& key)
+    {
+        auto it = memo_keys.find(name);
+        if (it != memo_keys.end() && it->second == key)
+            return true;
+        memo_keys[name] = key;
+        return false;
+    }
+
+    // Named scratch buffer, grown on demand (steady state allocates nothing).
+    template <typename T>
+    T* buf(const std::string& name, size_t count)
+    {
+        const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+        DevBuf& b = bufs[name];
+        if (b.cap < bytes) {
+            if (b.p) {
+                STPGPU_CUDA_TRY(cudaStreamSynchronize(stream));
+                STPGPU_CUDA_TRY(cudaFree(b.p));
+                b.p = nullptr;
+                b.cap = 0;
+            }
+            const size_t want = bytes + bytes / 8;
+            STPGPU_CUDA_TRY(cudaMalloc(&b.p, want));
+            b.cap = want;
+            memo_keys.erase(name);
+        }
+        return reinterpret_cast<T*>(b.p);
+    }
+
+    template <typename T>
+    T* host_stage(size_t count)
+    {
+        const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+        if (pinned_cap < bytes) {
+            if (pinned) {
+                STPGPU_CUDA_TRY(cudaStreamSynchronize(stream));
+                cudaFreeHost(pinned);
+            }
+            pinned = nullptr;
+            pinned_cap = 0;
+            STPGPU_CUDA_TRY(cudaMallocHost(&pinned, bytes));
+            pinned_cap = bytes;
+        }
+        return reinterpret_cast<T*>(pinned);
+    }
+
+    cufftHandle plan(int N, cufftType type)
+    {
+        const auto key = std::make_tuple(N, int(type));
+        auto it = plans.find(key);
+        if (it != plans.end())
+            return it->second;
+        cufftHandle h;
+        cufftResult r = cufftPlan2d(&h, N, N, type);
+        if (r != CUFFT_SUCCESS)
+            fail(STPGPU_ERR_CUFFT, "cufftPlan2d failed (" + std::to_string(int(r)) + ") for N=" + std::to_string(N));
+        r = cufftSetStream(h, stream);
+        if (r != CUFFT_SUCCESS)
+            fail(STPGPU_ERR_CUFFT, "cufftSetStream failed");
+        plans[key] = h;
+        return h;
+    }
+
+    void release()
+    {
+        if (stream)
+            cudaStreamSynchronize(stream);
+        for (auto& kv : plans)
+            cufftDestroy(kv.second);
+        plans.clear();
+        for (auto& kv : bufs)
+            if (kv.second.p)
+                cudaFree(kv.second.p);
+        bufs.clear();
+        memo_keys.clear();
+    }
+};
+
+namespace {
+
+std::string fkey(double v)
+{
+    char b[64];
+    std::snprintf(b, sizeof(b), "%a", v);
+    return b;
+}
+
+inline unsigned grid1d(int64_t n, int threads) { return unsigned(std::max<int64_t>(1, ceil_div(n, threads))); }
+
+stpgpu_status guard(stpgpu_context* ctx, const std::function<void()>& f)
+{
+    if (!ctx)
+        return STPGPU_ERR_INVALID_ARG;
+    try {
+        STPGPU_CUDA_TRY(cudaSetDevice(ctx->device));
+        f();
+        ctx->err.clear();
+        return STPGPU_OK;
+    } catch (const Error& e) {
+        ctx->err = e.msg;
+        if (ctx->stream)
+            cudaStreamSynchronize(ctx->stream);
+        return e.status;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return STPGPU_ERR_CUDA;
+    }
+}
+
+double arc_sec_to_rad(double v) { return (v / 3600.0) * (M_PI / 180.0); } // gridder.h:20
+
+// ------------------------------------------------------------------ imager
+
+struct ImagerSetup {
+    int kf = kPSWF;
+    double trunc = 0.0; // functor argument
+    int support = 0;    // AA kernel support
+    int N = 0;          // padded (grid) size
+    int kernel_exact = 0;
+    int os = 1;
+    int shift_uv = 1, halfplane = 1, beam = 0;
+    int analytic = 0;
+    double cell_size = 0.0;
+    int nplanes = 0, max_support = 0, undersampling = 1, wmedian = 0;
+    double trunc_perc = 0.0;
+};
+
+struct GridOut {
+    void* grid = nullptr;
+    void* beam = nullptr;
+    int image_rows = 0;
+    double* d_total = nullptr;             // [0] sample_grid_total
+    unsigned long long* d_ngood = nullptr; // [0] good visibilities
+    uint32_t* d_nitems = nullptr;          // tile-list entries
+    unsigned int* d_err = nullptr;
+    int* d_plane_support = nullptr;
+    int nplanes = 0;
+};
+
+void check_pars(const ImagerSetup& s)
+{
+    if (s.N <= 0 || (s.N % 2) != 0)
+        fail(STPGPU_ERR_INVALID_ARG, "grid size must be a positive even number");
+    if (s.support <= 0)
+        fail(STPGPU_ERR_INVALID_ARG, "kernel_support must be > 0");
+    if (s.nplanes > 0 && s.max_support <= 0)
+        fail(STPGPU_ERR_INVALID_ARG, "max_wpconv_support must be > 0 with W-projection");
+    if (s.nplanes > 65535)
+        fail(STPGPU_ERR_INVALID_ARG, "num_wplanes too large");
+    if (s.nplanes > 0 && s.max_support > 32)
+        fail(STPGPU_ERR_UNSUPPORTED, "max_wpconv_support > 32 is outside the GPU path");
+    if (s.nplanes == 0 && s.support > 32)
+        fail(STPGPU_ERR_UNSUPPORTED, "kernel_support > 32 is outside the GPU path");
+    if (s.os > 4096)
+        fail(STPGPU_ERR_INVALID_ARG, "oversampling too large");
+}
+
+// convolve_to_grid (gridder.h:240-997): grids into context buffers "grid"
+// and "beamgrid" of precision R (complex), image_rows x N column-major.
+template <typename R, int COMP>
+GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, int vis_c64, const double* d_wts,
+    const double* d_uv, int uv_is_pixels, int64_t n)
+{
+    using C2 = typename Cplx<R>::T;
+    check_pars(s);
+    cudaStream_t st = c->stream;
+    GridOut g;
+    const int N = s.N;
+    const bool wproj = s.nplanes > 0;
+    const int conv_support = wproj ? s.max_support : s.support;
+    const int kernel_exact = wproj ? 0 : s.kernel_exact;
+    int os = s.os;
+    if (kernel_exact) {
+        os = 1;
+    } else {
+        os = (os >> 1) << 1;
+        if (os == 0)
+            os = 1;
+    }
+    const int cs = (os / 2) * 2 + 1;
+    const int image_rows = s.halfplane ? N / 2 + 1 : N;
+    g.image_rows = image_rows;
+    const int64_t nn = std::max<int64_t>(n, 1);
+    c->mark(0);
+
+    // ---- prepass (gridder.h:369-423, :504)
+    Item<R>* items = c->buf<Item<R>>("items", nn);
+    const unsigned nb_pre = grid1d(n, GRID_THREADS);
+    double* wpart = c->buf<double>("wpart", nb_pre);
+    unsigned long long* npart = c->buf<unsigned long long>("npart", nb_pre);
+    g.d_total = c->buf<double>("total", 2);
+    g.d_ngood = c->buf<unsigned long long>("ngood", 2);
+    g.d_err = c->buf<unsigned int>("err", 2);
+    STPGPU_CUDA_TRY(cudaMemsetAsync(g.d_err, 0, sizeof(unsigned int), st));
+    PrepassParams pp {};
+    pp.n = n;
+    pp.vis = d_vis;
+    pp.vis_c64 = vis_c64;
+    pp.weights = d_wts;
+    pp.uv = d_uv;
+    pp.uv_is_pixels = uv_is_pixels;
+    pp.inv_px = arc_sec_to_rad(s.cell_size) * double(N); // imager.h:293
+    pp.N = N;
+    pp.conv_support = conv_support;
+    pp.halfplane = s.halfplane;
+    pp.shift_uv = s.shift_uv;
+    pp.kernel_exact = kernel_exact;
+    pp.os = os;
+    pp.keep_w = wproj ? 1 : 0;
+    pp.frac = kernel_exact ? c->buf<double>("frac", 2 * nn) : nullptr;
+    pp.wsum_part = wpart;
+    pp.ngood_part = npart;
+    pp.absw_key = wproj ? c->buf<double>("absw", nn) : nullptr;
+    pp.w_out = nullptr;
+    if (n > 0) {
+        k_prepass<R><<<nb_pre, GRID_THREADS, 0, st>>>(pp, items);
+        STPGPU_CHECK_LAUNCH();
+    }
+    k_finish_wsum<<<1, 1024, 0, st>>>(wpart, npart, n > 0 ? int(nb_pre) : 0, g.d_total, g.d_ngood);
+    STPGPU_CHECK_LAUNCH();
+
+    // ---- kernels
+    const uint32_t* sorted_perm = nullptr;
+    const R* k1d = nullptr;
+    const C2* wconv = nullptr;
+    const R* winv = nullptr;
+    int lh = 0;
+    int* plane_support = nullptr;
+    if (!wproj && !kernel_exact) {
+        // populate_kernel_cache (gridder.h:73-105) as a 1-D table, FP64 on the device
+        const int K = 2 * s.support + 1;
+        const std::string key = std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(s.support)
+            + "/" + std::to_string(os);
+        double* t64 = c->buf<double>("k1d64", size_t(cs) * K);
+        if (!c->memo("k1d64", key)) {
+            k_kernel_table<<<grid1d(cs, 64), 64, 0, st>>>(s.kf, s.trunc, s.support, os, t64);
+            STPGPU_CHECK_LAUNCH();
+        }
+        if (sizeof(R) == 8) {
+            k1d = reinterpret_cast<const R*>(t64);
+        } else {
+            float* t32 = c->buf<float>("k1d32", size_t(cs) * K);
+            if (!c->memo("k1d32", key)) {
+                k_d2f<<<grid1d(int64_t(cs) * K, 256), 256, 0, st>>>(t64, t32, int64_t(cs) * K);
+                STPGPU_CHECK_LAUNCH();
+            }
+            k1d = reinterpret_cast<const R*>(t32);
+        }
+    }
+    if (wproj && n > 0) {
+        const int P = s.nplanes;
+        // |w| order: stable radix sort of the IEEE bits of |w| (non-negative
+        // doubles order as their bit patterns), gridder.h:311-367.
+        const unsigned long long* keys_in = reinterpret_cast<const unsigned long long*>(pp.absw_key);
+        unsigned long long* keys_out = c->buf<unsigned long long>("absw_sorted", nn);
+        uint32_t* perm_in = c->buf<uint32_t>("perm_in", nn);
+        uint32_t* perm = c->buf<uint32_t>("perm", nn);
+        k_iota_u32<<<grid1d(n, 256), 256, 0, st>>>(perm_in, n);
+        STPGPU_CHECK_LAUNCH();
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, perm_in, perm, int(n), 0, 64, st);
+        void* tmp = c->buf<unsigned char>("cubtmp", tb);
+        if (cub::DeviceRadixSort::SortPairs(tmp, tb, keys_in, keys_out, perm_in, perm, int(n), 0, 64, st)
+            != cudaSuccess)
+            fail(STPGPU_ERR_CUDA, "radix sort failed");
+        uint8_t* good_sorted = c->buf<uint8_t>("good_sorted", nn);
+        uint32_t* gflag = c->buf<uint32_t>("gflag", nn + 1);
+        uint32_t* cgood = c->buf<uint32_t>("cgood", nn + 1);
+        k_gather_good<R><<<grid1d(n, 256), 256, 0, st>>>(perm, items, n, good_sorted, gflag);
+        STPGPU_CHECK_LAUNCH();
+        STPGPU_CUDA_TRY(cudaMemsetAsync(gflag + n, 0, sizeof(uint32_t), st));
+        size_t tb2 = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb2, gflag, cgood, int(n + 1), st);
+        void* tmp2 = c->buf<unsigned char>("cubtmp2", tb2);
+        if (cub::DeviceScan::ExclusiveSum(tmp2, tb2, gflag, cgood, int(n + 1), st) != cudaSuccess)
+            fail(STPGPU_ERR_CUDA, "scan failed");
+        int64_t* first = c->buf<int64_t>("pfirst", P);
+        int64_t* last = c->buf<int64_t>("plast", P);
+        double* w_avg = c->buf<double>("wavg", P);
+        const double* absw_sorted = reinterpret_cast<const double*>(keys_out);
+        k_wplanes<<<1, 1, 0, st>>>(cgood, absw_sorted, n, P, s.wmedian, first, last);
+        STPGPU_CHECK_LAUNCH();
+        k_wplane_values<<<P, 256, 0, st>>>(cgood, absw_sorted, good_sorted, first, last, n, P, s.wmedian, w_avg);
+        STPGPU_CHECK_LAUNCH();
+        k_assign_planes<R><<<grid1d(n, 256), 256, 0, st>>>(perm, first, P, n, items);
+        STPGPU_CHECK_LAUNCH();
+        sorted_perm = perm;
+
+        // W-kernels in FP64 (WideFieldImaging, aw_projection.cpp:19-111,173-210,366-452)
+        const int K = 2 * s.max_support + 1;
+        const int u = s.undersampling > 0 ? int(std::pow(2, s.undersampling - 1)) : 0;
+        int workarea = 2;
+        if (u > 0) {
+            while ((workarea / u) < K)
+                workarea *= 2;
+        } else {
+            while (workarea < N)
+                workarea *= 2;
+        }
+        if (workarea < K)
+            fail(STPGPU_ERR_INVALID_ARG, "W-kernel workarea smaller than the kernel size");
+        const double scaling = double(N) / double(workarea);
+        const int arr = workarea * os;
+        if (arr % 2)
+            fail(STPGPU_ERR_INVALID_ARG, "array_size must be multiple of 2 for WideFieldImaging generation.");
+        if (int64_t(arr) * arr > (int64_t(1) << 31))
+            fail(STPGPU_ERR_UNSUPPORTED, "W-kernel array too large");
+        const int half = workarea / 2;
+        const int Lh = std::min(s.max_support * os + os / 2 + 1, arr / 2 + 1);
+        double* aa = c->buf<double>("aa", workarea);
+        if (!c->memo("aa", std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(workarea) + "/"
+                               + std::to_string(s.analytic))) {
+            // ImgDomKernel(kernel_creator, workarea) (gridder.h:486)
+            const int centre = workarea / 2;
+            const int dmax = int(std::floor(s.trunc)) + 1;
+            double ssum = 0.0;
+            for (int d = -std::min(dmax, centre); d <= std::min(dmax, workarea - centre - 1); d++)
+                ssum += kernel_value(s.kf, s.trunc, double(d));
+            const double ksum_inv = ssum > 0.0 ? 1.0 / ssum : 1.0;
+            k_imgdom_kernel<<<grid1d(workarea, 128), 128, 0, st>>>(s.kf, s.trunc, workarea, s.analytic, ksum_inv,
+                dmax, aa);
+            STPGPU_CHECK_LAUNCH();
+        }
+        double* ctab = c->buf<double>("ctab", arr);
+        if (!c->memo("ctab", std::to_string(arr))) {
+            k_cos_table<<<grid1d(arr, 256), 256, 0, st>>>(arr, ctab);
+            STPGPU_CHECK_LAUNCH();
+        }
+        WkParams wq {};
+        wq.w_avg = w_avg;
+        wq.aa = aa;
+        wq.ctab = ctab;
+        wq.half = half;
+        wq.arr = arr;
+        wq.os = os;
+        wq.cs = cs;
+        wq.max_support = s.max_support;
+        wq.lh_max = Lh;
+        // WideFieldImaging gets real_t(arc_sec_to_rad(cell)), scaled by N/workarea
+        wq.scaled_cell = arc_sec_to_rad(s.cell_size) * scaling;
+        wq.trunc_perc = s.trunc_perc;
+        wq.Qs = c->buf<double2>("wkQ", size_t(P) * half * half);
+        wq.Ts = c->buf<double2>("wkT", size_t(P) * Lh * half);
+        wq.convd = c->buf<double2>("wkconv", size_t(P) * Lh * Lh);
+        wq.invd = c->buf<double>("wkinv", size_t(P) * cs * cs);
+        plane_support = c->buf<int>("psupport", P);
+        wq.support = plane_support;
+        k_wkernel_plane<<<P, 256, 0, st>>>(wq);
+        STPGPU_CHECK_LAUNCH();
+        if (sizeof(R) == 8) {
+            wconv = reinterpret_cast<const C2*>(wq.convd);
+            winv = reinterpret_cast<const R*>(wq.invd);
+        } else {
+            float2* cf = c->buf<float2>("wkconv32", size_t(P) * Lh * Lh);
+            float* inf = c->buf<float>("wkinv32", size_t(P) * cs * cs);
+            const int64_t nconv = int64_t(P) * Lh * Lh, ninv = int64_t(P) * cs * cs;
+            k_wk_to_f32<<<grid1d(std::max(nconv, ninv), 256), 256, 0, st>>>(wq.convd, wq.invd, nconv, ninv, cf, inf);
+            STPGPU_CHECK_LAUNCH();
+            wconv = reinterpret_cast<const C2*>(cf);
+            winv = reinterpret_cast<const R*>(inf);
+        }
+        lh = Lh;
+        g.d_plane_support = plane_support;
+        g.nplanes = P;
+    }
+
+    // ---- binning into 32x32 uv tiles
+    const int tiles_r = int(ceil_div(image_rows, TILE_R));
+    const int tiles_c = int(ceil_div(N, TILE_C));
+    const int ntiles = tiles_r * tiles_c;
+    uint32_t* tcount = c->buf<uint32_t>("tcount", ntiles + 1);
+    uint32_t* toff = c->buf<uint32_t>("toff", ntiles + 1);
+    uint32_t* tcur = c->buf<uint32_t>("tcur", ntiles + 1);
+    const int Kx = 2 * conv_support + 1;
+    const uint64_t per_dim = uint64_t(ceil_div(Kx - 1, std::min(TILE_R, TILE_C))) + 2;
+    const uint64_t cap = std::max<uint64_t>(1, uint64_t(nn) * 2 * per_dim * per_dim);
+    if (cap > 0xffffffffull)
+        fail(STPGPU_ERR_INVALID_ARG, "too many visibilities for one snapshot");
+    uint32_t* list = c->buf<uint32_t>("tlist", cap);
+    BinParams bp {};
+    bp.N = N;
+    bp.image_rows = image_rows;
+    bp.tiles_r = tiles_r;
+    bp.tiles_c = tiles_c;
+    bp.support = s.support;
+    bp.plane_support = plane_support;
+    bp.exact = kernel_exact;
+    bp.n = n;
+    bp.tile_count = tcount;
+    bp.tile_off = toff;
+    bp.tile_cursor = tcur;
+    bp.list = list;
+    bp.list_capacity = cap;
+    bp.err = g.d_err;
+    STPGPU_CUDA_TRY(cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (ntiles + 1), st));
+    STPGPU_CUDA_TRY(cudaMemsetAsync(tcur, 0, sizeof(uint32_t) * (ntiles + 1), st));
+    if (n > 0) {
+        k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items);
+        STPGPU_CHECK_LAUNCH();
+    }
+    k_scan_single<<<1, 1024, 0, st>>>(tcount, toff, ntiles);
+    STPGPU_CHECK_LAUNCH();
+    if (n > 0) {
+        k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, wproj ? sorted_perm : nullptr);
+        STPGPU_CHECK_LAUNCH();
+    }
+    g.d_nitems = toff + ntiles;
+
+    // ---- tile gridding
+    C2* grid = c->buf<C2>("grid", size_t(image_rows) * N);
+    C2* beam = s.beam ? c->buf<C2>("beamgrid", size_t(image_rows) * N) : nullptr;
+    GridParams<R> gp {};
+    gp.N = N;
+    gp.image_rows = image_rows;
+    gp.tiles_r = tiles_r;
+    gp.support = s.support;
+    gp.os = os;
+    gp.cs = cs;
+    gp.exact_wrap = kernel_exact;
+    gp.items = items;
+    gp.tile_off = toff;
+    gp.list = list;
+    gp.k1d = k1d;
+    gp.kf = s.kf;
+    gp.trunc = s.trunc;
+    gp.frac = pp.frac;
+    gp.n = n;
+    gp.wconv = wconv;
+    gp.winv = winv;
+    gp.lh = lh;
+    gp.plane_support = plane_support;
+    gp.grid = grid;
+    gp.beam = beam;
+    using A = Acc<R, COMP>;
+    size_t smem = size_t(TILE_R) * TILE_C * sizeof(A) * (s.beam ? 2 : 1);
+    if (!wproj && !kernel_exact)
+        smem += sizeof(R) * size_t(cs) * (2 * s.support + 1);
+    auto launch = [&](auto kern) {
+        if (smem > 48 * 1024)
+            STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        c->mark(1);
+        kern<<<ntiles, 32, smem, st>>>(gp);
+        STPGPU_CHECK_LAUNCH();
+        c->mark(2);
+    };
+    if (2 * conv_support + 1 > 65)
+        fail(STPGPU_ERR_UNSUPPORTED, "kernel support > 32 is outside the GPU path");
+    if (wproj && n > 0) {
+        if (s.beam)
+            launch(k_grid_tiles<R, COMP, KM_WPROJ, true>);
+        else
+            launch(k_grid_tiles<R, COMP, KM_WPROJ, false>);
+    } else if (kernel_exact) {
+        if (s.beam)
+            launch(k_grid_tiles<R, COMP, KM_EXACT, true>);
+        else
+            launch(k_grid_tiles<R, COMP, KM_EXACT, false>);
+    } else if (!wproj) {
+        if (s.beam)
+            launch(k_grid_tiles<R, COMP, KM_SEP, true>);
+        else
+            launch(k_grid_tiles<R, COMP, KM_SEP, false>);
+    } else {
+        STPGPU_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(C2) * size_t(image_rows) * N, st));
+        if (beam)
+            STPGPU_CUDA_TRY(cudaMemsetAsync(beam, 0, sizeof(C2) * size_t(image_rows) * N, st));
+    }
+    g.grid = grid;
+    g.beam = beam;
+    return g;
+}
+
+struct ScalarsBack {
+    double total;
+    unsigned long long ngood;
+    uint32_t nitems;
+    unsigned int err;
+    int max_support;
+};
+
+ScalarsBack read_back(stpgpu_context* c, const GridOut& g)
+{
+    std::vector<int> sup(g.nplanes);
+    struct Stage {
+        double total;
+        unsigned long long ngood;
+        uint32_t nitems;
+        unsigned int err;
+    };
+    Stage* h = c->host_stage<Stage>(1);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&h->total, g.d_total, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    STPGPU_CUDA_TRY(
+        cudaMemcpyAsync(&h->ngood, g.d_ngood, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&h->nitems, g.d_nitems, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&h->err, g.d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
+    if (g.nplanes > 0)
+        STPGPU_CUDA_TRY(
+            cudaMemcpyAsync(sup.data(), g.d_plane_support, sizeof(int) * g.nplanes, cudaMemcpyDeviceToHost, c->stream));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    ScalarsBack r { h->total, h->ngood, h->nitems, h->err, 0 };
+    for (int v : sup)
+        r.max_support = std::max(r.max_support, v);
+    if (r.err)
+        fail(STPGPU_ERR_DEVICE, "gridder reported internal error flags " + std::to_string(r.err));
+    return r;
+}
+
+template <typename R>
+const double* device_gcf(stpgpu_context* c, const ImagerSetup& s)
+{
+    double* gcf = c->buf<double>("gcf", s.N);
+    if (c->memo("gcf", std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(s.N) + "/"
+                          + std::to_string(s.analytic)))
+        return gcf;
+    double ksum_inv = 1.0;
+    const int dmax = int(std::floor(s.trunc)) + 1;
+    if (!s.analytic) {
+        const int centre = s.N / 2;
+        double ssum = 0.0;
+        for (int d = -std::min(dmax, centre); d <= std::min(dmax, s.N - centre - 1); d++)
+            ssum += kernel_value(s.kf, s.trunc, double(d));
+        ksum_inv = ssum > 0.0 ? 1.0 / ssum : 1.0;
+    }
+    k_imgdom_kernel<<<grid1d(s.N, 256), 256, 0, c->stream>>>(s.kf, s.trunc, s.N, s.analytic, ksum_inv, dmax, gcf);
+    STPGPU_CHECK_LAUNCH();
+    return gcf;
+}
+
+// stp::image_visibilities (imager.h:233-376) on device buffers.  The whole
+// pipeline is enqueued without a host round trip; the normalisation reads
+// the sampling total on the device, and the scalars are read back once at
+// the end (an empty result, imager.h:355, is reported then).
+template <typename R, int COMP>
+void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const void* d_vis,
+    int vis_c64, const double* d_wts, const double* d_uvw, int64_t n, void* d_image, void* d_beam, int out_f32,
+    stpgpu_imager_info* info)
+{
+    if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
+        fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
+    cudaStream_t st = c->stream;
+    GridOut g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n);
+    const int N = s.N;
+    R* img = c->buf<R>("fftimg", size_t(N) * N);
+    const cufftType type = sizeof(R) == 8 ? CUFFT_Z2D : CUFFT_C2R;
+    cufftHandle h = c->plan(N, type);
+    auto exec = [&](void* in, R* out) {
+        cufftResult r;
+        if (sizeof(R) == 8)
+            r = cufftExecZ2D(h, reinterpret_cast<cufftDoubleComplex*>(in), reinterpret_cast<cufftDoubleReal*>(out));
+        else
+            r = cufftExecC2R(h, reinterpret_cast<cufftComplex*>(in), reinterpret_cast<cufftReal*>(out));
+        if (r != CUFFT_SUCCESS)
+            fail(STPGPU_ERR_CUFFT, "cuFFT c2r execution failed (" + std::to_string(int(r)) + ")");
+    };
+    const double* gcf = correction ? device_gcf<R>(c, s) : nullptr;
+    const dim3 ngrid(grid1d(image_size, 256), image_size);
+    auto normalise = [&](void* out) {
+        if (out_f32)
+            k_normalise<R, float><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, gcf, correction,
+                reinterpret_cast<float*>(out));
+        else
+            k_normalise<R, double><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, gcf, correction,
+                reinterpret_cast<double*>(out));
+        STPGPU_CHECK_LAUNCH();
+    };
+    exec(g.grid, img);
+    c->mark(3);
+    normalise(d_image);
+    c->mark(4);
+    if (s.beam && d_beam) {
+        exec(g.beam, img);
+        normalise(d_beam);
+    }
+    const ScalarsBack sb = read_back(c, g);
+    if (info) {
+        info->sample_grid_total = sb.total;
+        info->n_good_vis = int64_t(sb.ngood);
+        info->n_grid_items = sb.nitems;
+        info->padded_image_size = N;
+        info->num_wplanes = s.nplanes;
+        info->max_plane_support = sb.max_support;
+        info->image_size = sb.total > 0.0 ? image_size : 0;
+        if (c->timing) {
+            float ms[4] = { 0, 0, 0, 0 };
+            for (int k = 0; k < 4; k++)
+                STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms[k], c->pev[k], c->pev[k + 1]));
+            for (int k = 0; k < 4; k++)
+                info->phase_ms[k] = ms[k];
+        }
+    }
+}
+
+ImagerSetup setup_from(const stpgpu_imager_pars* p, const stpgpu_wproj_pars* w, const stpgpu_aproj_pars* a,
+    int& image_size)
+{
+    if (!p)
+        fail(STPGPU_ERR_INVALID_ARG, "null imager parameters");
+    if (a && a->num_timesteps > 0)
+        fail(STPGPU_ERR_UNSUPPORTED, "A-projection is outside the GPU path");
+    if (w && w->num_wplanes > 0 && w->hankel_opt)
+        fail(STPGPU_ERR_UNSUPPORTED, "Hankel-transform W-kernels are outside the GPU path");
+    if (p->kernel_function < 0 || p->kernel_function > 5)
+        fail(STPGPU_ERR_INVALID_ARG, "unknown kernel function");
+    if (!(p->cell_size > 0.0))
+        fail(STPGPU_ERR_INVALID_ARG, "cell_size must be > 0");
+    if (!(p->padding_factor >= 1.0))
+        fail(STPGPU_ERR_INVALID_ARG, "padding_factor must be >= 1");
+    ImagerSetup s;
+    image_size = p->image_size;
+    s.N = p->padded_image_size > 0 ? p->padded_image_size : int(unsigned(double(image_size) * p->padding_factor));
+    s.kf = p->kernel_function;
+    s.support = p->kernel_support;
+    s.trunc = double(p->kernel_support);
+    s.kernel_exact = p->kernel_exact;
+    s.os = p->oversampling;
+    s.beam = p->generate_beam;
+    s.analytic = p->analytic_gcf;
+    s.cell_size = p->cell_size;
+    s.shift_uv = 1;
+    s.halfplane = 1;
+    if (w && w->num_wplanes > 0) {
+        if (p->kernel_exact)
+            fail(STPGPU_ERR_INVALID_ARG, "W-projection cannot be used with kernel_exact (imager.h:287)");
+        s.nplanes = w->num_wplanes;
+        s.max_support = w->max_wpconv_support;
+        s.undersampling = w->undersampling_opt;
+        s.trunc_perc = w->kernel_trunc_perc;
+        s.wmedian = w->wplanes_median;
+    }
+    if (!p->kernel_exact && p->oversampling < 1)
+        fail(STPGPU_ERR_INVALID_ARG, "oversampling must be >= 1 when kernel_exact is false");
+    return s;
+}
+
+template <typename T>
+T* to_device(stpgpu_context* c, const char* name, const void* host, size_t count)
+{
+    T* d = c->buf<T>(name, count);
+    if (count)
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(d, host, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
+    return d;
+}
+
+// ------------------------------------------------------------------ source finder
+
+// Exact k-th order statistic (0-based) by 16-bit radix select.
+template <typename T>
+double select_kth(stpgpu_context* c, const T* x, int64_t n, unsigned long long k)
+{
+    cudaStream_t st = c->stream;
+    unsigned int* hist = c->buf<unsigned int>("rsel_hist", 65536);
+    unsigned long long* state = c->buf<unsigned long long>("rsel_state", 3);
+    unsigned long long h0[3] = { k, 0ull, 0ull };
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(state, h0, sizeof(h0), cudaMemcpyHostToDevice, st));
+    unsigned long long* hs = c->host_stage<unsigned long long>(3);
+    for (int pass = 3; pass >= 0; pass--) {
+        const int shift = pass * 16;
+        STPGPU_CUDA_TRY(cudaMemsetAsync(hist, 0, sizeof(unsigned int) * 65536, st));
+        // prefix/mask are read on the host after each pass
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hs, state, sizeof(h0), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+        k_radix_hist<T><<<std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 16), SF_THREADS, 0, st>>>(x, n, hs[1],
+            hs[2], shift, hist);
+        STPGPU_CHECK_LAUNCH();
+        k_radix_pick<<<1, 1024, 0, st>>>(hist, shift, state);
+        STPGPU_CHECK_LAUNCH();
+    }
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(hs, state, sizeof(h0), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    // key -> double
+    const unsigned long long key = hs[1];
+    const unsigned long long u = (key >> 63) ? (key & 0x7fffffffffffffffull) : ~key;
+    double v;
+    std::memcpy(&v, &u, sizeof(v));
+    return v;
+}
+
+// mat_median_exact (matrix_math.cpp:20-48)
+template <typename T>
+double median_exact(stpgpu_context* c, const T* x, int64_t n)
+{
+    const unsigned long long k = (unsigned long long)(n / 2);
+    const double v1 = select_kth(c, x, n, k);
+    if (n & 1)
+        return v1;
+    const double v2 = select_kth(c, x, n, k - 1);
+    return (v1 + v2) / 2;
+}
+
+template <typename T>
+void mean_sigma(stpgpu_context* c, const T* x, int64_t n, double& mean, double& sigma)
+{
+    cudaStream_t st = c->stream;
+    const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8);
+    double* part = c->buf<double>("sf_part", 3 * size_t(nb));
+    double* out = c->buf<double>("sf_out", 4);
+    k_sum_sq<T><<<nb, SF_THREADS, 0, st>>>(x, n, part);
+    STPGPU_CHECK_LAUNCH();
+    k_finish_parts<2><<<1, 256, 0, st>>>(part, int(nb), out);
+    STPGPU_CHECK_LAUNCH();
+    double* h = c->host_stage<double>(4);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    mean = h[0] / double(n);
+    sigma = std::sqrt(h[1] / double(n) - mean * mean);
+}
+
+// mat_median_binapprox (matrix_math.cpp:334-455)
+template <typename T>
+double median_binapprox(stpgpu_context* c, const T* x, int64_t n, double mean, double sigma)
+{
+    const int N = BINS_N;
+    if ((sigma * 2) < 0.0001)
+        return median_exact(c, x, n);
+    cudaStream_t st = c->stream;
+    const double scalefactor = double(N) / (2 * sigma);
+    const double leftend = mean - sigma;
+    unsigned long long* bins = c->buf<unsigned long long>("sf_bins", N + 2);
+    STPGPU_CUDA_TRY(cudaMemsetAsync(bins, 0, sizeof(unsigned long long) * (N + 2), st));
+    k_hist<T><<<std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8), SF_THREADS, 0, st>>>(x, n, leftend, scalefactor,
+        bins);
+    STPGPU_CHECK_LAUNCH();
+    unsigned long long* h = c->host_stage<unsigned long long>(N + 2);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, bins, sizeof(unsigned long long) * (N + 2), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<unsigned long long> b(h, h + N + 1);
+    const unsigned long long bottom = h[N + 1];
+    if (n & 1) {
+        const unsigned long long k = (unsigned long long)(n + 1) / 2;
+        unsigned long long count = bottom;
+        for (int i = 0; i < N + 1; i++) {
+            count += b[i];
+            if (count >= k)
+                return double(i + 0.5) / scalefactor + leftend;
+        }
+    } else {
+        const unsigned long long k = (unsigned long long)n / 2;
+        unsigned long long count = bottom;
+        for (int i = 0; i < N + 1; i++) {
+            count += b[i];
+            if (count >= k) {
+                int j = i;
+                while (count == k) {
+                    j++;
+                    count += b[j];
+                    if (j == N)
+                        break;
+                }
+                return double(i + j + 1) / (2 * scalefactor) + leftend;
+            }
+        }
+    }
+    return median_exact(c, x, n);
+}
+
+// estimate_rms (sourcefind.cpp:22-154), num_sigma = 3
+template <typename T>
+double estimate_rms(stpgpu_context* c, const T* x, int64_t n, double num_sigma, int iters, double mean, double sigma,
+    double median)
+{
+    cudaStream_t st = c->stream;
+    const double m = mean - median;
+    double s = sigma;
+    double d1 = m * double(n), d2 = (s * s + m * m) * double(n);
+    unsigned long long valid = (unsigned long long)n;
+    double prev_upper = 1.7976931348623157e308;
+    const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8);
+    double* part = c->buf<double>("sf_part", 3 * size_t(nb));
+    double* out = c->buf<double>("sf_out", 4);
+    double* h = c->host_stage<double>(4);
+    for (int it = 0; it < iters; it++) {
+        const double upper = num_sigma * s;
+        k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, median, upper, prev_upper, part);
+        STPGPU_CHECK_LAUNCH();
+        k_finish_parts<3><<<1, 256, 0, st>>>(part, int(nb), out);
+        STPGPU_CHECK_LAUNCH();
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(h, out, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+        const unsigned long long rem = (unsigned long long)(h[2] + 0.5);
+        if (rem == 0)
+            break;
+        valid -= rem;
+        d1 -= h[0];
+        d2 -= h[1];
+        s = std::sqrt(d2 / double(valid) - (d1 / double(valid)) * (d1 / double(valid)));
+        prev_upper = upper;
+    }
+    return s;
+}
+
+unsigned long long host_okey(double v)
+{
+    unsigned long long u;
+    std::memcpy(&u, &v, sizeof(u));
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+// Gaussian2dParams::convert_to_constrained_parameters (fitting.cpp:32-57)
+void constrain(double* g)
+{
+    const double half_pi = M_PI / 2.0;
+    g[3] = std::fabs(g[3]);
+    g[4] = std::fabs(g[4]);
+    if (g[3] < g[4]) {
+        std::swap(g[3], g[4]);
+        g[5] += half_pi;
+    }
+    double t = std::fmod(g[5], M_PI);
+    if (t <= -half_pi)
+        t += M_PI;
+    else if (t > half_pi)
+        t -= M_PI;
+    g[5] = t;
+}
+
+// IslandParams::estimate_moments_fit (sourcefind.cpp:691-717)
+void moments_fit(int sign, double extremum, const double* mb, double rms, double ana_sigma, double* g)
+{
+    const double xx = mb[2], yy = mb[3], xy = mb[4];
+    const double w1 = (xx + yy) / 2.0;
+    const double w2 = std::sqrt(((xx - yy) * (xx - yy) / 4) + xy * xy);
+    const double tmaj = w1 + w2, tmin = w1 - w2;
+    const double thr = ana_sigma * rms;
+    const double ratio = sign * extremum / thr;
+    const double scale = 1.0 - std::log(ratio) / (ratio - 1.0);
+    double theta = 0.5 * std::atan(2.0 * xy / (xx - yy));
+    if (theta * xy < 0.0)
+        theta += M_PI / 2.0;
+    g[0] = extremum;
+    g[1] = mb[0];
+    g[2] = mb[1];
+    g[3] = std::sqrt(tmaj / scale);
+    g[4] = std::sqrt(tmin / scale);
+    g[5] = theta;
+    constrain(g);
+}
+
+template <typename T>
+void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, const stpgpu_sf_pars& p, int32_t* d_labels,
+    std::vector<stpgpu_island>& islands, stpgpu_sf_info& info)
+{
+    if (rows <= 0 || cols <= 0 || (rows % 2) || (cols % 2))
+        fail(STPGPU_ERR_INVALID_ARG, "image dimensions must be positive and even (ccl.h:116-117)");
+    if (rows > 65536 || cols > 65536 || int64_t(rows) * cols >= (int64_t(1) << 32))
+        fail(STPGPU_ERR_INVALID_ARG, "image too large for the labeler (ccl.h:118-119)");
+    if (p.gaussian_fitting)
+        fail(STPGPU_ERR_UNSUPPORTED, "Gaussian least-squares fitting (Ceres) is outside the GPU path");
+    cudaStream_t st = c->stream;
+    const int64_t n = int64_t(rows) * cols;
+    double mean = 0.0, sigma = 0.0, median = 0.0;
+    bool have_ms = false;
+    switch (p.median_method) {
+    case STPGPU_ZEROMEDIAN:
+        median = 0.0;
+        break;
+    case STPGPU_BINAPPROX:
+        mean_sigma(c, d_img, n, mean, sigma);
+        have_ms = true;
+        median = median_binapprox(c, d_img, n, mean, sigma);
+        break;
+    case STPGPU_BINMEDIAN: // successive binning ends in nth_element: the exact median
+        mean_sigma(c, d_img, n, mean, sigma);
+        have_ms = true;
+        median = median_exact(c, d_img, n);
+        break;
+    case STPGPU_NTHELEMENT:
+        median = median_exact(c, d_img, n);
+        break;
+    default:
+        fail(STPGPU_ERR_INVALID_ARG, "unknown median method");
+    }
+    const double bg = median;
+    double rms;
+    if (std::fabs(p.rms_est) > 0.0) {
+        rms = p.rms_est;
+    } else {
+        if (!have_ms)
+            mean_sigma(c, d_img, n, mean, sigma);
+        rms = estimate_rms(c, d_img, n, 3, p.sigma_clip_iters, mean, sigma, median);
+    }
+    info.bg_level = bg;
+    info.rms_est = rms;
+    info.mean = mean;
+    info.sigma = sigma;
+    // thresholds (sourcefind.cpp:298-301)
+    const double a_pos = bg + p.analysis_n_sigma * rms;
+    const double a_neg = bg - p.analysis_n_sigma * rms;
+    const double d_pos = bg + p.detection_n_sigma * rms;
+    const double d_neg = bg - p.detection_n_sigma * rms;
+
+    // ---- connected components
+    CclGeom geom { rows, cols, rows / 2, cols / 2 };
+    uint8_t* cls = c->buf<uint8_t>("ccl_cls", n);
+    uint32_t* P = c->buf<uint32_t>("ccl_P", n);
+    uint32_t* R = c->buf<uint32_t>("ccl_R", n);
+    unsigned int* err = c->buf<unsigned int>("ccl_err", 2);
+    int32_t* L = d_labels ? d_labels : c->buf<int32_t>("ccl_L", n);
+    STPGPU_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), st));
+    const int slice = p.ccl_slice_cols > 0 ? p.ccl_slice_cols : std::max(2, cols / 8);
+    k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, geom, a_pos, a_neg, p.find_negative_sources, cls, P);
+    STPGPU_CHECK_LAUNCH();
+    k_ccl_union<<<grid1d(n, 256), 256, 0, st>>>(cls, geom, p.ccl_4connectivity, slice, P, err);
+    STPGPU_CHECK_LAUNCH();
+    k_ccl_flatten<<<grid1d(n, 256), 256, 0, st>>>(cls, n, P, err);
+    STPGPU_CHECK_LAUNCH();
+    const int nchunks = int(ceil_div(n, RANK_CHUNK));
+    uint32_t* cpos = c->buf<uint32_t>("ccl_cpos", nchunks + 1);
+    uint32_t* cneg = c->buf<uint32_t>("ccl_cneg", nchunks + 1);
+    uint32_t* opos = c->buf<uint32_t>("ccl_opos", nchunks + 1);
+    uint32_t* oneg = c->buf<uint32_t>("ccl_oneg", nchunks + 1);
+    k_ccl_rootcount<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, cpos, cneg);
+    STPGPU_CHECK_LAUNCH();
+    k_scan_single<<<1, 1024, 0, st>>>(cpos, opos, nchunks);
+    k_scan_single<<<1, 1024, 0, st>>>(cneg, oneg, nchunks);
+    STPGPU_CHECK_LAUNCH();
+    k_ccl_rank<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, opos, oneg, R);
+    STPGPU_CHECK_LAUNCH();
+    k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(cls, P, R, geom, L);
+    STPGPU_CHECK_LAUNCH();
+    uint32_t* hcnt = c->host_stage<uint32_t>(4);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[0], opos + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[1], oneg + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[2], err, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hcnt[2])
+        fail(STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)");
+    const int np = int(hcnt[0]), nneg = int(hcnt[1]);
+    info.n_labels_pos = np;
+    info.n_labels_neg = nneg;
+
+    // ---- extrema, detection filter, moments (sourcefind.cpp:342-628)
+    const int nl = std::max(1, np + nneg);
+    unsigned long long* ext = c->buf<unsigned long long>("sf_ext", nl);
+    unsigned long long* eidx = c->buf<unsigned long long>("sf_eidx", nl);
+    double* mom = c->buf<double>("sf_mom", 6 * size_t(nl));
+    int* ns = c->buf<int>("sf_ns", nl);
+    uint32_t* flags = c->buf<uint32_t>("sf_flags", nl + 1);
+    uint32_t* foff = c->buf<uint32_t>("sf_foff", nl + 1);
+    uint32_t* nvalid = c->buf<uint32_t>("sf_nvalid", 2);
+    unsigned long long* ext_pos = ext;
+    unsigned long long* ext_neg = ext + np;
+    const unsigned long long kpos = host_okey(d_pos), kneg = host_okey(d_neg);
+    {
+        std::vector<unsigned long long> init(nl);
+        for (int i = 0; i < np; i++)
+            init[i] = kpos;
+        for (int i = np; i < np + nneg; i++)
+            init[i] = kneg;
+        unsigned long long* hi = c->host_stage<unsigned long long>(nl);
+        std::memcpy(hi, init.data(), sizeof(unsigned long long) * nl);
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(ext, hi, sizeof(unsigned long long) * nl, cudaMemcpyHostToDevice, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    hcnt = c->host_stage<uint32_t>(4); // the staging area may have been reallocated above
+    STPGPU_CUDA_TRY(cudaMemsetAsync(eidx, 0xff, sizeof(unsigned long long) * nl, st));
+    STPGPU_CUDA_TRY(cudaMemsetAsync(mom, 0, sizeof(double) * 6 * nl, st));
+    STPGPU_CUDA_TRY(cudaMemsetAsync(ns, 0, sizeof(int) * nl, st));
+    STPGPU_CUDA_TRY(cudaMemsetAsync(nvalid, 0, sizeof(uint32_t), st));
+    k_extrema<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg);
+    STPGPU_CHECK_LAUNCH();
+    k_extrema_idx<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg, kpos, kneg, eidx, eidx + np);
+    STPGPU_CHECK_LAUNCH();
+    {
+        // ordered (deterministic) moments: compact -> stable sort by label -> per-label sums
+        uint32_t* fcnt = c->buf<uint32_t>("fg_cnt", nchunks + 1);
+        uint32_t* foffs = c->buf<uint32_t>("fg_off", nchunks + 1);
+        k_fg_count<<<nchunks, SF_THREADS, 0, st>>>(L, n, np, ext_pos, ext_neg, kpos, kneg, fcnt);
+        STPGPU_CHECK_LAUNCH();
+        k_scan_single<<<1, 1024, 0, st>>>(fcnt, foffs, nchunks);
+        STPGPU_CHECK_LAUNCH();
+        uint32_t* hk = c->host_stage<uint32_t>(4);
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hk, foffs + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+        const int64_t nk = hk[0];
+        const int64_t nkk = std::max<int64_t>(nk, 1);
+        uint32_t* k0 = c->buf<uint32_t>("fg_k0", nkk);
+        uint32_t* v0 = c->buf<uint32_t>("fg_v0", nkk);
+        uint32_t* k1 = c->buf<uint32_t>("fg_k1", nkk);
+        uint32_t* v1 = c->buf<uint32_t>("fg_v1", nkk);
+        k_fg_compact<<<nchunks, SF_THREADS, 0, st>>>(L, n, np, ext_pos, ext_neg, kpos, kneg, p.generate_labelmap,
+            foffs, k0, v0);
+        STPGPU_CHECK_LAUNCH();
+        uint32_t* sb = c->buf<uint32_t>("fg_sb", nl);
+        uint32_t* se = c->buf<uint32_t>("fg_se", nl);
+        STPGPU_CUDA_TRY(cudaMemsetAsync(sb, 0, sizeof(uint32_t) * nl, st));
+        STPGPU_CUDA_TRY(cudaMemsetAsync(se, 0, sizeof(uint32_t) * nl, st));
+        if (nk > 0) {
+            int end_bit = 1;
+            while (end_bit < 32 && (uint64_t(1) << end_bit) < uint64_t(nl))
+                end_bit++;
+            size_t tb = 0;
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, int(nk), 0, end_bit, st);
+            void* tmp = c->buf<unsigned char>("cubtmp_sf", tb);
+            if (cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, v0, v1, int(nk), 0, end_bit, st) != cudaSuccess)
+                fail(STPGPU_ERR_CUDA, "label sort failed");
+            k_seg_bounds<<<grid1d(nk, 256), 256, 0, st>>>(k1, nk, sb, se);
+            STPGPU_CHECK_LAUNCH();
+        }
+        k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, mom, ns);
+        STPGPU_CHECK_LAUNCH();
+    }
+    k_island_flags<<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext_pos, ext_neg, kpos, kneg, ns, ns + np,
+        p.source_min_area, flags, nvalid);
+    STPGPU_CHECK_LAUNCH();
+    k_scan_single<<<1, 1024, 0, st>>>(flags, foff, np + nneg);
+    STPGPU_CHECK_LAUNCH();
+    IslandRaw* raw = c->buf<IslandRaw>("sf_raw", nl);
+    k_island_scatter<<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, flags, foff, ext_pos, ext_neg, eidx, eidx + np, ns,
+        ns + np, mom, mom + 6 * size_t(np), raw);
+    STPGPU_CHECK_LAUNCH();
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[0], foff + (np + nneg), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[1], nvalid, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    const int nis = int(hcnt[0]);
+    info.n_valid_labels = int(hcnt[1]);
+    info.n_islands = nis;
+    std::vector<IslandRaw> hr(nis);
+    if (nis)
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hr.data(), raw, sizeof(IslandRaw) * nis, cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    islands.resize(nis);
+    const int vs = rows / 2, hs = cols / 2;
+    for (int i = 0; i < nis; i++) {
+        const IslandRaw& r = hr[i];
+        stpgpu_island& o = islands[i];
+        std::memset(&o, 0, sizeof(o));
+        o.label_idx = r.label;
+        o.sign = r.label < 0 ? -1 : 1;
+        o.extremum_val = r.extremum_val;
+        const int row = int(r.extremum_idx % rows), col = int(r.extremum_idx / rows);
+        o.extremum_y_idx = row < vs ? row + vs : row - vs; // sourcefind.cpp:243-244
+        o.extremum_x_idx = col < hs ? col + hs : col - hs;
+        o.num_samples = r.num_samples;
+        // moment normalisation (sourcefind.cpp:591-604)
+        const double* a = r.mom;
+        double mb[5];
+        mb[0] = a[0] / a[5];
+        mb[1] = a[1] / a[5];
+        mb[2] = a[2] / a[5] - mb[0] * mb[0];
+        mb[3] = a[3] / a[5] - mb[1] * mb[1];
+        mb[4] = a[4] / a[5] - mb[0] * mb[1];
+        moments_fit(o.sign, o.extremum_val, mb, rms, p.analysis_n_sigma, o.moments_fit);
+    }
+}
+
+} // namespace
+
+// ====================================================================== C ABI
+
+extern "C" {
+
+int stpgpu_abi_version(void) { return STPGPU_ABI_VERSION; }
+
+stpgpu_status stpgpu_create(int device, stpgpu_context** out)
+{
+    if (!out)
+        return STPGPU_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return STPGPU_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev)
+        return STPGPU_ERR_INVALID_ARG;
+    stpgpu_context* c = new stpgpu_context();
+    c->device = device;
+    stpgpu_status s = guard(c, [&] {
+        STPGPU_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        STPGPU_CUDA_TRY(cudaEventCreate(&c->ev0));
+        STPGPU_CUDA_TRY(cudaEventCreate(&c->ev1));
+    });
+    if (s != STPGPU_OK) {
+        delete c;
+        return s;
+    }
+    *out = c;
+    return STPGPU_OK;
+}
+
+stpgpu_status stpgpu_destroy(stpgpu_context* c)
+{
+    if (!c)
+        return STPGPU_OK;
+    cudaSetDevice(c->device);
+    c->release();
+    if (c->pinned)
+        cudaFreeHost(c->pinned);
+    if (c->ev0)
+        cudaEventDestroy(c->ev0);
+    if (c->ev1)
+        cudaEventDestroy(c->ev1);
+    for (auto& e : c->pev)
+        if (e)
+            cudaEventDestroy(e);
+    if (c->stream)
+        cudaStreamDestroy(c->stream);
+    delete c;
+    return STPGPU_OK;
+}
+
+const char* stpgpu_last_error(const stpgpu_context* c) { return c ? c->err.c_str() : "null context"; }
+
+void* stpgpu_stream(stpgpu_context* c) { return c ? reinterpret_cast<void*>(c->stream) : nullptr; }
+
+stpgpu_status stpgpu_trim(stpgpu_context* c)
+{
+    return guard(c, [&] { c->release(); });
+}
+
+stpgpu_status stpgpu_image_visibilities_ex(stpgpu_context* c, const void* vis, int vis_dtype, const double* weights,
+    const double* uvw, int64_t n_vis, const stpgpu_imager_pars* pars, const stpgpu_wproj_pars* wproj,
+    const stpgpu_aproj_pars* aproj, int precision, void* image, void* beam, int out_dtype, int device_ptrs,
+    stpgpu_imager_info* info)
+{
+    return guard(c, [&] {
+        int image_size = 0;
+        ImagerSetup s = setup_from(pars, wproj, aproj, image_size);
+        if (n_vis < 0 || (n_vis > 0 && (!vis || !weights || !uvw)) || !image)
+            fail(STPGPU_ERR_INVALID_ARG, "null buffer");
+        if (vis_dtype != STPGPU_C128 && vis_dtype != STPGPU_C64)
+            fail(STPGPU_ERR_INVALID_ARG, "vis_dtype");
+        if (out_dtype != STPGPU_F64 && out_dtype != STPGPU_F32)
+            fail(STPGPU_ERR_INVALID_ARG, "out_dtype");
+        const int vc64 = vis_dtype == STPGPU_C64;
+        const size_t vbytes = vc64 ? 8 : 16;
+        const void* dv = vis;
+        const double* dw = weights;
+        const double* duvw = uvw;
+        const bool timed = !device_ptrs;
+        if (timed)
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+        if (!device_ptrs) {
+            dv = to_device<unsigned char>(c, "in_vis", vis, vbytes * size_t(n_vis));
+            dw = to_device<double>(c, "in_w", weights, size_t(n_vis));
+            duvw = to_device<double>(c, "in_uvw", uvw, 3 * size_t(n_vis));
+        }
+        const int64_t npix = int64_t(image_size) * image_size;
+        const size_t obytes = out_dtype == STPGPU_F32 ? 4 : 8;
+        void* dimg = image;
+        void* dbeam = beam;
+        if (!device_ptrs) {
+            dimg = c->buf<unsigned char>("out_img", obytes * size_t(std::max<int64_t>(npix, 1)));
+            dbeam = (s.beam && beam) ? c->buf<unsigned char>("out_beam", obytes * size_t(std::max<int64_t>(npix, 1)))
+                                     : nullptr;
+        }
+        stpgpu_imager_info local {};
+        stpgpu_imager_info* inf = info ? info : &local;
+        std::memset(inf, 0, sizeof(*inf));
+        g_launches = 0;
+        const int f32 = out_dtype == STPGPU_F32;
+        s.beam = s.beam && beam != nullptr;
+        switch (precision) {
+        case STPGPU_FP64:
+            run_imager<double, 0>(c, s, image_size, pars->gridding_correction, dv, vc64, dw, duvw, n_vis, dimg, dbeam,
+                f32, inf);
+            break;
+        case STPGPU_FP32:
+            run_imager<float, 0>(c, s, image_size, pars->gridding_correction, dv, vc64, dw, duvw, n_vis, dimg, dbeam,
+                f32, inf);
+            break;
+        case STPGPU_FP32C:
+            run_imager<float, 1>(c, s, image_size, pars->gridding_correction, dv, vc64, dw, duvw, n_vis, dimg, dbeam,
+                f32, inf);
+            break;
+        default:
+            fail(STPGPU_ERR_INVALID_ARG, "precision");
+        }
+        if (!device_ptrs && inf->image_size > 0) {
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(image, dimg, obytes * npix, cudaMemcpyDeviceToHost, c->stream));
+            if (dbeam)
+                STPGPU_CUDA_TRY(cudaMemcpyAsync(beam, dbeam, obytes * npix, cudaMemcpyDeviceToHost, c->stream));
+        }
+        if (timed)
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (timed) {
+            float ms = 0.f;
+            STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            inf->device_ms = ms;
+        }
+        inf->n_launches = g_launches;
+    });
+}
+
+stpgpu_status stpgpu_set_timing(stpgpu_context* c, int enable)
+{
+    return guard(c, [&] {
+        if (enable)
+            for (auto& e : c->pev)
+                if (!e)
+                    STPGPU_CUDA_TRY(cudaEventCreate(&e));
+        c->timing = enable != 0;
+    });
+}
+
+stpgpu_status stpgpu_image_visibilities(stpgpu_context* c, const double* vis, const double* weights, const double* uvw,
+    int64_t n_vis, const stpgpu_imager_pars* pars, const stpgpu_wproj_pars* wproj, const stpgpu_aproj_pars* aproj,
+    double* image, double* beam, stpgpu_imager_info* info)
+{
+    return stpgpu_image_visibilities_ex(c, vis, STPGPU_C128, weights, uvw, n_vis, pars, wproj, aproj, STPGPU_FP64,
+        image, beam, STPGPU_F64, 0, info);
+}
+
+stpgpu_status stpgpu_convolve_to_grid(stpgpu_context* c, int kernel_function, double kernel_trunc, int support,
+    int image_size, const double* uv, const double* vis, const double* weights, int64_t n_vis, int kernel_exact,
+    int oversampling, int shift_uv, int halfplane, int generate_beam, const stpgpu_wproj_pars* wproj, const double* w,
+    double cell_size, int analytic_gcf, double* vis_grid, double* sampling_grid, double* sample_grid_total)
+{
+    return guard(c, [&] {
+        if (kernel_function < 0 || kernel_function > 5)
+            fail(STPGPU_ERR_INVALID_ARG, "unknown kernel function");
+        if (n_vis < 0 || (n_vis > 0 && (!uv || !vis || !weights)) || !vis_grid)
+            fail(STPGPU_ERR_INVALID_ARG, "null buffer");
+        ImagerSetup s;
+        s.kf = kernel_function;
+        s.trunc = kernel_trunc;
+        s.support = support;
+        s.N = image_size;
+        s.kernel_exact = kernel_exact;
+        s.os = oversampling;
+        s.shift_uv = shift_uv;
+        s.halfplane = halfplane;
+        s.beam = generate_beam && sampling_grid;
+        s.analytic = analytic_gcf;
+        s.cell_size = cell_size;
+        const bool wp = wproj && wproj->num_wplanes > 0;
+        if (wp) {
+            if (!w)
+                fail(STPGPU_ERR_INVALID_ARG, "W-projection needs w");
+            if (wproj->hankel_opt)
+                fail(STPGPU_ERR_UNSUPPORTED, "Hankel-transform W-kernels are outside the GPU path");
+            if (!(cell_size > 0.0))
+                fail(STPGPU_ERR_INVALID_ARG, "W-projection needs cell_size > 0");
+            s.nplanes = wproj->num_wplanes;
+            s.max_support = wproj->max_wpconv_support;
+            s.undersampling = wproj->undersampling_opt;
+            s.trunc_perc = wproj->kernel_trunc_perc;
+            s.wmedian = wproj->wplanes_median;
+        }
+        if (!kernel_exact && !wp && oversampling < 1)
+            fail(STPGPU_ERR_INVALID_ARG, "oversampling must be >= 1");
+        // uv (n x 2) [+ w] in pixels as an n x 3 device array
+        double* duv = c->buf<double>("in_uv", 3 * size_t(std::max<int64_t>(n_vis, 1)));
+        if (n_vis) {
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(duv, uv, sizeof(double) * 2 * n_vis, cudaMemcpyHostToDevice, c->stream));
+            if (wp)
+                STPGPU_CUDA_TRY(
+                    cudaMemcpyAsync(duv + 2 * n_vis, w, sizeof(double) * n_vis, cudaMemcpyHostToDevice, c->stream));
+        }
+        const double* dvis = to_device<double>(c, "in_vis", vis, 2 * size_t(n_vis));
+        const double* dw = to_device<double>(c, "in_w", weights, size_t(n_vis));
+        GridOut g = run_gridder<double, 0>(c, s, dvis, 0, dw, duv, 1, n_vis);
+        ScalarsBack sb = read_back(c, g);
+        const size_t cells = size_t(g.image_rows) * size_t(image_size);
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(vis_grid, g.grid, sizeof(double2) * cells, cudaMemcpyDeviceToHost, c->stream));
+        if (s.beam)
+            STPGPU_CUDA_TRY(
+                cudaMemcpyAsync(sampling_grid, g.beam, sizeof(double2) * cells, cudaMemcpyDeviceToHost, c->stream));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (sample_grid_total)
+            *sample_grid_total = sb.total;
+    });
+}
+
+stpgpu_status stpgpu_source_find_ex(stpgpu_context* c, const void* image, int image_dtype, int32_t rows, int32_t cols,
+    const stpgpu_sf_pars* pars, int32_t* label_map, int device_ptrs, stpgpu_island* islands, int32_t capacity,
+    int32_t* n_islands, stpgpu_sf_info* info)
+{
+    return guard(c, [&] {
+        if (!image || !pars || !n_islands)
+            fail(STPGPU_ERR_INVALID_ARG, "null argument");
+        if (image_dtype != STPGPU_F64 && image_dtype != STPGPU_F32)
+            fail(STPGPU_ERR_INVALID_ARG, "image_dtype");
+        const int64_t n = int64_t(rows) * cols;
+        const size_t eb = image_dtype == STPGPU_F32 ? 4 : 8;
+        if (!device_ptrs)
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+        const void* dimg = image;
+        if (!device_ptrs && n > 0)
+            dimg = to_device<unsigned char>(c, "sf_in", image, eb * size_t(n));
+        int32_t* dl = device_ptrs ? label_map : nullptr;
+        std::vector<stpgpu_island> isl;
+        stpgpu_sf_info local {};
+        stpgpu_sf_info* inf = info ? info : &local;
+        std::memset(inf, 0, sizeof(*inf));
+        if (image_dtype == STPGPU_F32)
+            run_source_find<float>(c, reinterpret_cast<const float*>(dimg), rows, cols, *pars, dl, isl, *inf);
+        else
+            run_source_find<double>(c, reinterpret_cast<const double*>(dimg), rows, cols, *pars, dl, isl, *inf);
+        if (!device_ptrs && label_map) {
+            const int32_t* src = c->buf<int32_t>("ccl_L", n);
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(label_map, src, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->stream));
+        }
+        if (!device_ptrs)
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (!device_ptrs) {
+            float ms = 0.f;
+            STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            inf->device_ms = ms;
+        }
+        *n_islands = int32_t(isl.size());
+        if (int32_t(isl.size()) > capacity)
+            fail(STPGPU_ERR_CAPACITY, "island buffer too small: need " + std::to_string(isl.size()));
+        if (!isl.empty())
+            std::memcpy(islands, isl.data(), sizeof(stpgpu_island) * isl.size());
+    });
+}
+
+stpgpu_status stpgpu_source_find(stpgpu_context* c, const double* image, int32_t rows, int32_t cols,
+    const stpgpu_sf_pars* pars, int32_t* label_map, stpgpu_island* islands, int32_t capacity, int32_t* n_islands,
+    stpgpu_sf_info* info)
+{
+    return stpgpu_source_find_ex(c, image, STPGPU_F64, rows, cols, pars, label_map, 0, islands, capacity, n_islands,
+        info);
+}
+
+} // extern "C"

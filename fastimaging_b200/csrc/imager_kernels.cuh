@@ -1,0 +1,1077 @@
+// Device kernels of the snapshot imager.
+//
+// Pipeline (one snapshot):
+//   k_prepass      uvw -> pixel scaling, half-plane conversion, rint split,
+//                  bounds check, uv shift, oversampled index  (gridder.h:369-504)
+//   [W-proj]       |w| sort (CUB), plane boundaries/averages, FP64 W-kernels
+//   k_count_tiles  footprint -> uv tiles it overlaps (counting pass)
+//   k_scan_*       tile offsets
+//   k_fill_tiles   tile -> item lists
+//   k_grid_tiles   one CTA per 32x32 tile of the half-plane grid: all items
+//                  whose footprint touches the tile accumulate in shared
+//                  memory, then the tile is written once with coalesced
+//                  stores (no memset, no global atomics)          (gridder.h:596-994)
+//   cuFFT Z2D/C2R  (fft.cpp:45-135)
+//   k_normalise    crop + 1/sum + gcf division                    (imager.h:97-150)
+#pragma once
+
+#include "common.cuh"
+
+namespace stpgpu {
+
+constexpr int TILE_R = 32; // tile rows (v, the fast grid axis)
+constexpr int TILE_C = 32; // tile columns (u)
+constexpr int GRID_THREADS = 256;
+
+enum KMode { KM_SEP = 0, KM_EXACT = 1, KM_WPROJ = 2 };
+
+// Per-visibility record written by the prepass.  flags: bit0 conj(kernel)
+// for the original item (w < 0), bit1 conj(kernel) for the mirrored item
+// (-w < 0).  The visibility is stored conjugated when the half-plane
+// conversion flipped it.
+template <typename R>
+struct Item {
+    R vr, vi, w;
+    int32_t gcx, gcy;
+    int16_t cpx, cpy;
+    uint16_t plane;
+    uint8_t good, flags;
+};
+
+struct PrepassParams {
+    int64_t n;
+    const void* vis; // complex128 or complex64
+    int vis_c64;
+    const double* weights;
+    const double* uv; // either uvw (n x 3, lambda) or uv (n x 2, pixels)
+    int uv_is_pixels;
+    double inv_px; // lambda -> pixel factor when uv_is_pixels == 0
+    int N, conv_support, halfplane, shift_uv, kernel_exact, os;
+    int keep_w;
+    double* frac;      // 2n (exact mode only), may be null
+    double* wsum_part; // per-block partial sums of good weights
+    unsigned long long* ngood_part;
+    double* absw_key; // n |w| (W-proj only), may be null
+    double* w_out;    // n half-plane-converted w (W-proj), may be null
+};
+
+template <typename R>
+__global__ void k_prepass(PrepassParams p, Item<R>* items)
+{
+    __shared__ double s_w[GRID_THREADS / 32];
+    __shared__ unsigned long long s_n[GRID_THREADS / 32];
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    double wgood = 0.0;
+    unsigned long long ngood = 0;
+    if (i < p.n) {
+        double u, v, w = 0.0;
+        if (p.uv_is_pixels) {
+            u = p.uv[i];
+            v = p.uv[p.n + i];
+            if (p.keep_w)
+                w = p.uv[2 * p.n + i];
+        } else {
+            u = p.uv[i] * p.inv_px;
+            v = p.uv[p.n + i] * p.inv_px;
+            w = p.uv[2 * p.n + i];
+        }
+        double vr, vi;
+        if (p.vis_c64) {
+            float2 t = reinterpret_cast<const float2*>(p.vis)[i];
+            vr = t.x;
+            vi = t.y;
+        } else {
+            double2 t = reinterpret_cast<const double2*>(p.vis)[i];
+            vr = t.x;
+            vi = t.y;
+        }
+        const double wt = p.weights[i];
+        int good = 1;
+        const int S = p.conv_support;
+        if (p.halfplane) {
+            if (v < 0.0) {
+                if (v > -(S + 1))
+                    good = 2;
+                u *= -1;
+                v *= -1;
+                w *= -1;
+                vi = -vi;
+            } else if (v < (S + 1)) {
+                good = 2;
+            }
+        }
+        const int half = p.N / 2;
+        bool finite = isfinite(u) && isfinite(v);
+        double ru = rint(u), rv = rint(v);
+        // int(rint(x)) with the out-of-range behaviour of x86 (INT_MIN) kept
+        // for the bounds check: such centres are always out of bounds.
+        long long vx = (finite && fabs(ru) < 1.0e9) ? (long long)ru : (long long)INT32_MIN;
+        long long vy = (finite && fabs(rv) < 1.0e9) ? (long long)rv : (long long)INT32_MIN;
+        double fx = u - double(vx), fy = v - double(vy);
+        long long kx = vx + half, ky = vy + half;
+        if (!finite || (kx - S) <= 0 || (ky - S) <= 0 || (kx + S) >= p.N || (ky + S) >= p.N)
+            good = 0;
+        if (p.shift_uv) {
+            kx = kx < half ? kx + half : kx - half;
+            ky = ky < half ? ky + half : ky - half;
+        }
+        int cpx = 0, cpy = 0;
+        if (!p.kernel_exact) {
+            const int rmax = p.os / 2;
+            int ox = int(rint(fx * p.os)), oy = int(rint(fy * p.os));
+            ox = ox > rmax ? rmax : (ox < -rmax ? -rmax : ox);
+            oy = oy > rmax ? rmax : (oy < -rmax ? -rmax : oy);
+            cpx = ox + rmax;
+            cpy = oy + rmax;
+        }
+        if (p.frac) {
+            p.frac[i] = fx;
+            p.frac[p.n + i] = fy;
+        }
+        if (p.absw_key)
+            p.absw_key[i] = fabs(w);
+        if (p.w_out)
+            p.w_out[i] = w;
+        Item<R> it;
+        it.vr = R(vr);
+        it.vi = R(vi);
+        it.w = R(wt);
+        it.gcx = good ? int32_t(kx) : 0;
+        it.gcy = good ? int32_t(ky) : 0;
+        it.cpx = int16_t(cpx);
+        it.cpy = int16_t(cpy);
+        it.plane = 0;
+        it.good = uint8_t(good);
+        it.flags = uint8_t((w < 0.0 ? 1 : 0) | (-w < 0.0 ? 2 : 0));
+        items[i] = it;
+        if (good) {
+            wgood = wt;
+            ngood = 1;
+        }
+    }
+    // deterministic block partial sums
+    for (int o = 16; o > 0; o >>= 1) {
+        wgood += __shfl_down_sync(0xffffffffu, wgood, o);
+        ngood += __shfl_down_sync(0xffffffffu, ngood, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        s_w[threadIdx.x >> 5] = wgood;
+        s_n[threadIdx.x >> 5] = ngood;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        unsigned long long c = 0;
+        for (int k = 0; k < int(blockDim.x >> 5); k++) {
+            t += s_w[k];
+            c += s_n[k];
+        }
+        p.wsum_part[blockIdx.x] = t;
+        p.ngood_part[blockIdx.x] = c;
+    }
+}
+
+// Sum of block partials in a fixed order (one block).  out[0] = 2 * sum
+// (the half-plane doubling of gridder.h:423), out_n[0] = count.
+__global__ void k_finish_wsum(const double* part, const unsigned long long* npart, int nb, double* out,
+    unsigned long long* out_n)
+{
+    __shared__ double s[1024];
+    __shared__ unsigned long long sn[1024];
+    double t = 0.0;
+    unsigned long long c = 0;
+    for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+        t += part[k];
+        c += npart[k];
+    }
+    s[threadIdx.x] = t;
+    sn[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s[threadIdx.x] += s[threadIdx.x + o];
+            sn[threadIdx.x] += sn[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = s[0] * 2.0;
+        out_n[0] = sn[0];
+    }
+}
+
+// ---------------------------------------------------------------- footprint segments
+
+// Footprint index mapping (gridder.h:645-667 columns/rows, :970-983 exact).
+// Column tap j of a kernel whose left edge is cb lands in grid column
+// cb + j wrapped once into [0, N).  Row tap i lands in cb-style wrapped row
+// rb + i, except that negative rows are skipped by the oversampled gridder
+// and wrapped by the exact one; rows >= `rows` (half plane) are dropped.
+// Returns -1 when the tap is not gridded.
+__device__ __forceinline__ int map_col(int raw, int N)
+{
+    return raw < 0 ? raw + N : (raw >= N ? raw - N : raw);
+}
+__device__ __forceinline__ int map_row(int raw, int N, int rows, bool wrap_neg)
+{
+    if (raw < 0) {
+        if (!wrap_neg)
+            return -1;
+        raw += N;
+    } else if (raw >= N) {
+        raw -= N;
+    }
+    return raw < rows ? raw : -1;
+}
+
+struct BinParams {
+    int N, image_rows, tiles_r, tiles_c;
+    int support;             // non-W-proj support
+    const int* plane_support; // W-proj truncated support per plane (nullable)
+    int exact;               // rows wrap negative (exact gridder)
+    int64_t n;
+    uint32_t* tile_count;
+    const uint32_t* tile_off;
+    uint32_t* tile_cursor;
+    uint32_t* list;
+    uint64_t list_capacity;
+    unsigned int* err;
+};
+
+template <typename R>
+__device__ __forceinline__ void item_centre(const Item<R>& it, int mir, int N, int& cx, int& cy)
+{
+    cx = mir ? N - it.gcx : it.gcx;
+    cy = mir ? N - it.gcy : it.gcy;
+}
+
+// Tiles overlapped by one item: calls f(tile) once per distinct tile.  The
+// tile rows / columns of the mapped taps form at most a few runs; distinct
+// values are collected in small register bitmasks (tile ids relative to the
+// first one seen, plus a wrap-around run).
+template <typename R, typename F>
+__device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, const BinParams& p, F f)
+{
+    const int S = p.plane_support ? p.plane_support[it.plane] : p.support;
+    const int K = 2 * S + 1;
+    int cx, cy;
+    item_centre(it, mir, p.N, cx, cy);
+    // distinct tile rows / cols: at most 2 runs each (before and after a wrap)
+    int tr0 = -1, tr1 = -1, tr0e = -1, tr1e = -1;
+    for (int i = 0; i < K; i++) {
+        const int r = map_row(cy - S + i, p.N, p.image_rows, p.exact != 0);
+        if (r < 0)
+            continue;
+        const int t = r / TILE_R;
+        if (tr0 < 0) {
+            tr0 = tr0e = t;
+        } else if (t == tr0e + 1 || t == tr0e) {
+            tr0e = t;
+        } else if (tr1 < 0) {
+            tr1 = tr1e = t;
+        } else {
+            tr1e = t;
+        }
+    }
+    int tc0 = -1, tc1 = -1, tc0e = -1, tc1e = -1;
+    for (int j = 0; j < K; j++) {
+        const int c = map_col(cx - S + j, p.N);
+        const int t = c / TILE_C;
+        if (tc0 < 0) {
+            tc0 = tc0e = t;
+        } else if (t == tc0e + 1 || t == tc0e) {
+            tc0e = t;
+        } else if (tc1 < 0) {
+            tc1 = tc1e = t;
+        } else {
+            tc1e = t;
+        }
+    }
+    if (tr0 < 0)
+        return;
+    for (int rr = 0; rr < 2; rr++) {
+        const int rlo = rr ? tr1 : tr0, rhi = rr ? tr1e : tr0e;
+        if (rlo < 0)
+            continue;
+        for (int tr = rlo; tr <= rhi; tr++) {
+            if (rr && tr >= tr0 && tr <= tr0e)
+                continue;
+            for (int cc = 0; cc < 2; cc++) {
+                const int clo = cc ? tc1 : tc0, chi = cc ? tc1e : tc0e;
+                if (clo < 0)
+                    continue;
+                for (int tc = clo; tc <= chi; tc++) {
+                    if (cc && tc >= tc0 && tc <= tc0e)
+                        continue;
+                    f(uint32_t(tc) * uint32_t(p.tiles_r) + uint32_t(tr));
+                }
+            }
+        }
+    }
+}
+
+template <typename R>
+__global__ void k_count_tiles(BinParams p, const Item<R>* items)
+{
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= p.n)
+        return;
+    const Item<R> it = items[i];
+    for (int mir = 0; mir < int(it.good); mir++)
+        for_item_tiles(it, mir, p, [&](uint32_t t) { atomicAdd(&p.tile_count[t], 1u); });
+}
+
+// Lists are filled in the order given by `order` when non-null (the |w|
+// order for W-projection), so that a warp's items mostly share one plane.
+template <typename R>
+__global__ void k_fill_tiles(BinParams p, const Item<R>* items, const uint32_t* order)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= p.n)
+        return;
+    const int64_t i = order ? int64_t(order[k]) : k;
+    const Item<R> it = items[i];
+    for (int mir = 0; mir < int(it.good); mir++)
+        for_item_tiles(it, mir, p, [&](uint32_t t) {
+            const uint32_t slot = atomicAdd(&p.tile_cursor[t], 1u);
+            const uint64_t pos = uint64_t(p.tile_off[t]) + slot;
+            if (pos < p.list_capacity)
+                p.list[pos] = uint32_t(i) * 2u + uint32_t(mir);
+            else
+                atomicOr(p.err, 1u);
+        });
+}
+
+// Exclusive scan of n counts into off[0..n] (single block, n up to a few
+// hundred thousand).  off[n] = total.
+__global__ void k_scan_single(const uint32_t* cnt, uint32_t* off, int n)
+{
+    __shared__ uint32_t s[1024];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += 1024 * 8) {
+        // each thread scans 8 consecutive elements
+        uint32_t v[8];
+        uint32_t loc = 0;
+        const int b0 = base + threadIdx.x * 8;
+        for (int k = 0; k < 8; k++) {
+            v[k] = (b0 + k < n) ? cnt[b0 + k] : 0u;
+            loc += v[k];
+        }
+        s[threadIdx.x] = loc;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {
+            uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
+            __syncthreads();
+            s[threadIdx.x] += t;
+            __syncthreads();
+        }
+        uint32_t excl = carry + s[threadIdx.x] - loc;
+        for (int k = 0; k < 8; k++) {
+            if (b0 + k < n)
+                off[b0 + k] = excl;
+            excl += v[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023)
+            carry += s[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        off[n] = carry;
+}
+
+// ---------------------------------------------------------------- accumulators
+
+// Shared-memory cell accumulators.  Each cell is owned by one warp and
+// updated with plain read-modify-write (no atomics), so the two-sum
+// compensation of FP32C is exact: s + c carries the full sum.
+template <typename R, int COMP>
+struct Acc;
+template <>
+struct __align__(16) Acc<double, 0> {
+    double2 s;
+};
+template <>
+struct __align__(8) Acc<float, 0> {
+    float2 s;
+};
+template <>
+struct __align__(16) Acc<float, 1> {
+    float2 s, c;
+};
+
+// Knuth's TwoSum error term with explicit rounding (no contraction).
+__device__ __forceinline__ float two_sum_err(float a, float b, float s)
+{
+    const float bb = __fsub_rn(s, a);
+    return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+}
+
+__device__ __forceinline__ void acc_rmw(Acc<double, 0>* a, double re, double im)
+{
+    double2 v = a->s;
+    v.x += re;
+    v.y += im;
+    a->s = v;
+}
+__device__ __forceinline__ void acc_rmw(Acc<float, 0>* a, float re, float im)
+{
+    float2 v = a->s;
+    v.x += re;
+    v.y += im;
+    a->s = v;
+}
+__device__ __forceinline__ void acc_rmw(Acc<float, 1>* a, float re, float im)
+{
+    Acc<float, 1> v = *a;
+    const float sx = __fadd_rn(v.s.x, re), sy = __fadd_rn(v.s.y, im);
+    v.c.x = __fadd_rn(v.c.x, two_sum_err(v.s.x, re, sx));
+    v.c.y = __fadd_rn(v.c.y, two_sum_err(v.s.y, im, sy));
+    v.s.x = sx;
+    v.s.y = sy;
+    *a = v;
+}
+template <typename R, int COMP>
+__device__ __forceinline__ void acc_zero(Acc<R, COMP>* a)
+{
+    *a = Acc<R, COMP> {};
+}
+__device__ __forceinline__ double2 acc_value(const Acc<double, 0>& a) { return a.s; }
+__device__ __forceinline__ float2 acc_value(const Acc<float, 0>& a) { return a.s; }
+__device__ __forceinline__ float2 acc_value(const Acc<float, 1>& a)
+{
+    return make_float2(__fadd_rn(a.s.x, a.c.x), __fadd_rn(a.s.y, a.c.y));
+}
+
+template <typename R>
+struct Cplx;
+template <>
+struct Cplx<double> {
+    using T = double2;
+};
+template <>
+struct Cplx<float> {
+    using T = float2;
+};
+
+// ---------------------------------------------------------------- gridder
+
+template <typename R>
+struct GridParams {
+    int N, image_rows, tiles_r;
+    int support, os, cs; // cs = cache size per dimension = (os/2)*2+1
+    int exact_wrap;      // exact gridder row wrap
+    const Item<R>* items;
+    const uint32_t* tile_off;
+    const uint32_t* list;
+    // KM_SEP: 1-D kernel table [cs][K] (R)
+    const R* k1d;
+    // KM_EXACT: functor + per-visibility fractions
+    int kf;
+    double trunc;
+    const double* frac;
+    int64_t n;
+    // KM_WPROJ: per plane the W-kernel quadrant conv[p][l][k] (stride lh,
+    // |offsets| index it) and 1/sum(Re) per oversampled offset inv[p][y][x]:
+    // the cached kernel of aw_projection.cpp:415-448 is conv * inv.
+    const typename Cplx<R>::T* wconv;
+    const R* winv;
+    int lh;
+    const int* plane_support;
+    typename Cplx<R>::T* grid; // image_rows x N column-major
+    typename Cplx<R>::T* beam; // nullable
+};
+
+// One warp per 32x32 tile of the (half-plane) grid.  Lanes take 32 items of
+// the tile's list at a time and walk their K x K footprints in lockstep, so
+// at every step distinct lanes touch distinct cells unless two items share a
+// kernel corner; such items are deferred to a later round (match_any).  The
+// tile is zeroed in shared memory, accumulated with plain read-modify-write,
+// and stored once with coalesced 512-byte column writes: no memset of the
+// grid, no global or shared atomics, and every cell of the grid is written
+// exactly once.  (Gridding semantics: gridder.h:596-994.)
+// Kernel value of tap (i, j) of the lane's item, times the visibility weight.
+template <typename R, int KMODE>
+struct TapCtx {
+    int K, S, cpx, cpy;
+    R wt, winv;
+    bool conj_k;
+    const typename Cplx<R>::T* wconv;
+    double fx, fy, ksum;
+};
+
+template <typename R, int KMODE>
+__device__ __forceinline__ void tap_value(const GridParams<R>& p, const R* tab, const TapCtx<R, KMODE>& t, int i, int j,
+    R& kr, R& ki)
+{
+    if (KMODE == KM_SEP) {
+        kr = tab[t.cpy * t.K + i] * tab[t.cpx * t.K + j];
+        ki = R(0);
+    } else if (KMODE == KM_EXACT) {
+        // make_kernel_array (conv_func.h:279-303): outer product / accu
+        const double y = kernel_value(p.kf, p.trunc, (double(i) - t.S) - t.fy);
+        const double x = kernel_value(p.kf, p.trunc, (double(j) - t.S) - t.fx);
+        kr = R((y * x) / t.ksum);
+        ki = R(0);
+    } else {
+        int oy = (i - t.S) * p.os + p.os / 2 - t.cpy;
+        int ox = (j - t.S) * p.os + p.os / 2 - t.cpx;
+        oy = oy < 0 ? -oy : oy;
+        ox = ox < 0 ? -ox : ox;
+        const typename Cplx<R>::T cv = t.wconv[size_t(oy) * p.lh + ox];
+        kr = cv.x * t.winv;
+        ki = t.conj_k ? -(cv.y * t.winv) : cv.y * t.winv;
+    }
+    kr = kr * t.wt;
+    ki = ki * t.wt;
+}
+
+template <typename R, int COMP, int KMODE, bool BEAM>
+__global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
+{
+    using A = Acc<R, COMP>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A* acc = reinterpret_cast<A*>(smem_raw);
+    A* bacc = acc + (BEAM ? TILE_R * TILE_C : 0);
+    R* tab = reinterpret_cast<R*>(acc + (BEAM ? 2 : 1) * TILE_R * TILE_C);
+    const int lane = threadIdx.x;
+    const int tile = blockIdx.x;
+    const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
+    const int r0 = tr * TILE_R, c0 = tc * TILE_C;
+    const bool wrap_neg = p.exact_wrap != 0;
+
+    for (int t = lane; t < TILE_R * TILE_C; t += 32) {
+        acc_zero(&acc[t]);
+        if (BEAM)
+            acc_zero(&bacc[t]);
+    }
+    if (KMODE == KM_SEP) {
+        const int K = 2 * p.support + 1;
+        for (int t = lane; t < p.cs * K; t += 32)
+            tab[t] = p.k1d[t];
+    }
+    __syncwarp();
+
+    const uint32_t beg = p.tile_off[tile], end = p.tile_off[tile + 1];
+    for (uint32_t base = beg; base < end; base += 32) {
+        const uint32_t e = base + lane;
+        const bool active = e < end;
+        TapCtx<R, KMODE> t;
+        t.K = 0;
+        t.S = 0;
+        t.cpx = t.cpy = 0;
+        t.wt = R(0);
+        t.winv = R(1);
+        t.conj_k = false;
+        t.wconv = nullptr;
+        t.fx = t.fy = 0.0;
+        t.ksum = 1.0;
+        R vr = R(0), vim = R(0);
+        int rb = 0, cb = 0;
+        unsigned long long key = ~0ull;
+        if (active) {
+            const uint32_t code = p.list[e];
+            const uint32_t vi = code >> 1;
+            const int mir = int(code & 1u);
+            const Item<R> it = p.items[vi];
+            int cx, cy;
+            item_centre(it, mir, p.N, cx, cy);
+            t.S = (KMODE == KM_WPROJ) ? p.plane_support[it.plane] : p.support;
+            t.K = 2 * t.S + 1;
+            t.cpx = it.cpx;
+            t.cpy = it.cpy;
+            if (mir && p.os > 1) {
+                t.cpx = p.os - t.cpx;
+                t.cpy = p.os - t.cpy;
+            }
+            vr = it.vr;
+            vim = mir ? -it.vi : it.vi;
+            t.wt = it.w;
+            rb = cy - t.S;
+            cb = cx - t.S;
+            const int krow = ((rb % p.N) + p.N) % p.N, kcol = ((cb % p.N) + p.N) % p.N;
+            key = (unsigned long long)krow * (unsigned long long)p.N + (unsigned long long)kcol;
+            if (KMODE == KM_WPROJ) {
+                t.conj_k = (it.flags >> (mir ? 1 : 0)) & 1u;
+                t.wconv = p.wconv + size_t(it.plane) * p.lh * p.lh;
+                t.winv = p.winv[(size_t(it.plane) * p.cs + t.cpy) * p.cs + t.cpx];
+            }
+            if (KMODE == KM_EXACT) {
+                t.fx = p.frac[vi];
+                t.fy = p.frac[p.n + vi];
+                if (mir) {
+                    t.fx *= -1;
+                    t.fy *= -1;
+                }
+                // arma::accu of the column-major outer product (two accumulators)
+                double a1 = 0.0, a2 = 0.0;
+                int lin = 0;
+                for (int c = 0; c < t.K; c++) {
+                    const double xc = kernel_value(p.kf, p.trunc, (double(c) - t.S) - t.fx);
+                    for (int r = 0; r < t.K; r++, lin++) {
+                        const double v = kernel_value(p.kf, p.trunc, (double(r) - t.S) - t.fy) * xc;
+                        if (lin & 1)
+                            a2 += v;
+                        else
+                            a1 += v;
+                    }
+                }
+                t.ksum = a1 + a2;
+            }
+        }
+        // rounds: one item per kernel corner per round, so that at every
+        // step of the lockstep walk distinct lanes touch distinct cells
+        unsigned pending = __ballot_sync(0xffffffffu, active);
+        while (pending) {
+            const unsigned peers
+                = __match_any_sync(0xffffffffu, (active && ((pending >> lane) & 1u)) ? key : ~0ull);
+            const bool mine = active && ((pending >> lane) & 1u) && (__ffs(peers & pending) - 1 == lane);
+            const unsigned sel = __ballot_sync(0xffffffffu, mine);
+            pending &= ~sel;
+            int kmax = mine ? t.K : 0;
+            for (int o = 16; o > 0; o >>= 1)
+                kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+            for (int i = 0; i < kmax; i++) {
+                const int rm = (mine && i < t.K) ? map_row(rb + i, p.N, p.image_rows, wrap_neg) : -1;
+                const int rl = rm - r0;
+                const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
+                for (int j = 0; j < kmax; j++) {
+                    const int cl = map_col(cb + j, p.N) - c0;
+                    if (rok && j < t.K && cl >= 0 && cl < TILE_C) {
+                        R kr, ki;
+                        tap_value<R, KMODE>(p, tab, t, i, j, kr, ki);
+                        const R re = vr * kr - vim * ki;
+                        const R im = vr * ki + vim * kr;
+                        acc_rmw(&acc[cl * TILE_R + rl], re, im);
+                        if (BEAM)
+                            acc_rmw(&bacc[cl * TILE_R + rl], kr, ki);
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    __syncwarp();
+    const int nr = min(TILE_R, p.image_rows - r0);
+    const int nc = min(TILE_C, p.N - c0);
+    for (int q = lane; q < TILE_R * TILE_C; q += 32) {
+        const int rl = q % TILE_R, cl = q / TILE_R;
+        if (rl < nr && cl < nc) {
+            const size_t g = size_t(c0 + cl) * p.image_rows + (r0 + rl);
+            p.grid[g] = acc_value(acc[q]);
+            if (BEAM)
+                p.beam[g] = acc_value(bacc[q]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- kernel tables
+
+// make_1D_kernel for every oversampled offset (populate_kernel_cache,
+// gridder.h:73-105): out[cs][K], normalised by accu (two accumulators).
+__global__ void k_kernel_table(int kf, double trunc, int support, int os, double* out)
+{
+    const int half = os / 2;
+    const int cs = half * 2 + 1;
+    const int K = 2 * support + 1;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cs)
+        return;
+    const double offset = (double(c) - half) / os;
+    double a1 = 0.0, a2 = 0.0;
+    for (int i = 0; i < K; i++) {
+        double d = (double(i) - support) / 1;
+        double v = kernel_value(kf, trunc, d - offset);
+        out[c * K + i] = v;
+        if (i & 1)
+            a2 += v;
+        else
+            a1 += v;
+    }
+    const double s = a1 + a2;
+    for (int i = 0; i < K; i++)
+        out[c * K + i] = out[c * K + i] / s;
+}
+
+__global__ void k_iota_u32(uint32_t* p, int64_t n)
+{
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n)
+        p[i] = uint32_t(i);
+}
+
+__global__ void k_d2f(const double* in, float* out, int64_t n)
+{
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = float(in[i]);
+}
+
+// ImgDomKernel (conv_func.h:351-412).  Analytic: gcf((i - c)/c).  Otherwise
+// the real part of the R2HC DFT of the normalised, wrapped 1-D kernel,
+// mirrored about the centre.  The kernel is exactly zero beyond `trunc`, so
+// the DFT is a short cosine sum, evaluated with exact argument reduction.
+__global__ void k_imgdom_kernel(int kf, double trunc, int n, int analytic, double ksum_inv, int dmax, double* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const int centre = n / 2;
+    if (analytic) {
+        out[i] = gcf_value(kf, (double(i) - centre) / centre);
+        return;
+    }
+    // aa[n/2 + m] = r_m (m < n/2), aa[n/2 - m] = r_m (1 <= m <= n/2)
+    int m = i >= centre ? i - centre : centre - i;
+    double r = 0.0;
+    // arr[j] = k1(j) (j < n/2), k1(j - n) (j >= n/2); r_m = sum_j arr[j] cos(2 pi j m / n)
+    for (int d = -dmax; d <= dmax; d++) {
+        if (d < -centre || d >= n - centre)
+            continue;
+        double kv = kernel_value(kf, trunc, double(d));
+        if (kv == 0.0)
+            continue;
+        kv = kv * ksum_inv;
+        long long jm = (long long)(d < 0 ? d + n : d) * m % n;
+        r += kv * cospi(2.0 * double(jm) / double(n));
+    }
+    out[i] = r;
+}
+
+// ---------------------------------------------------------------- normalise
+
+// normalise_image_beam_result_1D, non-FFTSHIFT branch (imager.h:97-150):
+// crop the padded image keeping the unshifted quadrant layout, multiply by
+// 1/sum and divide by gcf[ii]*gcf[jj].  blockIdx.y = output column; the
+// factor 1/sum is read from the device (0 when the sampling total is 0).
+template <typename RI, typename RO>
+__global__ void k_normalise(const RI* __restrict__ img, int padded, int image_size, const double* total,
+    const double* __restrict__ gcf, int corr, RO* __restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= image_size)
+        return;
+    const double tot = total[0];
+    const double nf = tot > 0.0 ? 1.0 / tot : 0.0;
+    const int hp = padded / 2, hs = image_size / 2;
+    const int oj = j < hs ? j : padded + j - image_size;
+    const int jj = j < hs ? j + hp : hp + j - image_size;
+    const int oi = i < hs ? i : padded - hs + (i - hs);
+    const int ii = i < hs ? hp + i : hp - hs + (i - hs);
+    const double v = double(img[size_t(oj) * padded + oi]);
+    out[size_t(j) * image_size + i] = RO(corr ? v * nf / (gcf[ii] * gcf[jj]) : v * nf);
+}
+
+// ---------------------------------------------------------------- W-projection
+
+// Plane boundaries and plane w (average_w_planes, gridder.cpp:68-146) from the
+// |w|-sorted order: cgood[k] = number of good visibilities among sorted[0..k).
+__global__ void k_wplanes(const uint32_t* cgood, const double* absw_sorted, int64_t n, int P, int median,
+    int64_t* first, int64_t* last)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    const uint64_t G = cgood[n];
+    uint64_t begin = 0;
+    if (G == uint64_t(n)) {
+        // every visibility is in bounds: sorted position == good count
+        for (int idx = 0; idx < P; idx++) {
+            const uint64_t plane_size = uint64_t(ceil(double(G - begin) / (P - idx)));
+            const uint64_t lo = min(uint64_t(n), begin + plane_size);
+            first[idx] = int64_t(begin);
+            last[idx] = int64_t(lo);
+            begin = lo;
+        }
+        return;
+    }
+    for (int idx = 0; idx < P; idx++) {
+        uint64_t plane_size = uint64_t(ceil(double(G - begin) / (P - idx)));
+        // k: first index with cgood[k] == cgood[begin] + plane_size (or n)
+        const uint64_t remaining = uint64_t(cgood[n]) - uint64_t(cgood[begin]);
+        uint64_t lo = begin, hi = uint64_t(n);
+        if (plane_size > remaining) {
+            lo = uint64_t(n);
+        } else {
+            const uint64_t target = uint64_t(cgood[begin]) + plane_size;
+            while (lo < hi) {
+                uint64_t mid = (lo + hi) / 2;
+                if (uint64_t(cgood[mid]) >= target)
+                    hi = mid;
+                else
+                    lo = mid + 1;
+            }
+        }
+        first[idx] = int64_t(begin);
+        last[idx] = int64_t(lo);
+        begin = lo;
+    }
+    (void)absw_sorted;
+    (void)median;
+}
+
+// One block per plane: plane w = mean |w| over good visibilities (or the
+// median rule), in the plane's sorted range.
+__global__ void k_wplane_values(const uint32_t* cgood, const double* absw_sorted, const uint8_t* good_sorted,
+    const int64_t* first, const int64_t* last, int64_t n, int P, int median, double* w_avg)
+{
+    const int p = blockIdx.x;
+    const int64_t b = first[p], e = last[p];
+    __shared__ double s[256];
+    if (!median) {
+        double t = 0.0;
+        for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x)
+            if (good_sorted[k])
+                t += absw_sorted[k];
+        s[threadIdx.x] = t;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o)
+                s[threadIdx.x] += s[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            uint64_t cnt = uint64_t(cgood[e]) - uint64_t(cgood[b]);
+            w_avg[p] = cnt > 0 ? s[0] / double(cnt) : 0.0;
+        }
+    } else if (threadIdx.x == 0) {
+        // median variant (gridder.cpp:79-118)
+        const uint64_t G = cgood[n];
+        uint64_t plane_size = uint64_t(ceil(double(G - uint64_t(b)) / (P - p)));
+        uint64_t middle = plane_size / 2;
+        if (uint64_t(b) + plane_size > G)
+            middle = (G - uint64_t(b)) / 2;
+        uint64_t counter = uint64_t(cgood[e]) - uint64_t(cgood[b]);
+        if (counter == 0) {
+            w_avg[p] = 0.0;
+            return;
+        }
+        // idx_mid: position of the (middle)-th good from b
+        uint64_t target = uint64_t(cgood[b]) + middle; // cgood[k] == target and good[k]
+        int64_t lo = b, hi = e;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) / 2;
+            if (uint64_t(cgood[mid + 1]) > target)
+                hi = mid;
+            else
+                lo = mid + 1;
+        }
+        int64_t idx_mid = lo;
+        if ((plane_size % 2) == 0 && idx_mid > 0)
+            w_avg[p] = (absw_sorted[idx_mid - 1] + absw_sorted[idx_mid]) / 2.0;
+        else
+            w_avg[p] = absw_sorted[idx_mid];
+    }
+}
+
+template <typename R>
+__global__ void k_assign_planes(const uint32_t* perm, const int64_t* first, int P, int64_t n, Item<R>* items)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    int lo = 0, hi = P - 1;
+    while (lo < hi) { // last plane whose first <= k
+        int mid = (lo + hi + 1) / 2;
+        if (first[mid] <= k)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    items[perm[k]].plane = uint16_t(lo);
+}
+
+template <typename R>
+__global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, int64_t n, uint8_t* good_sorted,
+    uint32_t* gflag)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    uint8_t g = items[perm[k]].good != 0;
+    good_sorted[k] = g;
+    gflag[k] = g;
+}
+
+// W-kernel generation for one plane per CTA (FP64), the non-Hankel path of
+// WideFieldImaging (aw_projection.cpp:50-111 image-domain kernel with
+// combine_2d_kernel_value :455-474, forward c2c FFT :194, truncation
+// :197-209, kernel cache :415-448).
+//
+// The image-domain kernel comb(a, b) is even in both indices (the reference
+// writes each value at (+-a, +-b)), non-zero only for |a|, |b| < half, so its
+// forward DFT is the separable cosine sum
+//   conv(k, l) = sum_{a,b >= 0} m_a m_b Q[a][b] cos(2 pi k a / arr) cos(2 pi l b / arr)
+// with m_0 = 1, m_{>0} = 2, and conv(+-k, +-l) = conv(|k|, |l|).  Only the
+// entries the cache samples are formed: first the l = 0 row for the
+// truncation, then the |offset| block of the truncated support.
+// Outputs per plane: support, conv quadrant conv[p][l][k] (stride lh_max)
+// and inv[p][y][x] = 1 / sum(Re) of each oversampled sub-kernel, so that the
+// reference's cached kernel value is conv * inv.
+struct WkParams {
+    const double* w_avg;
+    const double* aa; // image-domain AA kernel over the workarea
+    const double* ctab; // cos(2 pi t / arr), t < arr
+    int half, arr, os, cs, max_support, lh_max;
+    double scaled_cell, trunc_perc;
+    double2* Qs;   // scratch [P][half][half]
+    double2* Ts;   // scratch [P][lh_max][half]
+    double2* convd; // [P][lh_max][lh_max] FP64
+    double* invd;   // [P][cs][cs]
+    int* support;
+};
+
+__device__ __forceinline__ double2 wk_value(const WkParams& q, double w, int px, int py)
+{
+    const int half = q.half;
+    const double dx = double(px) * q.scaled_cell, dy = double(py) * q.scaled_cell;
+    const double r2 = dx * dx + dy * dy;
+    if (r2 >= 1.0)
+        return make_double2(q.aa[half + px] * q.aa[half + py], 0.0);
+    const double nn = sqrt(1.0 - r2);
+    const double ph = (-2.0 * 3.141592653589793238462643383279502884) * w * (nn - 1.0);
+    double sn, cn;
+    sincos(ph, &sn, &cn);
+    const double re = (cn / nn) * q.aa[half + px];
+    const double im = (sn / nn) * q.aa[half + px];
+    return make_double2(re * q.aa[half + py], im * q.aa[half + py]);
+}
+
+__global__ void __launch_bounds__(256) k_wkernel_plane(WkParams q)
+{
+    const int p = blockIdx.x;
+    const int half = q.half, arr = q.arr, os = q.os, lh = q.lh_max;
+    const double w = q.w_avg[p];
+    double2* Q = q.Qs + size_t(p) * half * half;
+    double2* T = q.Ts + size_t(p) * lh * half;
+    double2* conv = q.convd + size_t(p) * lh * lh;
+    __shared__ double2 row0[1024];
+    __shared__ int s_support;
+    auto C = [&](int t) { return q.ctab[t % arr]; };
+    // 1. image-domain quadrant Q[a][b] (row a, column b)
+    for (int t = threadIdx.x; t < half * half; t += blockDim.x) {
+        const int a = t % half, b = t / half;
+        double2 v;
+        if (a == 0 && b == 0)
+            v = make_double2(q.aa[half] * q.aa[half], 0.0);
+        else if (b == 0)
+            v = wk_value(q, w, a, 0);
+        else if (a == 0)
+            v = wk_value(q, w, b, 0); // output(0, i) reuses value(i, 0)
+        else
+            v = wk_value(q, w, a, b);
+        Q[size_t(b) * half + a] = v;
+    }
+    __syncthreads();
+    // 2. T[0][a] = sum_b m_b Q[a][b]
+    for (int a = threadIdx.x; a < half; a += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        for (int b = 0; b < half; b++) {
+            const double m = b == 0 ? 1.0 : 2.0;
+            const double2 v = Q[size_t(b) * half + a];
+            re += v.x * m;
+            im += v.y * m;
+        }
+        T[a] = make_double2(re, im);
+    }
+    __syncthreads();
+    // 3. conv(k, 0) at k = i*os for the truncation (k <= arr/2)
+    const int kmax0 = min(q.max_support * os, arr >> 1);
+    const int nrow = kmax0 / os + 1;
+    for (int t = threadIdx.x; t < nrow && t < 1024; t += blockDim.x) {
+        const int k = t * os;
+        double re = 0.0, im = 0.0;
+        for (int a = 0; a < half; a++) {
+            const double c = (a == 0 ? 1.0 : 2.0) * C(k * a);
+            re += T[a].x * c;
+            im += T[a].y * c;
+        }
+        row0[t] = make_double2(re, im);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int S = q.max_support;
+        if (q.trunc_perc > 0.0) {
+            const double minv = hypot(row0[0].x, row0[0].y) * (q.trunc_perc / 100.0);
+            unsigned i = unsigned(kmax0);
+            while (i > 0) {
+                const double2 v = row0[i / os];
+                if (hypot(v.x, v.y) > minv)
+                    break;
+                i -= os;
+            }
+            S = int(min(unsigned(i / os), unsigned(q.max_support)));
+        }
+        s_support = S;
+        q.support[p] = S;
+    }
+    __syncthreads();
+    const int S = s_support;
+    const int K = 2 * S + 1;
+    const int L = min(S * os + os / 2 + 1, (arr >> 1) + 1);
+    // 4. T[l][a] for l < L
+    for (int t = threadIdx.x; t < L * half; t += blockDim.x) {
+        const int a = t % half, l = t / half;
+        double re = 0.0, im = 0.0;
+        for (int b = 0; b < half; b++) {
+            const double c = (b == 0 ? 1.0 : 2.0) * C(l * b);
+            const double2 v = Q[size_t(b) * half + a];
+            re += v.x * c;
+            im += v.y * c;
+        }
+        T[size_t(l) * half + a] = make_double2(re, im);
+    }
+    __syncthreads();
+    // 5. conv(k, l) for k, l < L
+    for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
+        const int k = t % L, l = t / L;
+        double re = 0.0, im = 0.0;
+        const double2* Tl = T + size_t(l) * half;
+        for (int a = 0; a < half; a++) {
+            const double c = (a == 0 ? 1.0 : 2.0) * C(k * a);
+            re += Tl[a].x * c;
+            im += Tl[a].y * c;
+        }
+        conv[size_t(l) * lh + k] = make_double2(re, im);
+    }
+    __syncthreads();
+    // 6. 1/sum(Re) of each sub-kernel (ty outer, tx inner as in the reference)
+    const int cs = q.cs;
+    for (int t = threadIdx.x; t < cs * cs; t += blockDim.x) {
+        const int x = t % cs, y = t / cs;
+        double ks = 0.0;
+        for (int j = 0; j < K; j++) {
+            int ox = (j - S) * os + os / 2 - x;
+            ox = ox < 0 ? -ox : ox;
+            for (int i = 0; i < K; i++) {
+                int oy = (i - S) * os + os / 2 - y;
+                oy = oy < 0 ? -oy : oy;
+                ks += conv[size_t(oy) * lh + ox].x;
+            }
+        }
+        q.invd[(size_t(p) * cs + y) * cs + x] = 1 / ks;
+    }
+}
+
+__global__ void k_cos_table(int arr, double* c)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < arr)
+        c[t] = cospi(2.0 * double(t) / double(arr));
+}
+
+// FP32 copies of the W-kernel tables for the single-precision gridders.
+__global__ void k_wk_to_f32(const double2* convd, const double* invd, int64_t nconv, int64_t ninv, float2* convf,
+    float* invf)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < nconv)
+        convf[t] = make_float2(float(convd[t].x), float(convd[t].y));
+    if (t < ninv)
+        invf[t] = float(invd[t]);
+}
+
+} // namespace stpgpu

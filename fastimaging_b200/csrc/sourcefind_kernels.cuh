@@ -1,0 +1,662 @@
+// Device kernels of the source finder (src/stp/sourcefind/sourcefind.cpp:22-671,
+// src/stp/common/matrix_math.cpp:20-499, src/stp/common/ccl.h:19-773).
+#pragma once
+
+#include "common.cuh"
+
+namespace stpgpu {
+
+constexpr int SF_THREADS = 256;
+constexpr int BINS_N = 1000; // binapprox / binmedian bin count (matrix_math.cpp:54,339)
+constexpr uint32_t UF_MAX_STEPS = 1u << 26; // bound on union-find loops
+
+template <typename T>
+__device__ __forceinline__ double ld(const T* p, int64_t i)
+{
+    return double(p[i]);
+}
+
+// order-preserving 64-bit key of a double (non-NaN)
+__device__ __forceinline__ unsigned long long okey(double v)
+{
+    unsigned long long u = __double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double okey_inv(unsigned long long k)
+{
+    unsigned long long u = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double(u);
+}
+
+// x86 int(double) conversion (cvttsd2si): truncation, INT_MIN when out of range / NaN.
+__device__ __forceinline__ int int_trunc_x86(double t)
+{
+    if (!(t > -2147483649.0 && t < 2147483648.0))
+        return INT32_MIN;
+    return int(t);
+}
+
+// -------------------------------------------------- deterministic FP64 reductions
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sums(double (&v)[NV], double* out_part)
+{
+    __shared__ double s[NV][SF_THREADS / 32];
+    for (int q = 0; q < NV; q++) {
+        double w = warp_sum(v[q]);
+        if ((threadIdx.x & 31) == 0)
+            s[q][threadIdx.x >> 5] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double t = 0.0;
+        for (int k = 0; k < SF_THREADS / 32; k++)
+            t += s[threadIdx.x][k];
+        out_part[threadIdx.x] = t;
+    }
+}
+
+// sum x, sum x^2 (mat_mean_and_stddev, matrix_math.cpp:457-499)
+template <typename T>
+__global__ void __launch_bounds__(SF_THREADS) k_sum_sq(const T* x, int64_t n, double* part)
+{
+    double v[2] = { 0.0, 0.0 };
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        double a = ld(x, i);
+        v[0] += a;
+        v[1] += a * a;
+    }
+    block_sums<2>(v, part + 2 * blockIdx.x);
+}
+
+// Sum NV-wide partials of nb blocks in a fixed order (one block).
+template <int NV>
+__global__ void k_finish_parts(const double* part, int nb, double* out)
+{
+    __shared__ double s[NV][256];
+    for (int q = 0; q < NV; q++) {
+        double t = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x)
+            t += part[NV * k + q];
+        s[q][threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < NV; q++)
+                s[q][threadIdx.x] += s[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < NV; q++)
+            out[q] = s[q][0];
+}
+
+// Histogram over [leftend, leftend + N/scale] with N+1 bins plus the
+// bottom count (matrix_math.cpp:358-401): bin = int((x - leftend) * scale).
+template <typename T>
+__global__ void __launch_bounds__(SF_THREADS) k_hist(const T* x, int64_t n, double leftend, double scale,
+    unsigned long long* bins /* BINS_N + 2: [0..N] bins, [N+1] bottom */)
+{
+    __shared__ unsigned int h[BINS_N + 2];
+    for (int k = threadIdx.x; k < BINS_N + 2; k += blockDim.x)
+        h[k] = 0;
+    __syncthreads();
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int b = int_trunc_x86((ld(x, i) - leftend) * scale);
+        if (b < 0)
+            atomicAdd(&h[BINS_N + 1], 1u);
+        else if (b <= BINS_N)
+            atomicAdd(&h[b], 1u);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < BINS_N + 2; k += blockDim.x)
+        if (h[k])
+            atomicAdd(&bins[k], (unsigned long long)h[k]);
+}
+
+// -------------------------------------------------- exact selection (nth_element)
+
+// Radix select, 16-bit digits over order keys.  pass: digit index 3..0
+// (most significant first); prefix/mask select the candidates.
+template <typename T>
+__global__ void __launch_bounds__(SF_THREADS) k_radix_hist(const T* x, int64_t n, unsigned long long prefix,
+    unsigned long long mask, int shift, unsigned int* hist /* 65536 */)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const unsigned long long k = okey(ld(x, i));
+        if ((k & mask) == prefix)
+            atomicAdd(&hist[(k >> shift) & 0xffffull], 1u);
+    }
+}
+
+// Single block: find the digit bucket containing rank `state[0]` (0-based
+// among candidates); update prefix/mask/rank in `state`
+// (state: [0] rank, [1] prefix, [2] mask).
+__global__ void k_radix_pick(const unsigned int* hist, int shift, unsigned long long* state)
+{
+    __shared__ unsigned long long s[1024];
+    const unsigned long long rank = state[0]; // read before any thread updates it
+    // each thread owns 64 consecutive digits
+    unsigned long long loc = 0;
+    const int d0 = threadIdx.x * 64;
+    for (int k = 0; k < 64; k++)
+        loc += hist[d0 + k];
+    s[threadIdx.x] = loc;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        unsigned long long t = threadIdx.x >= o ? s[threadIdx.x - o] : 0ull;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    const unsigned long long incl = s[threadIdx.x], excl = incl - loc;
+    if (rank >= excl && rank < incl) {
+        unsigned long long c = excl;
+        for (int k = 0; k < 64; k++) {
+            const unsigned long long h = hist[d0 + k];
+            if (rank < c + h) {
+                state[0] = rank - c;
+                state[1] |= (unsigned long long)(d0 + k) << shift;
+                state[2] |= 0xffffull << shift;
+                break;
+            }
+            c += h;
+        }
+    }
+}
+
+// -------------------------------------------------- sigma clip (estimate_rms)
+
+// One clipping pass (sourcefind.cpp:54-134): samples with
+// |x - median| > upper and not > prev_upper; sums of v, v^2 and the count.
+template <typename T>
+__global__ void __launch_bounds__(SF_THREADS) k_clip_pass(const T* x, int64_t n, double median, double upper,
+    double prev_upper, double* part)
+{
+    double v[3] = { 0.0, 0.0, 0.0 };
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const double d = ld(x, i) - median;
+        const double a = fabs(d);
+        if (a > upper && !(a > prev_upper)) {
+            v[0] += d;
+            v[1] += d * d;
+            v[2] += 1.0;
+        }
+    }
+    block_sums<3>(v, part + 3 * blockIdx.x);
+}
+
+// -------------------------------------------------- connected components
+
+// Scan key of memory pixel (mr, mc): the reference scans display columns
+// c_i = (mc + cols/2) mod cols in order, rows in memory order (ccl.h:162-183).
+struct CclGeom {
+    int rows, cols, rshift, cshift;
+    __device__ __forceinline__ int64_t mem_of_key(int64_t s) const
+    {
+        const int ci = int(s / rows), r = int(s % rows);
+        const int mc = ci >= cshift ? ci - cshift : ci + cshift;
+        return int64_t(mc) * rows + r;
+    }
+};
+
+template <typename T>
+__global__ void k_ccl_init(const T* img, CclGeom g, double tp, double tn, int findneg, uint8_t* cls, uint32_t* P)
+{
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t n = int64_t(g.rows) * g.cols;
+    if (s >= n)
+        return;
+    const double v = ld(img, g.mem_of_key(s));
+    uint8_t c = 0;
+    if (v > tp)
+        c = 1;
+    else if (findneg && v < tn)
+        c = 2;
+    cls[s] = c;
+    P[s] = uint32_t(s);
+}
+
+__device__ __forceinline__ uint32_t uf_find(const uint32_t* P, uint32_t x, unsigned* err)
+{
+    for (uint32_t it = 0; it < UF_MAX_STEPS; it++) {
+        const uint32_t y = P[x];
+        if (y == x)
+            return x;
+        x = y;
+    }
+    atomicOr(err, 2u);
+    return x;
+}
+
+// Lock-free union by minimum root (links the larger root under the smaller),
+// so every component's root is its smallest scan key.
+__device__ __forceinline__ void uf_union(uint32_t* P, uint32_t a, uint32_t b, unsigned* err)
+{
+    for (uint32_t it = 0; it < UF_MAX_STEPS; it++) {
+        a = uf_find(P, a, err);
+        b = uf_find(P, b, err);
+        if (a == b)
+            return;
+        if (a < b) {
+            const uint32_t old = atomicMin(&P[b], a);
+            if (old == b)
+                return;
+            b = old;
+        } else {
+            const uint32_t old = atomicMin(&P[a], b);
+            if (old == a)
+                return;
+            a = old;
+        }
+    }
+    atomicOr(err, 4u);
+}
+
+// Links of the reference's labeling graph, non-FFTSHIFT build
+// (ccl.h:162-342 scan + row border merge, :355-448 column border merge;
+// 4-connectivity :545-745).  With s = (c_i, r):
+//   left       (c_i-1, r)                      c_i >= 1
+//   top        (c_i, r-1)                      r not in {0, rows/2}
+//   row wrap   (c_i, rows-1)                   r == 0
+//   8-conn only:
+//   top-left   (c_i-1, r-1)                    c_i >= 1, r not in {0, rows/2}
+//   bottom-left(c_i-1, r+1)                    c_i >= 1, r not in {rows/2-1, rows-1}
+//   wrap t-left(c_i-1, rows-1)                 c_i >= 1, r == 0
+//   slice link (c_i-1, 0)                      r == rows-1, c_i a slice start
+__global__ void k_ccl_union(const uint8_t* cls, CclGeom g, int conn4, int slice_cols, uint32_t* P, unsigned* err)
+{
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t n = int64_t(g.rows) * g.cols;
+    if (s >= n)
+        return;
+    const uint8_t my = cls[s];
+    if (!my)
+        return;
+    const int rows = g.rows;
+    const int ci = int(s / rows), r = int(s % rows);
+    auto link = [&](int64_t q) {
+        if (cls[q] == my)
+            uf_union(P, uint32_t(s), uint32_t(q), err);
+    };
+    if (ci >= 1)
+        link(s - rows);
+    if (r != 0 && r != g.rshift)
+        link(s - 1);
+    if (r == 0)
+        link(s + rows - 1);
+    if (!conn4 && ci >= 1) {
+        if (r != 0 && r != g.rshift)
+            link(s - rows - 1);
+        if (r != g.rshift - 1 && r != rows - 1)
+            link(s - rows + 1);
+        if (r == 0)
+            link(s - 1);
+        if (r == rows - 1 && (ci % slice_cols) == 0)
+            link(s - 2 * int64_t(rows) + 1);
+    }
+}
+
+__global__ void k_ccl_flatten(const uint8_t* cls, int64_t n, uint32_t* P, unsigned* err)
+{
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= n || !cls[s])
+        return;
+    P[s] = uf_find(P, uint32_t(s), err);
+}
+
+// Per block of SF_THREADS*8 keys: number of positive / negative roots.
+constexpr int RANK_CHUNK = SF_THREADS * 8;
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_rootcount(const uint8_t* cls, const uint32_t* P, int64_t n,
+    uint32_t* cnt_pos, uint32_t* cnt_neg)
+{
+    __shared__ uint32_t sp, sn;
+    if (threadIdx.x == 0)
+        sp = sn = 0;
+    __syncthreads();
+    uint32_t lp = 0, ln = 0;
+    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
+    for (int k = threadIdx.x; k < RANK_CHUNK; k += blockDim.x) {
+        const int64_t s = b0 + k;
+        if (s < n && cls[s] && P[s] == uint32_t(s)) {
+            if (cls[s] == 1)
+                lp++;
+            else
+                ln++;
+        }
+    }
+    atomicAdd(&sp, lp);
+    atomicAdd(&sn, ln);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cnt_pos[blockIdx.x] = sp;
+        cnt_neg[blockIdx.x] = sn;
+    }
+}
+
+// Final label number of each root: 1 + its rank among roots of the same sign
+// in scan order (ccl.h:452-480 numbers roots in increasing provisional-label
+// order, which is scan order of each component's first pixel).
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_rank(const uint8_t* cls, const uint32_t* P, int64_t n,
+    const uint32_t* off_pos, const uint32_t* off_neg, uint32_t* R)
+{
+    __shared__ uint32_t wp[SF_THREADS / 32], wn[SF_THREADS / 32];
+    __shared__ uint32_t base_p, base_n;
+    if (threadIdx.x == 0) {
+        base_p = off_pos[blockIdx.x];
+        base_n = off_neg[blockIdx.x];
+    }
+    __syncthreads();
+    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int round = 0; round < RANK_CHUNK / SF_THREADS; round++) {
+        const int64_t s = b0 + int64_t(round) * SF_THREADS + threadIdx.x;
+        bool isroot = s < n && cls[s] && P[s] == uint32_t(s);
+        const bool pos = isroot && cls[s] == 1;
+        const bool neg = isroot && cls[s] == 2;
+        const unsigned bp = __ballot_sync(0xffffffffu, pos), bn = __ballot_sync(0xffffffffu, neg);
+        if (lane == 0) {
+            wp[warp] = __popc(bp);
+            wn[warp] = __popc(bn);
+        }
+        __syncthreads();
+        uint32_t ep = base_p, en = base_n;
+        for (int w = 0; w < warp; w++) {
+            ep += wp[w];
+            en += wn[w];
+        }
+        const unsigned lm = (1u << lane) - 1u;
+        if (pos)
+            R[s] = ep + __popc(bp & lm) + 1;
+        if (neg)
+            R[s] = en + __popc(bn & lm) + 1;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 0; w < SF_THREADS / 32; w++) {
+                base_p += wp[w];
+                base_n += wn[w];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Label map in memory order: +rank (positive) / -rank (negative), 0 = background.
+__global__ void k_ccl_label(const uint8_t* cls, const uint32_t* P, const uint32_t* R, CclGeom g, int32_t* L)
+{
+    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t n = int64_t(g.rows) * g.cols;
+    if (s >= n)
+        return;
+    const int64_t m = g.mem_of_key(s);
+    const uint8_t c = cls[s];
+    L[m] = c == 0 ? 0 : (c == 1 ? int32_t(R[P[s]]) : -int32_t(R[P[s]]));
+}
+
+// -------------------------------------------------- label analysis
+
+// Extrema (sourcefind.cpp:342-378): init = detection threshold, strict compare.
+template <typename T>
+__global__ void k_extrema(const T* img, const int32_t* L, int64_t n, unsigned long long* ext_pos,
+    unsigned long long* ext_neg)
+{
+    const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (m >= n)
+        return;
+    const int32_t l = L[m];
+    if (l == 0)
+        return;
+    const unsigned long long k = okey(ld(img, m));
+    if (l > 0)
+        atomicMax(&ext_pos[l - 1], k);
+    else
+        atomicMin(&ext_neg[-l - 1], k);
+}
+
+// First memory index holding the extremum (the serial reference keeps the
+// first occurrence in memory order).
+template <typename T>
+__global__ void k_extrema_idx(const T* img, const int32_t* L, int64_t n, const unsigned long long* ext_pos,
+    const unsigned long long* ext_neg, unsigned long long det_pos_key, unsigned long long det_neg_key,
+    unsigned long long* idx_pos, unsigned long long* idx_neg)
+{
+    const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (m >= n)
+        return;
+    const int32_t l = L[m];
+    if (l == 0)
+        return;
+    const unsigned long long k = okey(ld(img, m));
+    if (l > 0) {
+        if (k > det_pos_key && k == ext_pos[l - 1])
+            atomicMin(&idx_pos[l - 1], (unsigned long long)m);
+    } else {
+        if (k < det_neg_key && k == ext_neg[-l - 1])
+            atomicMin(&idx_neg[-l - 1], (unsigned long long)m);
+    }
+}
+
+// Deterministic moments (sourcefind.cpp:457-569).  The foreground pixels of
+// valid labels are compacted in memory order, stably sorted by label, and
+// each label's sums are accumulated sequentially in memory order -- the
+// order of the reference's single-range loop -- with explicitly rounded
+// operations (no FMA contraction), so the sums are bit-identical to it.
+//
+// Pass 1: per chunk of RANK_CHUNK pixels, the number of kept pixels.
+__global__ void __launch_bounds__(SF_THREADS) k_fg_count(const int32_t* L, int64_t n, int np,
+    const unsigned long long* ext_pos, const unsigned long long* ext_neg, unsigned long long det_pos_key,
+    unsigned long long det_neg_key, uint32_t* cnt)
+{
+    __shared__ uint32_t sc;
+    if (threadIdx.x == 0)
+        sc = 0;
+    __syncthreads();
+    uint32_t loc = 0;
+    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
+    for (int k = threadIdx.x; k < RANK_CHUNK; k += blockDim.x) {
+        const int64_t m = b0 + k;
+        if (m >= n)
+            break;
+        const int32_t l = L[m];
+        if (l > 0 ? ext_pos[l - 1] > det_pos_key : (l < 0 && ext_neg[-l - 1] < det_neg_key))
+            loc++;
+    }
+    atomicAdd(&sc, loc);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        cnt[blockIdx.x] = sc;
+    (void)np;
+}
+
+// Pass 2: ordered compaction; key = label code (positives 0..np-1, negatives
+// np..np+nn-1), value = memory index.  Invalid labels are zeroed in the map
+// when generate_labelmap.
+__global__ void __launch_bounds__(SF_THREADS) k_fg_compact(int32_t* L, int64_t n, int np,
+    const unsigned long long* ext_pos, const unsigned long long* ext_neg, unsigned long long det_pos_key,
+    unsigned long long det_neg_key, int generate_labelmap, const uint32_t* off, uint32_t* keys, uint32_t* vals)
+{
+    __shared__ uint32_t wc[SF_THREADS / 32];
+    __shared__ uint32_t base;
+    if (threadIdx.x == 0)
+        base = off[blockIdx.x];
+    __syncthreads();
+    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int round = 0; round < RANK_CHUNK / SF_THREADS; round++) {
+        const int64_t m = b0 + int64_t(round) * SF_THREADS + threadIdx.x;
+        int32_t l = 0;
+        bool keep = false;
+        if (m < n) {
+            l = L[m];
+            if (l != 0) {
+                keep = l > 0 ? ext_pos[l - 1] > det_pos_key : ext_neg[-l - 1] < det_neg_key;
+                if (!keep && generate_labelmap)
+                    L[m] = 0;
+            }
+        }
+        const unsigned b = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0)
+            wc[warp] = __popc(b);
+        __syncthreads();
+        uint32_t e = base;
+        for (int w = 0; w < warp; w++)
+            e += wc[w];
+        if (keep) {
+            const uint32_t pos = e + __popc(b & ((1u << lane) - 1u));
+            keys[pos] = l > 0 ? uint32_t(l - 1) : uint32_t(np + (-l - 1));
+            vals[pos] = uint32_t(m);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int w = 0; w < SF_THREADS / 32; w++)
+                base += wc[w];
+        __syncthreads();
+    }
+}
+
+// Segment starts of the label-sorted list.
+__global__ void k_seg_bounds(const uint32_t* keys, int64_t nk, uint32_t* seg_begin, uint32_t* seg_end)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= nk)
+        return;
+    const uint32_t k = keys[t];
+    if (t == 0 || keys[t - 1] != k)
+        seg_begin[k] = uint32_t(t);
+    if (t == nk - 1 || keys[t + 1] != k)
+        seg_end[k] = uint32_t(t + 1);
+}
+
+// One thread per label: ordered sums over its pixels.  mom: 6 doubles per
+// label code: sum x v, y v, x^2 v, y^2 v, x y v, v (display coordinates).
+template <typename T>
+__global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uint32_t* vals,
+    const uint32_t* seg_begin, const uint32_t* seg_end, double* mom, int* ns)
+{
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nl)
+        return;
+    const uint32_t b = seg_begin[l], e = seg_end[l];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
+    const int vs = rows / 2, hs = cols / 2;
+    for (uint32_t t = b; t < e; t++) {
+        const int64_t m = vals[t];
+        const double val = ld(img, m);
+        const int r = int(m % rows), c = int(m / rows);
+        const double y = r < vs ? double(r + vs) : double(r - vs);
+        const double x = c < hs ? double(c + hs) : double(c - hs);
+        const double xb = __dmul_rn(x, val), yb = __dmul_rn(y, val);
+        a0 = __dadd_rn(a0, xb);
+        a1 = __dadd_rn(a1, yb);
+        a2 = __dadd_rn(a2, __dmul_rn(xb, x));
+        a3 = __dadd_rn(a3, __dmul_rn(yb, y));
+        a4 = __dadd_rn(a4, __dmul_rn(xb, y));
+        a5 = __dadd_rn(a5, val);
+    }
+    double* mo = mom + 6 * size_t(l);
+    mo[0] = a0;
+    mo[1] = a1;
+    mo[2] = a2;
+    mo[3] = a3;
+    mo[4] = a4;
+    mo[5] = a5;
+    ns[l] = int(e - b);
+}
+
+// Moments / sample counts over valid labels with atomics (unordered sums);
+// kept for reference, superseded by the ordered path above.
+template <typename T>
+__global__ void k_moments(const T* img, int32_t* L, int rows, int cols, unsigned long long det_pos_key,
+    unsigned long long det_neg_key, const unsigned long long* ext_pos, const unsigned long long* ext_neg,
+    int generate_labelmap, double* mom_pos, double* mom_neg, int* ns_pos, int* ns_neg)
+{
+    const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t n = int64_t(rows) * cols;
+    if (m >= n)
+        return;
+    const int32_t l = L[m];
+    if (l == 0)
+        return;
+    const bool pos = l > 0;
+    const int idx = pos ? l - 1 : -l - 1;
+    const bool valid = pos ? (ext_pos[idx] > det_pos_key) : (ext_neg[idx] < det_neg_key);
+    if (!valid) {
+        if (generate_labelmap)
+            L[m] = 0;
+        return;
+    }
+    const double val = ld(img, m);
+    const int r = int(m % rows), c = int(m / rows);
+    const int vs = rows / 2, hs = cols / 2;
+    const double y = r < vs ? double(r + vs) : double(r - vs);
+    const double x = c < hs ? double(c + hs) : double(c - hs);
+    const double xb = x * val, yb = y * val;
+    double* mo = (pos ? mom_pos : mom_neg) + 6 * size_t(idx);
+    atomicAdd(pos ? &ns_pos[idx] : &ns_neg[idx], 1);
+    atomicAdd(&mo[0], xb);
+    atomicAdd(&mo[1], yb);
+    atomicAdd(&mo[2], xb * x);
+    atomicAdd(&mo[3], yb * y);
+    atomicAdd(&mo[4], xb * y);
+    atomicAdd(&mo[5], val);
+}
+
+struct IslandRaw {
+    int32_t label;
+    int32_t num_samples;
+    double extremum_val;
+    long long extremum_idx;
+    double mom[6];
+};
+
+// flags for island compaction: positives [0, np), negatives [np, np+nn)
+__global__ void k_island_flags(int np, int nn, const unsigned long long* ext_pos, const unsigned long long* ext_neg,
+    unsigned long long det_pos_key, unsigned long long det_neg_key, const int* ns_pos, const int* ns_neg,
+    int min_area, uint32_t* flags, uint32_t* nvalid)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np + nn)
+        return;
+    bool valid, keep;
+    if (t < np) {
+        valid = ext_pos[t] > det_pos_key;
+        keep = valid && ns_pos[t] >= min_area;
+    } else {
+        valid = ext_neg[t - np] < det_neg_key;
+        keep = valid && ns_neg[t - np] >= min_area;
+    }
+    flags[t] = keep ? 1u : 0u;
+    if (valid)
+        atomicAdd(nvalid, 1u);
+}
+
+__global__ void k_island_scatter(int np, int nn, const uint32_t* flags, const uint32_t* off,
+    const unsigned long long* ext_pos, const unsigned long long* ext_neg, const unsigned long long* idx_pos,
+    const unsigned long long* idx_neg, const int* ns_pos, const int* ns_neg, const double* mom_pos,
+    const double* mom_neg, IslandRaw* out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= np + nn || !flags[t])
+        return;
+    IslandRaw r;
+    const bool pos = t < np;
+    const int i = pos ? t : t - np;
+    r.label = pos ? (i + 1) : -(i + 1);
+    r.num_samples = pos ? ns_pos[i] : ns_neg[i];
+    r.extremum_val = okey_inv(pos ? ext_pos[i] : ext_neg[i]);
+    r.extremum_idx = (long long)(pos ? idx_pos[i] : idx_neg[i]);
+    const double* mo = (pos ? mom_pos : mom_neg) + 6 * size_t(i);
+    for (int q = 0; q < 6; q++)
+        r.mom[q] = mo[q];
+    out[off[t]] = r;
+}
+
+} // namespace stpgpu

@@ -1,0 +1,235 @@
+/*
+ * stpgpu.h -- C ABI of the B200 snapshot imager and source finder.
+ *
+ * Drop-in boundary for the hot path of the Slow Transients Pipeline (STP):
+ *   stp::image_visibilities / stp::ImageVisibilities  (src/stp/imager/imager.h:233-411)
+ *   stp::convolve_to_grid                             (src/stp/gridder/gridder.h:240-997)
+ *   stp::SourceFindImage                              (src/stp/sourcefind/sourcefind.h:143-216)
+ * Plain pointers and sizes only.  All matrices are column-major (Armadillo
+ * layout): element (r, c) of an R x C matrix is at c*R + r.
+ *
+ * Every entry point returns an stpgpu_status (0 = success).  On failure
+ * stpgpu_last_error(ctx) returns a message.  A context is bound to one CUDA
+ * device and owns one stream; calls on one context must be serialised by the
+ * caller, different contexts are independent.
+ */
+#ifndef STPGPU_H
+#define STPGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define STPGPU_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define STPGPU_API __attribute__((visibility("default")))
+#else
+#define STPGPU_API
+#endif
+
+typedef enum {
+    STPGPU_OK = 0,
+    STPGPU_ERR_INVALID_ARG = 1, /* bad sizes / parameters (the reference asserts) */
+    STPGPU_ERR_UNSUPPORTED = 2, /* option outside the GPU path (A-projection, Hankel, Ceres fit) */
+    STPGPU_ERR_CUDA = 3,        /* CUDA runtime error */
+    STPGPU_ERR_CUFFT = 4,       /* cuFFT plan / exec failure (reference: std::runtime_error, fft.cpp:100-103) */
+    STPGPU_ERR_OOM = 5,         /* device allocation failed or admission budget exceeded */
+    STPGPU_ERR_CAPACITY = 6,    /* caller buffer too small; required size returned */
+    STPGPU_ERR_DEVICE = 7,      /* a kernel reported an internal error (bounded loop gave up) */
+    STPGPU_ERR_TIMEOUT = 8,     /* a bounded wait expired */
+    STPGPU_ERR_NO_DEVICE = 9    /* no CUDA device / driver */
+} stpgpu_status;
+
+/* Enum values are those of src/stp/types.h:32-89. */
+typedef enum { STPGPU_TOPHAT = 0, STPGPU_TRIANGLE, STPGPU_SINC, STPGPU_GAUSSIAN, STPGPU_GAUSSIANSINC, STPGPU_PSWF } stpgpu_kernel_function;
+typedef enum { STPGPU_ZEROMEDIAN = 0, STPGPU_BINMEDIAN, STPGPU_BINAPPROX, STPGPU_NTHELEMENT } stpgpu_median_method;
+
+/* Arithmetic of the imager.  FP64 is the plain form matched to the
+ * reference's double build; FP32 uses single-precision visibilities, kernel
+ * weights, grid and FFT; FP32C adds two-sum compensated accumulation of the
+ * grid cells.  uvw -> pixel scaling, W-kernel generation and the final
+ * normalisation stay FP64 in all modes. */
+typedef enum { STPGPU_FP64 = 0, STPGPU_FP32 = 1, STPGPU_FP32C = 2 } stpgpu_precision;
+
+typedef enum { STPGPU_C128 = 0, STPGPU_C64 = 1 } stpgpu_vis_dtype;
+typedef enum { STPGPU_F64 = 0, STPGPU_F32 = 1 } stpgpu_real_dtype;
+
+/* stp::ImagerPars, src/stp/types.h:93-177.  padded_image_size = 0 means
+ * image_size * padding_factor (types.h:157).  r_fft is accepted and ignored
+ * (cuFFT replaces the FFTW planner modes, fft.cpp:53-76). */
+typedef struct {
+    int32_t image_size;
+    int32_t padded_image_size;
+    double cell_size; /* arcsec */
+    double padding_factor;
+    int32_t kernel_function; /* stpgpu_kernel_function */
+    int32_t kernel_support;
+    int32_t kernel_exact;
+    int32_t oversampling;
+    int32_t generate_beam;
+    int32_t gridding_correction;
+    int32_t analytic_gcf;
+    int32_t r_fft;
+} stpgpu_imager_pars;
+
+/* stp::W_ProjectionPars, src/stp/types.h:182-250.  hankel_opt must be 0. */
+typedef struct {
+    int32_t num_wplanes;
+    int32_t max_wpconv_support;
+    int32_t undersampling_opt;
+    double kernel_trunc_perc;
+    int32_t hankel_opt;
+    int32_t hankel_proj_slice;
+    int32_t interp_type;
+    int32_t wplanes_median;
+} stpgpu_wproj_pars;
+
+/* stp::A_ProjectionPars, src/stp/types.h:255-316.  num_timesteps must be 0
+ * (A-projection is outside the GPU path). */
+typedef struct {
+    int32_t num_timesteps;
+    double obs_dec;
+    double obs_ra;
+    int32_t aproj_opt;
+    double aproj_mask_perc;
+} stpgpu_aproj_pars;
+
+/* Per-call imaging report. */
+typedef struct {
+    double sample_grid_total;   /* 2 * sum of good weights (gridder.h:417-423) */
+    int64_t n_good_vis;         /* visibilities that passed the bounds check */
+    int64_t n_grid_items;       /* gridded items incl. mirrored duplicates */
+    int32_t padded_image_size;
+    int32_t image_size;
+    int32_t num_wplanes;
+    int32_t max_plane_support; /* largest truncated W-kernel support */
+    double device_ms;           /* device time of the call (CUDA events) */
+    /* With stpgpu_set_timing(ctx, 1): device time of the phases the
+     * reference reports (reduce/common_functions.cpp:164-228), ms:
+     * [0] grid init (prepass, W-planes and W-kernels, binning),
+     * [1] grid loop (the tile gridder kernel), [2] FFT, [3] normalise. */
+    double phase_ms[4];
+    int32_t n_launches; /* kernels this library launched (cuFFT's excluded) */
+    int32_t reserved;
+} stpgpu_imager_info;
+
+/* One island, stp::IslandParams (src/stp/sourcefind/sourcefind.h:63-133).
+ * moments = Gaussian2dParams from estimate_moments_fit:
+ * {amplitude, x_centre, y_centre, semimajor, semiminor, theta}. */
+typedef struct {
+    int32_t label_idx;
+    int32_t sign;
+    double extremum_val;
+    int32_t extremum_y_idx;
+    int32_t extremum_x_idx;
+    int32_t num_samples;
+    int32_t bbox_top, bbox_bottom, bbox_left, bbox_right;
+    double moments_fit[6];
+    double leastsq_fit[6];
+} stpgpu_island;
+
+/* SourceFindImage ctor arguments, src/stp/sourcefind/sourcefind.h:188-201.
+ * ccl_slice_cols: width of the reference's TBB column slices, which decides
+ * one 8-connectivity link (src/stp/common/ccl.h:207 vs :386); 0 = the
+ * decomposition of an 8-thread host, max(2, cols/8). */
+typedef struct {
+    double detection_n_sigma;
+    double analysis_n_sigma;
+    double rms_est;
+    int32_t find_negative_sources;
+    int32_t sigma_clip_iters;
+    int32_t median_method; /* stpgpu_median_method */
+    int32_t gaussian_fitting; /* must be 0 (Ceres fit outside the GPU path) */
+    int32_t ccl_4connectivity;
+    int32_t generate_labelmap;
+    int32_t source_min_area;
+    int32_t ccl_slice_cols;
+} stpgpu_sf_pars;
+
+typedef struct {
+    double bg_level;
+    double rms_est;
+    double mean;
+    double sigma;
+    int32_t n_labels_pos; /* CCL labels before the detection filter */
+    int32_t n_labels_neg;
+    int32_t n_valid_labels;
+    int32_t n_islands;
+    double device_ms;
+} stpgpu_sf_info;
+
+typedef struct stpgpu_context stpgpu_context;
+
+STPGPU_API int stpgpu_abi_version(void);
+
+/* Create a context on `device` (its own CUDA stream). */
+STPGPU_API stpgpu_status stpgpu_create(int device, stpgpu_context** ctx);
+STPGPU_API stpgpu_status stpgpu_destroy(stpgpu_context* ctx);
+STPGPU_API const char* stpgpu_last_error(const stpgpu_context* ctx);
+/* The context's stream (cudaStream_t), for callers that order work around it. */
+STPGPU_API void* stpgpu_stream(stpgpu_context* ctx);
+/* Record per-phase CUDA events in subsequent imaging calls (info->phase_ms). */
+STPGPU_API stpgpu_status stpgpu_set_timing(stpgpu_context* ctx, int enable);
+/* Release cached device buffers, cuFFT plans and W-kernel caches. */
+STPGPU_API stpgpu_status stpgpu_trim(stpgpu_context* ctx);
+
+/* stp::image_visibilities through stp_python.image_visibilities_wrapper
+ * (src/stp-python/stp_python.cpp:17-140), FP64, host buffers:
+ *   vis      n_vis complex128 (interleaved re, im)
+ *   weights  n_vis float64
+ *   uvw      n_vis x 3 float64, column-major (u[], v[], w[])
+ *   image    image_size^2 float64 out, column-major, unshifted (DC at [0,0])
+ *   beam     nullable; image_size^2 float64 when generate_beam
+ * Sizes are used as given (stp::ImagerPars semantics); the Python binding
+ * rounds them up to multiples of 4 first as stp_python does
+ * (stp_python.cpp:60-67).  When the sampling total is zero the reference
+ * returns empty matrices (imager.h:355); then info->image_size is 0 and
+ * nothing is written. */
+STPGPU_API stpgpu_status stpgpu_image_visibilities(stpgpu_context* ctx, const double* vis, const double* weights, const double* uvw,
+    int64_t n_vis, const stpgpu_imager_pars* pars, const stpgpu_wproj_pars* wproj, const stpgpu_aproj_pars* aproj,
+    double* image, double* beam, stpgpu_imager_info* info);
+
+/* Same computation with explicit precision and memory location.
+ * vis_dtype: STPGPU_C128 or STPGPU_C64; out_dtype: STPGPU_F64 or STPGPU_F32.
+ * device_ptrs != 0: all pointers are device pointers on the context's
+ * device and the call is asynchronous on the context's stream except for
+ * the small scalar read-backs it needs; info->device_ms is then 0. */
+STPGPU_API stpgpu_status stpgpu_image_visibilities_ex(stpgpu_context* ctx, const void* vis, int vis_dtype, const double* weights,
+    const double* uvw, int64_t n_vis, const stpgpu_imager_pars* pars, const stpgpu_wproj_pars* wproj,
+    const stpgpu_aproj_pars* aproj, int precision, void* image, void* beam, int out_dtype, int device_ptrs,
+    stpgpu_imager_info* info);
+
+/* stp::convolve_to_grid (src/stp/gridder/gridder.h:240-997), FP64, host
+ * buffers.  uv: n_vis x 2 column-major in pixels; w: nullable (W-projection
+ * only).  kernel_trunc is the functor's own parameter (truncation radius or
+ * half_base_width).  Grids: rows x image_size complex128 column-major with
+ * rows = image_size/2+1 when halfplane else image_size. */
+STPGPU_API stpgpu_status stpgpu_convolve_to_grid(stpgpu_context* ctx, int kernel_function, double kernel_trunc, int support,
+    int image_size, const double* uv, const double* vis, const double* weights, int64_t n_vis, int kernel_exact,
+    int oversampling, int shift_uv, int halfplane, int generate_beam, const stpgpu_wproj_pars* wproj, const double* w,
+    double cell_size, int analytic_gcf, double* vis_grid, double* sampling_grid, double* sample_grid_total);
+
+/* stp::SourceFindImage (src/stp/sourcefind/sourcefind.cpp:156-292), host
+ * buffers.  image: rows x cols float64 column-major, as produced by the
+ * imager (unshifted).  label_map: nullable rows x cols int32 out.  islands:
+ * capacity entries; *n_islands receives the count (STPGPU_ERR_CAPACITY when
+ * it exceeds capacity, nothing else written). */
+STPGPU_API stpgpu_status stpgpu_source_find(stpgpu_context* ctx, const double* image, int32_t rows, int32_t cols,
+    const stpgpu_sf_pars* pars, int32_t* label_map, stpgpu_island* islands, int32_t capacity, int32_t* n_islands,
+    stpgpu_sf_info* info);
+
+/* Same with image_dtype (STPGPU_F64 / STPGPU_F32) and device pointers for
+ * image and label_map when device_ptrs != 0 (islands stay host memory). */
+STPGPU_API stpgpu_status stpgpu_source_find_ex(stpgpu_context* ctx, const void* image, int image_dtype, int32_t rows, int32_t cols,
+    const stpgpu_sf_pars* pars, int32_t* label_map, int device_ptrs, stpgpu_island* islands, int32_t capacity,
+    int32_t* n_islands, stpgpu_sf_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STPGPU_H */

@@ -1,0 +1,570 @@
+"""CPU oracle for the FastImaging snapshot imager and source finder.
+
+TEST INFRASTRUCTURE ONLY: the checker that the CUDA product is compared with.
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.  It is never on the product path.
+
+The loops live in ``stp_oracle.cpp`` (built into ``liboracle.so``); this
+module orchestrates them the way the reference's ``stp::image_visibilities``
+(``src/stp/imager/imager.h:233-376``), ``stp::convolve_to_grid``
+(``src/stp/gridder/gridder.h:240-997``) and ``stp::SourceFindImage``
+(``src/stp/sourcefind/sourcefind.cpp:156-292``) do, with ``scipy.fft`` in place
+of FFTW 3.3.5 (unnormalised transforms with FFTW's sign conventions).
+
+Parity pins: the restatement is checked against every inline known answer of
+the reference's own gtest suite (tests/golden/reference_pins.json, generated
+from the reference test sources by tests/golden/make_reference_pins.py).  The
+reference's NPZ golden images (the ``test-data`` submodule) are not in the
+reference tree, so whole-imager parity against the original binary is
+unpinned; the imager is pinned through the gridder/kernel/conv unit pins.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.fft
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# Enum values, same order as src/stp/types.h:32-89.
+TopHat, Triangle, Sinc, Gaussian, GaussianSinc, PSWF = range(6)
+ZEROMEDIAN, BINMEDIAN, BINAPPROX, NTHELEMENT = range(4)
+
+_lib_lock = threading.Lock()
+_libs: dict = {}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+def _build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib(fast: bool = False):
+    """Load (building on first use) the oracle shared library."""
+    name = "liboracle_fast.so" if fast else "liboracle.so"
+    with _lib_lock:
+        if name in _libs:
+            return _libs[name]
+        path = os.path.join(HERE, name)
+        src = os.path.join(HERE, "stp_oracle.cpp")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            _build()
+        L = ctypes.CDLL(path)
+        L.orc_grid_prepass.restype = ctypes.c_double
+        L.orc_median_exact.restype = ctypes.c_double
+        L.orc_estimate_rms.restype = ctypes.c_double
+        L.orc_wkernel_truncate.restype = ctypes.c_int
+        L.orc_num_threads.restype = ctypes.c_int
+        _libs[name] = L
+        return L
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _i32(a):
+    return a.ctypes.data_as(_i32p)
+
+
+def _u32(a):
+    return a.ctypes.data_as(_u32p)
+
+
+def _i64(a):
+    return a.ctypes.data_as(_i64p)
+
+
+def arc_sec_to_rad(v):
+    """gridder.h:20."""
+    return (v / 3600.0) * (math.pi / 180.0)
+
+
+# ------------------------------------------------------------------ kernels
+
+def kernel_eval(kf, trunc, r):
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    out = np.empty_like(r)
+    lib().orc_kernel_eval(ctypes.c_int(kf), ctypes.c_double(trunc), _d(r), _d(out), ctypes.c_int64(r.size))
+    return out
+
+
+def gcf_eval(kf, r):
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    out = np.empty_like(r)
+    lib().orc_gcf_eval(ctypes.c_int(kf), _d(r), _d(out), ctypes.c_int64(r.size))
+    return out
+
+
+def make_1d_kernel(kf, trunc, support, offset, oversampling=1, pad=False, normalize=True):
+    n = 2 * (support + (1 if pad else 0)) * oversampling + 1
+    out = np.empty(n)
+    lib().orc_make_1d_kernel(ctypes.c_int(kf), ctypes.c_double(trunc), ctypes.c_int(support), ctypes.c_double(offset),
+                             ctypes.c_int(oversampling), ctypes.c_int(int(pad)), ctypes.c_int(int(normalize)), _d(out))
+    return out
+
+
+def make_kernel_array(kf, trunc, support, offset, oversampling=1, pad=False, normalize=True):
+    n = 2 * (support + (1 if pad else 0)) * oversampling + 1
+    out = np.empty(n * n)
+    lib().orc_make_kernel_array(ctypes.c_int(kf), ctypes.c_double(trunc), ctypes.c_int(support),
+                                ctypes.c_double(offset[0]), ctypes.c_double(offset[1]), ctypes.c_int(oversampling),
+                                ctypes.c_int(int(pad)), ctypes.c_int(int(normalize)), _d(out))
+    return out.reshape((n, n), order="F")
+
+
+def kernel_table_1d(kf, trunc, support, oversampling):
+    cs = (oversampling // 2) * 2 + 1
+    out = np.empty(cs * (2 * support + 1))
+    lib().orc_kernel_table_1d(ctypes.c_int(kf), ctypes.c_double(trunc), ctypes.c_int(support),
+                              ctypes.c_int(oversampling), _d(out))
+    return out.reshape(cs, 2 * support + 1)
+
+
+def populate_kernel_cache(kf, trunc, support, oversampling):
+    """gridder.h:73-105 as a dict {(cp_y, cp_x): K x K matrix}."""
+    t = kernel_table_1d(kf, trunc, support, oversampling)
+    cs = t.shape[0]
+    return {(y, x): np.outer(t[y], t[x]) for y in range(cs) for x in range(cs)}
+
+
+def oversampled_indices(frac, oversampling):
+    frac = np.ascontiguousarray(frac, dtype=np.float64)
+    out = np.empty(frac.shape, dtype=np.int32)
+    lib().orc_oversampled_indices(_d(frac), ctypes.c_int64(frac.size), ctypes.c_int(oversampling), _i32(out))
+    return out
+
+
+def img_dom_kernel(kf, trunc, n, analytic_gcf):
+    """ImgDomKernel, conv_func.h:351-412 (normalize=false)."""
+    centre = n // 2
+    lin = np.arange(n, dtype=np.float64) - centre
+    if analytic_gcf:
+        return gcf_eval(kf, lin / centre)
+    k1 = kernel_eval(kf, trunc, lin)
+    s = float(np.sum(k1))
+    if s > 0.0:
+        k1 = k1 / s
+    arr = np.zeros(n)
+    arr[:centre] = k1[centre:centre + centre]
+    arr[n - centre:n - centre + centre] = k1[:centre]
+    # FFTW_R2HC real parts r_0..r_{n/2}
+    re = scipy.fft.rfft(arr).real
+    aa = np.zeros(n)
+    half = n // 2
+    aa[half:half + half] = re[:half]
+    aa[half - np.arange(1, half + 1)] = re[1:half + 1]
+    return aa
+
+
+# ------------------------------------------------------------------ gridder
+
+@dataclass
+class WProj:
+    num_wplanes: int = 0
+    max_wpconv_support: int = 0
+    undersampling_opt: int = 1
+    kernel_trunc_perc: float = 0.0
+    wplanes_median: bool = False
+
+    @property
+    def enabled(self):
+        return self.num_wplanes > 0
+
+
+@dataclass
+class GridResult:
+    vis_grid: np.ndarray
+    sampling_grid: np.ndarray
+    sample_grid_total: float
+    plane_supports: list = field(default_factory=list)
+    plane_w: list = field(default_factory=list)
+
+
+def _wkernel_workarea(image_size, kernel_size, undersampling_opt):
+    """gridder.h:467-483."""
+    u = int(2 ** (undersampling_opt - 1)) if undersampling_opt > 0 else 0
+    wa = 2
+    if u > 0:
+        while (wa // u) < kernel_size:
+            wa *= 2
+    else:
+        while wa < image_size:
+            wa *= 2
+    return wa
+
+
+def wkernel_plane(w_value, aa, workarea, oversampling, cell_size_arcsec, scaling, max_support, trunc_perc,
+                  current_support):
+    """One W-plane: aw_projection.cpp:173-210 then :366-452.
+
+    Returns (support, cache[cs*cs, K, K] complex, column-major K x K)."""
+    L = lib()
+    arr = workarea * oversampling
+    comb = np.empty(2 * arr * arr)
+    aa = np.ascontiguousarray(aa, dtype=np.float64)
+    L.orc_wkernel_image_domain(ctypes.c_double(w_value), _d(aa), ctypes.c_int(workarea), ctypes.c_int(oversampling),
+                               ctypes.c_double(arc_sec_to_rad(cell_size_arcsec)), ctypes.c_double(scaling), _d(comb))
+    M = comb.view(np.complex128).reshape((arr, arr), order="F")
+    conv = scipy.fft.fft2(M)
+    convF = np.asfortranarray(conv).reshape(-1, order="F").view(np.float64).copy()
+    support = L.orc_wkernel_truncate(_d(convF), ctypes.c_int64(arr), ctypes.c_int(max_support),
+                                     ctypes.c_int(oversampling), ctypes.c_double(trunc_perc),
+                                     ctypes.c_int(current_support))
+    cs = (oversampling // 2) * 2 + 1
+    K = 2 * support + 1
+    cache = np.empty(2 * cs * cs * K * K)
+    L.orc_wkernel_cache(_d(convF), ctypes.c_int64(arr), ctypes.c_int(support), ctypes.c_int(oversampling), _d(cache))
+    return support, cache
+
+
+def convolve_to_grid(kf, support, image_size, uv, vis, weights, kernel_exact=True, oversampling=1, shift_uv=True,
+                     halfplane=True, generate_beam=True, wproj: WProj | None = None, w=None, cell_size=0.0,
+                     analytic_gcf=True, threads=1, fast=False, trunc=None):
+    """stp::convolve_to_grid, gridder.h:240-997.  uv in pixels (n x 2).
+
+    ``trunc`` is the kernel functor's own parameter (truncation radius or
+    half_base_width); ImageVisibilities builds the functor with
+    trunc = kernel_support (imager.cpp:25-64), the default here."""
+    L = lib(fast)
+    trunc = float(support) if trunc is None else float(trunc)
+    wproj = wproj or WProj()
+    n = int(np.asarray(vis).size)
+    uvc = np.asfortranarray(np.asarray(uv, dtype=np.float64).reshape(n, 2)).reshape(-1, order="F").copy()
+    visc = np.ascontiguousarray(np.asarray(vis, dtype=np.complex128).reshape(-1)).view(np.float64).copy()
+    wts = np.ascontiguousarray(np.asarray(weights, dtype=np.float64).reshape(-1)).copy()
+    use_wproj = wproj.enabled
+    wc = np.zeros(n) if w is None else np.ascontiguousarray(np.asarray(w, dtype=np.float64).reshape(-1)).copy()
+    conv_support = support
+    if use_wproj:
+        conv_support = int(wproj.max_wpconv_support)
+        kernel_exact = False
+    if kernel_exact:
+        oversampling = 1
+    else:
+        oversampling = (oversampling >> 1) << 1
+        if oversampling == 0:
+            oversampling = 1
+    good = np.empty(n, dtype=np.int32)
+    kc = np.empty(2 * n, dtype=np.int32)
+    cp = np.empty(2 * n, dtype=np.int32)
+    frac = np.empty(2 * n)
+    total = L.orc_grid_prepass(ctypes.c_int64(n), _d(uvc), _d(visc), _d(wts), _d(wc), ctypes.c_int(int(use_wproj)),
+                               ctypes.c_int(conv_support), ctypes.c_int(image_size), ctypes.c_int(int(kernel_exact)),
+                               ctypes.c_int(oversampling), ctypes.c_int(int(shift_uv)), ctypes.c_int(int(halfplane)),
+                               _i32(good), _i32(kc), _i32(cp), _d(frac))
+    image_rows = image_size // 2 + 1 if halfplane else image_size
+    vg = np.zeros(2 * image_rows * image_size)
+    sg = np.zeros(2 * image_rows * image_size) if generate_beam else np.zeros(2)
+    empty = np.zeros(1)
+    res = GridResult(None, None, total)
+
+    def accumulate(kmode, k1d, wk, sup, b, e):
+        L.orc_grid_accumulate(ctypes.c_int(kmode), ctypes.c_int(kf), ctypes.c_double(trunc), _d(k1d), _d(wk),
+                              ctypes.c_int(sup), ctypes.c_int(image_size), ctypes.c_int(image_rows),
+                              ctypes.c_int(oversampling), ctypes.c_int64(n), ctypes.c_int64(b), ctypes.c_int64(e),
+                              _d(visc), _d(wts), _d(wc), _i32(good), _i32(kc), _i32(cp), _d(frac),
+                              ctypes.c_int(int(generate_beam)), _d(vg), _d(sg), ctypes.c_int(threads))
+
+    if kernel_exact:
+        accumulate(1, empty, empty, support, 0, n)
+    elif not use_wproj:
+        k1d = np.ascontiguousarray(kernel_table_1d(kf, trunc, support, oversampling)).reshape(-1)
+        accumulate(0, k1d, empty, support, 0, n)
+    else:
+        nplanes = int(wproj.num_wplanes)
+        w_avg = np.empty(nplanes)
+        first = np.empty(nplanes, dtype=np.int64)
+        absw = np.abs(wc)
+        L.orc_average_w_planes(_d(absw), _i32(good), ctypes.c_int64(n), ctypes.c_int(nplanes),
+                               ctypes.c_int(int(wproj.wplanes_median)), _d(w_avg), _i64(first))
+        kernel_size = 2 * conv_support + 1
+        workarea = _wkernel_workarea(image_size, kernel_size, wproj.undersampling_opt)
+        scaling = float(image_size) / float(workarea)
+        aa = img_dom_kernel(kf, trunc, workarea, analytic_gcf)
+        cur = int(wproj.max_wpconv_support)
+        for p in range(nplanes):
+            b = int(first[p])
+            e = n if p == nplanes - 1 else int(first[p + 1])
+            cur, cache = wkernel_plane(float(w_avg[p]), aa, workarea, oversampling, cell_size, scaling,
+                                       int(wproj.max_wpconv_support), float(wproj.kernel_trunc_perc), cur)
+            res.plane_supports.append(cur)
+            res.plane_w.append(float(w_avg[p]))
+            accumulate(2, empty, cache, cur, b, e)
+    res.vis_grid = vg.view(np.complex128).reshape((image_rows, image_size), order="F")
+    res.sampling_grid = (sg.view(np.complex128).reshape((image_rows, image_size), order="F") if generate_beam
+                         else np.zeros((0, 0), dtype=np.complex128))
+    return res
+
+
+def convolve_to_grid_functor(kf, trunc, support, image_size, uv, vis, weights, kernel_exact, oversampling, shift_uv,
+                             halfplane, generate_beam):
+    """convolve_to_grid with an explicitly parameterised functor (the
+    reference unit tests build e.g. TopHat(half_base_width) themselves)."""
+    return convolve_to_grid(kf, support, image_size, uv, vis, weights, kernel_exact, oversampling, shift_uv, halfplane,
+                            generate_beam, trunc=trunc)
+
+
+make_kernel_array_functor = make_kernel_array
+
+
+def populate_kernel_cache_functor(kf, trunc, support, oversampling):
+    t = kernel_table_1d(kf, trunc, support, oversampling)
+    cs = t.shape[0]
+    return {(y, x): np.outer(t[y], t[x]) for y in range(cs) for x in range(cs)}
+
+
+def c2r(grid, n, threads=1):
+    """fft_fftw_c2r, fft.cpp:45-135: unnormalised backward 2-D c2r of a
+    (n/2+1) x n column-major half-plane grid into an n x n column-major image."""
+    X = np.asarray(grid).T  # axis 0 = columns (slow FFTW dim), axis 1 = half axis
+    Y = scipy.fft.irfft2(X, s=(n, n), norm="forward", workers=threads)
+    return np.asfortranarray(Y.T)
+
+
+def normalise(img, padded, image_size, normalization_factor, gcf, grid_correction, threads=1, fast=False):
+    out = np.empty(image_size * image_size)
+    imgF = np.asfortranarray(img, dtype=np.float64)
+    g = np.ascontiguousarray(gcf if gcf is not None else np.ones(padded), dtype=np.float64)
+    lib(fast).orc_normalise(_d(imgF.reshape(-1, order="F")), ctypes.c_int64(padded), ctypes.c_int64(image_size),
+                            ctypes.c_double(normalization_factor), _d(g), ctypes.c_int(int(grid_correction)), _d(out),
+                            ctypes.c_int(threads))
+    return out.reshape((image_size, image_size), order="F")
+
+
+def image_visibilities(vis, weights, uvw, image_size, cell_size, padding_factor=1.0, kernel_func=PSWF,
+                       kernel_support=3, kernel_exact=True, oversampling=8, generate_beam=False,
+                       gridding_correction=True, analytic_gcf=False, num_wplanes=0, wplanes_median=False,
+                       max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, threads=1, fast=False,
+                       return_grid=False):
+    """stp_python.image_visibilities_wrapper (stp-python/stp_python.cpp:17-140)
+    -> ImageVisibilities (stp/imager/imager.cpp:12-68) -> image_visibilities
+    (stp/imager/imager.h:233-376).  Returns (image, beam)."""
+    image_size = int(image_size)
+    while image_size % 4:
+        image_size += 1
+    padded = int(float(image_size) * padding_factor)
+    while padded % 4:
+        padded += 1
+    uvw = np.asarray(uvw, dtype=np.float64).reshape(-1, 3)
+    inv = arc_sec_to_rad(cell_size) * float(padded)
+    uv = np.empty((uvw.shape[0], 2))
+    uv[:, 0] = uvw[:, 0] * inv
+    uv[:, 1] = uvw[:, 1] * inv
+    wp = WProj(num_wplanes, max_wpconv_support, undersampling_opt, kernel_trunc_perc, wplanes_median)
+    g = convolve_to_grid(kernel_func, kernel_support, padded, uv, vis, weights, kernel_exact, oversampling, True,
+                         True, generate_beam, wp, uvw[:, 2], cell_size, analytic_gcf, threads, fast)
+    img = c2r(g.vis_grid, padded, threads)
+    beam = c2r(g.sampling_grid, padded, threads) if generate_beam else None
+    out_img = np.zeros((0, 0))
+    out_beam = np.zeros((0, 0))
+    if g.sample_grid_total > 0.0:
+        nf = 1.0 / g.sample_grid_total
+        gcf = img_dom_kernel(kernel_func, float(kernel_support), padded, analytic_gcf) if gridding_correction else None
+        out_img = normalise(img, padded, image_size, nf, gcf, gridding_correction, threads, fast)
+        if generate_beam:
+            out_beam = normalise(beam, padded, image_size, nf, gcf, gridding_correction, threads, fast)
+    if return_grid:
+        return out_img, out_beam, g
+    return out_img, out_beam
+
+
+# ------------------------------------------------------------------ source finder
+
+def mean_std(x):
+    x = np.asfortranarray(x, dtype=np.float64).reshape(-1, order="F")
+    m = ctypes.c_double()
+    s = ctypes.c_double()
+    lib().orc_mean_std(_d(x), ctypes.c_int64(x.size), ctypes.byref(m), ctypes.byref(s))
+    return m.value, s.value
+
+
+def median_exact(x):
+    x = np.asfortranarray(x, dtype=np.float64).reshape(-1, order="F")
+    return lib().orc_median_exact(_d(x), ctypes.c_int64(x.size))
+
+
+def median_binapprox(x):
+    x = np.asfortranarray(x, dtype=np.float64).reshape(-1, order="F")
+    m, s, md = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    lib().orc_median_binapprox(_d(x), ctypes.c_int64(x.size), ctypes.byref(m), ctypes.byref(s), ctypes.byref(md))
+    return m.value, s.value, md.value
+
+
+def median_binmedian(x):
+    x = np.asfortranarray(x, dtype=np.float64).reshape(-1, order="F")
+    m, s, md = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    lib().orc_median_binmedian(_d(x), ctypes.c_int64(x.size), ctypes.byref(m), ctypes.byref(s), ctypes.byref(md))
+    return m.value, s.value, md.value
+
+
+def estimate_rms(x, num_sigma, iters, mean, sigma, median):
+    x = np.asfortranarray(x, dtype=np.float64).reshape(-1, order="F")
+    return lib().orc_estimate_rms(_d(x), ctypes.c_int64(x.size), ctypes.c_double(num_sigma), ctypes.c_int(iters),
+                                  ctypes.c_double(mean), ctypes.c_double(sigma), ctypes.c_double(median))
+
+
+def default_slice_cols(cols):
+    """Column-slice width of the reference's TBB scan on an 8-thread host:
+    static_partitioner over blocked_range(0, cols, max(cols/32, 2))."""
+    return max(2, cols // 8)
+
+
+def ccl(data, thr_pos, thr_neg, find_negative=True, conn4=False, slice_cols=0):
+    data = np.asfortranarray(data, dtype=np.float64)
+    rows, cols = data.shape
+    if slice_cols <= 0:
+        slice_cols = default_slice_cols(cols)
+    L = np.zeros(rows * cols, dtype=np.int32)
+    plen = cols * rows // 2
+    Pp = np.zeros(plen, dtype=np.uint32)
+    Pn = np.zeros(plen, dtype=np.uint32)
+    npos, nneg = ctypes.c_uint32(), ctypes.c_uint32()
+    lib().orc_ccl(_d(data.reshape(-1, order="F")), ctypes.c_int(rows), ctypes.c_int(cols), ctypes.c_double(thr_pos),
+                  ctypes.c_double(thr_neg), ctypes.c_int(int(find_negative)), ctypes.c_int(int(conn4)),
+                  ctypes.c_int(slice_cols), _i32(L), _u32(Pp), _u32(Pn), ctypes.byref(npos), ctypes.byref(nneg))
+    return L, Pp, Pn, npos.value, nneg.value
+
+
+@dataclass
+class Gaussian2dParams:
+    """fitting.h:90-150 (fields as bound by stp_python.cpp:224-235)."""
+    amplitude: float = 0.0
+    x_centre: float = 0.0
+    y_centre: float = 0.0
+    semimajor: float = 0.0
+    semiminor: float = 0.0
+    theta: float = 0.0
+
+    def convert_to_constrained_parameters(self):
+        """fitting.cpp:32-57."""
+        half_pi = math.pi / 2.0
+        self.semimajor = math.fabs(self.semimajor)
+        self.semiminor = math.fabs(self.semiminor)
+        if self.semimajor < self.semiminor:
+            self.semimajor, self.semiminor = self.semiminor, self.semimajor
+            self.theta += half_pi
+        t = math.fmod(self.theta, math.pi)
+        if t <= -half_pi:
+            t += math.pi
+        elif t > half_pi:
+            t -= math.pi
+        self.theta = t
+
+
+def _csqrt(x):
+    return math.sqrt(x) if x >= 0 else float("nan")
+
+
+def _clog(x):
+    if x > 0:
+        return math.log(x)
+    return float("-inf") if x == 0 else float("nan")
+
+
+def moments_fit(sign, extremum_val, x_bar, y_bar, xx_bar, yy_bar, xy_bar, rms_est, analysis_n_sigma):
+    """IslandParams::estimate_moments_fit, sourcefind.cpp:691-717."""
+    w1 = (xx_bar + yy_bar) / 2.0
+    w2 = _csqrt(((xx_bar - yy_bar) * (xx_bar - yy_bar) / 4) + xy_bar * xy_bar)
+    tmaj = w1 + w2
+    tmin = w1 - w2
+    thr = analysis_n_sigma * rms_est
+    ratio = sign * extremum_val / thr
+    with np.errstate(all="ignore"):
+        scale = 1.0 - _clog(ratio) / (ratio - 1.0) if ratio != 1.0 else float("nan")
+        smaj = _csqrt(tmaj / scale) if scale != 0 else float("inf")
+        smin = _csqrt(tmin / scale) if scale != 0 else float("inf")
+        den = xx_bar - yy_bar
+        arg = 2.0 * xy_bar / den if den != 0 else math.copysign(float("inf"), 2.0 * xy_bar) if xy_bar != 0 else float("nan")
+        theta = 0.5 * math.atan(arg) if not math.isnan(arg) else float("nan")
+    if theta * xy_bar < 0.0:
+        theta += math.pi / 2.0
+    g = Gaussian2dParams(extremum_val, x_bar, y_bar, smaj, smin, theta)
+    g.convert_to_constrained_parameters()
+    return g
+
+
+@dataclass
+class SourceFindResult:
+    islands: list
+    label_map: np.ndarray
+    bg_level: float
+    rms_est: float
+    n_pos: int
+    n_neg: int
+    label_valid_pos: np.ndarray
+    label_valid_neg: np.ndarray
+
+
+def source_find(image, detection_n_sigma, analysis_n_sigma, rms_est=0.0, find_negative_sources=True,
+                sigma_clip_iters=5, median_method=BINAPPROX, gaussian_fitting=False, ccl_4connectivity=False,
+                generate_labelmap=True, source_min_area=5, slice_cols=0):
+    """SourceFindImage ctor, sourcefind.cpp:156-292 (+ the python tuple layout,
+    stp_python.cpp:142-179).  Islands: (sign, extremum_val, x_idx, y_idx,
+    num_samples, moments_fit, leastsq_fit, ceres_report)."""
+    if gaussian_fitting:
+        raise NotImplementedError("Gaussian fitting (Ceres) is not restated")
+    data = np.asfortranarray(image, dtype=np.float64)
+    rows, cols = data.shape
+    mean = sigma = None
+    if median_method == ZEROMEDIAN:
+        median = 0.0
+    elif median_method == BINAPPROX:
+        mean, sigma, median = median_binapprox(data)
+    elif median_method == BINMEDIAN:
+        mean, sigma, median = median_binmedian(data)
+    elif median_method == NTHELEMENT:
+        median = median_exact(data)
+    else:
+        raise ValueError("median_method")
+    bg = median
+    if abs(rms_est) > 0.0:
+        rms = rms_est
+    else:
+        if mean is None:
+            mean, sigma = mean_std(data)
+        rms = estimate_rms(data, 3.0, sigma_clip_iters, mean, sigma, median)
+    a_pos = bg + analysis_n_sigma * rms
+    a_neg = bg - analysis_n_sigma * rms
+    d_pos = bg + detection_n_sigma * rms
+    d_neg = bg - detection_n_sigma * rms
+    L, Pp, Pn, npos, nneg = ccl(data, a_pos, a_neg, find_negative_sources, ccl_4connectivity, slice_cols)
+    ev_p = np.empty(npos)
+    ei_p = np.empty(npos, dtype=np.int64)
+    mo_p = np.empty(5 * npos)
+    ns_p = np.empty(npos, dtype=np.int32)
+    va_p = np.empty(npos, dtype=np.int32)
+    ev_n = np.empty(nneg)
+    ei_n = np.empty(nneg, dtype=np.int64)
+    mo_n = np.empty(5 * nneg)
+    ns_n = np.empty(nneg, dtype=np.int32)
+    va_n = np.empty(nneg, dtype=np.int32)
+    dataflat = data.reshape(-1, order="F")
+    lib().orc_label_analysis(_d(dataflat), ctypes.c_int(rows), ctypes.c_int(cols), _i32(L), _u32(Pp), _u32(Pn),
+                             ctypes.c_uint32(npos), ctypes.c_uint32(nneg), ctypes.c_double(d_pos),
+                             ctypes.c_double(d_neg), ctypes.c_int(int(generate_labelmap)), _d(ev_p), _i64(ei_p),
+                             _d(mo_p), _i32(ns_p), _i32(va_p), _d(ev_n), _i64(ei_n), _d(mo_n), _i32(ns_n), _i32(va_n))
+    islands = []
+    vs, hs = rows // 2, cols // 2
+    for sign, n_l, ev, ei, mo, ns, va in ((1, npos, ev_p, ei_p, mo_p, ns_p, va_p), (-1, nneg, ev_n, ei_n, mo_n, ns_n, va_n)):
+        for i in range(n_l):
+            if not va[i]:
+                continue
+            r, c = int(ei[i] % rows), int(ei[i] // rows)
+            y = r + vs if r < vs else r - vs
+            x = c + hs if c < hs else c - hs
+            if ns[i] >= source_min_area:
+                m = mo[5 * i:5 * i + 5]
+                g = moments_fit(sign, float(ev[i]), m[0], m[1], m[2], m[3], m[4], rms, analysis_n_sigma)
+                islands.append((sign, float(ev[i]), x, y, int(ns[i]), g, Gaussian2dParams(), ""))
+    return SourceFindResult(islands, L.reshape((rows, cols), order="F"), bg, rms, npos, nneg, va_p, va_n)

@@ -1,0 +1,163 @@
+"""GPU parity of the imager through the C ABI, against the CPU oracle.
+
+Tolerances: FP64 path within 1e-10 peak-relative error of the oracle (the
+reference's fptolerance for double builds, src/stp/types.h:26); FP32 and
+compensated FP32 within 1e-5 peak-relative of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from fastimaging_b200 import capi
+from fastimaging_b200.synthetic import make_snapshot
+from oracle import stp_oracle as orc
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-10
+TOL32 = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+def peak_rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+KF = {"TopHat": 0, "Triangle": 1, "Sinc": 2, "Gaussian": 3, "GaussianSinc": 4, "PSWF": 5}
+
+
+@pytest.mark.parametrize("name", ["SmallPillbox", "MultiPixelPillbox", "MultipleComplexVis", "NearbyComplexVis",
+                                  "SinglePixelOverlapPillbox"])
+def test_gridder_reference_pins(ctx, pins, name):
+    c = next(x for x in pins["gridder"] if x["name"] == name)
+    vis = np.array([complex(a, b) for a, b in c["vis"]])
+    vg, sg, tot = ctx.convolve_to_grid(KF[c["kernel"]], c["hbw"], c["support"], c["image_size"], np.array(c["uv"]),
+                                       vis, np.array(c["weights"]), c["kernel_exact"], c["oversampling"],
+                                       c["shift_uv"], c["halfplane"], True)
+    assert np.max(np.abs(vg.real - np.array(c["expect_vis_grid_real"]))) < TOL64
+    if c["expect_sampling_real"] is not None:
+        assert np.max(np.abs(sg.real - np.array(c["expect_sampling_real"]))) < TOL64
+
+
+def test_gridder_halfplane_shifted_pin(ctx, pins):
+    c = next(x for x in pins["gridder"] if x["name"] == "HalfPlaneShiftedGridding")
+    vis = np.ones(2, complex)
+    for exact in (False, True):
+        vg, sg, tot = ctx.convolve_to_grid(0, c["hbw"], c["support"], 8, np.array(c["uv"]), vis, np.ones(2), exact,
+                                           c["oversampling"], True, True, True)
+        assert np.max(np.abs(np.roll(vg, 4, axis=1).real - np.array(c["expect_vis_grid_real"]))) < TOL64
+
+
+@pytest.mark.parametrize("mode", ["oversampled", "exact", "fullplane_noshift", "exact_fullplane"])
+@pytest.mark.parametrize("kf", [4, 5, 1])
+def test_gridder_random_vs_oracle(ctx, mode, kf):
+    rng = np.random.default_rng(11 + kf)
+    N, n, S = 64, 300, 3
+    uv = rng.uniform(-N / 2 + 1, N / 2 - 1, size=(n, 2))
+    uv[:20, 1] = rng.uniform(-S - 1.2, S + 1.2, size=20)  # near v = 0: mirrored duplicates
+    vis = rng.normal(size=n) + 1j * rng.normal(size=n)
+    w = rng.uniform(0.5, 2.0, size=n)
+    exact = mode.startswith("exact")
+    half = mode in ("oversampled", "exact")
+    shift = half
+    g, s, t = ctx.convolve_to_grid(kf, float(S), S, N, uv, vis, w, exact, 8, shift, half, True)
+    r = orc.convolve_to_grid(kf, S, N, uv, vis, w, exact, 8, shift, half, True)
+    assert abs(t - r.sample_grid_total) <= 1e-12 * abs(r.sample_grid_total)
+    assert peak_rel(g, r.vis_grid) < 1e-12
+    assert peak_rel(s, r.sampling_grid) < 1e-12
+
+
+def _imager_case(seed, N, n, **kw):
+    return make_snapshot(seed, n, N, 2.0, n_src=4, flux=(1.0, 5.0), noise_sigma=0.05, **kw)
+
+
+@pytest.mark.parametrize("kf,exact,analytic", [(4, False, False), (5, False, True), (5, False, False),
+                                                (4, True, False), (2, False, False), (3, False, True)])
+def test_imager_fp64_vs_oracle(ctx, kf, exact, analytic):
+    s = _imager_case(5 + kf, 256, 3000)
+    kw = dict(kernel_func=kf, kernel_support=3, kernel_exact=exact, oversampling=8, gridding_correction=True,
+              analytic_gcf=analytic, generate_beam=True)
+    img, beam, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    ri, rb = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, oversampling=8, **{
+        k: v for k, v in kw.items() if k != "oversampling"})
+    assert info.image_size == 256
+    assert peak_rel(img, ri) < TOL64
+    assert peak_rel(beam, rb) < TOL64
+
+
+def test_imager_padding_crop(ctx):
+    s = _imager_case(21, 192, 2500)
+    kw = dict(kernel_func=5, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=True)
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 192, s.cell_size, padding_factor=1.5, **kw)
+    ri, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 192, s.cell_size, padding_factor=1.5, **kw)
+    assert info.padded_image_size == 288
+    assert peak_rel(img, ri) < TOL64
+
+
+@pytest.mark.parametrize("median", [False, True])
+def test_imager_wproj_fp64_vs_oracle(ctx, median):
+    s = _imager_case(31, 256, 6000, w_range=(-800.0, 800.0))
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              num_wplanes=6, max_wpconv_support=8, undersampling_opt=1, kernel_trunc_perc=1.0,
+              wplanes_median=median)
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    ri, _, g = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, return_grid=True, **kw)
+    assert info.max_plane_support == max(g.plane_supports)
+    assert peak_rel(img, ri) < TOL64
+
+
+def test_imager_wproj_untruncated(ctx):
+    s = _imager_case(33, 128, 3000, w_range=(-3000.0, 3000.0))
+    kw = dict(kernel_func=5, kernel_support=3, kernel_exact=False, oversampling=4, analytic_gcf=True,
+              num_wplanes=4, max_wpconv_support=5, kernel_trunc_perc=0.0)
+    img, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 128, s.cell_size, **kw)
+    ri, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 128, s.cell_size, **kw)
+    assert peak_rel(img, ri) < TOL64
+
+
+@pytest.mark.parametrize("precision", [capi.FP32, capi.FP32C])
+def test_imager_fp32_vs_fp64_oracle(ctx, precision):
+    s = _imager_case(41, 512, 20000, w_range=(-500.0, 500.0))
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              num_wplanes=4, max_wpconv_support=8, kernel_trunc_perc=1.0)
+    img, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 512, s.cell_size, precision=precision,
+                                       out_dtype=capi.F32, **kw)
+    ri, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 512, s.cell_size, **kw)
+    assert peak_rel(img.astype(np.float64), ri) < TOL32
+
+
+def test_imager_empty_and_out_of_bounds(ctx):
+    """No good visibilities -> the reference returns empty matrices (imager.h:355)."""
+    uvw = np.asfortranarray(np.array([[1e9, 1e9, 0.0], [-1e9, 0.0, 0.0]]))
+    img, beam, info = ctx.image_visibilities(np.ones(2, complex), np.ones(2), uvw, 64, 1.0, kernel_exact=False,
+                                             oversampling=8)
+    assert info.image_size == 0 and img.size == 0
+    img, beam, info = ctx.image_visibilities(np.zeros(0, complex), np.zeros(0), np.zeros((0, 3)), 64, 1.0,
+                                             kernel_exact=False, oversampling=8)
+    assert info.image_size == 0
+
+
+def test_imager_rejects_unsupported(ctx):
+    s = _imager_case(1, 64, 100)
+    with pytest.raises(capi.StpGpuError) as e:
+        ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, num_wplanes=2, max_wpconv_support=4,
+                               kernel_exact=False, hankel_opt=True)
+    assert e.value.status == 2
+    with pytest.raises(capi.StpGpuError) as e:
+        ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, aproj_numtimesteps=2, kernel_exact=False)
+    assert e.value.status == 2
+    with pytest.raises(capi.StpGpuError) as e:
+        ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, -1.0)
+    assert e.value.status == 1
+
+
+def test_imager_repeatable(ctx):
+    """Two calls on the same context give the same image (cached buffers reused)."""
+    s = _imager_case(3, 256, 4000)
+    a, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, kernel_exact=False)
+    b, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, kernel_exact=False)
+    assert peak_rel(a, b) < 1e-13

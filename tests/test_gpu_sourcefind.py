@@ -1,0 +1,106 @@
+"""GPU parity of the source finder through the C ABI: labels bit-exact to the
+oracle (and to the reference's own expected label maps), statistics within
+1e-10 relative."""
+import numpy as np
+import pytest
+
+from fastimaging_b200 import capi
+from fastimaging_b200.synthetic import make_snapshot
+from oracle import stp_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("idx", range(12))
+def test_labeling_reference_maps(ctx, pins, idx):
+    c = pins["labeling"][idx]
+    img = np.array(c["img"], dtype=np.float64)
+    exp = np.array(c["expected_map"], dtype=np.int32)
+    for sgn in (1, -1):
+        data = np.fft.fftshift(sgn * img)
+        isl, lab, info = ctx.source_find(data, c["detection_n_sigma"], c["analysis_n_sigma"], c["rms_est"], True, 5,
+                                         capi.ZEROMEDIAN, False, c["conn4"], c["generate_labelmap"],
+                                         c["source_min_area"])
+        assert len(isl) == c["expected_total_islands"], (c["name"], sgn)
+        assert np.array_equal(np.fft.fftshift(lab), sgn * exp), (c["name"], sgn)
+
+
+def _compare(isl, ref, lab, rl, rtol=1e-9):
+    assert np.array_equal(lab, rl)
+    assert len(isl) == len(ref.islands)
+    for a, b in zip(isl, ref.islands):
+        sign, val, x, y, ns, mom, _, _ = b
+        assert a.sign == sign and a.extremum_x_idx == x and a.extremum_y_idx == y and a.num_samples == ns
+        assert a.extremum_val == val
+        got = np.array(a.moments_fit[:])
+        want = np.array([mom.amplitude, mom.x_centre, mom.y_centre, mom.semimajor, mom.semiminor, mom.theta])
+        ok = np.isclose(got, want, rtol=rtol, atol=1e-9) | (np.isnan(got) & np.isnan(want))
+        assert ok.all(), (got, want)
+
+
+@pytest.mark.parametrize("conn4", [False, True])
+@pytest.mark.parametrize("slice_cols", [0, 1, 64])
+def test_labels_injected_thresholds(ctx, conn4, slice_cols):
+    """Thresholds fixed (ZEROMEDIAN + given rms): labels must be bit-exact."""
+    rng = np.random.default_rng(5)
+    img = rng.normal(size=(256, 256))
+    img[100:110, 30:38] += 8.0
+    img[0:3, :] += 4.0  # structures across the shifted-topology seams
+    img[:, 127:130] -= 5.0
+    ref = orc.source_find(img, 4.0, 2.5, 1.0, True, 5, orc.ZEROMEDIAN, False, conn4, True, 3, slice_cols)
+    isl, lab, info = ctx.source_find(img, 4.0, 2.5, 1.0, True, 5, capi.ZEROMEDIAN, False, conn4, True, 3, slice_cols)
+    assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
+    _compare(isl, ref, lab, ref.label_map)
+
+
+@pytest.mark.parametrize("method", [capi.BINAPPROX, capi.BINMEDIAN, capi.NTHELEMENT, capi.ZEROMEDIAN])
+def test_source_find_end_to_end(ctx, method):
+    """Median + sigma-clip RMS estimated on the device; bg and rms match the
+    oracle to 1e-10 relative, labels bit-exact (no pixel lies within rounding
+    distance of a threshold, checked)."""
+    s = make_snapshot(7, 20000, 256, 2.0, n_src=6, flux=(2.0, 8.0), noise_sigma=0.3, n_extended=2)
+    img, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, kernel_func=5, kernel_exact=False,
+                                    oversampling=8, analytic_gcf=True)
+    ref = orc.source_find(img, 5.0, 3.0, 0.0, True, 5, method, False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, 5, method, False, False, True, 5)
+    assert abs(info.bg_level - ref.bg_level) <= 1e-10 * max(1e-300, abs(ref.rms_est))
+    assert abs(info.rms_est - ref.rms_est) <= 1e-10 * abs(ref.rms_est)
+    thr = [ref.bg_level + k * ref.rms_est for k in (3.0, -3.0, 5.0, -5.0)]
+    near = min(float(np.min(np.abs(img - t))) for t in thr)
+    if near < 1e-9 * ref.rms_est:
+        pytest.skip("a pixel sits on a threshold")
+    _compare(isl, ref, lab, ref.label_map)
+
+
+def test_source_find_float32_input(ctx):
+    rng = np.random.default_rng(9)
+    img = rng.normal(size=(128, 192)).astype(np.float32)
+    img[40:44, 50:55] += 9
+    ref = orc.source_find(img.astype(np.float64), 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5)
+    assert abs(info.rms_est - ref.rms_est) <= 1e-10 * ref.rms_est
+    _compare(isl, ref, lab, ref.label_map)
+
+
+def test_source_find_no_labelmap_cleanup(ctx):
+    rng = np.random.default_rng(13)
+    img = rng.normal(size=(64, 64))
+    img[10:12, 10:12] += 10
+    ref = orc.source_find(img, 5.0, 3.0, 1.0, False, 5, orc.ZEROMEDIAN, False, False, False, 1)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 1.0, False, 5, capi.ZEROMEDIAN, False, False, False, 1)
+    _compare(isl, ref, lab, ref.label_map)
+
+
+def test_source_find_rejects(ctx):
+    with pytest.raises(capi.StpGpuError):
+        ctx.source_find(np.zeros((7, 8)), 5, 3)
+    with pytest.raises(capi.StpGpuError) as e:
+        ctx.source_find(np.zeros((8, 8)), 5, 3, gaussian_fitting=True)
+    assert e.value.status == 2
