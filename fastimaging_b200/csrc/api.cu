@@ -563,9 +563,14 @@ template <typename R>
 const double* device_gcf(stpgpu_context* c, const ImagerSetup& s)
 {
     double* gcf = c->buf<double>("gcf", s.N);
+    c->buf<double>("gcfinv", s.N);
     if (c->memo("gcf", std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(s.N) + "/"
-                          + std::to_string(s.analytic)))
+                          + std::to_string(s.analytic))
+        && c->memo("gcfinv", std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(s.N) + "/"
+            + std::to_string(s.analytic)))
         return gcf;
+    c->memo("gcfinv", std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(s.N) + "/"
+            + std::to_string(s.analytic));
     double ksum_inv = 1.0;
     const int dmax = int(std::floor(s.trunc)) + 1;
     if (!s.analytic) {
@@ -576,6 +581,9 @@ const double* device_gcf(stpgpu_context* c, const ImagerSetup& s)
         ksum_inv = ssum > 0.0 ? 1.0 / ssum : 1.0;
     }
     k_imgdom_kernel<<<grid1d(s.N, 256), 256, 0, c->stream>>>(s.kf, s.trunc, s.N, s.analytic, ksum_inv, dmax, gcf);
+    STPGPU_CHECK_LAUNCH();
+    double* ginv = c->buf<double>("gcfinv", s.N);
+    k_reciprocal<<<grid1d(s.N, 256), 256, 0, c->stream>>>(gcf, ginv, s.N);
     STPGPU_CHECK_LAUNCH();
     return gcf;
 }
@@ -607,13 +615,15 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
             fail(STPGPU_ERR_CUFFT, "cuFFT c2r execution failed (" + std::to_string(int(r)) + ")");
     };
     const double* gcf = correction ? device_gcf<R>(c, s) : nullptr;
-    const dim3 ngrid(grid1d(image_size, 256), image_size);
+    const double* ginv = correction ? c->buf<double>("gcfinv", s.N) : nullptr;
+    (void)gcf;
+    const dim3 ngrid(std::min<unsigned>(grid1d(image_size, 256), 4), image_size);
     auto normalise = [&](void* out) {
         if (out_f32)
-            k_normalise<R, float><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, gcf, correction,
+            k_normalise<R, float><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, ginv, correction,
                 reinterpret_cast<float*>(out));
         else
-            k_normalise<R, double><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, gcf, correction,
+            k_normalise<R, double><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, ginv, correction,
                 reinterpret_cast<double*>(out));
         STPGPU_CHECK_LAUNCH();
     };
@@ -1371,3 +1381,4 @@ stpgpu_status stpgpu_source_find(stpgpu_context* c, const double* image, int32_t
 }
 
 } // extern "C"
+

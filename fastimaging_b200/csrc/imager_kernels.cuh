@@ -571,6 +571,8 @@ __global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
         t.ksum = 1.0;
         R vr = R(0), vim = R(0);
         int rb = 0, cb = 0;
+        int cbase = 0, jlo = 0, jhi = 0;
+        bool cwrap = false;
         unsigned long long key = ~0ull;
         if (active) {
             const uint32_t code = p.list[e];
@@ -592,6 +594,12 @@ __global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
             t.wt = it.w;
             rb = cy - t.S;
             cb = cx - t.S;
+            // column window of the footprint inside this tile; only footprints
+            // crossing the grid edge need the per-tap wrap
+            cwrap = cb < 0 || cb + t.K > p.N;
+            cbase = cb - c0;
+            jlo = cwrap ? 0 : max(0, -cbase);
+            jhi = cwrap ? t.K : min(t.K, TILE_C - cbase);
             const int krow = ((rb % p.N) + p.N) % p.N, kcol = ((cb % p.N) + p.N) % p.N;
             key = (unsigned long long)krow * (unsigned long long)p.N + (unsigned long long)kcol;
             if (KMODE == KM_WPROJ) {
@@ -634,22 +642,63 @@ __global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
             int kmax = mine ? t.K : 0;
             for (int o = 16; o > 0; o >>= 1)
                 kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-            for (int i = 0; i < kmax; i++) {
-                const int rm = (mine && i < t.K) ? map_row(rb + i, p.N, p.image_rows, wrap_neg) : -1;
-                const int rl = rm - r0;
-                const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
-                for (int j = 0; j < kmax; j++) {
-                    const int cl = map_col(cb + j, p.N) - c0;
-                    if (rok && j < t.K && cl >= 0 && cl < TILE_C) {
-                        R kr, ki;
-                        tap_value<R, KMODE>(p, tab, t, i, j, kr, ki);
-                        const R re = vr * kr - vim * ki;
-                        const R im = vr * ki + vim * kr;
-                        acc_rmw(&acc[cl * TILE_R + rl], re, im);
-                        if (BEAM)
-                            acc_rmw(&bacc[cl * TILE_R + rl], kr, ki);
+            if (KMODE != KM_EXACT) {
+                // tabulated kernels: the lane's kernel row is fetched into
+                // registers eight taps at a time, so the loads are in flight
+                // together, then accumulated tap by tap in lockstep
+                for (int i = 0; i < kmax; i++) {
+                    const int rm = (mine && i < t.K) ? map_row(rb + i, p.N, p.image_rows, wrap_neg) : -1;
+                    const int rl = rm - r0;
+                    const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
+                    for (int j0 = 0; j0 < kmax; j0 += 8) {
+                        R kr[8], ki[8];
+#pragma unroll
+                        for (int jj = 0; jj < 8; jj++) {
+                            const int j = j0 + jj;
+                            kr[jj] = R(0);
+                            ki[jj] = R(0);
+                            if (rok && j < t.K && j >= jlo && j < jhi)
+                                tap_value<R, KMODE>(p, tab, t, i, j, kr[jj], ki[jj]);
+                        }
+#pragma unroll
+                        for (int jj = 0; jj < 8; jj++) {
+                            const int j = j0 + jj;
+                            if (j < kmax) {
+                                if (rok && j < t.K && j >= jlo && j < jhi) {
+                                    const int cl = cwrap ? map_col(cb + j, p.N) - c0 : cbase + j;
+                                    if (cl >= 0 && cl < TILE_C) {
+                                        const R re = vr * kr[jj] - vim * ki[jj];
+                                        const R im = vr * ki[jj] + vim * kr[jj];
+                                        acc_rmw(&acc[cl * TILE_R + rl], re, im);
+                                        if (BEAM)
+                                            acc_rmw(&bacc[cl * TILE_R + rl], kr[jj], ki[jj]);
+                                    }
+                                }
+                                __syncwarp();
+                            }
+                        }
                     }
-                    __syncwarp();
+                }
+            } else {
+                for (int i = 0; i < kmax; i++) {
+                    const int rm = (mine && i < t.K) ? map_row(rb + i, p.N, p.image_rows, wrap_neg) : -1;
+                    const int rl = rm - r0;
+                    const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
+                    for (int j = 0; j < kmax; j++) {
+                        if (rok && j < t.K && j >= jlo && j < jhi) {
+                            const int cl = cwrap ? map_col(cb + j, p.N) - c0 : cbase + j;
+                            if (cl >= 0 && cl < TILE_C) {
+                                R kr, ki;
+                                tap_value<R, KMODE>(p, tab, t, i, j, kr, ki);
+                                const R re = vr * kr - vim * ki;
+                                const R im = vr * ki + vim * kr;
+                                acc_rmw(&acc[cl * TILE_R + rl], re, im);
+                                if (BEAM)
+                                    acc_rmw(&bacc[cl * TILE_R + rl], kr, ki);
+                            }
+                        }
+                        __syncwarp();
+                    }
                 }
             }
         }
@@ -748,22 +797,32 @@ __global__ void k_imgdom_kernel(int kf, double trunc, int n, int analytic, doubl
 // 1/sum and divide by gcf[ii]*gcf[jj].  blockIdx.y = output column; the
 // factor 1/sum is read from the device (0 when the sampling total is 0).
 template <typename RI, typename RO>
-__global__ void k_normalise(const RI* __restrict__ img, int padded, int image_size, const double* total,
-    const double* __restrict__ gcf, int corr, RO* __restrict__ out)
+__global__ void __launch_bounds__(256) k_normalise(const RI* __restrict__ img, int padded, int image_size,
+    const double* total, const double* __restrict__ ginv, int corr, RO* __restrict__ out)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
-    if (i >= image_size)
-        return;
     const double tot = total[0];
     const double nf = tot > 0.0 ? 1.0 / tot : 0.0;
     const int hp = padded / 2, hs = image_size / 2;
     const int oj = j < hs ? j : padded + j - image_size;
     const int jj = j < hs ? j + hp : hp + j - image_size;
-    const int oi = i < hs ? i : padded - hs + (i - hs);
-    const int ii = i < hs ? hp + i : hp - hs + (i - hs);
-    const double v = double(img[size_t(oj) * padded + oi]);
-    out[size_t(j) * image_size + i] = RO(corr ? v * nf / (gcf[ii] * gcf[jj]) : v * nf);
+    // value * (1/sum) / (gcf[ii] * gcf[jj]) as value * (nf * 1/gcf[jj]) * 1/gcf[ii]
+    const double fj = corr ? nf * ginv[jj] : nf;
+    const RI* src = img + size_t(oj) * padded;
+    RO* dst = out + size_t(j) * image_size;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < image_size; i += gridDim.x * blockDim.x) {
+        const int oi = i < hs ? i : padded - hs + (i - hs);
+        const int ii = i < hs ? hp + i : hp - hs + (i - hs);
+        const double v = double(src[oi]) * fj;
+        dst[i] = RO(corr ? v * ginv[ii] : v);
+    }
+}
+
+__global__ void k_reciprocal(const double* in, double* out, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = 1.0 / in[i];
 }
 
 // ---------------------------------------------------------------- W-projection
