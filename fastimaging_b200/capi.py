@@ -85,7 +85,8 @@ class SfInfo(ctypes.Structure):
 
 EXPORTED = ["stpgpu_abi_version", "stpgpu_create", "stpgpu_destroy", "stpgpu_last_error", "stpgpu_stream",
             "stpgpu_set_timing", "stpgpu_trim", "stpgpu_image_visibilities", "stpgpu_image_visibilities_ex", "stpgpu_convolve_to_grid",
-            "stpgpu_source_find", "stpgpu_source_find_ex"]
+            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_label_noalloc"]
+NOALLOC_MAX_PIXELS = 1024 * 1024
 
 _lock = threading.Lock()
 _lib = None
@@ -126,6 +127,10 @@ def load():
         L.stpgpu_source_find_ex.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(SfPars), vp, ctypes.c_int, vp, ctypes.c_int32,
                                             ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(SfInfo)]
+        L.stpgpu_label_noalloc.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
         return L
 
@@ -274,3 +279,19 @@ class Context:
             break
         islands = [buf[i] for i in range(nis.value)]
         return islands, labels, info
+
+
+def label_noalloc(device, stream, image_ptr, image_dtype, rows, cols, thresh_pos, thresh_neg, find_negative_sources=True,
+                  ccl_4connectivity=False, ccl_slice_cols=0, label_ptr=None):
+    """Allocation-free labelling (stpgpu_label_noalloc): device image in, device
+    int32 label map out (both raw device addresses).  Returns (n_pos, n_neg)."""
+    L = load()
+    npos, nneg = ctypes.c_int32(), ctypes.c_int32()
+    msg = ctypes.create_string_buffer(256)
+    st = L.stpgpu_label_noalloc(int(device), ctypes.c_void_p(stream or 0), ctypes.c_void_p(image_ptr),
+                                int(image_dtype), int(rows), int(cols), float(thresh_pos), float(thresh_neg),
+                                int(bool(find_negative_sources)), int(bool(ccl_4connectivity)), int(ccl_slice_cols),
+                                ctypes.c_void_p(label_ptr), ctypes.byref(npos), ctypes.byref(nneg), msg, len(msg))
+    if st != 0:
+        raise StpGpuError(st, msg.value.decode(errors="replace"))
+    return npos.value, nneg.value

@@ -12,6 +12,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <type_traits>
@@ -1382,3 +1383,171 @@ stpgpu_status stpgpu_source_find(stpgpu_context* c, const double* image, int32_t
 
 } // extern "C"
 
+// ------------------------------------------------------- allocation-free labelling
+//
+// stpgpu_label_noalloc runs the connected-component labeller (k_ccl_* above)
+// with its working arrays in one file-scope device array instead of
+// context-owned buffers.  It exists for callers that must not allocate:
+//  * a real-time detection stage that runs between the imaging launches of a
+//    stream-ordered pipeline: cudaMalloc/cudaFree synchronise the whole device
+//    and would stall the imaging streams that share it, breaking the snapshot
+//    cadence;
+//  * a process whose device memory is already owned by another allocator (a
+//    caching allocator or a memory pool that reserved the free HBM up front),
+//    where an allocation by this library could fail with out-of-memory in the
+//    middle of a run;
+// neither can create a stpgpu_context, which allocates its buffers, stream and
+// events.  The call makes no cudaMalloc, cudaFree or allocating library call;
+// host-side it uses no heap either (no exceptions, strings or containers).
+//
+// Scratch layout for n = rows * cols pixels (byte offsets, 256-aligned):
+//   cls  n bytes        pixel class (0 background, 1 positive, 2 negative)
+//   P    n uint32       union-find parents
+//   R    n uint32       final label number of each root
+//   err  2 uint32       union-find step-bound flag; MUST start at zero, so
+//                       every call clears it before the first kernel
+//   cpos, cneg, opos, oneg   (nchunks + 1) uint32 each: roots per chunk of
+//                       RANK_CHUNK keys and their exclusive scans
+// Everything except err is fully written before it is read in each call.
+// The array is shared by every call on a device: two calls whose kernels
+// overlap on the GPU (different streams, or different host threads) race on
+// it and give wrong labels.
+
+namespace stpgpu {
+
+constexpr size_t noalloc_align(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t noalloc_chunks(size_t n) { return (n + RANK_CHUNK - 1) / RANK_CHUNK; }
+constexpr size_t noalloc_bytes(size_t n)
+{
+    return noalloc_align(n) + 2 * noalloc_align(4 * n) + 256 + 4 * noalloc_align(4 * (noalloc_chunks(n) + 1));
+}
+constexpr size_t kNoallocScratchBytes = noalloc_bytes(STPGPU_NOALLOC_MAX_PIXELS);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static unsigned char* g_noalloc_ptr[kNoallocMaxDevices] = {};
+
+static stpgpu_status noalloc_msg(char* buf, size_t len, stpgpu_status s, const char* what, cudaError_t e)
+{
+    if (buf && len)
+        std::snprintf(buf, len, "%s%s%s", what, e == cudaSuccess ? "" : ": ",
+            e == cudaSuccess ? "" : cudaGetErrorString(e));
+    return s;
+}
+
+template <typename T>
+static cudaError_t noalloc_label_run(unsigned char* base, cudaStream_t st, const T* img, int rows, int cols,
+    double tp, double tn, int findneg, int conn4, int slice, int32_t* L, uint32_t* h)
+{
+    const int64_t n = int64_t(rows) * cols;
+    const size_t nch = noalloc_chunks(size_t(n));
+    size_t o = 0;
+    uint8_t* cls = base + o;
+    o += noalloc_align(size_t(n));
+    uint32_t* P = reinterpret_cast<uint32_t*>(base + o);
+    o += noalloc_align(4 * size_t(n));
+    uint32_t* R = reinterpret_cast<uint32_t*>(base + o);
+    o += noalloc_align(4 * size_t(n));
+    unsigned int* err = reinterpret_cast<unsigned int*>(base + o);
+    o += 256;
+    uint32_t* cnt[4];
+    for (int k = 0; k < 4; k++) {
+        cnt[k] = reinterpret_cast<uint32_t*>(base + o);
+        o += noalloc_align(4 * (nch + 1));
+    }
+    cudaError_t e = cudaMemsetAsync(err, 0, 2 * sizeof(unsigned int), st);
+    if (e != cudaSuccess)
+        return e;
+    const CclGeom geom { rows, cols, rows / 2, cols / 2 };
+    const int nchunks = int(nch);
+    k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(img, geom, tp, tn, findneg, cls, P);
+    k_ccl_union<<<grid1d(n, 256), 256, 0, st>>>(cls, geom, conn4, slice, P, err);
+    k_ccl_flatten<<<grid1d(n, 256), 256, 0, st>>>(cls, n, P, err);
+    k_ccl_rootcount<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, cnt[0], cnt[1]);
+    k_scan_single<<<1, 1024, 0, st>>>(cnt[0], cnt[2], nchunks);
+    k_scan_single<<<1, 1024, 0, st>>>(cnt[1], cnt[3], nchunks);
+    k_ccl_rank<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, cnt[2], cnt[3], R);
+    k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(cls, P, R, geom, L);
+    g_launches += 8;
+    if ((e = cudaGetLastError()) != cudaSuccess)
+        return e;
+    // counts and the step-bound flag, read back into host stack memory
+    if ((e = cudaMemcpyAsync(&h[0], cnt[2] + nchunks, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(&h[1], cnt[3] + nchunks, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemcpyAsync(&h[2], err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return e;
+    return cudaStreamSynchronize(st);
+}
+
+} // namespace stpgpu
+
+extern "C" stpgpu_status stpgpu_label_noalloc(int device, void* stream, const void* image, int image_dtype,
+    int32_t rows, int32_t cols, double analysis_thresh_pos, double analysis_thresh_neg, int find_negative_sources,
+    int ccl_4connectivity, int ccl_slice_cols, int32_t* label_map, int32_t* n_labels_pos, int32_t* n_labels_neg,
+    char* err_msg, size_t err_msg_len)
+{
+    using namespace stpgpu;
+    if (err_msg && err_msg_len)
+        err_msg[0] = '\0';
+    if (!image || !label_map)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_INVALID_ARG, "null image or label_map", cudaSuccess);
+    if (image_dtype != STPGPU_F64 && image_dtype != STPGPU_F32)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_INVALID_ARG, "image_dtype", cudaSuccess);
+    if (rows <= 0 || cols <= 0 || (rows % 2) || (cols % 2) || rows > 65536 || cols > 65536)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_INVALID_ARG,
+            "image dimensions must be positive, even and at most 65536 (ccl.h:116-119)", cudaSuccess);
+    if (int64_t(rows) * cols > int64_t(STPGPU_NOALLOC_MAX_PIXELS)) {
+        if (err_msg && err_msg_len)
+            std::snprintf(err_msg, err_msg_len,
+                "image of %lld pixels exceeds the allocation-free labeller's maximum of %lld pixels",
+                (long long)(int64_t(rows) * cols), (long long)STPGPU_NOALLOC_MAX_PIXELS);
+        return STPGPU_ERR_INVALID_ARG;
+    }
+    if (device < 0 || device >= kNoallocMaxDevices)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_INVALID_ARG, "device ordinal", cudaSuccess);
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_NO_DEVICE, "cudaGetDevice", e);
+    if ((e = cudaSetDevice(device)) != cudaSuccess)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_NO_DEVICE, "cudaSetDevice", e);
+    unsigned char* base = nullptr;
+    {
+        // set-up, once per device, with that device current
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[device]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                cudaSetDevice(prev);
+                return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_CUDA, "cudaGetSymbolAddress(scratch)", e);
+            }
+            g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+        }
+        base = g_noalloc_ptr[device];
+    }
+    const int slice = ccl_slice_cols > 0 ? ccl_slice_cols : std::max(2, cols / 8);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint32_t h[3] = { 0, 0, 0 }; // positive labels, negative labels, step-bound flag
+    if (image_dtype == STPGPU_F32)
+        e = noalloc_label_run<float>(base, st, static_cast<const float*>(image), rows, cols, analysis_thresh_pos,
+            analysis_thresh_neg, find_negative_sources, ccl_4connectivity, slice, label_map, h);
+    else
+        e = noalloc_label_run<double>(base, st, static_cast<const double*>(image), rows, cols, analysis_thresh_pos,
+            analysis_thresh_neg, find_negative_sources, ccl_4connectivity, slice, label_map, h);
+    cudaSetDevice(prev);
+    if (e != cudaSuccess)
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_CUDA, "labelling", e);
+    if (h[2])
+        return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)",
+            cudaSuccess);
+    if (n_labels_pos)
+        *n_labels_pos = int32_t(h[0]);
+    if (n_labels_neg)
+        *n_labels_neg = int32_t(h[1]);
+    return STPGPU_OK;
+}

@@ -228,6 +228,30 @@ STPGPU_API stpgpu_status stpgpu_source_find_ex(stpgpu_context* ctx, const void* 
     const stpgpu_sf_pars* pars, int32_t* label_map, int device_ptrs, stpgpu_island* islands, int32_t capacity,
     int32_t* n_islands, stpgpu_sf_info* info);
 
+/* Allocation-free connected-component labelling.  No counterpart in the
+ * reference: it is the labelling step of stpgpu_source_find (the reference's
+ * labeling_8con / labeling_4con, src/stp/common/ccl.h:107-504) for callers
+ * that cannot allocate device memory (a detection stage between the launches
+ * of a stream-ordered imaging pipeline, where cudaMalloc/cudaFree would
+ * synchronise the device; a process whose HBM is already reserved by another
+ * allocator).  It needs no context, allocates nothing, and keeps its working
+ * arrays in one static device array of 9 bytes per pixel plus the per-chunk
+ * counts; images above STPGPU_NOALLOC_MAX_PIXELS pixels are rejected with
+ * STPGPU_ERR_INVALID_ARG.  image (rows x cols, column-major, image_dtype
+ * STPGPU_F64 / STPGPU_F32) and label_map (rows x cols int32) are device
+ * pointers on `device`; stream is a cudaStream_t (NULL: the legacy default
+ * stream).  Pixels > analysis_thresh_pos are positive, < analysis_thresh_neg
+ * negative (when find_negative_sources); labels are numbered as
+ * stpgpu_source_find numbers them before its detection filter, and
+ * ccl_slice_cols <= 0 selects max(2, cols / 8).  The call returns after the
+ * labels are written.  The scratch array is shared by all calls on a device:
+ * calls whose work overlaps on the GPU race on it.  err_msg (nullable)
+ * receives a message on failure. */
+#define STPGPU_NOALLOC_MAX_PIXELS (1024 * 1024)
+STPGPU_API stpgpu_status stpgpu_label_noalloc(int device, void* stream, const void* image, int image_dtype, int32_t rows,
+    int32_t cols, double analysis_thresh_pos, double analysis_thresh_neg, int find_negative_sources, int ccl_4connectivity,
+    int ccl_slice_cols, int32_t* label_map, int32_t* n_labels_pos, int32_t* n_labels_neg, char* err_msg, size_t err_msg_len);
+
 #ifdef __cplusplus
 }
 #endif
