@@ -1411,7 +1411,9 @@ stpgpu_status stpgpu_source_find(stpgpu_context* c, const double* image, int32_t
 // Everything except err is fully written before it is read in each call.
 // The array is shared by every call on a device: two calls whose kernels
 // overlap on the GPU (different streams, or different host threads) race on
-// it and give wrong labels.
+// it and give wrong labels.  The first call on a device resolves the array's
+// device address (cudaGetSymbolAddress, that device current) and caches it;
+// that first call should come before any stream capture.
 
 namespace stpgpu {
 

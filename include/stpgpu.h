@@ -244,9 +244,12 @@ STPGPU_API stpgpu_status stpgpu_source_find_ex(stpgpu_context* ctx, const void* 
  * negative (when find_negative_sources); labels are numbered as
  * stpgpu_source_find numbers them before its detection filter, and
  * ccl_slice_cols <= 0 selects max(2, cols / 8).  The call returns after the
- * labels are written.  The scratch array is shared by all calls on a device:
- * calls whose work overlaps on the GPU race on it.  err_msg (nullable)
- * receives a message on failure. */
+ * labels are written.  The scratch array is shared by all calls on a device
+ * and keeps the previous call's contents (each call clears what must start at
+ * zero): calls whose work overlaps on the GPU race on it.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.
+ * err_msg (nullable) receives a message on failure. */
 #define STPGPU_NOALLOC_MAX_PIXELS (1024 * 1024)
 STPGPU_API stpgpu_status stpgpu_label_noalloc(int device, void* stream, const void* image, int image_dtype, int32_t rows,
     int32_t cols, double analysis_thresh_pos, double analysis_thresh_neg, int find_negative_sources, int ccl_4connectivity,
