@@ -83,9 +83,33 @@ class SfInfo(ctypes.Structure):
                 ("n_valid_labels", ctypes.c_int32), ("n_islands", ctypes.c_int32), ("device_ms", ctypes.c_double)]
 
 
+class Snapshot(ctypes.Structure):
+    _fields_ = [("vis", ctypes.c_void_p), ("vis_dtype", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("weights", ctypes.c_void_p), ("uvw", ctypes.c_void_p), ("n_vis", ctypes.c_int64),
+                ("pars", ImagerPars), ("wproj", WProjPars), ("image", ctypes.c_void_p)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("device_ms", ctypes.c_double), ("graph", ctypes.c_int32), ("gridder_launches", ctypes.c_int32),
+                ("tuned_classes", ctypes.c_int32), ("n_launches", ctypes.c_int32)]
+
+
+def imager_pars(image_size, cell_size, padding_factor=1.0, kernel_func=PSWF, kernel_support=3, kernel_exact=True,
+                oversampling=8, generate_beam=False, gridding_correction=True, analytic_gcf=False, num_wplanes=0,
+                wplanes_median=False, max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0,
+                padded_image_size=0, **_):
+    """(ImagerPars, WProjPars) from image_visibilities-style keywords."""
+    ip = ImagerPars(int(image_size), int(padded_image_size), float(cell_size), float(padding_factor),
+                    int(kernel_func), int(kernel_support), int(bool(kernel_exact)), int(oversampling),
+                    int(bool(generate_beam)), int(bool(gridding_correction)), int(bool(analytic_gcf)), 0)
+    wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc), 0, 0,
+                   0, int(bool(wplanes_median)))
+    return ip, wp
+
+
 EXPORTED = ["stpgpu_abi_version", "stpgpu_create", "stpgpu_destroy", "stpgpu_last_error", "stpgpu_stream",
             "stpgpu_set_timing", "stpgpu_trim", "stpgpu_image_visibilities", "stpgpu_image_visibilities_ex", "stpgpu_convolve_to_grid",
-            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_label_noalloc"]
+            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_image_batch", "stpgpu_label_noalloc"]
 NOALLOC_MAX_PIXELS = 1024 * 1024
 
 _lock = threading.Lock()
@@ -127,6 +151,8 @@ def load():
         L.stpgpu_source_find_ex.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(SfPars), vp, ctypes.c_int, vp, ctypes.c_int32,
                                             ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(SfInfo)]
+        L.stpgpu_image_batch.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
+                                         ctypes.POINTER(BatchInfo)]
         L.stpgpu_label_noalloc.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
@@ -221,6 +247,43 @@ class Context:
         if info.image_size == 0:
             return np.zeros((0, 0)), np.zeros((0, 0)), info
         return img, (beam if beam is not None else np.zeros((0, 0))), info
+
+    def image_batch(self, snapshots, precision=FP32C, out_dtype=F32, device_ptrs=True):
+        """stpgpu_image_batch over a list of dicts, one per snapshot:
+        vis, weights, uvw, image (torch CUDA tensors when device_ptrs, uvw
+        (3, n) contiguous; numpy arrays otherwise, uvw (n, 3)), plus the
+        image_visibilities keywords (image_size, cell_size, kernel_func, ...).
+        Returns (images, infos, batch_info); images are the given outputs
+        (device) or new F-ordered arrays (host)."""
+        n = len(snapshots)
+        arr = (Snapshot * n)()
+        keep, outs = [], []
+        odt = np.float32 if out_dtype == F32 else np.float64
+        for i, sd in enumerate(snapshots):
+            ip, wp = imager_pars(**{k: v for k, v in sd.items() if k not in ("vis", "weights", "uvw", "image")})
+            if device_ptrs:
+                vis, w, uvw, img = sd["vis"], sd["weights"], sd["uvw"], sd["image"]
+                nv = int(w.numel())
+                vdt = C64 if str(vis.dtype).endswith("complex64") else C128
+            else:
+                vis = np.ascontiguousarray(sd["vis"])
+                if vis.dtype not in (np.complex128, np.complex64):
+                    vis = vis.astype(np.complex128)
+                vdt = C64 if vis.dtype == np.complex64 else C128
+                nv = vis.size
+                w = np.ascontiguousarray(sd["weights"], dtype=np.float64).reshape(-1)
+                uvw = np.asfortranarray(np.asarray(sd["uvw"], dtype=np.float64).reshape(nv, 3))
+                img = sd.get("image")
+                if img is None:
+                    img = np.empty((int(sd["image_size"]), int(sd["image_size"])), dtype=odt, order="F")
+            keep += [vis, w, uvw, img]
+            outs.append(img)
+            arr[i] = Snapshot(_ptr(vis), vdt, 0, _ptr(w), _ptr(uvw), nv, ip, wp, _ptr(img))
+        infos = (ImagerInfo * n)()
+        bi = BatchInfo()
+        self._check(self.L.stpgpu_image_batch(self.h, arr, n, int(precision), int(out_dtype), int(bool(device_ptrs)),
+                                               infos, ctypes.byref(bi)))
+        return outs, list(infos), bi
 
     def convolve_to_grid(self, kernel_func, kernel_trunc, support, image_size, uv, vis, weights, kernel_exact=True,
                          oversampling=1, shift_uv=True, halfplane=True, generate_beam=True, num_wplanes=0,

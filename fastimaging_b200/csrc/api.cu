@@ -45,7 +45,34 @@ struct stpgpu_context {
             STPGPU_CUDA_TRY(cudaEventRecord(pev[k], stream));
     }
     std::map<std::string, DevBuf> bufs;
-    std::map<std::tuple<int, int>, cufftHandle> plans; // (N, cufftType)
+    std::map<std::tuple<int, int, cudaStream_t>, cufftHandle> plans; // (N, cufftType, stream)
+    // Prefix of buffer and memo names: the batch path gives every snapshot
+    // slot its own buffers ("b<i>/"); single calls use "".
+    std::string ns;
+
+    // batch path: worker streams, fork/join events, the captured graph of
+    // the last batch signature, the tile-width choice per size class and a
+    // pinned staging area (gridder parameter tables, scalar read-back)
+    std::vector<cudaStream_t> wstreams;
+    std::vector<cudaEvent_t> wevents;
+    cudaEvent_t fork_ev = nullptr;
+    std::string batch_sig;
+    int batch_calls = 0;
+    cudaGraph_t batch_graph = nullptr;
+    cudaGraphExec_t batch_exec = nullptr;
+    std::map<std::string, int> tune;
+    void* batch_host = nullptr;
+    size_t batch_host_cap = 0;
+
+    void drop_graph()
+    {
+        if (batch_exec)
+            cudaGraphExecDestroy(batch_exec);
+        if (batch_graph)
+            cudaGraphDestroy(batch_graph);
+        batch_exec = nullptr;
+        batch_graph = nullptr;
+    }
     void* pinned = nullptr;
     size_t pinned_cap = 0;
     std::map<std::string, std::string> memo_keys; // buffer name -> key of its current contents
@@ -54,10 +81,10 @@ struct stpgpu_context {
     // (static tables: gcf, kernel tables, cos tables); records `key`.
     bool memo(const std::string& name, const std::string& key)
     {
-        auto it = memo_keys.find(name);
+        auto it = memo_keys.find(ns + name);
         if (it != memo_keys.end() && it->second == key)
             return true;
-        memo_keys[name] = key;
+        memo_keys[ns + name] = key;
         return false;
     }
 
@@ -66,7 +93,7 @@ struct stpgpu_context {
     T* buf(const std::string& name, size_t count)
     {
         const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
-        DevBuf& b = bufs[name];
+        DevBuf& b = bufs[ns + name];
         if (b.cap < bytes) {
             if (b.p) {
                 STPGPU_CUDA_TRY(cudaStreamSynchronize(stream));
@@ -77,7 +104,7 @@ struct stpgpu_context {
             const size_t want = bytes + bytes / 8;
             STPGPU_CUDA_TRY(cudaMalloc(&b.p, want));
             b.cap = want;
-            memo_keys.erase(name);
+            memo_keys.erase(ns + name);
         }
         return reinterpret_cast<T*>(b.p);
     }
@@ -99,9 +126,11 @@ struct stpgpu_context {
         return reinterpret_cast<T*>(pinned);
     }
 
+    // One plan per (size, type, stream): a plan's work area must not be
+    // shared by transforms running concurrently on different streams.
     cufftHandle plan(int N, cufftType type)
     {
-        const auto key = std::make_tuple(N, int(type));
+        const auto key = std::make_tuple(N, int(type), stream);
         auto it = plans.find(key);
         if (it != plans.end())
             return it->second;
@@ -120,6 +149,11 @@ struct stpgpu_context {
     {
         if (stream)
             cudaStreamSynchronize(stream);
+        for (auto w : wstreams)
+            cudaStreamSynchronize(w);
+        drop_graph();
+        batch_sig.clear();
+        batch_calls = 0;
         for (auto& kv : plans)
             cufftDestroy(kv.second);
         plans.clear();
@@ -139,6 +173,8 @@ std::string fkey(double v)
     std::snprintf(b, sizeof(b), "%a", v);
     return b;
 }
+
+constexpr size_t pad256(size_t b) { return (b + 255) / 256 * 256; }
 
 inline unsigned grid1d(int64_t n, int threads) { return unsigned(std::max<int64_t>(1, ceil_div(n, threads))); }
 
@@ -210,12 +246,29 @@ void check_pars(const ImagerSetup& s)
         fail(STPGPU_ERR_INVALID_ARG, "oversampling too large");
 }
 
+// Gridder launch prepared by run_gridder when the caller launches it itself
+// (the batch path merges the tiles of many snapshots into one launch).
+enum GridKind { GK_NONE = 0, GK_SEP, GK_EXACT, GK_WPROJ };
+template <typename R>
+struct GridLaunch {
+    int kind = GK_NONE;
+    int beam = 0;
+    int tile_c = TILE_C_DEFAULT;
+    int ntiles = 0;
+    size_t smem = 0;
+    GridParams<R> gp {};
+};
+
 // convolve_to_grid (gridder.h:240-997): grids into context buffers "grid"
 // and "beamgrid" of precision R (complex), image_rows x N column-major.
+// tile_c: grid columns per tile (32 or 16).  With `defer` the gridder kernel
+// is not launched: its parameters are returned there instead.
 template <typename R, int COMP>
 GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, int vis_c64, const double* d_wts,
-    const double* d_uv, int uv_is_pixels, int64_t n)
+    const double* d_uv, int uv_is_pixels, int64_t n, int tile_c = TILE_C_DEFAULT, GridLaunch<R>* defer = nullptr)
 {
+    if (tile_c != 32 && tile_c != 16)
+        fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32");
     using C2 = typename Cplx<R>::T;
     check_pars(s);
     cudaStream_t st = c->stream;
@@ -421,13 +474,13 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
 
     // ---- binning into 32x32 uv tiles
     const int tiles_r = int(ceil_div(image_rows, TILE_R));
-    const int tiles_c = int(ceil_div(N, TILE_C));
+    const int tiles_c = int(ceil_div(N, tile_c));
     const int ntiles = tiles_r * tiles_c;
     uint32_t* tcount = c->buf<uint32_t>("tcount", ntiles + 1);
     uint32_t* toff = c->buf<uint32_t>("toff", ntiles + 1);
     uint32_t* tcur = c->buf<uint32_t>("tcur", ntiles + 1);
     const int Kx = 2 * conv_support + 1;
-    const uint64_t per_dim = uint64_t(ceil_div(Kx - 1, std::min(TILE_R, TILE_C))) + 2;
+    const uint64_t per_dim = uint64_t(ceil_div(Kx - 1, std::min(TILE_R, tile_c))) + 2;
     const uint64_t cap = std::max<uint64_t>(1, uint64_t(nn) * 2 * per_dim * per_dim);
     if (cap > 0xffffffffull)
         fail(STPGPU_ERR_INVALID_ARG, "too many visibilities for one snapshot");
@@ -437,6 +490,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     bp.image_rows = image_rows;
     bp.tiles_r = tiles_r;
     bp.tiles_c = tiles_c;
+    bp.tile_c = tile_c;
     bp.support = s.support;
     bp.plane_support = plane_support;
     bp.exact = kernel_exact;
@@ -487,38 +541,47 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     gp.grid = grid;
     gp.beam = beam;
     using A = Acc<R, COMP>;
-    size_t smem = size_t(TILE_R) * TILE_C * sizeof(A) * (s.beam ? 2 : 1);
+    size_t smem = size_t(TILE_R) * tile_c * sizeof(A) * (s.beam ? 2 : 1);
     if (!wproj && !kernel_exact)
         smem += sizeof(R) * size_t(cs) * (2 * s.support + 1);
-    auto launch = [&](auto kern) {
-        if (smem > 48 * 1024)
-            STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        c->mark(1);
-        kern<<<ntiles, 32, smem, st>>>(gp);
-        STPGPU_CHECK_LAUNCH();
-        c->mark(2);
-    };
     if (2 * conv_support + 1 > 65)
         fail(STPGPU_ERR_UNSUPPORTED, "kernel support > 32 is outside the GPU path");
-    if (wproj && n > 0) {
-        if (s.beam)
-            launch(k_grid_tiles<R, COMP, KM_WPROJ, true>);
-        else
-            launch(k_grid_tiles<R, COMP, KM_WPROJ, false>);
-    } else if (kernel_exact) {
-        if (s.beam)
-            launch(k_grid_tiles<R, COMP, KM_EXACT, true>);
-        else
-            launch(k_grid_tiles<R, COMP, KM_EXACT, false>);
-    } else if (!wproj) {
-        if (s.beam)
-            launch(k_grid_tiles<R, COMP, KM_SEP, true>);
-        else
-            launch(k_grid_tiles<R, COMP, KM_SEP, false>);
-    } else {
+    const int kind = (wproj && n > 0) ? GK_WPROJ : (kernel_exact ? GK_EXACT : (!wproj ? GK_SEP : GK_NONE));
+    if (kind == GK_NONE) {
         STPGPU_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(C2) * size_t(image_rows) * N, st));
         if (beam)
             STPGPU_CUDA_TRY(cudaMemsetAsync(beam, 0, sizeof(C2) * size_t(image_rows) * N, st));
+    }
+    if (defer) {
+        defer->kind = kind;
+        defer->beam = s.beam ? 1 : 0;
+        defer->tile_c = tile_c;
+        defer->ntiles = kind == GK_NONE ? 0 : ntiles;
+        defer->smem = smem;
+        defer->gp = gp;
+    } else if (kind != GK_NONE) {
+        auto launch = [&](auto kern) {
+            if (smem > 48 * 1024)
+                STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+            c->mark(1);
+            kern<<<ntiles, 32, smem, st>>>(gp);
+            STPGPU_CHECK_LAUNCH();
+            c->mark(2);
+        };
+        const bool b = s.beam != 0;
+        const bool t32 = tile_c == 32;
+        if (kind == GK_WPROJ)
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16>));
+        else if (kind == GK_EXACT)
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_EXACT, true, 32>) : launch(k_grid_tiles<R, COMP, KM_EXACT, true, 16>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_EXACT, false, 32>) : launch(k_grid_tiles<R, COMP, KM_EXACT, false, 16>));
+        else
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, true, 32>) : launch(k_grid_tiles<R, COMP, KM_SEP, true, 16>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, false, 32>) : launch(k_grid_tiles<R, COMP, KM_SEP, false, 16>));
+    } else {
+        c->mark(1);
+        c->mark(2);
     }
     g.grid = grid;
     g.beam = beam;
@@ -589,19 +652,13 @@ const double* device_gcf(stpgpu_context* c, const ImagerSetup& s)
     return gcf;
 }
 
-// stp::image_visibilities (imager.h:233-376) on device buffers.  The whole
-// pipeline is enqueued without a host round trip; the normalisation reads
-// the sampling total on the device, and the scalars are read back once at
-// the end (an empty result, imager.h:355, is reported then).
-template <typename R, int COMP>
-void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const void* d_vis,
-    int vis_c64, const double* d_wts, const double* d_uvw, int64_t n, void* d_image, void* d_beam, int out_f32,
-    stpgpu_imager_info* info)
+// c2r FFT + crop/normalise of a gridded snapshot (fft.cpp:45-135,
+// imager.h:97-213) on the context's current stream.
+template <typename R>
+void finish_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const GridOut& g,
+    void* d_image, void* d_beam, int out_f32)
 {
-    if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
-        fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
     cudaStream_t st = c->stream;
-    GridOut g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n);
     const int N = s.N;
     R* img = c->buf<R>("fftimg", size_t(N) * N);
     const cufftType type = sizeof(R) == 8 ? CUFFT_Z2D : CUFFT_C2R;
@@ -636,6 +693,22 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         exec(g.beam, img);
         normalise(d_beam);
     }
+}
+
+// stp::image_visibilities (imager.h:233-376) on device buffers.  The whole
+// pipeline is enqueued without a host round trip; the normalisation reads
+// the sampling total on the device, and the scalars are read back once at
+// the end (an empty result, imager.h:355, is reported then).
+template <typename R, int COMP>
+void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const void* d_vis,
+    int vis_c64, const double* d_wts, const double* d_uvw, int64_t n, void* d_image, void* d_beam, int out_f32,
+    stpgpu_imager_info* info)
+{
+    if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
+        fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
+    GridOut g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n);
+    finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+    const int N = s.N;
     const ScalarsBack sb = read_back(c, g);
     if (info) {
         info->sample_grid_total = sb.total;
@@ -704,6 +777,373 @@ T* to_device(stpgpu_context* c, const char* name, const void* host, size_t count
     if (count)
         STPGPU_CUDA_TRY(cudaMemcpyAsync(d, host, sizeof(T) * count, cudaMemcpyHostToDevice, c->stream));
     return d;
+}
+
+// ------------------------------------------------------------------ batch
+
+constexpr int kBatchStreams = 4;
+
+struct BatchSnap {
+    ImagerSetup s;
+    int image_size = 0;
+    int correction = 1;
+    const void* vis = nullptr; // caller's pointers (device or host)
+    int c64 = 0;
+    const double* wts = nullptr;
+    const double* uvw = nullptr;
+    int64_t n = 0;
+    void* image = nullptr;
+    std::string cls; // size class of the tile autotuner
+    int tile_c = TILE_C_DEFAULT;
+};
+
+void batch_streams(stpgpu_context* c)
+{
+    if (!c->wstreams.empty())
+        return;
+    for (int k = 0; k < kBatchStreams; k++) {
+        cudaStream_t w;
+        STPGPU_CUDA_TRY(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking));
+        c->wstreams.push_back(w);
+        cudaEvent_t e;
+        STPGPU_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->wevents.push_back(e);
+    }
+    STPGPU_CUDA_TRY(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+}
+
+// main stream -> every worker stream
+void batch_fork(stpgpu_context* c, cudaStream_t main)
+{
+    STPGPU_CUDA_TRY(cudaEventRecord(c->fork_ev, main));
+    for (auto w : c->wstreams)
+        STPGPU_CUDA_TRY(cudaStreamWaitEvent(w, c->fork_ev, 0));
+}
+
+// every worker stream -> main stream
+void batch_join(stpgpu_context* c, cudaStream_t main)
+{
+    for (size_t k = 0; k < c->wstreams.size(); k++) {
+        STPGPU_CUDA_TRY(cudaEventRecord(c->wevents[k], c->wstreams[k]));
+        STPGPU_CUDA_TRY(cudaStreamWaitEvent(main, c->wevents[k], 0));
+    }
+}
+
+template <typename R, int COMP, int KMODE, int TC>
+void launch_grid_batch(cudaStream_t st, size_t smem, const GridParams<R>* ps, const uint32_t* tb, int nsnap,
+    uint32_t* counter, uint32_t total_tiles, bool capturing)
+{
+    auto kern = k_grid_batch<R, COMP, KMODE, false, TC>;
+    if (!capturing && smem > 48 * 1024)
+        STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        STPGPU_CUDA_TRY(cudaGetDevice(&dev));
+        STPGPU_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    int per_sm = 0;
+    STPGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
+    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(total_tiles, uint32_t(std::max(per_sm, 1) * sms)));
+    kern<<<blocks, 32, smem, st>>>(ps, tb, nsnap, counter);
+    STPGPU_CHECK_LAUNCH();
+}
+
+template <typename R, int COMP>
+void launch_group(cudaStream_t st, int kind, int tc, size_t smem, const GridParams<R>* ps, const uint32_t* tb,
+    int nsnap, uint32_t* counter, uint32_t total, bool capturing)
+{
+    if (kind == GK_WPROJ)
+        tc == 32 ? launch_grid_batch<R, COMP, KM_WPROJ, 32>(st, smem, ps, tb, nsnap, counter, total, capturing)
+                 : launch_grid_batch<R, COMP, KM_WPROJ, 16>(st, smem, ps, tb, nsnap, counter, total, capturing);
+    else if (kind == GK_EXACT)
+        tc == 32 ? launch_grid_batch<R, COMP, KM_EXACT, 32>(st, smem, ps, tb, nsnap, counter, total, capturing)
+                 : launch_grid_batch<R, COMP, KM_EXACT, 16>(st, smem, ps, tb, nsnap, counter, total, capturing);
+    else
+        tc == 32 ? launch_grid_batch<R, COMP, KM_SEP, 32>(st, smem, ps, tb, nsnap, counter, total, capturing)
+                 : launch_grid_batch<R, COMP, KM_SEP, 16>(st, smem, ps, tb, nsnap, counter, total, capturing);
+}
+
+// Enqueue one batch: preparation of every snapshot on the worker streams,
+// persistent gridder launches on the main stream (one per kernel variant,
+// or one per size class when class_ms is given, each timed), then c2r +
+// normalisation per snapshot on the worker streams, and the scalars of every
+// snapshot gathered into `scal` (pinned host memory) by the main stream.
+template <typename R, int COMP>
+int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int device_ptrs, bool capturing,
+    BatchScalars* scal, unsigned char* host_params, std::map<std::string, float>* class_ms)
+{
+    const cudaStream_t main = c->stream;
+    const int nb = int(B.size());
+    const int K = int(c->wstreams.size());
+    const size_t vb = 16;
+    std::vector<GridLaunch<R>> L(nb);
+    std::vector<GridOut> G(nb);
+    std::vector<void*> dimg(nb);
+    batch_fork(c, main);
+    for (int i = 0; i < nb; i++) {
+        c->stream = c->wstreams[i % K];
+        c->ns = "b" + std::to_string(i) + "/";
+        BatchSnap& b = B[i];
+        const void* dv = b.vis;
+        const double* dw = b.wts;
+        const double* duvw = b.uvw;
+        dimg[i] = b.image;
+        if (!device_ptrs) {
+            const size_t vbytes = b.c64 ? 8 : vb;
+            dv = to_device<unsigned char>(c, "in_vis", b.vis, vbytes * size_t(b.n));
+            dw = to_device<double>(c, "in_w", b.wts, size_t(b.n));
+            duvw = to_device<double>(c, "in_uvw", b.uvw, 3 * size_t(b.n));
+            dimg[i] = c->buf<unsigned char>("out_img", (out_f32 ? 4 : 8) * size_t(b.image_size) * b.image_size);
+        }
+        G[i] = run_gridder<R, COMP>(c, b.s, dv, b.c64, dw, duvw, 0, b.n, b.tile_c, &L[i]);
+    }
+    c->stream = main;
+    c->ns = "batch/";
+    batch_join(c, main);
+
+    // ---- persistent gridder launches over (snapshot, tile) work queues
+    std::map<std::string, std::vector<int>> groups;
+    for (int i = 0; i < nb; i++) {
+        if (L[i].kind == GK_NONE || L[i].ntiles == 0)
+            continue;
+        std::string key = std::to_string(L[i].kind) + "/" + std::to_string(L[i].tile_c);
+        if (class_ms)
+            key += "|" + B[i].cls;
+        groups[key].push_back(i);
+    }
+    size_t hoff = 0;
+    int gi = 0;
+    for (auto& kv : groups) {
+        const std::vector<int>& mem = kv.second;
+        const int m = int(mem.size());
+        GridParams<R>* hp = reinterpret_cast<GridParams<R>*>(host_params + hoff);
+        hoff += pad256(sizeof(GridParams<R>) * m);
+        uint32_t* htb = reinterpret_cast<uint32_t*>(host_params + hoff);
+        hoff += pad256(sizeof(uint32_t) * (m + 1));
+        size_t smem = 0;
+        uint32_t tot = 0;
+        for (int k = 0; k < m; k++) {
+            const GridLaunch<R>& l = L[mem[k]];
+            hp[k] = l.gp; // a captured copy reads these host bytes at every replay
+            htb[k] = tot;
+            tot += uint32_t(l.ntiles);
+            smem = std::max(smem, l.smem);
+        }
+        htb[m] = tot;
+        const std::string gname = "g" + std::to_string(gi++);
+        GridParams<R>* dps = c->buf<GridParams<R>>(gname + "ps", m);
+        uint32_t* dtb = c->buf<uint32_t>(gname + "tb", m + 1);
+        uint32_t* ctr = c->buf<uint32_t>(gname + "ctr", 1);
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(dps, hp, sizeof(GridParams<R>) * m, cudaMemcpyHostToDevice, main));
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(dtb, htb, sizeof(uint32_t) * (m + 1), cudaMemcpyHostToDevice, main));
+        STPGPU_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), main));
+        if (class_ms)
+            STPGPU_CUDA_TRY(cudaEventRecord(c->pev[0], main));
+        const GridLaunch<R>& l0 = L[mem[0]];
+        launch_group<R, COMP>(main, l0.kind, l0.tile_c, smem, dps, dtb, m, ctr, tot, capturing);
+        if (class_ms) {
+            STPGPU_CUDA_TRY(cudaEventRecord(c->pev[1], main));
+            STPGPU_CUDA_TRY(cudaEventSynchronize(c->pev[1]));
+            float ms = 0.f;
+            STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->pev[0], c->pev[1]));
+            (*class_ms)[B[mem[0]].cls] += ms;
+        }
+    }
+
+    // ---- c2r + normalise per snapshot, scalars
+    batch_fork(c, main);
+    for (int i = 0; i < nb; i++) {
+        c->stream = c->wstreams[i % K];
+        c->ns = "b" + std::to_string(i) + "/";
+        BatchSnap& b = B[i];
+        finish_imager<R>(c, b.s, b.image_size, b.correction, G[i], dimg[i], nullptr, out_f32);
+        BatchScalars* ds = c->buf<BatchScalars>("scal", 1);
+        k_collect_scalars<<<1, 1, 0, c->stream>>>(G[i].d_total, G[i].d_ngood, G[i].d_nitems, G[i].d_err,
+            G[i].d_plane_support ? G[i].d_plane_support : reinterpret_cast<const int*>(G[i].d_err),
+            G[i].d_plane_support ? G[i].nplanes : 0, ds);
+        STPGPU_CHECK_LAUNCH();
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(&scal[i], ds, sizeof(BatchScalars), cudaMemcpyDeviceToHost, c->stream));
+        if (!device_ptrs)
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(b.image, dimg[i], (out_f32 ? 4 : 8) * size_t(b.image_size) * b.image_size,
+                cudaMemcpyDeviceToHost, c->stream));
+    }
+    c->stream = main;
+    c->ns = "";
+    batch_join(c, main);
+    return int(groups.size());
+}
+
+std::string size_class(const ImagerSetup& s, int precision)
+{
+    const int conv = s.nplanes > 0 ? s.max_support : s.support;
+    return "p" + std::to_string(precision) + "/k" + std::to_string(s.nplanes > 0 ? 2 : (s.kernel_exact ? 1 : 0))
+        + "/N" + std::to_string(s.N) + "/S" + std::to_string(conv) + "/os" + std::to_string(s.os);
+}
+
+template <typename R, int COMP>
+void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precision, int out_f32, int device_ptrs,
+    stpgpu_imager_info* infos, stpgpu_batch_info* bi)
+{
+    batch_streams(c);
+    std::vector<BatchSnap> B(nb);
+    std::string sig;
+    auto put = [&](const void* p, size_t n) { sig.append(reinterpret_cast<const char*>(p), n); };
+    put(&precision, sizeof(int));
+    put(&out_f32, sizeof(int));
+    put(&device_ptrs, sizeof(int));
+    for (int i = 0; i < nb; i++) {
+        const stpgpu_snapshot& x = sn[i];
+        BatchSnap& b = B[i];
+        b.s = setup_from(&x.pars, &x.wproj, nullptr, b.image_size);
+        if (x.pars.generate_beam)
+            fail(STPGPU_ERR_UNSUPPORTED, "generate_beam is not supported by the batch path");
+        if (b.image_size <= 0 || b.image_size > b.s.N || (b.image_size % 2) != 0)
+            fail(STPGPU_ERR_INVALID_ARG, "snapshot " + std::to_string(i) + ": image_size must be even, > 0 and <= padded size");
+        if (x.n_vis < 0 || (x.n_vis > 0 && (!x.vis || !x.weights || !x.uvw)) || !x.image)
+            fail(STPGPU_ERR_INVALID_ARG, "snapshot " + std::to_string(i) + ": null buffer");
+        if (x.vis_dtype != STPGPU_C128 && x.vis_dtype != STPGPU_C64)
+            fail(STPGPU_ERR_INVALID_ARG, "snapshot " + std::to_string(i) + ": vis_dtype");
+        b.correction = x.pars.gridding_correction;
+        b.vis = x.vis;
+        b.c64 = x.vis_dtype == STPGPU_C64;
+        b.wts = x.weights;
+        b.uvw = x.uvw;
+        b.n = x.n_vis;
+        b.image = x.image;
+        b.cls = size_class(b.s, precision);
+        put(&x.pars, sizeof(x.pars));
+        put(&x.wproj, sizeof(x.wproj));
+        put(&x.n_vis, sizeof(x.n_vis));
+        put(&x.vis_dtype, sizeof(x.vis_dtype));
+        put(&x.vis, sizeof(void*));
+        put(&x.weights, sizeof(void*));
+        put(&x.uvw, sizeof(void*));
+        put(&x.image, sizeof(void*));
+    }
+    if (sig != c->batch_sig) {
+        for (auto w : c->wstreams)
+            STPGPU_CUDA_TRY(cudaStreamSynchronize(w));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        c->drop_graph();
+        c->batch_sig = sig;
+        c->batch_calls = 0;
+    }
+    c->batch_calls++;
+    // pinned staging: gridder parameter tables (<= 2 per snapshot) + scalars
+    const size_t need = size_t(nb) * (pad256(sizeof(GridParams<R>)) + 2 * 256) * 2
+        + pad256(sizeof(BatchScalars) * nb) + 4096;
+    if (c->batch_host_cap < need) {
+        if (c->batch_host) {
+            for (auto w : c->wstreams)
+                STPGPU_CUDA_TRY(cudaStreamSynchronize(w));
+            STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            c->drop_graph();
+            cudaFreeHost(c->batch_host);
+            c->batch_host = nullptr;
+            c->batch_host_cap = 0;
+        }
+        STPGPU_CUDA_TRY(cudaMallocHost(&c->batch_host, need));
+        c->batch_host_cap = need;
+    }
+    BatchScalars* scal = reinterpret_cast<BatchScalars*>(c->batch_host);
+    unsigned char* hparams = reinterpret_cast<unsigned char*>(c->batch_host) + pad256(sizeof(BatchScalars) * nb);
+    const bool saved_timing = c->timing;
+    c->timing = false;
+    struct Restore {
+        stpgpu_context* c;
+        cudaStream_t main;
+        bool timing;
+        ~Restore()
+        {
+            c->stream = main;
+            c->ns = "";
+            c->timing = timing;
+        }
+    } restore { c, c->stream, saved_timing };
+    const cudaStream_t main = c->stream;
+    int tuned = 0, glaunch = 0, graph = 0;
+    g_launches = 0;
+    if (device_ptrs && c->batch_exec) {
+        // replay
+        STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
+        STPGPU_CUDA_TRY(cudaGraphLaunch(c->batch_exec, main));
+        STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, main));
+        graph = 1;
+    } else {
+        // tile autotuner: time both tile widths for classes not seen before
+        std::vector<std::string> fresh;
+        for (auto& b : B)
+            if (!c->tune.count(b.cls) && std::find(fresh.begin(), fresh.end(), b.cls) == fresh.end())
+                fresh.push_back(b.cls);
+        if (!fresh.empty()) {
+            std::map<std::string, float> t32, t16;
+            for (int cand : { 32, 16 }) {
+                for (auto& b : B)
+                    b.tile_c = c->tune.count(b.cls) ? c->tune[b.cls] : cand;
+                for (int k = 0; k < 5; k++)
+                    if (!c->pev[k])
+                        STPGPU_CUDA_TRY(cudaEventCreate(&c->pev[k]));
+                batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, cand == 32 ? &t32 : &t16);
+                STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
+            }
+            for (auto& cls : fresh)
+                c->tune[cls] = t16[cls] < t32[cls] ? 16 : 32;
+            tuned = int(fresh.size());
+        }
+        for (auto& b : B)
+            b.tile_c = c->tune[b.cls];
+        if (device_ptrs && c->batch_calls >= 2 && tuned == 0) {
+            // capture the batch (buffers, plans and tables exist from the previous call)
+            STPGPU_CUDA_TRY(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+            try {
+                glaunch = batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, true, scal, hparams, nullptr);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(main, &g);
+                if (g)
+                    cudaGraphDestroy(g);
+                throw;
+            }
+            STPGPU_CUDA_TRY(cudaStreamEndCapture(main, &c->batch_graph));
+            STPGPU_CUDA_TRY(cudaGraphInstantiate(&c->batch_exec, c->batch_graph, 0));
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
+            STPGPU_CUDA_TRY(cudaGraphLaunch(c->batch_exec, main));
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, main));
+            graph = 1;
+        } else {
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
+            glaunch = batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, nullptr);
+            STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, main));
+        }
+    }
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
+    float ms = 0.f;
+    STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    for (int i = 0; i < nb; i++) {
+        if (scal[i].err)
+            fail(STPGPU_ERR_DEVICE, "snapshot " + std::to_string(i) + ": gridder reported internal error flags "
+                    + std::to_string(scal[i].err));
+        if (infos) {
+            stpgpu_imager_info& f = infos[i];
+            std::memset(&f, 0, sizeof(f));
+            f.sample_grid_total = scal[i].total;
+            f.n_good_vis = int64_t(scal[i].ngood);
+            f.n_grid_items = scal[i].nitems;
+            f.padded_image_size = B[i].s.N;
+            f.num_wplanes = B[i].s.nplanes;
+            f.max_plane_support = scal[i].max_support;
+            f.image_size = scal[i].total > 0.0 ? B[i].image_size : 0;
+        }
+    }
+    if (bi) {
+        std::memset(bi, 0, sizeof(*bi));
+        bi->device_ms = ms;
+        bi->graph = graph;
+        bi->gridder_launches = glaunch;
+        bi->tuned_classes = tuned;
+        bi->n_launches = g_launches;
+    }
 }
 
 // ------------------------------------------------------------------ source finder
@@ -1151,6 +1591,14 @@ stpgpu_status stpgpu_destroy(stpgpu_context* c)
     c->release();
     if (c->pinned)
         cudaFreeHost(c->pinned);
+    if (c->batch_host)
+        cudaFreeHost(c->batch_host);
+    for (auto w : c->wstreams)
+        cudaStreamDestroy(w);
+    for (auto e : c->wevents)
+        cudaEventDestroy(e);
+    if (c->fork_ev)
+        cudaEventDestroy(c->fork_ev);
     if (c->ev0)
         cudaEventDestroy(c->ev0);
     if (c->ev1)
@@ -1245,6 +1693,31 @@ stpgpu_status stpgpu_image_visibilities_ex(stpgpu_context* c, const void* vis, i
             inf->device_ms = ms;
         }
         inf->n_launches = g_launches;
+    });
+}
+
+stpgpu_status stpgpu_image_batch(stpgpu_context* c, const stpgpu_snapshot* snapshots, int32_t n_snapshots,
+    int precision, int out_dtype, int device_ptrs, stpgpu_imager_info* infos, stpgpu_batch_info* batch_info)
+{
+    return guard(c, [&] {
+        if (!snapshots || n_snapshots <= 0)
+            fail(STPGPU_ERR_INVALID_ARG, "empty batch");
+        if (out_dtype != STPGPU_F64 && out_dtype != STPGPU_F32)
+            fail(STPGPU_ERR_INVALID_ARG, "out_dtype");
+        const int f32 = out_dtype == STPGPU_F32;
+        switch (precision) {
+        case STPGPU_FP64:
+            run_batch<double, 0>(c, snapshots, n_snapshots, precision, f32, device_ptrs, infos, batch_info);
+            break;
+        case STPGPU_FP32:
+            run_batch<float, 0>(c, snapshots, n_snapshots, precision, f32, device_ptrs, infos, batch_info);
+            break;
+        case STPGPU_FP32C:
+            run_batch<float, 1>(c, snapshots, n_snapshots, precision, f32, device_ptrs, infos, batch_info);
+            break;
+        default:
+            fail(STPGPU_ERR_INVALID_ARG, "precision");
+        }
     });
 }
 

@@ -20,7 +20,7 @@
 namespace stpgpu {
 
 constexpr int TILE_R = 32; // tile rows (v, the fast grid axis)
-constexpr int TILE_C = 32; // tile columns (u)
+constexpr int TILE_C_DEFAULT = 32; // tile columns (u); 16-column tiles are the other tuned shape
 constexpr int GRID_THREADS = 256;
 
 enum KMode { KM_SEP = 0, KM_EXACT = 1, KM_WPROJ = 2 };
@@ -226,6 +226,7 @@ __device__ __forceinline__ int map_row(int raw, int N, int rows, bool wrap_neg)
 
 struct BinParams {
     int N, image_rows, tiles_r, tiles_c;
+    int tile_c;              // tile width in grid columns (TILE_R rows per tile)
     int support;             // non-W-proj support
     const int* plane_support; // W-proj truncated support per plane (nullable)
     int exact;               // rows wrap negative (exact gridder)
@@ -276,7 +277,7 @@ __device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, const
     int tc0 = -1, tc1 = -1, tc0e = -1, tc1e = -1;
     for (int j = 0; j < K; j++) {
         const int c = map_col(cx - S + j, p.N);
-        const int t = c / TILE_C;
+        const int t = c / p.tile_c;
         if (tc0 < 0) {
             tc0 = tc0e = t;
         } else if (t == tc0e + 1 || t == tc0e) {
@@ -529,16 +530,14 @@ __device__ __forceinline__ void tap_value(const GridParams<R>& p, const R* tab, 
     ki = ki * t.wt;
 }
 
-template <typename R, int COMP, int KMODE, bool BEAM>
-__global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
+__device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsigned char* smem_raw)
 {
     using A = Acc<R, COMP>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     A* acc = reinterpret_cast<A*>(smem_raw);
     A* bacc = acc + (BEAM ? TILE_R * TILE_C : 0);
     R* tab = reinterpret_cast<R*>(acc + (BEAM ? 2 : 1) * TILE_R * TILE_C);
     const int lane = threadIdx.x;
-    const int tile = blockIdx.x;
     const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
     const int r0 = tr * TILE_R, c0 = tc * TILE_C;
     const bool wrap_neg = p.exact_wrap != 0;
@@ -714,6 +713,45 @@ __global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
             if (BEAM)
                 p.beam[g] = acc_value(bacc[q]);
         }
+    }
+}
+
+// One CTA (one warp) per tile of one snapshot.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
+__global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    grid_tile<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
+}
+
+// Persistent gridder over the tiles of many snapshots: a (snapshot, tile)
+// work queue.  Work item w is tile w - tile_base[s] of the snapshot s with
+// tile_base[s] <= w < tile_base[s + 1]; warps take items from one atomic
+// counter (zeroed before the launch) until the queue is empty.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
+__global__ void __launch_bounds__(32) k_grid_batch(const GridParams<R>* __restrict__ ps,
+    const uint32_t* __restrict__ tile_base, int nsnap, uint32_t* counter)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t total = tile_base[nsnap];
+    for (;;) {
+        uint32_t w = 0;
+        if (threadIdx.x == 0)
+            w = atomicAdd(counter, 1u);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= total)
+            break;
+        int lo = 0, hi = nsnap - 1;
+        while (lo < hi) { // last snapshot whose first tile <= w
+            const int mid = (lo + hi + 1) / 2;
+            if (tile_base[mid] <= w)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        __syncwarp();
+        grid_tile<R, COMP, KMODE, BEAM, TILE_C>(ps[lo], int(w - tile_base[lo]), smem_raw);
+        __syncwarp();
     }
 }
 
@@ -1131,6 +1169,34 @@ __global__ void k_wk_to_f32(const double2* convd, const double* invd, int64_t nc
         convf[t] = make_float2(float(convd[t].x), float(convd[t].y));
     if (t < ninv)
         invf[t] = float(invd[t]);
+}
+
+// Per-snapshot scalars of a batch, gathered for one read-back.
+struct BatchScalars {
+    double total;
+    unsigned long long ngood;
+    uint32_t nitems;
+    uint32_t err;
+    int32_t max_support;
+    int32_t pad;
+};
+
+__global__ void k_collect_scalars(const double* total, const unsigned long long* ngood, const uint32_t* nitems,
+    const unsigned int* err, const int* psup, int nplanes, BatchScalars* out)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    BatchScalars b;
+    b.total = total[0];
+    b.ngood = ngood[0];
+    b.nitems = nitems[0];
+    b.err = err[0];
+    int m = 0;
+    for (int p = 0; p < nplanes; p++)
+        m = max(m, psup[p]);
+    b.max_support = m;
+    b.pad = 0;
+    *out = b;
 }
 
 } // namespace stpgpu

@@ -228,6 +228,45 @@ STPGPU_API stpgpu_status stpgpu_source_find_ex(stpgpu_context* ctx, const void* 
     const stpgpu_sf_pars* pars, int32_t* label_map, int device_ptrs, stpgpu_island* islands, int32_t capacity,
     int32_t* n_islands, stpgpu_sf_info* info);
 
+/* One snapshot of a batch (stpgpu_image_batch).  Pointers are device
+ * pointers when the batch call's device_ptrs != 0, else host pointers.
+ * vis_dtype: STPGPU_C128 / STPGPU_C64; uvw n_vis x 3 column-major; image:
+ * image_size^2 out, column-major, of the batch's out_dtype.  generate_beam
+ * must be 0 (the batch path images the visibilities only). */
+typedef struct {
+    const void* vis;
+    int32_t vis_dtype;
+    int32_t reserved;
+    const double* weights;
+    const double* uvw;
+    int64_t n_vis;
+    stpgpu_imager_pars pars;
+    stpgpu_wproj_pars wproj;
+    void* image;
+} stpgpu_snapshot;
+
+typedef struct {
+    double device_ms;        /* device time of the whole batch (CUDA events) */
+    int32_t graph;           /* 1: ran as a replay of a captured CUDA graph */
+    int32_t gridder_launches; /* persistent gridder launches (one per kernel variant) */
+    int32_t tuned_classes;   /* size classes the tile autotuner measured in this call */
+    int32_t n_launches;      /* kernels this library launched when not replayed (cuFFT's excluded) */
+} stpgpu_batch_info;
+
+/* Many snapshots of uneven sizes in one call: per-snapshot preparation on
+ * parallel streams, ONE persistent gridder launch per kernel variant over a
+ * (snapshot, tile) work queue, then the c2r transforms and normalisation of
+ * every snapshot.  Results equal stpgpu_image_visibilities_ex on each
+ * snapshot alone.  The tile width (32 or 16 grid columns) of each size class
+ * (padded size, kernel mode, precision, support) is chosen by an autotuner
+ * that times both shapes on the first batch containing that class.  With
+ * device pointers, the second and later calls with the same snapshots
+ * (sizes, parameters and pointers) replay a CUDA graph captured from the
+ * previous one.  infos: nullable, n_snapshots entries. No counterpart in the
+ * reference (it images one snapshot per call, imager.h:233-376). */
+STPGPU_API stpgpu_status stpgpu_image_batch(stpgpu_context* ctx, const stpgpu_snapshot* snapshots, int32_t n_snapshots,
+    int precision, int out_dtype, int device_ptrs, stpgpu_imager_info* infos, stpgpu_batch_info* batch_info);
+
 /* Allocation-free connected-component labelling.  No counterpart in the
  * reference: it is the labelling step of stpgpu_source_find (the reference's
  * labeling_8con / labeling_4con, src/stp/common/ccl.h:107-504) for callers

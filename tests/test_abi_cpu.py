@@ -40,9 +40,9 @@ def test_struct_sizes_match_header():
     src = r"""
 #include <stdio.h>
 #include "stpgpu.h"
-int main(){printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(stpgpu_imager_pars), sizeof(stpgpu_wproj_pars),
+int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(stpgpu_imager_pars), sizeof(stpgpu_wproj_pars),
  sizeof(stpgpu_aproj_pars), sizeof(stpgpu_imager_info), sizeof(stpgpu_island), sizeof(stpgpu_sf_pars),
- sizeof(stpgpu_sf_info));return 0;}
+ sizeof(stpgpu_sf_info), sizeof(stpgpu_snapshot), sizeof(stpgpu_batch_info));return 0;}
 """
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
@@ -53,7 +53,7 @@ int main(){printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(stpgpu_imager_pars), s
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
     sizes = [int(x) for x in out]
     py = [ctypes.sizeof(t) for t in (capi.ImagerPars, capi.WProjPars, capi.AProjPars, capi.ImagerInfo, capi.Island,
-                                     capi.SfPars, capi.SfInfo)]
+                                     capi.SfPars, capi.SfInfo, capi.Snapshot, capi.BatchInfo)]
     assert sizes == py
 
 

@@ -1,0 +1,123 @@
+"""Batched imaging (stpgpu_image_batch): snapshots of uneven sizes and modes
+in one call must give the images of the single-snapshot entry point, in
+eager mode, in the captured CUDA graph and in its replays, with device or
+host buffers."""
+import numpy as np
+import pytest
+
+from fastimaging_b200 import capi
+from fastimaging_b200.synthetic import make_snapshot
+from oracle import stp_oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(0)
+    yield c
+    c.close()
+
+
+def peak_rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def _cases():
+    """(snapshot, keywords) of uneven sizes, kernels and W-projection."""
+    out = []
+    s = make_snapshot(41, 3000, 256, 2.0, n_src=3)
+    out.append((s, dict(image_size=256, cell_size=s.cell_size, kernel_func=capi.GaussianSinc, kernel_support=3,
+                        kernel_exact=False, oversampling=8)))
+    s = make_snapshot(42, 5000, 512, 1.0, n_src=4, w_range=(-300.0, 300.0))
+    out.append((s, dict(image_size=512, cell_size=s.cell_size, kernel_func=capi.GaussianSinc, kernel_support=3,
+                        kernel_exact=False, oversampling=8, num_wplanes=4, max_wpconv_support=8,
+                        kernel_trunc_perc=1.0)))
+    s = make_snapshot(43, 2000, 256, 2.0, n_src=2)
+    out.append((s, dict(image_size=256, cell_size=s.cell_size, kernel_func=capi.PSWF, kernel_support=4,
+                        kernel_exact=False, oversampling=16, analytic_gcf=True)))
+    s = make_snapshot(44, 4000, 384, 2.0, n_src=3)
+    out.append((s, dict(image_size=384, padded_image_size=576, padding_factor=1.5, cell_size=s.cell_size,
+                        kernel_func=capi.GaussianSinc, kernel_support=3, kernel_exact=False, oversampling=8)))
+    s = make_snapshot(45, 300, 128, 2.0, n_src=1)
+    s.uvw[:, :2] *= 1e6  # every visibility out of bounds: empty result
+    out.append((s, dict(image_size=128, cell_size=s.cell_size, kernel_func=capi.GaussianSinc, kernel_support=3,
+                        kernel_exact=False, oversampling=8)))
+    return out
+
+
+def _single(ctx, s, kw, precision=capi.FP64):
+    single_kw = {k: v for k, v in kw.items() if k not in ("image_size", "cell_size")}
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, kw["image_size"], kw["cell_size"],
+                                          precision=precision, **single_kw)
+    return img, info
+
+
+def test_batch_device_eager_graph_and_replay_match_single(ctx):
+    import torch
+
+    cases = _cases()
+    refs = [_single(ctx, s, kw) for s, kw in cases]
+    snaps = []
+    for s, kw in cases:
+        d = dict(kw)
+        d["vis"] = torch.from_numpy(s.vis).cuda()
+        d["weights"] = torch.from_numpy(s.weights).cuda()
+        d["uvw"] = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+        d["image"] = torch.zeros(kw["image_size"] ** 2, dtype=torch.float64, device="cuda")
+        snaps.append(d)
+    graphs = []
+    for call in range(4):
+        for d in snaps:
+            d["image"].fill_(-1.0)
+        torch.cuda.synchronize()
+        outs, infos, bi = ctx.image_batch(snaps, precision=capi.FP64, out_dtype=capi.F64, device_ptrs=True)
+        graphs.append(bi.graph)
+        if call == 0:
+            assert bi.tuned_classes >= 1
+        for (s, kw), out, info, (ref, rinfo) in zip(cases, outs, infos, refs):
+            n = kw["image_size"]
+            assert info.sample_grid_total == rinfo.sample_grid_total
+            assert info.n_good_vis == rinfo.n_good_vis
+            assert info.image_size == rinfo.image_size
+            if rinfo.image_size == 0:
+                continue
+            got = out.cpu().numpy().reshape(n, n).T
+            assert peak_rel(got, ref) < 1e-12, (call, n)
+    assert graphs[0] == 0 and graphs[2] == 1 and graphs[3] == 1
+
+
+def test_batch_fp32c_host_buffers_against_oracle(ctx):
+    cases = _cases()[:3]
+    snaps = []
+    for s, kw in cases:
+        d = dict(kw)
+        d.update(vis=s.vis, weights=s.weights, uvw=s.uvw)
+        snaps.append(d)
+    outs, infos, bi = ctx.image_batch(snaps, precision=capi.FP32C, out_dtype=capi.F32, device_ptrs=False)
+    assert bi.graph == 0
+    for (s, kw), img in zip(cases, outs):
+        okw = {k: v for k, v in kw.items() if k not in ("image_size", "cell_size", "padded_image_size")}
+        ref, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, kw["image_size"], kw["cell_size"], **okw)
+        single, _ = _single(ctx, s, kw, precision=capi.FP32C)
+        img = img.astype(np.float64)
+        # same arithmetic as the single-snapshot call (accumulation order may differ)
+        assert peak_rel(img, single.astype(np.float64)) < 1e-6
+        # FP32 against the FP64 oracle: 1e-5, except where the analytic PSWF
+        # grid correction divides the field corners by gcf(1)^2 ~ 1.6e-5,
+        # which magnifies single-precision rounding of the uncorrected image
+        # (the FP64 path shows the same magnification at the 1e-13 level)
+        tol = 5e-4 if kw.get("analytic_gcf") else 1e-5
+        assert peak_rel(img, ref) < tol
+
+
+def test_batch_rejects_beam_and_bad_sizes(ctx):
+    s, kw = _cases()[0]
+    d = dict(kw, vis=s.vis, weights=s.weights, uvw=s.uvw, generate_beam=True)
+    with pytest.raises(capi.StpGpuError) as e:
+        ctx.image_batch([d], device_ptrs=False)
+    assert e.value.status == 2
+    d = dict(kw, vis=s.vis, weights=s.weights, uvw=s.uvw, image_size=255,
+             image=np.empty((255, 255), np.float32, order="F"))
+    with pytest.raises(capi.StpGpuError):
+        ctx.image_batch([d], device_ptrs=False)
