@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -61,6 +62,7 @@ struct stpgpu_context {
     cudaGraph_t batch_graph = nullptr;
     cudaGraphExec_t batch_exec = nullptr;
     std::map<std::string, int> tune;
+    cudaEvent_t tev[2] = { nullptr, nullptr };
     void* batch_host = nullptr;
     size_t batch_host_cap = 0;
 
@@ -244,6 +246,14 @@ void check_pars(const ImagerSetup& s)
         fail(STPGPU_ERR_UNSUPPORTED, "kernel_support > 32 is outside the GPU path");
     if (s.os > 4096)
         fail(STPGPU_ERR_INVALID_ARG, "oversampling too large");
+}
+
+// Key of the tile autotuner: calls of one class share the tile width.
+std::string size_class(const ImagerSetup& s, int precision)
+{
+    const int conv = s.nplanes > 0 ? s.max_support : s.support;
+    return "p" + std::to_string(precision) + "/k" + std::to_string(s.nplanes > 0 ? 2 : (s.kernel_exact ? 1 : 0))
+        + "/N" + std::to_string(s.N) + "/S" + std::to_string(conv) + "/os" + std::to_string(s.os);
 }
 
 // Gridder launch prepared by run_gridder when the caller launches it itself
@@ -706,7 +716,37 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
 {
     if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
         fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
-    GridOut g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n);
+    // tile width: the autotuned choice of this size class; the first call of
+    // a class grids with both widths, times them, keeps the faster for later
+    // calls (every pass produces the complete grid; the last one is used)
+    const int precision = sizeof(R) == 8 ? STPGPU_FP64 : (COMP ? STPGPU_FP32C : STPGPU_FP32);
+    const std::string cls = size_class(s, precision);
+    GridOut g;
+    auto it = c->tune.find(cls);
+    if (it != c->tune.end() || c->timing) {
+        g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n,
+            it != c->tune.end() ? (it->second & 0xff) : TILE_C_DEFAULT);
+    } else {
+        for (auto& e : c->tev)
+            if (!e)
+                STPGPU_CUDA_TRY(cudaEventCreate(&e));
+        // an untimed pass first grows every buffer (16 columns: the most
+        // tiles) and fills the cached tables, so neither timed pass pays that
+        float ms[2] = { 0.f, 0.f };
+        const int widths[2] = { 32, 16 };
+        g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, 16);
+        for (int k = 0; k < 2; k++) {
+            STPGPU_CUDA_TRY(cudaEventRecord(c->tev[0], c->stream));
+            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, widths[k]);
+            STPGPU_CUDA_TRY(cudaEventRecord(c->tev[1], c->stream));
+            STPGPU_CUDA_TRY(cudaEventSynchronize(c->tev[1]));
+            STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms[k], c->tev[0], c->tev[1]));
+        }
+        c->tune[cls] = ms[1] < ms[0] ? 16 : 32;
+        if (std::getenv("STPGPU_LOG_TUNING"))
+            std::fprintf(stderr, "stpgpu tile tuner: %s  32 cols %.3f ms  16 cols %.3f ms  -> %d (single call)\n",
+                cls.c_str(), double(ms[0]), double(ms[1]), c->tune[cls]);
+    }
     finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
     const int N = s.N;
     const ScalarsBack sb = read_back(c, g);
@@ -781,7 +821,7 @@ T* to_device(stpgpu_context* c, const char* name, const void* host, size_t count
 
 // ------------------------------------------------------------------ batch
 
-constexpr int kBatchStreams = 4;
+constexpr int kBatchStreams = 8;
 
 struct BatchSnap {
     ImagerSetup s;
@@ -795,6 +835,7 @@ struct BatchSnap {
     void* image = nullptr;
     std::string cls; // size class of the tile autotuner
     int tile_c = TILE_C_DEFAULT;
+    int persist = 0;
 };
 
 void batch_streams(stpgpu_context* c)
@@ -829,39 +870,54 @@ void batch_join(stpgpu_context* c, cudaStream_t main)
     }
 }
 
-template <typename R, int COMP, int KMODE, int TC>
-void launch_grid_batch(cudaStream_t st, size_t smem, const GridParams<R>* ps, const uint32_t* tb, int nsnap,
-    uint32_t* counter, uint32_t total_tiles, bool capturing)
+template <typename R, int COMP, int KMODE, int TC, bool PERSIST>
+void launch_grid_batch(cudaStream_t st, size_t smem, const BatchGridParams<R>& P, uint32_t total_tiles, bool capturing)
 {
-    auto kern = k_grid_batch<R, COMP, KMODE, false, TC>;
+    auto kern = k_grid_batch<R, COMP, KMODE, false, TC, PERSIST>;
     if (!capturing && smem > 48 * 1024)
         STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        STPGPU_CUDA_TRY(cudaGetDevice(&dev));
-        STPGPU_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    uint32_t blocks = std::max<uint32_t>(1, total_tiles);
+    if (PERSIST) {
+        static int sms = 0;
+        if (sms == 0) {
+            int dev = 0;
+            STPGPU_CUDA_TRY(cudaGetDevice(&dev));
+            STPGPU_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        int per_sm = 0;
+        STPGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
+        blocks = std::min<uint32_t>(blocks, uint32_t(std::max(per_sm, 1) * sms));
     }
-    int per_sm = 0;
-    STPGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, smem));
-    const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(total_tiles, uint32_t(std::max(per_sm, 1) * sms)));
-    kern<<<blocks, 32, smem, st>>>(ps, tb, nsnap, counter);
+    kern<<<blocks, 32, smem, st>>>(P);
     STPGPU_CHECK_LAUNCH();
 }
 
+// Tuned gridder layout: tile width (32 or 16 grid columns) and whether the
+// batch gridder is persistent, packed as width | persistent << 8.
+constexpr int kLayoutPersist = 1 << 8;
+
+template <typename R, int COMP, int KMODE>
+void launch_mode(cudaStream_t st, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total, bool cap)
+{
+    const bool t32 = (layout & 0xff) == 32;
+    if (layout & kLayoutPersist)
+        t32 ? launch_grid_batch<R, COMP, KMODE, 32, true>(st, smem, P, total, cap)
+            : launch_grid_batch<R, COMP, KMODE, 16, true>(st, smem, P, total, cap);
+    else
+        t32 ? launch_grid_batch<R, COMP, KMODE, 32, false>(st, smem, P, total, cap)
+            : launch_grid_batch<R, COMP, KMODE, 16, false>(st, smem, P, total, cap);
+}
+
 template <typename R, int COMP>
-void launch_group(cudaStream_t st, int kind, int tc, size_t smem, const GridParams<R>* ps, const uint32_t* tb,
-    int nsnap, uint32_t* counter, uint32_t total, bool capturing)
+void launch_group(cudaStream_t st, int kind, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total,
+    bool capturing)
 {
     if (kind == GK_WPROJ)
-        tc == 32 ? launch_grid_batch<R, COMP, KM_WPROJ, 32>(st, smem, ps, tb, nsnap, counter, total, capturing)
-                 : launch_grid_batch<R, COMP, KM_WPROJ, 16>(st, smem, ps, tb, nsnap, counter, total, capturing);
+        launch_mode<R, COMP, KM_WPROJ>(st, layout, smem, P, total, capturing);
     else if (kind == GK_EXACT)
-        tc == 32 ? launch_grid_batch<R, COMP, KM_EXACT, 32>(st, smem, ps, tb, nsnap, counter, total, capturing)
-                 : launch_grid_batch<R, COMP, KM_EXACT, 16>(st, smem, ps, tb, nsnap, counter, total, capturing);
+        launch_mode<R, COMP, KM_EXACT>(st, layout, smem, P, total, capturing);
     else
-        tc == 32 ? launch_grid_batch<R, COMP, KM_SEP, 32>(st, smem, ps, tb, nsnap, counter, total, capturing)
-                 : launch_grid_batch<R, COMP, KM_SEP, 16>(st, smem, ps, tb, nsnap, counter, total, capturing);
+        launch_mode<R, COMP, KM_SEP>(st, layout, smem, P, total, capturing);
 }
 
 // Enqueue one batch: preparation of every snapshot on the worker streams,
@@ -907,47 +963,44 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
     for (int i = 0; i < nb; i++) {
         if (L[i].kind == GK_NONE || L[i].ntiles == 0)
             continue;
-        std::string key = std::to_string(L[i].kind) + "/" + std::to_string(L[i].tile_c);
+        std::string key = std::to_string(L[i].kind) + "/" + std::to_string(L[i].tile_c) + "/"
+            + std::to_string(B[i].persist);
         if (class_ms)
             key += "|" + B[i].cls;
         groups[key].push_back(i);
     }
-    size_t hoff = 0;
-    int gi = 0;
+    int gi = 0, nlaunch = 0;
     for (auto& kv : groups) {
-        const std::vector<int>& mem = kv.second;
-        const int m = int(mem.size());
-        GridParams<R>* hp = reinterpret_cast<GridParams<R>*>(host_params + hoff);
-        hoff += pad256(sizeof(GridParams<R>) * m);
-        uint32_t* htb = reinterpret_cast<uint32_t*>(host_params + hoff);
-        hoff += pad256(sizeof(uint32_t) * (m + 1));
-        size_t smem = 0;
-        uint32_t tot = 0;
-        for (int k = 0; k < m; k++) {
-            const GridLaunch<R>& l = L[mem[k]];
-            hp[k] = l.gp; // a captured copy reads these host bytes at every replay
-            htb[k] = tot;
-            tot += uint32_t(l.ntiles);
-            smem = std::max(smem, l.smem);
-        }
-        htb[m] = tot;
-        const std::string gname = "g" + std::to_string(gi++);
-        GridParams<R>* dps = c->buf<GridParams<R>>(gname + "ps", m);
-        uint32_t* dtb = c->buf<uint32_t>(gname + "tb", m + 1);
-        uint32_t* ctr = c->buf<uint32_t>(gname + "ctr", 1);
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(dps, hp, sizeof(GridParams<R>) * m, cudaMemcpyHostToDevice, main));
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(dtb, htb, sizeof(uint32_t) * (m + 1), cudaMemcpyHostToDevice, main));
-        STPGPU_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), main));
-        if (class_ms)
-            STPGPU_CUDA_TRY(cudaEventRecord(c->pev[0], main));
-        const GridLaunch<R>& l0 = L[mem[0]];
-        launch_group<R, COMP>(main, l0.kind, l0.tile_c, smem, dps, dtb, m, ctr, tot, capturing);
-        if (class_ms) {
-            STPGPU_CUDA_TRY(cudaEventRecord(c->pev[1], main));
-            STPGPU_CUDA_TRY(cudaEventSynchronize(c->pev[1]));
-            float ms = 0.f;
-            STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->pev[0], c->pev[1]));
-            (*class_ms)[B[mem[0]].cls] += ms;
+        const std::vector<int>& all = kv.second;
+        for (size_t c0 = 0; c0 < all.size(); c0 += kBatchGrid) {
+            const int m = int(std::min<size_t>(kBatchGrid, all.size() - c0));
+            auto* P = reinterpret_cast<BatchGridParams<R>*>(host_params); // host-side scratch, copied by value
+            size_t smem = 0;
+            uint32_t tot = 0;
+            for (int k = 0; k < m; k++) {
+                const GridLaunch<R>& l = L[all[c0 + k]];
+                P->ps[k] = l.gp;
+                P->tile_base[k] = tot;
+                tot += uint32_t(l.ntiles);
+                smem = std::max(smem, l.smem);
+            }
+            P->tile_base[m] = tot;
+            P->nsnap = m;
+            P->counter = c->buf<uint32_t>("g" + std::to_string(gi++) + "ctr", 1);
+            STPGPU_CUDA_TRY(cudaMemsetAsync(P->counter, 0, sizeof(uint32_t), main));
+            if (class_ms)
+                STPGPU_CUDA_TRY(cudaEventRecord(c->pev[0], main));
+            const GridLaunch<R>& l0 = L[all[c0]];
+            launch_group<R, COMP>(main, l0.kind, l0.tile_c | (B[all[c0]].persist ? kLayoutPersist : 0), smem, *P,
+                tot, capturing);
+            nlaunch++;
+            if (class_ms) {
+                STPGPU_CUDA_TRY(cudaEventRecord(c->pev[1], main));
+                STPGPU_CUDA_TRY(cudaEventSynchronize(c->pev[1]));
+                float ms = 0.f;
+                STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->pev[0], c->pev[1]));
+                (*class_ms)[B[all[c0]].cls] += ms;
+            }
         }
     }
 
@@ -971,15 +1024,9 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
     c->stream = main;
     c->ns = "";
     batch_join(c, main);
-    return int(groups.size());
+    return nlaunch;
 }
 
-std::string size_class(const ImagerSetup& s, int precision)
-{
-    const int conv = s.nplanes > 0 ? s.max_support : s.support;
-    return "p" + std::to_string(precision) + "/k" + std::to_string(s.nplanes > 0 ? 2 : (s.kernel_exact ? 1 : 0))
-        + "/N" + std::to_string(s.N) + "/S" + std::to_string(conv) + "/os" + std::to_string(s.os);
-}
 
 template <typename R, int COMP>
 void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precision, int out_f32, int device_ptrs,
@@ -1011,7 +1058,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         b.uvw = x.uvw;
         b.n = x.n_vis;
         b.image = x.image;
-        b.cls = size_class(b.s, precision);
+        b.cls = size_class(b.s, precision) + "/batch";
         put(&x.pars, sizeof(x.pars));
         put(&x.wproj, sizeof(x.wproj));
         put(&x.n_vis, sizeof(x.n_vis));
@@ -1030,9 +1077,9 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         c->batch_calls = 0;
     }
     c->batch_calls++;
-    // pinned staging: gridder parameter tables (<= 2 per snapshot) + scalars
-    const size_t need = size_t(nb) * (pad256(sizeof(GridParams<R>)) + 2 * 256) * 2
-        + pad256(sizeof(BatchScalars) * nb) + 4096;
+    // pinned staging: scalars read back by the device + host scratch for the
+    // by-value gridder parameter block
+    const size_t need = pad256(sizeof(BatchScalars) * nb) + pad256(sizeof(BatchGridParams<R>)) + 4096;
     if (c->batch_host_cap < need) {
         if (c->batch_host) {
             for (auto w : c->wstreams)
@@ -1077,22 +1124,39 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             if (!c->tune.count(b.cls) && std::find(fresh.begin(), fresh.end(), b.cls) == fresh.end())
                 fresh.push_back(b.cls);
         if (!fresh.empty()) {
-            std::map<std::string, float> t32, t16;
-            for (int cand : { 32, 16 }) {
-                for (auto& b : B)
-                    b.tile_c = c->tune.count(b.cls) ? c->tune[b.cls] : cand;
-                for (int k = 0; k < 5; k++)
-                    if (!c->pev[k])
-                        STPGPU_CUDA_TRY(cudaEventCreate(&c->pev[k]));
-                batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, cand == 32 ? &t32 : &t16);
+            const int layouts[4] = { 32, 16, 32 | kLayoutPersist, 16 | kLayoutPersist };
+            std::map<std::string, float> t[4];
+            for (int k = 0; k < 5; k++)
+                if (!c->pev[k])
+                    STPGPU_CUDA_TRY(cudaEventCreate(&c->pev[k]));
+            for (int cand = 0; cand < 4; cand++) {
+                for (auto& b : B) {
+                    const int lay = c->tune.count(b.cls) ? c->tune[b.cls] : layouts[cand];
+                    b.tile_c = lay & 0xff;
+                    b.persist = (lay & kLayoutPersist) ? 1 : 0;
+                }
+                batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, &t[cand]);
                 STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
             }
-            for (auto& cls : fresh)
-                c->tune[cls] = t16[cls] < t32[cls] ? 16 : 32;
+            static const bool log_tuning = std::getenv("STPGPU_LOG_TUNING") != nullptr;
+            for (auto& cls : fresh) {
+                int best = 0;
+                for (int cand = 1; cand < 4; cand++)
+                    if (t[cand][cls] < t[best][cls])
+                        best = cand;
+                c->tune[cls] = layouts[best];
+                if (log_tuning)
+                    std::fprintf(stderr,
+                        "stpgpu gridder tuner: %s  32/16 cols %.3f/%.3f ms, persistent %.3f/%.3f ms -> %d%s\n",
+                        cls.c_str(), double(t[0][cls]), double(t[1][cls]), double(t[2][cls]), double(t[3][cls]),
+                        layouts[best] & 0xff, (layouts[best] & kLayoutPersist) ? " persistent" : "");
+            }
             tuned = int(fresh.size());
         }
-        for (auto& b : B)
-            b.tile_c = c->tune[b.cls];
+        for (auto& b : B) {
+            b.tile_c = c->tune[b.cls] & 0xff;
+            b.persist = (c->tune[b.cls] & kLayoutPersist) ? 1 : 0;
+        }
         if (device_ptrs && c->batch_calls >= 2 && tuned == 0) {
             // capture the batch (buffers, plans and tables exist from the previous call)
             STPGPU_CUDA_TRY(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
@@ -1599,6 +1663,9 @@ stpgpu_status stpgpu_destroy(stpgpu_context* c)
         cudaEventDestroy(e);
     if (c->fork_ev)
         cudaEventDestroy(c->fork_ev);
+    for (auto e : c->tev)
+        if (e)
+            cudaEventDestroy(e);
     if (c->ev0)
         cudaEventDestroy(c->ev0);
     if (c->ev1)

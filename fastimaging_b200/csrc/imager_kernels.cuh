@@ -497,7 +497,7 @@ struct GridParams {
 // Kernel value of tap (i, j) of the lane's item, times the visibility weight.
 template <typename R, int KMODE>
 struct TapCtx {
-    int K, S, cpx, cpy;
+    int K, S, cpx, cpy, os, lh;
     R wt, winv;
     bool conj_k;
     const typename Cplx<R>::T* wconv;
@@ -518,11 +518,11 @@ __device__ __forceinline__ void tap_value(const GridParams<R>& p, const R* tab, 
         kr = R((y * x) / t.ksum);
         ki = R(0);
     } else {
-        int oy = (i - t.S) * p.os + p.os / 2 - t.cpy;
-        int ox = (j - t.S) * p.os + p.os / 2 - t.cpx;
+        int oy = (i - t.S) * t.os + t.os / 2 - t.cpy;
+        int ox = (j - t.S) * t.os + t.os / 2 - t.cpx;
         oy = oy < 0 ? -oy : oy;
         ox = ox < 0 ? -ox : ox;
-        const typename Cplx<R>::T cv = t.wconv[size_t(oy) * p.lh + ox];
+        const typename Cplx<R>::T cv = t.wconv[size_t(oy) * t.lh + ox];
         kr = cv.x * t.winv;
         ki = t.conj_k ? -(cv.y * t.winv) : cv.y * t.winv;
     }
@@ -538,6 +538,9 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
     A* bacc = acc + (BEAM ? TILE_R * TILE_C : 0);
     R* tab = reinterpret_cast<R*>(acc + (BEAM ? 2 : 1) * TILE_R * TILE_C);
     const int lane = threadIdx.x;
+    // hot scalars in registers (the batch kernel reads p from parameter
+    // space with a run-time index, which costs a load per use)
+    const int gN = p.N, grows = p.image_rows, gos = p.os, glh = p.lh;
     const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
     const int r0 = tr * TILE_R, c0 = tc * TILE_C;
     const bool wrap_neg = p.exact_wrap != 0;
@@ -562,6 +565,8 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
         t.K = 0;
         t.S = 0;
         t.cpx = t.cpy = 0;
+        t.os = gos;
+        t.lh = glh;
         t.wt = R(0);
         t.winv = R(1);
         t.conj_k = false;
@@ -579,14 +584,14 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
             const int mir = int(code & 1u);
             const Item<R> it = p.items[vi];
             int cx, cy;
-            item_centre(it, mir, p.N, cx, cy);
+            item_centre(it, mir, gN, cx, cy);
             t.S = (KMODE == KM_WPROJ) ? p.plane_support[it.plane] : p.support;
             t.K = 2 * t.S + 1;
             t.cpx = it.cpx;
             t.cpy = it.cpy;
-            if (mir && p.os > 1) {
-                t.cpx = p.os - t.cpx;
-                t.cpy = p.os - t.cpy;
+            if (mir && gos > 1) {
+                t.cpx = gos - t.cpx;
+                t.cpy = gos - t.cpy;
             }
             vr = it.vr;
             vim = mir ? -it.vi : it.vi;
@@ -595,15 +600,15 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
             cb = cx - t.S;
             // column window of the footprint inside this tile; only footprints
             // crossing the grid edge need the per-tap wrap
-            cwrap = cb < 0 || cb + t.K > p.N;
+            cwrap = cb < 0 || cb + t.K > gN;
             cbase = cb - c0;
             jlo = cwrap ? 0 : max(0, -cbase);
             jhi = cwrap ? t.K : min(t.K, TILE_C - cbase);
-            const int krow = ((rb % p.N) + p.N) % p.N, kcol = ((cb % p.N) + p.N) % p.N;
-            key = (unsigned long long)krow * (unsigned long long)p.N + (unsigned long long)kcol;
+            const int krow = ((rb % gN) + gN) % gN, kcol = ((cb % gN) + gN) % gN;
+            key = (unsigned long long)krow * (unsigned long long)gN + (unsigned long long)kcol;
             if (KMODE == KM_WPROJ) {
                 t.conj_k = (it.flags >> (mir ? 1 : 0)) & 1u;
-                t.wconv = p.wconv + size_t(it.plane) * p.lh * p.lh;
+                t.wconv = p.wconv + size_t(it.plane) * glh * glh;
                 t.winv = p.winv[(size_t(it.plane) * p.cs + t.cpy) * p.cs + t.cpx];
             }
             if (KMODE == KM_EXACT) {
@@ -646,7 +651,7 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
                 // registers eight taps at a time, so the loads are in flight
                 // together, then accumulated tap by tap in lockstep
                 for (int i = 0; i < kmax; i++) {
-                    const int rm = (mine && i < t.K) ? map_row(rb + i, p.N, p.image_rows, wrap_neg) : -1;
+                    const int rm = (mine && i < t.K) ? map_row(rb + i, gN, grows, wrap_neg) : -1;
                     const int rl = rm - r0;
                     const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
                     for (int j0 = 0; j0 < kmax; j0 += 8) {
@@ -664,7 +669,7 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
                             const int j = j0 + jj;
                             if (j < kmax) {
                                 if (rok && j < t.K && j >= jlo && j < jhi) {
-                                    const int cl = cwrap ? map_col(cb + j, p.N) - c0 : cbase + j;
+                                    const int cl = cwrap ? map_col(cb + j, gN) - c0 : cbase + j;
                                     if (cl >= 0 && cl < TILE_C) {
                                         const R re = vr * kr[jj] - vim * ki[jj];
                                         const R im = vr * ki[jj] + vim * kr[jj];
@@ -680,12 +685,12 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
                 }
             } else {
                 for (int i = 0; i < kmax; i++) {
-                    const int rm = (mine && i < t.K) ? map_row(rb + i, p.N, p.image_rows, wrap_neg) : -1;
+                    const int rm = (mine && i < t.K) ? map_row(rb + i, gN, grows, wrap_neg) : -1;
                     const int rl = rm - r0;
                     const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
                     for (int j = 0; j < kmax; j++) {
                         if (rok && j < t.K && j >= jlo && j < jhi) {
-                            const int cl = cwrap ? map_col(cb + j, p.N) - c0 : cbase + j;
+                            const int cl = cwrap ? map_col(cb + j, gN) - c0 : cbase + j;
                             if (cl >= 0 && cl < TILE_C) {
                                 R kr, ki;
                                 tap_value<R, KMODE>(p, tab, t, i, j, kr, ki);
@@ -703,12 +708,12 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
         }
     }
     __syncwarp();
-    const int nr = min(TILE_R, p.image_rows - r0);
-    const int nc = min(TILE_C, p.N - c0);
+    const int nr = min(TILE_R, grows - r0);
+    const int nc = min(TILE_C, gN - c0);
     for (int q = lane; q < TILE_R * TILE_C; q += 32) {
         const int rl = q % TILE_R, cl = q / TILE_R;
         if (rl < nr && cl < nc) {
-            const size_t g = size_t(c0 + cl) * p.image_rows + (r0 + rl);
+            const size_t g = size_t(c0 + cl) * grows + (r0 + rl);
             p.grid[g] = acc_value(acc[q]);
             if (BEAM)
                 p.beam[g] = acc_value(bacc[q]);
@@ -717,40 +722,61 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
 }
 
 // One CTA (one warp) per tile of one snapshot.
+// Residency target: the shared-memory tile allows ~28 CTAs per SM at 16
+// columns (8 KB FP32/FP32C cell tile) and ~14 at 32; registers are capped to match.
 template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
-__global__ void __launch_bounds__(32) k_grid_tiles(GridParams<R> p)
+__global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) : 14) k_grid_tiles(GridParams<R> p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     grid_tile<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
 }
 
+// Parameters of one persistent gridder launch: up to kBatchGrid snapshots,
+// passed by value (kernel parameter space, read through the constant cache
+// with a warp-uniform index).
+constexpr int kBatchGrid = 64;
+template <typename R>
+struct BatchGridParams {
+    GridParams<R> ps[kBatchGrid];
+    uint32_t tile_base[kBatchGrid + 1];
+    int nsnap;
+    uint32_t* counter;
+};
+
 // Persistent gridder over the tiles of many snapshots: a (snapshot, tile)
 // work queue.  Work item w is tile w - tile_base[s] of the snapshot s with
 // tile_base[s] <= w < tile_base[s + 1]; warps take items from one atomic
 // counter (zeroed before the launch) until the queue is empty.
-template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
-__global__ void __launch_bounds__(32) k_grid_batch(const GridParams<R>* __restrict__ ps,
-    const uint32_t* __restrict__ tile_base, int nsnap, uint32_t* counter)
+// PERSIST = false: one CTA per work item (w = blockIdx.x), the hardware
+// block scheduler being the queue; the autotuner picks the faster form.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, bool PERSIST>
+__global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) : 14) k_grid_batch(const __grid_constant__ BatchGridParams<R> P)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const uint32_t total = tile_base[nsnap];
-    for (;;) {
+    const uint32_t total = P.tile_base[P.nsnap];
+    for (int once = 0;; once++) {
         uint32_t w = 0;
-        if (threadIdx.x == 0)
-            w = atomicAdd(counter, 1u);
-        w = __shfl_sync(0xffffffffu, w, 0);
+        if (PERSIST) {
+            if (threadIdx.x == 0)
+                w = atomicAdd(P.counter, 1u);
+            w = __shfl_sync(0xffffffffu, w, 0);
+        } else {
+            if (once)
+                break;
+            w = blockIdx.x;
+        }
         if (w >= total)
             break;
-        int lo = 0, hi = nsnap - 1;
+        int lo = 0, hi = P.nsnap - 1;
         while (lo < hi) { // last snapshot whose first tile <= w
             const int mid = (lo + hi + 1) / 2;
-            if (tile_base[mid] <= w)
+            if (P.tile_base[mid] <= w)
                 lo = mid;
             else
                 hi = mid - 1;
         }
         __syncwarp();
-        grid_tile<R, COMP, KMODE, BEAM, TILE_C>(ps[lo], int(w - tile_base[lo]), smem_raw);
+        grid_tile<R, COMP, KMODE, BEAM, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw);
         __syncwarp();
     }
 }

@@ -134,3 +134,24 @@ CONFIG1_IMAGER = dict(kernel_func=4, kernel_support=3, kernel_exact=False, overs
                       analytic_gcf=False)
 CONFIG3_IMAGER = dict(kernel_func=5, kernel_support=4, kernel_exact=False, oversampling=16, gridding_correction=True,
                       analytic_gcf=True)
+
+
+def config4(seed=4, n_snapshots=64, n_src=5):
+    """Batched snapshots: visibility counts log-uniform in 50k-2M, image sizes from {1024, 2048, 4096, 8192},
+    w ~ U[-w_max, w_max] with w_max ~ U[0, 2000] lambda per snapshot, kernels alternating GaussianSinc / PSWF by a
+    seeded coin; W-projection with 16 planes, W-kernel support <= 16 (1 % truncation), os 8.
+    Returns [(Snapshot, imager keywords)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_snapshots):
+        n_vis = int(round(math.exp(rng.uniform(math.log(5e4), math.log(2e6)))))
+        size = int(rng.choice([1024, 2048, 4096, 8192]))
+        w_max = float(rng.uniform(0.0, 2000.0))
+        kf = 4 if rng.random() < 0.5 else 5
+        s = make_snapshot(seed * 1000 + i, n_vis, size, 1.0, n_src=n_src, flux=(0.5, 10.0), noise_sigma=0.05,
+                          w_range=(-w_max, w_max))
+        kw = dict(image_size=size, cell_size=1.0, kernel_func=kf, kernel_support=3, kernel_exact=False,
+                  oversampling=8, gridding_correction=True, analytic_gcf=False, num_wplanes=16,
+                  max_wpconv_support=16, undersampling_opt=1, kernel_trunc_perc=1.0)
+        out.append((s, kw))
+    return out
