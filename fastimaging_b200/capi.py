@@ -107,9 +107,37 @@ def imager_pars(image_size, cell_size, padding_factor=1.0, kernel_func=PSWF, ker
     return ip, wp
 
 
+class ServerPars(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("slots", ctypes.c_int32), ("hbm_budget_bytes", ctypes.c_int64),
+                ("precision", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("vis", ctypes.c_void_p), ("vis_dtype", ctypes.c_int32), ("out_dtype", ctypes.c_int32),
+                ("weights", ctypes.c_void_p), ("uvw", ctypes.c_void_p), ("n_vis", ctypes.c_int64),
+                ("pars", ImagerPars), ("wproj", WProjPars), ("image", ctypes.c_void_p),
+                ("find_sources", ctypes.c_int32), ("island_capacity", ctypes.c_int32), ("sf", SfPars),
+                ("label_map", ctypes.c_void_p), ("islands", ctypes.c_void_p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("n_islands", ctypes.c_int32), ("est_bytes", ctypes.c_int64),
+                ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double), ("done_ms", ctypes.c_double),
+                ("imager", ImagerInfo), ("sf", SfInfo), ("error", ctypes.c_char * 160)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("in_flight", ctypes.c_int64), ("queued", ctypes.c_int64), ("peak_in_flight", ctypes.c_int64),
+                ("peak_admitted_bytes", ctypes.c_int64), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("throughput_rps", ctypes.c_double)]
+
+
 EXPORTED = ["stpgpu_abi_version", "stpgpu_create", "stpgpu_destroy", "stpgpu_last_error", "stpgpu_stream",
             "stpgpu_set_timing", "stpgpu_trim", "stpgpu_image_visibilities", "stpgpu_image_visibilities_ex", "stpgpu_convolve_to_grid",
-            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_image_batch", "stpgpu_label_noalloc"]
+            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_image_batch", "stpgpu_server_create",
+            "stpgpu_server_destroy", "stpgpu_server_submit", "stpgpu_server_wait", "stpgpu_server_stats_get",
+            "stpgpu_label_noalloc"]
 NOALLOC_MAX_PIXELS = 1024 * 1024
 
 _lock = threading.Lock()
@@ -153,6 +181,11 @@ def load():
                                             ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(SfInfo)]
         L.stpgpu_image_batch.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                          ctypes.POINTER(BatchInfo)]
+        L.stpgpu_server_create.argtypes = [ctypes.POINTER(ServerPars), ctypes.POINTER(vp)]
+        L.stpgpu_server_destroy.argtypes = [vp]
+        L.stpgpu_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]
+        L.stpgpu_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Result)]
+        L.stpgpu_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
         L.stpgpu_label_noalloc.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                            vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
@@ -358,3 +391,81 @@ def label_noalloc(device, stream, image_ptr, image_dtype, rows, cols, thresh_pos
     if st != 0:
         raise StpGpuError(st, msg.value.decode(errors="replace"))
     return npos.value, nneg.value
+
+
+class Server:
+    """Request loop over one GPU (stpgpu_server_*): submit imaging (+ source
+    finding) requests from host buffers, wait for their results."""
+
+    def __init__(self, device=0, slots=4, hbm_budget_bytes=32 << 30, precision=FP32C):
+        self.L = load()
+        self.h = ctypes.c_void_p()
+        st = self.L.stpgpu_server_create(ctypes.byref(ServerPars(int(device), int(slots), int(hbm_budget_bytes),
+                                                                    int(precision), 0)), ctypes.byref(self.h))
+        if st != 0:
+            raise StpGpuError(st, "server create")
+        self._keep = {}
+
+    def submit(self, vis, weights, uvw, find_sources=False, out_dtype=F32, sf=None, want_labels=False,
+               island_capacity=4096, **imager_kw):
+        """imager_kw: image_size, cell_size and the image_visibilities keywords.
+        sf: dict of source_find keywords (detection_n_sigma, analysis_n_sigma, ...).
+        Returns a ticket."""
+        vis = np.ascontiguousarray(vis)
+        if vis.dtype not in (np.complex128, np.complex64):
+            vis = vis.astype(np.complex128)
+        n = vis.size
+        w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
+        uvwF = np.asfortranarray(np.asarray(uvw, dtype=np.float64).reshape(n, 3))
+        ip, wp = imager_pars(**imager_kw)
+        size = int(imager_kw["image_size"])
+        img = np.empty((size, size), dtype=np.float32 if out_dtype == F32 else np.float64, order="F")
+        sfd = dict(detection_n_sigma=5.0, analysis_n_sigma=3.0, rms_est=0.0, find_negative_sources=True,
+                   sigma_clip_iters=5, median_method=BINAPPROX, gaussian_fitting=False, ccl_4connectivity=False,
+                   generate_labelmap=True, source_min_area=5, ccl_slice_cols=0)
+        sfd.update(sf or {})
+        sp = SfPars(float(sfd["detection_n_sigma"]), float(sfd["analysis_n_sigma"]), float(sfd["rms_est"]),
+                    int(bool(sfd["find_negative_sources"])), int(sfd["sigma_clip_iters"]), int(sfd["median_method"]),
+                    int(bool(sfd["gaussian_fitting"])), int(bool(sfd["ccl_4connectivity"])),
+                    int(bool(sfd["generate_labelmap"])), int(sfd["source_min_area"]), int(sfd["ccl_slice_cols"]))
+        labels = np.empty((size, size), dtype=np.int32, order="F") if (find_sources and want_labels) else None
+        isl = (Island * max(1, int(island_capacity)))()
+        req = Request(_ptr(vis), C64 if vis.dtype == np.complex64 else C128, int(out_dtype), _ptr(w), _ptr(uvwF), n,
+                      ip, wp, _ptr(img), int(bool(find_sources)), int(island_capacity), sp, _ptr(labels),
+                      ctypes.cast(isl, ctypes.c_void_p))
+        t = ctypes.c_int64()
+        st = self.L.stpgpu_server_submit(self.h, ctypes.byref(req), ctypes.byref(t))
+        if st != 0:
+            raise StpGpuError(st, "submit")
+        self._keep[t.value] = (vis, w, uvwF, img, labels, isl, req)
+        return t.value
+
+    def wait(self, ticket, timeout_s=-1.0):
+        """-> (image, label_map or None, [Island], Result); raises on failure."""
+        res = Result()
+        st = self.L.stpgpu_server_wait(self.h, int(ticket), float(timeout_s), ctypes.byref(res))
+        if st == 8:
+            raise StpGpuError(st, "not done")
+        vis, w, uvwF, img, labels, isl, req = self._keep.pop(int(ticket))
+        if st != 0:
+            raise StpGpuError(st, res.error.decode(errors="replace"))
+        islands = [isl[i] for i in range(min(res.n_islands, len(isl)))] if req.find_sources else []
+        if res.imager.image_size == 0:
+            img = np.zeros((0, 0))
+        return img, labels, islands, res
+
+    def stats(self):
+        s = ServerStats()
+        self.L.stpgpu_server_stats_get(self.h, ctypes.byref(s))
+        return s
+
+    def close(self):
+        if self.h:
+            self.L.stpgpu_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

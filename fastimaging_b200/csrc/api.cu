@@ -13,6 +13,12 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <unordered_map>
+#include <chrono>
+#include <thread>
+#include <memory>
+#include <deque>
+#include <condition_variable>
 #include <mutex>
 #include <string>
 #include <tuple>
@@ -339,10 +345,14 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
 
     // ---- kernels
     const uint32_t* sorted_perm = nullptr;
+    const int64_t* plane_first = nullptr;
+    int nplanes = 0;
     const R* k1d = nullptr;
     const C2* wconv = nullptr;
     const R* winv = nullptr;
     int lh = 0;
+    C2* wk = nullptr;
+    uint32_t* wk_off = nullptr;
     int* plane_support = nullptr;
     if (!wproj && !kernel_exact) {
         // populate_kernel_cache (gridder.h:73-105) as a 1-D table, FP64 on the device
@@ -398,11 +408,21 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         const double* absw_sorted = reinterpret_cast<const double*>(keys_out);
         k_wplanes<<<1, 1, 0, st>>>(cgood, absw_sorted, n, P, s.wmedian, first, last);
         STPGPU_CHECK_LAUNCH();
-        k_wplane_values<<<P, 256, 0, st>>>(cgood, absw_sorted, good_sorted, first, last, n, P, s.wmedian, w_avg);
-        STPGPU_CHECK_LAUNCH();
-        k_assign_planes<R><<<grid1d(n, 256), 256, 0, st>>>(perm, first, P, n, items);
-        STPGPU_CHECK_LAUNCH();
+        if (s.wmedian) {
+            k_wplane_values<<<P, 256, 0, st>>>(cgood, absw_sorted, good_sorted, first, last, n, P, 1, w_avg);
+            STPGPU_CHECK_LAUNCH();
+        } else {
+            const int nblk = int(std::min<int64_t>(1024, ceil_div(n, 2048)));
+            const int64_t chunk = ceil_div(n, nblk);
+            double* partial = c->buf<double>("wpartial", size_t(P) * nblk);
+            k_wplane_partial<<<nblk, 256, 0, st>>>(absw_sorted, good_sorted, first, last, n, P, chunk, nblk, partial);
+            STPGPU_CHECK_LAUNCH();
+            k_wplane_finish<<<P, 256, 0, st>>>(partial, cgood, first, last, chunk, nblk, w_avg);
+            STPGPU_CHECK_LAUNCH();
+        }
         sorted_perm = perm;
+        plane_first = first;
+        nplanes = P;
 
         // W-kernels in FP64 (WideFieldImaging, aw_projection.cpp:19-111,173-210,366-452)
         const int K = 2 * s.max_support + 1;
@@ -465,18 +485,15 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         wq.support = plane_support;
         k_wkernel_plane<<<P, 256, 0, st>>>(wq);
         STPGPU_CHECK_LAUNCH();
-        if (sizeof(R) == 8) {
-            wconv = reinterpret_cast<const C2*>(wq.convd);
-            winv = reinterpret_cast<const R*>(wq.invd);
-        } else {
-            float2* cf = c->buf<float2>("wkconv32", size_t(P) * Lh * Lh);
-            float* inf = c->buf<float>("wkinv32", size_t(P) * cs * cs);
-            const int64_t nconv = int64_t(P) * Lh * Lh, ninv = int64_t(P) * cs * cs;
-            k_wk_to_f32<<<grid1d(std::max(nconv, ninv), 256), 256, 0, st>>>(wq.convd, wq.invd, nconv, ninv, cf, inf);
-            STPGPU_CHECK_LAUNCH();
-            wconv = reinterpret_cast<const C2*>(cf);
-            winv = reinterpret_cast<const R*>(inf);
-        }
+        // per-offset K x K tables in the gridder's precision (worst-case
+        // capacity: every plane at the maximum support)
+        const uint64_t cap_wk = uint64_t(P) * cs * cs * uint64_t(K) * K;
+        if (cap_wk * sizeof(C2) > (uint64_t(2) << 30) || cap_wk > 0xffffffffull)
+            fail(STPGPU_ERR_UNSUPPORTED, "W-kernel tables exceed 2 GB (planes x oversampling^2 x support^2)");
+        wk = c->buf<C2>("wkexp", cap_wk);
+        wk_off = c->buf<uint32_t>("wkoff", P);
+        k_wk_expand<R><<<dim3(P, cs * cs), 64, 0, st>>>(wq.convd, wq.invd, plane_support, P, cs, os, Lh, wk, wk_off);
+        STPGPU_CHECK_LAUNCH();
         lh = Lh;
         g.d_plane_support = plane_support;
         g.nplanes = P;
@@ -514,13 +531,13 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     STPGPU_CUDA_TRY(cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (ntiles + 1), st));
     STPGPU_CUDA_TRY(cudaMemsetAsync(tcur, 0, sizeof(uint32_t) * (ntiles + 1), st));
     if (n > 0) {
-        k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items);
+        k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
     }
     k_scan_single<<<1, 1024, 0, st>>>(tcount, toff, ntiles);
     STPGPU_CHECK_LAUNCH();
     if (n > 0) {
-        k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, wproj ? sorted_perm : nullptr);
+        k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
     }
     g.d_nitems = toff + ntiles;
@@ -548,6 +565,8 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     gp.winv = winv;
     gp.lh = lh;
     gp.plane_support = plane_support;
+    gp.wk = wk;
+    gp.wk_off = wk_off;
     gp.grid = grid;
     gp.beam = beam;
     using A = Acc<R, COMP>;
@@ -1919,6 +1938,307 @@ stpgpu_status stpgpu_source_find(stpgpu_context* c, const double* image, int32_t
 {
     return stpgpu_source_find_ex(c, image, STPGPU_F64, rows, cols, pars, label_map, 0, islands, capacity, n_islands,
         info);
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------ serving
+
+namespace {
+
+struct ServerJob {
+    int64_t ticket = 0;
+    stpgpu_request req {};
+    stpgpu_result res {};
+    bool done = false;
+};
+
+// Device working set of one request (inputs, items, tile lists, W-planes and
+// W-kernel tables, grid, FFT output, image, source-finder arrays), bytes.
+int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c64, int precision, int find_sources)
+{
+    const int64_t rb = precision == STPGPU_FP64 ? 8 : 4;
+    const int64_t N = s.N, rows = N / 2 + 1;
+    const int conv = s.nplanes > 0 ? s.max_support : s.support;
+    int64_t b = n * ((vis_c64 ? 8 : 16) + 8 + 24) + n * (rb == 8 ? 40 : 28);
+    const int64_t per_dim = ceil_div(2 * conv, 16) + 2;
+    b += std::max<int64_t>(n, 1) * 2 * per_dim * per_dim * 4; // tile-list capacity
+    if (s.nplanes > 0) {
+        const int64_t os = std::max(1, (s.os >> 1) << 1), cs = (os / 2) * 2 + 1, K = 2 * conv + 1;
+        const int64_t lh = conv * os + os / 2 + 1;
+        b += n * 41;                                                  // |w| sort, planes
+        b += int64_t(s.nplanes) * (cs * cs * K * K * 2 * rb + lh * lh * 16 + 64 * 64 * 16);
+    }
+    b += rows * N * 2 * rb + N * N * rb + int64_t(image_size) * image_size * rb;
+    if (find_sources)
+        b += int64_t(image_size) * image_size * 29;
+    return b + (int64_t(8) << 20);
+}
+
+// One request on one slot context (host buffers in and out).
+template <typename R, int COMP>
+void serve_request(stpgpu_context* c, const stpgpu_request& r, stpgpu_result& res)
+{
+    int image_size = 0;
+    ImagerSetup s = setup_from(&r.pars, &r.wproj, nullptr, image_size);
+    s.beam = 0;
+    const int c64 = r.vis_dtype == STPGPU_C64;
+    const int f32 = r.out_dtype == STPGPU_F32;
+    const int64_t n = r.n_vis;
+    const void* dv = to_device<unsigned char>(c, "in_vis", r.vis, (c64 ? 8 : 16) * size_t(n));
+    const double* dw = to_device<double>(c, "in_w", r.weights, size_t(n));
+    const double* duvw = to_device<double>(c, "in_uvw", r.uvw, 3 * size_t(n));
+    const int64_t npix = int64_t(image_size) * image_size;
+    const size_t ob = f32 ? 4 : 8;
+    void* dimg = c->buf<unsigned char>("srv_img", ob * size_t(std::max<int64_t>(npix, 1)));
+    run_imager<R, COMP>(c, s, image_size, r.pars.gridding_correction, dv, c64, dw, duvw, n, dimg, nullptr, f32,
+        &res.imager);
+    if (res.imager.image_size > 0) {
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(r.image, dimg, ob * npix, cudaMemcpyDeviceToHost, c->stream));
+        if (r.find_sources) {
+            std::vector<stpgpu_island> isl;
+            if (f32)
+                run_source_find<float>(c, reinterpret_cast<const float*>(dimg), image_size, image_size, r.sf, nullptr,
+                    isl, res.sf);
+            else
+                run_source_find<double>(c, reinterpret_cast<const double*>(dimg), image_size, image_size, r.sf,
+                    nullptr, isl, res.sf);
+            if (r.label_map)
+                STPGPU_CUDA_TRY(cudaMemcpyAsync(r.label_map, c->buf<int32_t>("ccl_L", npix), sizeof(int32_t) * npix,
+                    cudaMemcpyDeviceToHost, c->stream));
+            res.n_islands = int32_t(isl.size());
+            if (int32_t(isl.size()) > r.island_capacity)
+                fail(STPGPU_ERR_CAPACITY, "island buffer too small: need " + std::to_string(isl.size()));
+            if (!isl.empty())
+                std::memcpy(r.islands, isl.data(), sizeof(stpgpu_island) * isl.size());
+        }
+    }
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+}
+
+} // namespace
+
+struct stpgpu_server {
+    stpgpu_server_pars pars {};
+    std::vector<stpgpu_context*> slots;
+    std::vector<std::thread> workers;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<ServerJob*> queue;
+    std::unordered_map<int64_t, std::unique_ptr<ServerJob>> jobs;
+    int64_t next_ticket = 1;
+    int64_t inflight = 0, inflight_bytes = 0;
+    bool stop = false;
+    std::chrono::steady_clock::time_point t0;
+    std::vector<double> latency_ms;
+    double first_submit = -1.0, last_done = 0.0;
+    stpgpu_server_stats st {};
+
+    double now_ms() const
+    {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    void worker(int k)
+    {
+        stpgpu_context* c = slots[k];
+        cudaSetDevice(c->device);
+        for (;;) {
+            ServerJob* job = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                // first-in first-out: the head starts once its working set fits
+                cv_work.wait(lk, [&] {
+                    return stop
+                        || (!queue.empty() && inflight_bytes + queue.front()->res.est_bytes <= pars.hbm_budget_bytes);
+                });
+                if (queue.empty() && stop)
+                    return;
+                if (queue.empty() || inflight_bytes + queue.front()->res.est_bytes > pars.hbm_budget_bytes)
+                    continue;
+                job = queue.front();
+                queue.pop_front();
+                inflight++;
+                inflight_bytes += job->res.est_bytes;
+                st.peak_in_flight = std::max(st.peak_in_flight, inflight);
+                st.peak_admitted_bytes = std::max(st.peak_admitted_bytes, inflight_bytes);
+                job->res.admit_ms = now_ms();
+            }
+            const stpgpu_status status = guard(c, [&] {
+                g_launches = 0;
+                switch (pars.precision) {
+                case STPGPU_FP64:
+                    serve_request<double, 0>(c, job->req, job->res);
+                    break;
+                case STPGPU_FP32:
+                    serve_request<float, 0>(c, job->req, job->res);
+                    break;
+                default:
+                    serve_request<float, 1>(c, job->req, job->res);
+                    break;
+                }
+            });
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                job->res.status = status;
+                if (status != STPGPU_OK)
+                    std::snprintf(job->res.error, sizeof(job->res.error), "%s", c->err.c_str());
+                job->res.done_ms = now_ms();
+                job->done = true;
+                inflight--;
+                inflight_bytes -= job->res.est_bytes;
+                if (status == STPGPU_OK) {
+                    st.completed++;
+                    latency_ms.push_back(job->res.done_ms - job->res.submit_ms);
+                    last_done = std::max(last_done, job->res.done_ms);
+                } else {
+                    st.failed++;
+                }
+            }
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+    }
+};
+
+extern "C" {
+
+stpgpu_status stpgpu_server_create(const stpgpu_server_pars* pars, stpgpu_server** out)
+{
+    if (!pars || !out || pars->slots < 1 || pars->hbm_budget_bytes <= 0)
+        return STPGPU_ERR_INVALID_ARG;
+    if (pars->precision < STPGPU_FP64 || pars->precision > STPGPU_FP32C)
+        return STPGPU_ERR_INVALID_ARG;
+    *out = nullptr;
+    auto* sv = new stpgpu_server();
+    sv->pars = *pars;
+    sv->t0 = std::chrono::steady_clock::now();
+    for (int k = 0; k < pars->slots; k++) {
+        stpgpu_context* c = nullptr;
+        const stpgpu_status s = stpgpu_create(pars->device, &c);
+        if (s != STPGPU_OK) {
+            for (auto x : sv->slots)
+                stpgpu_destroy(x);
+            delete sv;
+            return s;
+        }
+        sv->slots.push_back(c);
+    }
+    for (int k = 0; k < pars->slots; k++)
+        sv->workers.emplace_back([sv, k] { sv->worker(k); });
+    *out = sv;
+    return STPGPU_OK;
+}
+
+stpgpu_status stpgpu_server_destroy(stpgpu_server* sv)
+{
+    if (!sv)
+        return STPGPU_OK;
+    {
+        std::unique_lock<std::mutex> lk(sv->mu);
+        sv->cv_done.wait(lk, [&] { return sv->queue.empty() && sv->inflight == 0; });
+        sv->stop = true;
+    }
+    sv->cv_work.notify_all();
+    for (auto& t : sv->workers)
+        t.join();
+    for (auto c : sv->slots)
+        stpgpu_destroy(c);
+    delete sv;
+    return STPGPU_OK;
+}
+
+stpgpu_status stpgpu_server_submit(stpgpu_server* sv, const stpgpu_request* r, int64_t* ticket)
+{
+    if (!sv || !r || !ticket)
+        return STPGPU_ERR_INVALID_ARG;
+    int64_t est = 0;
+    try {
+        int image_size = 0;
+        ImagerSetup s = setup_from(&r->pars, &r->wproj, nullptr, image_size);
+        if (r->pars.generate_beam)
+            return STPGPU_ERR_UNSUPPORTED;
+        if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
+            return STPGPU_ERR_INVALID_ARG;
+        if (r->n_vis < 0 || (r->n_vis > 0 && (!r->vis || !r->weights || !r->uvw)) || !r->image)
+            return STPGPU_ERR_INVALID_ARG;
+        if ((r->vis_dtype != STPGPU_C128 && r->vis_dtype != STPGPU_C64)
+            || (r->out_dtype != STPGPU_F64 && r->out_dtype != STPGPU_F32))
+            return STPGPU_ERR_INVALID_ARG;
+        if (r->find_sources && (r->island_capacity < 0 || (r->island_capacity > 0 && !r->islands)))
+            return STPGPU_ERR_INVALID_ARG;
+        est = request_bytes(s, image_size, r->n_vis, r->vis_dtype == STPGPU_C64, sv->pars.precision, r->find_sources);
+    } catch (const Error& e) {
+        return e.status;
+    }
+    if (est > sv->pars.hbm_budget_bytes)
+        return STPGPU_ERR_OOM;
+    auto job = std::make_unique<ServerJob>();
+    job->req = *r;
+    job->res.est_bytes = est;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        job->ticket = sv->next_ticket++;
+        job->res.submit_ms = sv->now_ms();
+        if (sv->first_submit < 0)
+            sv->first_submit = job->res.submit_ms;
+        sv->st.submitted++;
+        *ticket = job->ticket;
+        sv->queue.push_back(job.get());
+        sv->jobs[job->ticket] = std::move(job);
+    }
+    sv->cv_work.notify_all();
+    return STPGPU_OK;
+}
+
+stpgpu_status stpgpu_server_wait(stpgpu_server* sv, int64_t ticket, double timeout_s, stpgpu_result* out)
+{
+    if (!sv)
+        return STPGPU_ERR_INVALID_ARG;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(ticket);
+    if (it == sv->jobs.end())
+        return STPGPU_ERR_INVALID_ARG;
+    ServerJob* job = it->second.get();
+    if (timeout_s < 0)
+        sv->cv_done.wait(lk, [&] { return job->done; });
+    else if (!sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return job->done; }))
+        return STPGPU_ERR_TIMEOUT;
+    if (out)
+        *out = job->res;
+    const stpgpu_status s = stpgpu_status(job->res.status);
+    sv->jobs.erase(it);
+    return s;
+}
+
+stpgpu_status stpgpu_server_stats_get(stpgpu_server* sv, stpgpu_server_stats* out)
+{
+    if (!sv || !out)
+        return STPGPU_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    stpgpu_server_stats s = sv->st;
+    s.in_flight = sv->inflight;
+    s.queued = int64_t(sv->queue.size());
+    std::vector<double> l = sv->latency_ms;
+    if (!l.empty()) {
+        std::sort(l.begin(), l.end());
+        auto pct = [&](double q) {
+            const double pos = q * double(l.size() - 1);
+            const size_t i = size_t(pos);
+            const double f = pos - double(i);
+            return i + 1 < l.size() ? l[i] * (1.0 - f) + l[i + 1] * f : l[i];
+        };
+        s.p50_ms = pct(0.50);
+        s.p99_ms = pct(0.99);
+        double sum = 0.0;
+        for (double v : l)
+            sum += v;
+        s.mean_ms = sum / double(l.size());
+        const double span = sv->last_done - sv->first_submit;
+        s.throughput_rps = span > 0 ? double(s.completed) / (span / 1e3) : 0.0;
+    }
+    *out = s;
+    return STPGPU_OK;
 }
 
 } // extern "C"

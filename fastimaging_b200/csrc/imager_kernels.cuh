@@ -251,9 +251,8 @@ __device__ __forceinline__ void item_centre(const Item<R>& it, int mir, int N, i
 // values are collected in small register bitmasks (tile ids relative to the
 // first one seen, plus a wrap-around run).
 template <typename R, typename F>
-__device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, const BinParams& p, F f)
+__device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, int S, const BinParams& p, F f)
 {
-    const int S = p.plane_support ? p.plane_support[it.plane] : p.support;
     const int K = 2 * S + 1;
     int cx, cy;
     item_centre(it, mir, p.N, cx, cy);
@@ -311,29 +310,58 @@ __device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, const
     }
 }
 
-template <typename R>
-__global__ void k_count_tiles(BinParams p, const Item<R>* items)
+// W-plane of sorted position k: the last plane whose first position <= k.
+__device__ __forceinline__ int plane_of(const int64_t* first, int P, int64_t k)
 {
-    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= p.n)
-        return;
-    const Item<R> it = items[i];
-    for (int mir = 0; mir < int(it.good); mir++)
-        for_item_tiles(it, mir, p, [&](uint32_t t) { atomicAdd(&p.tile_count[t], 1u); });
+    int lo = 0, hi = P - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (first[mid] <= k)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
 }
 
-// Lists are filled in the order given by `order` when non-null (the |w|
-// order for W-projection), so that a warp's items mostly share one plane.
+// With W-projection (`order` = the |w| permutation, `first` = plane starts)
+// items are visited in |w| order and take the plane of their sorted
+// position; the fill pass records it in the item for the gridder.
 template <typename R>
-__global__ void k_fill_tiles(BinParams p, const Item<R>* items, const uint32_t* order)
+__global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t* order, const int64_t* first, int P)
 {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= p.n)
         return;
     const int64_t i = order ? int64_t(order[k]) : k;
     const Item<R> it = items[i];
+    if (!it.good)
+        return;
+    const int S = order ? p.plane_support[plane_of(first, P, k)] : p.support;
     for (int mir = 0; mir < int(it.good); mir++)
-        for_item_tiles(it, mir, p, [&](uint32_t t) {
+        for_item_tiles(it, mir, S, p, [&](uint32_t t) { atomicAdd(&p.tile_count[t], 1u); });
+}
+
+// Lists are filled in |w| order for W-projection, so that a warp's items
+// mostly share one plane.
+template <typename R>
+__global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order, const int64_t* first, int P)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= p.n)
+        return;
+    const int64_t i = order ? int64_t(order[k]) : k;
+    const Item<R> it = items[i];
+    if (!it.good)
+        return;
+    int S = p.support;
+    if (order) {
+        const int plane = plane_of(first, P, k);
+        S = p.plane_support[plane];
+        items[i].plane = uint16_t(plane);
+    }
+    for (int mir = 0; mir < int(it.good); mir++)
+        for_item_tiles(it, mir, S, p, [&](uint32_t t) {
             const uint32_t slot = atomicAdd(&p.tile_cursor[t], 1u);
             const uint64_t pos = uint64_t(p.tile_off[t]) + slot;
             if (pos < p.list_capacity)
@@ -343,44 +371,55 @@ __global__ void k_fill_tiles(BinParams p, const Item<R>* items, const uint32_t* 
         });
 }
 
-// Exclusive scan of n counts into off[0..n] (single block, n up to a few
-// hundred thousand).  off[n] = total.
-__global__ void k_scan_single(const uint32_t* cnt, uint32_t* off, int n)
+// Exclusive scan of n counts into off[0..n] (single block of 1024 threads,
+// n up to a few hundred thousand).  off[n] = total.  Each thread first
+// loads 16 elements (16 coalesced rows of 1024), then the rows are scanned
+// in order with warp shuffles and one shared-memory step per row.
+__global__ void __launch_bounds__(1024) k_scan_single(const uint32_t* cnt, uint32_t* off, int n)
 {
-    __shared__ uint32_t s[1024];
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0)
-        carry = 0;
-    __syncthreads();
-    for (int base = 0; base < n; base += 1024 * 8) {
-        // each thread scans 8 consecutive elements
-        uint32_t v[8];
-        uint32_t loc = 0;
-        const int b0 = base + threadIdx.x * 8;
-        for (int k = 0; k < 8; k++) {
-            v[k] = (b0 + k < n) ? cnt[b0 + k] : 0u;
-            loc += v[k];
+    __shared__ uint32_t wsum[32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint32_t carry = 0;
+    for (int base = 0; base < n; base += 1024 * 16) {
+        uint32_t v[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            const int idx = base + j * 1024 + tid;
+            v[j] = idx < n ? cnt[idx] : 0u;
         }
-        s[threadIdx.x] = loc;
-        __syncthreads();
-        for (int o = 1; o < 1024; o <<= 1) {
-            uint32_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0u;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            if (base + j * 1024 >= n)
+                break;
+            uint32_t x = v[j];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o)
+                    x += y;
+            }
+            if (lane == 31)
+                wsum[warp] = x;
             __syncthreads();
-            s[threadIdx.x] += t;
+            if (warp == 0) {
+                uint32_t t = wsum[lane];
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+                    if (lane >= o)
+                        t += y;
+                }
+                wsum[lane] = t;
+            }
+            __syncthreads();
+            const int idx = base + j * 1024 + tid;
+            if (idx < n)
+                off[idx] = carry + (warp ? wsum[warp - 1] : 0u) + x - v[j];
+            carry += wsum[31];
             __syncthreads();
         }
-        uint32_t excl = carry + s[threadIdx.x] - loc;
-        for (int k = 0; k < 8; k++) {
-            if (b0 + k < n)
-                off[b0 + k] = excl;
-            excl += v[k];
-        }
-        __syncthreads();
-        if (threadIdx.x == 1023)
-            carry += s[1023];
-        __syncthreads();
     }
-    if (threadIdx.x == 0)
+    if (tid == 0)
         off[n] = carry;
 }
 
@@ -482,6 +521,10 @@ struct GridParams {
     const R* winv;
     int lh;
     const int* plane_support;
+    // KM_WPROJ: per plane and oversampled offset pair (cpy, cpx) the K x K
+    // cached kernel (conv * inv, tap i*K + j) at wk + wk_off[plane] + (cpy*cs + cpx)*K*K
+    const typename Cplx<R>::T* wk;
+    const uint32_t* wk_off;
     typename Cplx<R>::T* grid; // image_rows x N column-major
     typename Cplx<R>::T* beam; // nullable
 };
@@ -518,13 +561,9 @@ __device__ __forceinline__ void tap_value(const GridParams<R>& p, const R* tab, 
         kr = R((y * x) / t.ksum);
         ki = R(0);
     } else {
-        int oy = (i - t.S) * t.os + t.os / 2 - t.cpy;
-        int ox = (j - t.S) * t.os + t.os / 2 - t.cpx;
-        oy = oy < 0 ? -oy : oy;
-        ox = ox < 0 ? -ox : ox;
-        const typename Cplx<R>::T cv = t.wconv[size_t(oy) * t.lh + ox];
-        kr = cv.x * t.winv;
-        ki = t.conj_k ? -(cv.y * t.winv) : cv.y * t.winv;
+        const typename Cplx<R>::T cv = t.wconv[i * t.K + j];
+        kr = cv.x;
+        ki = t.conj_k ? -cv.y : cv.y;
     }
     kr = kr * t.wt;
     ki = ki * t.wt;
@@ -608,8 +647,7 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
             key = (unsigned long long)krow * (unsigned long long)gN + (unsigned long long)kcol;
             if (KMODE == KM_WPROJ) {
                 t.conj_k = (it.flags >> (mir ? 1 : 0)) & 1u;
-                t.wconv = p.wconv + size_t(it.plane) * glh * glh;
-                t.winv = p.winv[(size_t(it.plane) * p.cs + t.cpy) * p.cs + t.cpx];
+                t.wconv = p.wk + p.wk_off[it.plane] + uint32_t((t.cpy * p.cs + t.cpx) * t.K * t.K);
             }
             if (KMODE == KM_EXACT) {
                 t.fx = p.frac[vi];
@@ -990,21 +1028,73 @@ __global__ void k_wplane_values(const uint32_t* cgood, const double* absw_sorted
     }
 }
 
-template <typename R>
-__global__ void k_assign_planes(const uint32_t* perm, const int64_t* first, int P, int64_t n, Item<R>* items)
+// Mean |w| per plane in two deterministic steps: block b sums the good |w|
+// of its slice [b*chunk, (b+1)*chunk) of the sorted array separately for
+// every plane the slice meets (partial[p][b]); then one block per plane adds
+// its partials in block order.
+__global__ void __launch_bounds__(256) k_wplane_partial(const double* __restrict__ absw_sorted,
+    const uint8_t* __restrict__ good_sorted, const int64_t* first, const int64_t* last, int64_t n, int P,
+    int64_t chunk, int nblk, double* partial)
 {
-    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (k >= n)
+    __shared__ double red[256];
+    const int64_t a = int64_t(blockIdx.x) * chunk;
+    const int64_t b = min(n, a + chunk);
+    if (a >= b)
         return;
-    int lo = 0, hi = P - 1;
-    while (lo < hi) { // last plane whose first <= k
-        int mid = (lo + hi + 1) / 2;
-        if (first[mid] <= k)
-            lo = mid;
-        else
-            hi = mid - 1;
+    int p = 0;
+    {
+        int lo = 0, hi = P - 1; // last plane with first <= a
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (first[mid] <= a)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        p = lo;
     }
-    items[perm[k]].plane = uint16_t(lo);
+    for (; p < P && first[p] < b; p++) {
+        const int64_t s0 = max(a, first[p]), s1 = min(b, last[p]);
+        double t = 0.0;
+        for (int64_t k = s0 + threadIdx.x; k < s1; k += blockDim.x)
+            if (good_sorted[k])
+                t += absw_sorted[k];
+        red[threadIdx.x] = t;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o)
+                red[threadIdx.x] += red[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            partial[int64_t(p) * nblk + blockIdx.x] = red[0];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) k_wplane_finish(const double* partial, const uint32_t* cgood,
+    const int64_t* first, const int64_t* last, int64_t chunk, int nblk, double* w_avg)
+{
+    __shared__ double red[256];
+    const int p = blockIdx.x;
+    const int64_t f = first[p], l = last[p];
+    double t = 0.0;
+    if (l > f) {
+        const int b0 = int(f / chunk), b1 = int((l - 1) / chunk);
+        for (int bb = b0 + int(threadIdx.x); bb <= b1; bb += blockDim.x)
+            t += partial[int64_t(p) * nblk + bb];
+    }
+    red[threadIdx.x] = t;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const uint64_t cnt = uint64_t(cgood[l]) - uint64_t(cgood[f]);
+        w_avg[p] = cnt > 0 ? red[0] / double(cnt) : 0.0;
+    }
 }
 
 template <typename R>
@@ -1187,16 +1277,6 @@ __global__ void k_cos_table(int arr, double* c)
 }
 
 // FP32 copies of the W-kernel tables for the single-precision gridders.
-__global__ void k_wk_to_f32(const double2* convd, const double* invd, int64_t nconv, int64_t ninv, float2* convf,
-    float* invf)
-{
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < nconv)
-        convf[t] = make_float2(float(convd[t].x), float(convd[t].y));
-    if (t < ninv)
-        invf[t] = float(invd[t]);
-}
-
 // Per-snapshot scalars of a batch, gathered for one read-back.
 struct BatchScalars {
     double total;
@@ -1223,6 +1303,44 @@ __global__ void k_collect_scalars(const double* total, const unsigned long long*
     b.max_support = m;
     b.pad = 0;
     *out = b;
+}
+
+// Expanded W-kernel tables for the gridder: one block per (plane, oversampled
+// offset pair); entry t = i*K + j holds the reference's cached kernel value
+// conv(|oy|, |ox|) * inv (aw_projection.cpp:415-448), formed in FP64 and
+// rounded once to R.  Plane p's tables start at off[p] = sum over q < p of
+// cs^2 * K_q^2.
+template <typename R>
+__global__ void k_wk_expand(const double2* convd, const double* invd, const int* support, int P, int cs, int os,
+    int lh, typename Cplx<R>::T* out, uint32_t* off)
+{
+    const int p = blockIdx.x;
+    const int pair = blockIdx.y;
+    const int cy = pair / cs, cx = pair % cs;
+    uint32_t base = 0;
+    for (int q = 0; q < p; q++) {
+        const uint32_t Kq = uint32_t(2 * support[q] + 1);
+        base += uint32_t(cs) * uint32_t(cs) * Kq * Kq;
+    }
+    if (pair == 0 && threadIdx.x == 0)
+        off[p] = base;
+    const int S = support[p];
+    const int K = 2 * S + 1;
+    const double inv = invd[(size_t(p) * cs + cy) * cs + cx];
+    const double2* conv = convd + size_t(p) * lh * lh;
+    typename Cplx<R>::T* dst = out + base + uint32_t(pair) * uint32_t(K * K);
+    for (int t = threadIdx.x; t < K * K; t += blockDim.x) {
+        const int i = t / K, j = t % K;
+        int oy = (i - S) * os + os / 2 - cy;
+        int ox = (j - S) * os + os / 2 - cx;
+        oy = oy < 0 ? -oy : oy;
+        ox = ox < 0 ? -ox : ox;
+        const double2 v = conv[size_t(oy) * lh + ox];
+        typename Cplx<R>::T o;
+        o.x = R(v.x * inv);
+        o.y = R(v.y * inv);
+        dst[t] = o;
+    }
 }
 
 } // namespace stpgpu

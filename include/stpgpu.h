@@ -267,6 +267,75 @@ typedef struct {
 STPGPU_API stpgpu_status stpgpu_image_batch(stpgpu_context* ctx, const stpgpu_snapshot* snapshots, int32_t n_snapshots,
     int precision, int out_dtype, int device_ptrs, stpgpu_imager_info* infos, stpgpu_batch_info* batch_info);
 
+/* ------------------------------------------------------------ serving
+ * A request loop over one GPU: imaging (+ optional source finding) requests
+ * are queued, admitted first-in first-out as soon as a slot is free and the
+ * request's estimated device working set fits in the HBM budget next to the
+ * requests in flight (continuous admission: a request that arrives while
+ * others run starts as soon as they release enough), and run concurrently,
+ * each slot on its own context and stream, so their kernels overlap on the
+ * device.  Slot contexts keep their buffers, cuFFT plans and W-kernel tables
+ * resident between requests.  A request's result does not depend on what
+ * else is in flight (up to floating-point summation order in the gridder).
+ * No counterpart in the reference (it is a library called once per snapshot). */
+typedef struct stpgpu_server stpgpu_server;
+
+typedef struct {
+    int32_t device;
+    int32_t slots;            /* requests in flight at most (>= 1) */
+    int64_t hbm_budget_bytes; /* admission budget for the working sets in flight */
+    int32_t precision;        /* stpgpu_precision of every request */
+    int32_t reserved;
+} stpgpu_server_pars;
+
+/* Host buffers, owned by the caller until the request completes. */
+typedef struct {
+    const void* vis;
+    int32_t vis_dtype;
+    int32_t out_dtype;        /* image dtype: STPGPU_F64 / STPGPU_F32 */
+    const double* weights;
+    const double* uvw;        /* n_vis x 3 column-major */
+    int64_t n_vis;
+    stpgpu_imager_pars pars;
+    stpgpu_wproj_pars wproj;
+    void* image;              /* image_size^2 out */
+    int32_t find_sources;     /* run the source finder on the image */
+    int32_t island_capacity;
+    stpgpu_sf_pars sf;
+    int32_t* label_map;       /* nullable, image_size^2 out */
+    stpgpu_island* islands;   /* island_capacity entries out */
+} stpgpu_request;
+
+typedef struct {
+    int32_t status;           /* stpgpu_status of the request */
+    int32_t n_islands;        /* may exceed island_capacity (then STPGPU_ERR_CAPACITY) */
+    int64_t est_bytes;        /* working-set estimate used for admission */
+    double submit_ms, admit_ms, done_ms; /* host clock, ms since the server started */
+    stpgpu_imager_info imager;
+    stpgpu_sf_info sf;
+    char error[160];
+} stpgpu_result;
+
+typedef struct {
+    int64_t submitted, completed, failed, in_flight, queued;
+    int64_t peak_in_flight;
+    int64_t peak_admitted_bytes; /* largest sum of working-set estimates in flight */
+    double p50_ms, p99_ms, mean_ms; /* submit -> done latency of completed requests */
+    double throughput_rps;          /* completed / (last done - first submit) */
+} stpgpu_server_stats;
+
+STPGPU_API stpgpu_status stpgpu_server_create(const stpgpu_server_pars* pars, stpgpu_server** server);
+/* Waits for every queued and running request, then releases the slots. */
+STPGPU_API stpgpu_status stpgpu_server_destroy(stpgpu_server* server);
+/* Queue a request; *ticket identifies it.  STPGPU_ERR_OOM when its working
+ * set alone exceeds the budget; STPGPU_ERR_INVALID_ARG for bad parameters. */
+STPGPU_API stpgpu_status stpgpu_server_submit(stpgpu_server* server, const stpgpu_request* request, int64_t* ticket);
+/* Wait up to timeout_s (< 0: forever) for a ticket; STPGPU_ERR_TIMEOUT if it
+ * is not done by then (the ticket stays valid).  On success *result holds
+ * the request's outcome and the ticket is released. */
+STPGPU_API stpgpu_status stpgpu_server_wait(stpgpu_server* server, int64_t ticket, double timeout_s, stpgpu_result* result);
+STPGPU_API stpgpu_status stpgpu_server_stats_get(stpgpu_server* server, stpgpu_server_stats* stats);
+
 /* Allocation-free connected-component labelling.  No counterpart in the
  * reference: it is the labelling step of stpgpu_source_find (the reference's
  * labeling_8con / labeling_4con, src/stp/common/ccl.h:107-504) for callers

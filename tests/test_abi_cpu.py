@@ -40,9 +40,10 @@ def test_struct_sizes_match_header():
     src = r"""
 #include <stdio.h>
 #include "stpgpu.h"
-int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(stpgpu_imager_pars), sizeof(stpgpu_wproj_pars),
+int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(stpgpu_imager_pars), sizeof(stpgpu_wproj_pars),
  sizeof(stpgpu_aproj_pars), sizeof(stpgpu_imager_info), sizeof(stpgpu_island), sizeof(stpgpu_sf_pars),
- sizeof(stpgpu_sf_info), sizeof(stpgpu_snapshot), sizeof(stpgpu_batch_info));return 0;}
+ sizeof(stpgpu_sf_info), sizeof(stpgpu_snapshot), sizeof(stpgpu_batch_info), sizeof(stpgpu_server_pars),
+ sizeof(stpgpu_request), sizeof(stpgpu_result), sizeof(stpgpu_server_stats));return 0;}
 """
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
@@ -53,7 +54,8 @@ int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(stpgpu_imager_
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
     sizes = [int(x) for x in out]
     py = [ctypes.sizeof(t) for t in (capi.ImagerPars, capi.WProjPars, capi.AProjPars, capi.ImagerInfo, capi.Island,
-                                     capi.SfPars, capi.SfInfo, capi.Snapshot, capi.BatchInfo)]
+                                     capi.SfPars, capi.SfInfo, capi.Snapshot, capi.BatchInfo,
+                                     capi.ServerPars, capi.Request, capi.Result, capi.ServerStats)]
     assert sizes == py
 
 
