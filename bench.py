@@ -298,6 +298,10 @@ def run_gpu(args):
         "gpu_launches": int(l32),
         "clocks": clocks,
     }
+    if ws == 1 and not args.headline_only:
+        line["batched"] = run_batched(ctx, min(args.steps, 10), args.warmup)
+        line["precision_study"] = run_precision(ctx)
+        line["serving"] = run_serving()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, snap)
     ctx.close()
@@ -308,6 +312,186 @@ def run_gpu(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_batched(ctx, steps, warmup):
+    """64 snapshots of uneven sizes (visibility counts log-uniform 50k-2M, images 1024^2-8192^2, W-projection)
+    through stpgpu_image_batch (FP32C, graph replay), and the same snapshots through single FP64 calls."""
+    import numpy as np
+    import torch
+
+    from fastimaging_b200 import capi
+    from fastimaging_b200.synthetic import config4
+
+    cases = config4()
+    nv = sum(s.vis.size for s, _ in cases)
+    snaps, outs64 = [], {}
+    for s, kw in cases:
+        d = dict(kw)
+        d["vis"] = torch.from_numpy(s.vis).cuda()
+        d["weights"] = torch.from_numpy(s.weights).cuda()
+        d["uvw"] = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+        d["image"] = torch.empty(kw["image_size"] ** 2, dtype=torch.float32, device="cuda")
+        snaps.append(d)
+    for _ in range(max(3, warmup)):
+        _, _, bi = ctx.image_batch(snaps, precision=capi.FP32C, out_dtype=capi.F32, device_ptrs=True)
+    ms = []
+    for _ in range(steps):
+        _, infos, bi = ctx.image_batch(snaps, precision=capi.FP32C, out_dtype=capi.F32, device_ptrs=True)
+        ms.append(bi.device_ms)
+    graph = bi.graph
+    st = torch.cuda.ExternalStream(ctx.stream)
+
+    def single_loop(prec):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for (s, kw), d in zip(cases, snaps):
+            k = {x: v for x, v in kw.items() if x not in ("image_size", "cell_size")}
+            if prec == capi.FP64:
+                out = outs64.setdefault(kw["image_size"], torch.empty(kw["image_size"] ** 2, dtype=torch.float64,
+                                                                      device="cuda"))
+                ctx.image_visibilities(d["vis"], d["weights"], d["uvw"], kw["image_size"], kw["cell_size"],
+                                       precision=capi.FP64, out_dtype=capi.F64, device_ptrs=True, image_out=out, **k)
+            else:
+                ctx.image_visibilities(d["vis"], d["weights"], d["uvw"], kw["image_size"], kw["cell_size"],
+                                       precision=capi.FP32C, out_dtype=capi.F32, device_ptrs=True,
+                                       image_out=d["image"], **k)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    single_loop(capi.FP64)  # tunes and allocates
+    t64 = min(single_loop(capi.FP64) for _ in range(2))
+    single_loop(capi.FP32C)
+    t32 = min(single_loop(capi.FP32C) for _ in range(2))
+    batch_ms = float(np.median(ms))
+    v = nv / (batch_ms / 1e3) / 1e6
+    v64 = nv / (t64 / 1e3) / 1e6
+    del snaps, outs64
+    torch.cuda.empty_cache()
+    return {"workload": "64 snapshots: visibilities log-uniform 50k-2M (total %d), images from {1024,2048,4096,8192}^2, "
+                        "w ~ U[-w_max, w_max], w_max ~ U[0, 2000], GaussianSinc/PSWF, W-projection 16 planes" % nv,
+            "value": round(v, 2), "unit": "Mvis/s", "ms_per_batch_p50": round(batch_ms, 3),
+            "ms_per_batch_p99": round(float(np.percentile(ms, 99)), 3), "graph_replay": bool(graph),
+            "fp64_single_calls": {"value": round(v64, 2), "ms": round(t64, 3)},
+            "fp32c_single_calls": {"value": round(nv / (t32 / 1e3) / 1e6, 2), "ms": round(t32, 3)},
+            "batched_fp32c_over_fp64_plain": round(v / v64, 3)}
+
+
+def run_serving(rates=(10.0, 50.0, 100.0, 200.0), seconds=3.0, slots=4):
+    """Poisson arrivals of imaging + source-finding requests (FP32C images, 5 sigma detection, 3 sigma
+    analysis, BINAPPROX, 8-connectivity) sampled from a pool of config-4-sized snapshots with 50 point and
+    5 extended sources; latency = submit -> done of each request (host clock)."""
+    import numpy as np
+
+    from fastimaging_b200 import capi
+    from fastimaging_b200.synthetic import config5_pool
+
+    import torch
+
+    # request inputs in page-locked host memory (as a receiving front end would hold them); the service
+    # returns the islands, not the images
+    pool = [((torch.from_numpy(s.vis).pin_memory(), torch.from_numpy(s.weights).pin_memory(),
+              torch.from_numpy(np.ascontiguousarray(s.uvw.T)).pin_memory()), kw, s.vis.size)
+            for s, kw in config5_pool()]
+    rng = np.random.default_rng(55)
+    out = []
+    for rate in rates:
+        srv = capi.Server(slots=slots, hbm_budget_bytes=64 << 30, precision=capi.FP32C)
+        try:
+            for (v, w, uvw), kw, _ in pool:  # warm every slot size class (plans, tables, buffers)
+                srv.wait(srv.submit(v, w, uvw, find_sources=True, want_image=False, **kw))
+            n_req = max(4, int(rate * seconds))
+            gaps = rng.exponential(1.0 / rate, size=n_req)
+            picks = rng.integers(0, len(pool), size=n_req)
+            t_start = time.perf_counter()
+            tickets, due = [], 0.0
+            for g, p in zip(gaps, picks):
+                due += g
+                delay = due - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                (v, w, uvw), kw, _ = pool[p]
+                tickets.append(srv.submit(v, w, uvw, find_sources=True, want_image=False, **kw))
+            lat, nvis, nisl = [], 0, 0
+            for t, p in zip(tickets, picks):
+                _, _, isl, res = srv.wait(t)
+                lat.append(res.done_ms - res.submit_ms)
+                nvis += pool[p][2]
+                nisl += len(isl)
+            wall = time.perf_counter() - t_start
+            st = srv.stats()
+        finally:
+            srv.close()
+        out.append({"offered_rps": rate, "requests": len(tickets), "completed_rps": round(len(tickets) / wall, 2),
+                    "p50_ms": round(float(np.percentile(lat, 50)), 2),
+                    "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(np.mean(lat)), 2),
+                    "Mvis_per_s": round(nvis / wall / 1e6, 1), "islands_per_request": round(nisl / len(tickets), 1),
+                    "peak_in_flight": int(st.peak_in_flight), "slots": slots})
+    return out
+
+
+def run_precision(ctx):
+    """8192^2 image, 4M complex64 visibilities Gaussian-concentrated in uv, PSWF S=4 os=16: FP32 naive and
+    FP32 compensated images against the FP64 image of the same library (itself pinned to the oracle)."""
+    import numpy as np
+    import torch
+
+    from fastimaging_b200 import capi
+    from fastimaging_b200.synthetic import CONFIG3_IMAGER, config3
+
+    s = config3()
+    N = s.image_size
+    dv = torch.from_numpy(s.vis).cuda()
+    dw = torch.from_numpy(s.weights).cuda()
+    duvw = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+    o64 = torch.empty(N * N, dtype=torch.float64, device="cuda")
+    o32 = torch.empty(N * N, dtype=torch.float32, device="cuda")
+    out = {"workload": "8192^2, 4M complex64 visibilities, uv Gaussian (sigma 0.25 of the radius), PSWF S=4 os=16, "
+                       "analytic gcf"}
+    ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=capi.FP64, out_dtype=capi.F64, device_ptrs=True,
+                           image_out=o64, **CONFIG3_IMAGER)
+    torch.cuda.synchronize()
+    ref = o64.clone()
+    peak = float(ref.abs().max())
+    norm = float(torch.linalg.vector_norm(ref))
+    # inner half of the field (|x|, |y| < N/4 from the phase centre; the image is unshifted, so these are the
+    # first and last N/4 rows and columns), away from the edges where the analytic PSWF correction is smallest
+    q = N // 4
+    idx = torch.cat([torch.arange(0, q), torch.arange(N - q, N)]).cuda()
+    for name, prec in (("fp32_naive", capi.FP32), ("fp32_compensated", capi.FP32C)):
+        ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=prec, out_dtype=capi.F32, device_ptrs=True,
+                               image_out=o32, **CONFIG3_IMAGER)
+        torch.cuda.synchronize()
+        d = o32.double() - ref
+        d2 = d.view(N, N).index_select(0, idx).index_select(1, idx)
+        out[name] = {"max_abs_over_peak": float(d.abs().max()) / peak,
+                     "rms_rel": float(torch.linalg.vector_norm(d)) / norm,
+                     "inner_half_field_max_abs_over_peak": float(d2.abs().max()) / peak}
+    for prec, name in ((capi.FP64, "fp64"), (capi.FP32C, "fp32c")):
+        t = []
+        for _ in range(3):
+            o = o64 if prec == capi.FP64 else o32
+            _, _, info = ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=prec,
+                                                out_dtype=capi.F64 if prec == capi.FP64 else capi.F32,
+                                                device_ptrs=True, image_out=o, **CONFIG3_IMAGER)
+        st = torch.cuda.ExternalStream(ctx.stream)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(3):
+            o = o64 if prec == capi.FP64 else o32
+            ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=prec,
+                                   out_dtype=capi.F64 if prec == capi.FP64 else capi.F32, device_ptrs=True,
+                                   image_out=o, **CONFIG3_IMAGER)
+        e1.record(st)
+        e1.synchronize()
+        t.append(e0.elapsed_time(e1) / 3)
+        out[name + "_Mvis_per_s"] = round(s.vis.size / (t[0] / 1e3) / 1e6, 1)
+    del dv, dw, duvw, o64, o32, ref
+    torch.cuda.empty_cache()
+    return out
 
 
 def _cpu_one(snap, threads, fast=True):
@@ -372,6 +556,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the batched, precision-study and serving sections")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3

@@ -407,19 +407,27 @@ class Server:
         self._keep = {}
 
     def submit(self, vis, weights, uvw, find_sources=False, out_dtype=F32, sf=None, want_labels=False,
-               island_capacity=4096, **imager_kw):
+               island_capacity=4096, want_image=True, **imager_kw):
         """imager_kw: image_size, cell_size and the image_visibilities keywords.
         sf: dict of source_find keywords (detection_n_sigma, analysis_n_sigma, ...).
-        Returns a ticket."""
-        vis = np.ascontiguousarray(vis)
-        if vis.dtype not in (np.complex128, np.complex64):
-            vis = vis.astype(np.complex128)
-        n = vis.size
-        w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
-        uvwF = np.asfortranarray(np.asarray(uvw, dtype=np.float64).reshape(n, 3))
+        Inputs: numpy arrays (uvw (n, 3)), or page-locked torch CPU tensors
+        (vis complex (n,), weights (n,), uvw (3, n) contiguous).  Returns a ticket."""
+        if hasattr(vis, "data_ptr"):
+            n = int(weights.numel())
+            vdt = C64 if str(vis.dtype).endswith("complex64") else C128
+            w, uvwF = weights, uvw
+        else:
+            vis = np.ascontiguousarray(vis)
+            if vis.dtype not in (np.complex128, np.complex64):
+                vis = vis.astype(np.complex128)
+            vdt = C64 if vis.dtype == np.complex64 else C128
+            n = vis.size
+            w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
+            uvwF = np.asfortranarray(np.asarray(uvw, dtype=np.float64).reshape(n, 3))
         ip, wp = imager_pars(**imager_kw)
         size = int(imager_kw["image_size"])
-        img = np.empty((size, size), dtype=np.float32 if out_dtype == F32 else np.float64, order="F")
+        img = (np.empty((size, size), dtype=np.float32 if out_dtype == F32 else np.float64, order="F")
+               if (want_image or not find_sources) else None)
         sfd = dict(detection_n_sigma=5.0, analysis_n_sigma=3.0, rms_est=0.0, find_negative_sources=True,
                    sigma_clip_iters=5, median_method=BINAPPROX, gaussian_fitting=False, ccl_4connectivity=False,
                    generate_labelmap=True, source_min_area=5, ccl_slice_cols=0)
@@ -430,7 +438,7 @@ class Server:
                     int(bool(sfd["generate_labelmap"])), int(sfd["source_min_area"]), int(sfd["ccl_slice_cols"]))
         labels = np.empty((size, size), dtype=np.int32, order="F") if (find_sources and want_labels) else None
         isl = (Island * max(1, int(island_capacity)))()
-        req = Request(_ptr(vis), C64 if vis.dtype == np.complex64 else C128, int(out_dtype), _ptr(w), _ptr(uvwF), n,
+        req = Request(_ptr(vis), vdt, int(out_dtype), _ptr(w), _ptr(uvwF), n,
                       ip, wp, _ptr(img), int(bool(find_sources)), int(island_capacity), sp, _ptr(labels),
                       ctypes.cast(isl, ctypes.c_void_p))
         t = ctypes.c_int64()
@@ -450,7 +458,7 @@ class Server:
         if st != 0:
             raise StpGpuError(st, res.error.decode(errors="replace"))
         islands = [isl[i] for i in range(min(res.n_islands, len(isl)))] if req.find_sources else []
-        if res.imager.image_size == 0:
+        if res.imager.image_size == 0 and img is not None:
             img = np.zeros((0, 0))
         return img, labels, islands, res
 

@@ -1994,7 +1994,8 @@ void serve_request(stpgpu_context* c, const stpgpu_request& r, stpgpu_result& re
     run_imager<R, COMP>(c, s, image_size, r.pars.gridding_correction, dv, c64, dw, duvw, n, dimg, nullptr, f32,
         &res.imager);
     if (res.imager.image_size > 0) {
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(r.image, dimg, ob * npix, cudaMemcpyDeviceToHost, c->stream));
+        if (r.image)
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(r.image, dimg, ob * npix, cudaMemcpyDeviceToHost, c->stream));
         if (r.find_sources) {
             std::vector<stpgpu_island> isl;
             if (f32)
@@ -2160,7 +2161,7 @@ stpgpu_status stpgpu_server_submit(stpgpu_server* sv, const stpgpu_request* r, i
             return STPGPU_ERR_UNSUPPORTED;
         if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
             return STPGPU_ERR_INVALID_ARG;
-        if (r->n_vis < 0 || (r->n_vis > 0 && (!r->vis || !r->weights || !r->uvw)) || !r->image)
+        if (r->n_vis < 0 || (r->n_vis > 0 && (!r->vis || !r->weights || !r->uvw)) || (!r->image && !r->find_sources))
             return STPGPU_ERR_INVALID_ARG;
         if ((r->vis_dtype != STPGPU_C128 && r->vis_dtype != STPGPU_C64)
             || (r->out_dtype != STPGPU_F64 && r->out_dtype != STPGPU_F32))

@@ -155,3 +155,24 @@ def config4(seed=4, n_snapshots=64, n_src=5):
                   max_wpconv_support=16, undersampling_opt=1, kernel_trunc_perc=1.0)
         out.append((s, kw))
     return out
+
+
+def config5_pool(seed=5, n_templates=12):
+    """Request templates of the serving workload: snapshot sizes drawn as in config4 (visibility counts
+    log-uniform 50k-2M, image sizes from {1024, 2048, 4096, 8192}, W-projection 16 planes), each sky with
+    50 point sources plus 5 extended elliptical Gaussians (sigma 2-6 px).  Requests sample this pool.
+    Returns [(Snapshot, imager keywords)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_templates):
+        n_vis = int(round(math.exp(rng.uniform(math.log(5e4), math.log(2e6)))))
+        size = int(rng.choice([1024, 2048, 4096, 8192]))
+        w_max = float(rng.uniform(0.0, 2000.0))
+        kf = 4 if rng.random() < 0.5 else 5
+        s = make_snapshot(seed * 1000 + i, n_vis, size, 1.0, n_src=50, flux=(0.5, 10.0), noise_sigma=0.05,
+                          w_range=(-w_max, w_max), n_extended=5)
+        kw = dict(image_size=size, cell_size=1.0, kernel_func=kf, kernel_support=3, kernel_exact=False,
+                  oversampling=8, gridding_correction=True, analytic_gcf=False, num_wplanes=16,
+                  max_wpconv_support=16, undersampling_opt=1, kernel_trunc_perc=1.0)
+        out.append((s, kw))
+    return out

@@ -288,7 +288,8 @@ typedef struct {
     int32_t reserved;
 } stpgpu_server_pars;
 
-/* Host buffers, owned by the caller until the request completes. */
+/* Host buffers, owned by the caller until the request completes (page-locked
+ * buffers make the copies asynchronous and several times faster). */
 typedef struct {
     const void* vis;
     int32_t vis_dtype;
@@ -298,7 +299,7 @@ typedef struct {
     int64_t n_vis;
     stpgpu_imager_pars pars;
     stpgpu_wproj_pars wproj;
-    void* image;              /* image_size^2 out */
+    void* image;              /* image_size^2 out; nullable when find_sources (islands only) */
     int32_t find_sources;     /* run the source finder on the image */
     int32_t island_capacity;
     stpgpu_sf_pars sf;
