@@ -222,6 +222,7 @@ struct ImagerSetup {
     double cell_size = 0.0;
     int nplanes = 0, max_support = 0, undersampling = 1, wmedian = 0;
     double trunc_perc = 0.0;
+    int full_wsort = 0; // |w| order from the 64-bit sort (fallback of the 32-bit sort + run fix-up)
 };
 
 struct GridOut {
@@ -335,6 +336,8 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     pp.wsum_part = wpart;
     pp.ngood_part = npart;
     pp.absw_key = wproj ? c->buf<double>("absw", nn) : nullptr;
+    pp.absw_key32 = (wproj && !s.full_wsort) ? c->buf<uint32_t>("absw32", nn) : nullptr;
+    pp.iota = wproj ? c->buf<uint32_t>("perm_in", nn) : nullptr;
     pp.w_out = nullptr;
     if (n > 0) {
         k_prepass<R><<<nb_pre, GRID_THREADS, 0, st>>>(pp, items);
@@ -377,24 +380,37 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     }
     if (wproj && n > 0) {
         const int P = s.nplanes;
-        // |w| order: stable radix sort of the IEEE bits of |w| (non-negative
-        // doubles order as their bit patterns), gridder.h:311-367.
-        const unsigned long long* keys_in = reinterpret_cast<const unsigned long long*>(pp.absw_key);
-        unsigned long long* keys_out = c->buf<unsigned long long>("absw_sorted", nn);
-        uint32_t* perm_in = c->buf<uint32_t>("perm_in", nn);
+        // |w| order (gridder.h:311-367): stable radix sort of float(|w|)
+        // rounded down (32-bit keys, half the passes of the 64-bit sort), then
+        // runs of equal 32-bit keys re-sorted by the full |w| bits; with
+        // full_wsort the IEEE bits of |w| themselves are sorted (64-bit keys;
+        // non-negative doubles order as their bit patterns).
+        const unsigned long long* keys64 = reinterpret_cast<const unsigned long long*>(pp.absw_key);
+        uint32_t* perm_in = pp.iota;
         uint32_t* perm = c->buf<uint32_t>("perm", nn);
-        k_iota_u32<<<grid1d(n, 256), 256, 0, st>>>(perm_in, n);
-        STPGPU_CHECK_LAUNCH();
         size_t tb = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, perm_in, perm, int(n), 0, 64, st);
-        void* tmp = c->buf<unsigned char>("cubtmp", tb);
-        if (cub::DeviceRadixSort::SortPairs(tmp, tb, keys_in, keys_out, perm_in, perm, int(n), 0, 64, st)
-            != cudaSuccess)
-            fail(STPGPU_ERR_CUDA, "radix sort failed");
+        if (s.full_wsort) {
+            unsigned long long* k64out = c->buf<unsigned long long>("absw64_sorted", nn);
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, keys64, k64out, perm_in, perm, int(n), 0, 64, st);
+            void* tmp = c->buf<unsigned char>("cubtmp", tb);
+            if (cub::DeviceRadixSort::SortPairs(tmp, tb, keys64, k64out, perm_in, perm, int(n), 0, 64, st)
+                != cudaSuccess)
+                fail(STPGPU_ERR_CUDA, "radix sort failed");
+        } else {
+            uint32_t* k32out = c->buf<uint32_t>("absw32_sorted", nn);
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, pp.absw_key32, k32out, perm_in, perm, int(n), 0, 32, st);
+            void* tmp = c->buf<unsigned char>("cubtmp", tb);
+            if (cub::DeviceRadixSort::SortPairs(tmp, tb, pp.absw_key32, k32out, perm_in, perm, int(n), 0, 32, st)
+                != cudaSuccess)
+                fail(STPGPU_ERR_CUDA, "radix sort failed");
+            k_fix_runs<<<grid1d(n, 256), 256, 0, st>>>(k32out, perm, keys64, n, g.d_err);
+            STPGPU_CHECK_LAUNCH();
+        }
         uint8_t* good_sorted = c->buf<uint8_t>("good_sorted", nn);
         uint32_t* gflag = c->buf<uint32_t>("gflag", nn + 1);
         uint32_t* cgood = c->buf<uint32_t>("cgood", nn + 1);
-        k_gather_good<R><<<grid1d(n, 256), 256, 0, st>>>(perm, items, n, good_sorted, gflag);
+        double* absw_sorted = c->buf<double>("absw_sorted", nn);
+        k_gather_good<R><<<grid1d(n, 256), 256, 0, st>>>(perm, items, pp.absw_key, n, good_sorted, gflag, absw_sorted);
         STPGPU_CHECK_LAUNCH();
         STPGPU_CUDA_TRY(cudaMemsetAsync(gflag + n, 0, sizeof(uint32_t), st));
         size_t tb2 = 0;
@@ -405,7 +421,6 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         int64_t* first = c->buf<int64_t>("pfirst", P);
         int64_t* last = c->buf<int64_t>("plast", P);
         double* w_avg = c->buf<double>("wavg", P);
-        const double* absw_sorted = reinterpret_cast<const double*>(keys_out);
         k_wplanes<<<1, 1, 0, st>>>(cgood, absw_sorted, n, P, s.wmedian, first, last);
         STPGPU_CHECK_LAUNCH();
         if (s.wmedian) {
@@ -647,7 +662,9 @@ ScalarsBack read_back(stpgpu_context* c, const GridOut& g)
     ScalarsBack r { h->total, h->ngood, h->nitems, h->err, 0 };
     for (int v : sup)
         r.max_support = std::max(r.max_support, v);
-    if (r.err)
+    // bit 4: the 32-bit |w| sort met a long run of distinct |w| (the caller
+    // repeats the gridding with the 64-bit sort); other bits are errors
+    if (r.err & ~4u)
         fail(STPGPU_ERR_DEVICE, "gridder reported internal error flags " + std::to_string(r.err));
     return r;
 }
@@ -768,7 +785,17 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     }
     finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
     const int N = s.N;
-    const ScalarsBack sb = read_back(c, g);
+    ScalarsBack sb = read_back(c, g);
+    if ((sb.err & 4u) && !s.full_wsort) {
+        // rare data (many distinct |w| within one single-precision step): redo with the 64-bit |w| sort
+        ImagerSetup s64 = s;
+        s64.full_wsort = 1;
+        auto t = c->tune.find(cls);
+        g = run_gridder<R, COMP>(c, s64, d_vis, vis_c64, d_wts, d_uvw, 0, n,
+            t != c->tune.end() ? (t->second & 0xff) : TILE_C_DEFAULT);
+        finish_imager<R>(c, s64, image_size, correction, g, d_image, d_beam, out_f32);
+        sb = read_back(c, g);
+    }
     if (info) {
         info->sample_grid_total = sb.total;
         info->n_good_vis = int64_t(sb.ngood);
@@ -1201,10 +1228,25 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         }
     }
     STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
+    bool redo = false;
+    for (int i = 0; i < nb; i++)
+        if (scal[i].err & 4u) { // long run of distinct |w| in the 32-bit sort: redo with the 64-bit sort
+            B[i].s.full_wsort = 1;
+            redo = true;
+        }
+    if (redo) {
+        c->drop_graph();
+        c->batch_calls = 0;
+        STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
+        glaunch = batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, nullptr);
+        STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, main));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
+        graph = 0;
+    }
     float ms = 0.f;
     STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     for (int i = 0; i < nb; i++) {
-        if (scal[i].err)
+        if (scal[i].err & ~4u)
             fail(STPGPU_ERR_DEVICE, "snapshot " + std::to_string(i) + ": gridder reported internal error flags "
                     + std::to_string(scal[i].err));
         if (infos) {
@@ -1876,6 +1918,11 @@ stpgpu_status stpgpu_convolve_to_grid(stpgpu_context* c, int kernel_function, do
         const double* dw = to_device<double>(c, "in_w", weights, size_t(n_vis));
         GridOut g = run_gridder<double, 0>(c, s, dvis, 0, dw, duv, 1, n_vis);
         ScalarsBack sb = read_back(c, g);
+        if (sb.err & 4u) { // redo with the 64-bit |w| sort
+            s.full_wsort = 1;
+            g = run_gridder<double, 0>(c, s, dvis, 0, dw, duv, 1, n_vis);
+            sb = read_back(c, g);
+        }
         const size_t cells = size_t(g.image_rows) * size_t(image_size);
         STPGPU_CUDA_TRY(cudaMemcpyAsync(vis_grid, g.grid, sizeof(double2) * cells, cudaMemcpyDeviceToHost, c->stream));
         if (s.beam)

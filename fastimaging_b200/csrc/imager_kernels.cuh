@@ -53,6 +53,8 @@ struct PrepassParams {
     unsigned long long* ngood_part;
     double* absw_key; // n |w| (W-proj only), may be null
     double* w_out;    // n half-plane-converted w (W-proj), may be null
+    uint32_t* absw_key32; // n float(|w|) rounded down, as bits (W-proj), may be null
+    uint32_t* iota;       // n identity permutation (W-proj), may be null
 };
 
 template <typename R>
@@ -130,6 +132,10 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
         }
         if (p.absw_key)
             p.absw_key[i] = fabs(w);
+        if (p.absw_key32) // monotone: |a| <= |b| implies key32(a) <= key32(b)
+            p.absw_key32[i] = __float_as_uint(__double2float_rd(fabs(w)));
+        if (p.iota)
+            p.iota[i] = uint32_t(i);
         if (p.w_out)
             p.w_out[i] = w;
         Item<R> it;
@@ -1098,15 +1104,70 @@ __global__ void __launch_bounds__(256) k_wplane_finish(const double* partial, co
 }
 
 template <typename R>
-__global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, int64_t n, uint8_t* good_sorted,
-    uint32_t* gflag)
+__global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, const double* absw, int64_t n,
+    uint8_t* good_sorted, uint32_t* gflag, double* absw_sorted)
 {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= n)
         return;
-    uint8_t g = items[perm[k]].good != 0;
+    const uint32_t i = perm[k];
+    uint8_t g = items[i].good != 0;
     good_sorted[k] = g;
     gflag[k] = g;
+    if (absw_sorted)
+        absw_sorted[k] = absw[i];
+}
+
+// The |w| order from a stable sort on 32-bit keys (float(|w|) rounded down)
+// is exact except inside runs of equal keys, whose members are in index
+// order.  Each run is re-sorted by the full 64-bit key (the bits of |w|),
+// keeping index order among equal |w|: the result is the stable order of the
+// 64-bit sort.  Runs longer than kFixRun whose |w| are not all equal set
+// bit 4 of *err (the caller then repeats the step with the 64-bit sort).
+constexpr int kFixRun = 32;
+__global__ void k_fix_runs(const uint32_t* __restrict__ key32, uint32_t* perm, const unsigned long long* __restrict__ key64,
+    int64_t n, unsigned int* err)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k + 1 >= n)
+        return;
+    const uint32_t kk = key32[k];
+    if ((k > 0 && key32[k - 1] == kk) || key32[k + 1] != kk)
+        return; // not the start of a run of length >= 2
+    int64_t e = k + 2;
+    while (e < n && e - k <= kFixRun && key32[e] == kk)
+        e++;
+    const int len = int(e - k);
+    if (len > kFixRun) {
+        const unsigned long long first = key64[perm[k]];
+        for (int64_t j = k + 1; j < n && key32[j] == kk; j++)
+            if (key64[perm[j]] != first) {
+                atomicOr(err, 4u);
+                return;
+            }
+        return; // all |w| equal: index order is already the stable order
+    }
+    unsigned long long kv[kFixRun];
+    uint32_t pv[kFixRun];
+    for (int a = 0; a < len; a++) {
+        pv[a] = perm[k + a];
+        kv[a] = key64[pv[a]];
+    }
+    // insertion sort by (key64, index): stable, so equal keys keep index order
+    for (int a = 1; a < len; a++) {
+        const unsigned long long x = kv[a];
+        const uint32_t y = pv[a];
+        int b = a - 1;
+        while (b >= 0 && kv[b] > x) {
+            kv[b + 1] = kv[b];
+            pv[b + 1] = pv[b];
+            b--;
+        }
+        kv[b + 1] = x;
+        pv[b + 1] = y;
+    }
+    for (int a = 0; a < len; a++)
+        perm[k + a] = pv[a];
 }
 
 // W-kernel generation for one plane per CTA (FP64), the non-Hankel path of

@@ -119,6 +119,37 @@ def test_imager_wproj_untruncated(ctx):
     assert peak_rel(img, ri) < TOL64
 
 
+@pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal"])
+def test_imager_wproj_near_tied_w(ctx, pattern):
+    """|w| values that are equal in single precision but distinct in double
+    (or exactly equal): the W-plane boundaries must follow the exact stable
+    double order of the reference's sort.  Short runs are re-sorted after the
+    32-bit key sort; a long run of distinct values takes the 64-bit sort;
+    exactly equal values keep index order."""
+    s = _imager_case(35, 256, 4000, w_range=(-600.0, 600.0))
+    uvw = np.array(s.uvw, order="F")
+    w = uvw[:, 2]
+    rng = np.random.default_rng(7)
+    nplanes = 6
+    if pattern == "short_runs":
+        for k in range(0, w.size - 1, 2):  # |w| of the pair one double step apart
+            w[k + 1] = np.copysign(np.nextafter(abs(w[k]), np.inf), w[k + 1])
+    else:
+        # a cluster placed across the first plane boundary
+        aw = np.sort(np.abs(w))
+        base = aw[w.size // nplanes]
+        idx = rng.choice(w.size, size=200 if pattern == "long_run" else 300, replace=False)
+        for j, k in enumerate(idx):
+            mag = base * (1.0 + j * 1e-15) if pattern == "long_run" else base
+            w[k] = mag if rng.random() < 0.5 else -mag
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              num_wplanes=nplanes, max_wpconv_support=8, undersampling_opt=1, kernel_trunc_perc=1.0)
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, uvw, 256, s.cell_size, **kw)
+    ri, _, g = orc.image_visibilities(s.vis, s.weights, uvw, 256, s.cell_size, return_grid=True, **kw)
+    assert info.max_plane_support == max(g.plane_supports)
+    assert peak_rel(img, ri) < TOL64
+
+
 @pytest.mark.parametrize("precision", [capi.FP32, capi.FP32C])
 def test_imager_fp32_vs_fp64_oracle(ctx, precision):
     s = _imager_case(41, 512, 20000, w_range=(-500.0, 500.0))
