@@ -722,7 +722,21 @@ void finish_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int 
     const double* ginv = correction ? c->buf<double>("gcfinv", s.N) : nullptr;
     (void)gcf;
     const dim3 ngrid(std::min<unsigned>(grid1d(image_size, 256), 4), image_size);
+    // 16-byte path: every 4-row group inside one crop segment and aligned
+    const bool vec4 = (image_size % 8) == 0 && (N % 4) == 0
+        && (reinterpret_cast<uintptr_t>(d_image) % 16) == 0 && (!d_beam || (reinterpret_cast<uintptr_t>(d_beam) % 16) == 0);
+    const dim3 ngrid4(grid1d(image_size / 4, 256), image_size);
     auto normalise = [&](void* out) {
+        if (vec4) {
+            if (out_f32)
+                k_normalise4<R, float><<<ngrid4, 256, 0, st>>>(img, N, image_size, g.d_total, ginv, correction,
+                    reinterpret_cast<float*>(out));
+            else
+                k_normalise4<R, double><<<ngrid4, 256, 0, st>>>(img, N, image_size, g.d_total, ginv, correction,
+                    reinterpret_cast<double*>(out));
+            STPGPU_CHECK_LAUNCH();
+            return;
+        }
         if (out_f32)
             k_normalise<R, float><<<ngrid, 256, 0, st>>>(img, N, image_size, g.d_total, ginv, correction,
                 reinterpret_cast<float*>(out));

@@ -253,67 +253,92 @@ __device__ __forceinline__ void item_centre(const Item<R>& it, int mir, int N, i
 }
 
 // Tiles overlapped by one item: calls f(tile) once per distinct tile.  The
-// tile rows / columns of the mapped taps form at most a few runs; distinct
-// values are collected in small register bitmasks (tile ids relative to the
-// first one seen, plus a wrap-around run).
+// footprint's raw rows [rb, rb+K) and columns [cb, cb+K) are split into the
+// segments that map_row / map_col send to distinct grid ranges (in place,
+// wrapped from >= N, and for the exact gridder wrapped from < 0; rows at or
+// beyond the half plane dropped); each segment becomes a range of tile
+// indices, overlapping ranges are merged, and the tiles of the row ranges x
+// column ranges are visited once each.
+struct TileRanges {
+    int lo[3], hi[3];
+    int n;
+    __device__ __forceinline__ void add(int l, int h)
+    {
+        if (l > h)
+            return;
+        for (int k = 0; k < n; k++) {
+            if (l <= hi[k] + 1 && h >= lo[k] - 1) { // overlapping or adjacent: merge
+                lo[k] = min(lo[k], l);
+                hi[k] = max(hi[k], h);
+                return;
+            }
+        }
+        lo[n] = l;
+        hi[n] = h;
+        n++;
+    }
+    // merge ranges that a later add made overlap
+    __device__ __forceinline__ void merge()
+    {
+        for (int a = 0; a < n; a++)
+            for (int b = a + 1; b < n; b++)
+                if (lo[b] <= hi[a] + 1 && hi[b] >= lo[a] - 1) {
+                    lo[a] = min(lo[a], lo[b]);
+                    hi[a] = max(hi[a], hi[b]);
+                    lo[b] = lo[n - 1];
+                    hi[b] = hi[n - 1];
+                    n--;
+                    b = a; // restart the scan of a
+                }
+    }
+};
+
 template <typename R, typename F>
 __device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, int S, const BinParams& p, F f)
 {
     const int K = 2 * S + 1;
     int cx, cy;
     item_centre(it, mir, p.N, cx, cy);
-    // distinct tile rows / cols: at most 2 runs each (before and after a wrap)
-    int tr0 = -1, tr1 = -1, tr0e = -1, tr1e = -1;
-    for (int i = 0; i < K; i++) {
-        const int r = map_row(cy - S + i, p.N, p.image_rows, p.exact != 0);
-        if (r < 0)
-            continue;
-        const int t = r / TILE_R;
-        if (tr0 < 0) {
-            tr0 = tr0e = t;
-        } else if (t == tr0e + 1 || t == tr0e) {
-            tr0e = t;
-        } else if (tr1 < 0) {
-            tr1 = tr1e = t;
-        } else {
-            tr1e = t;
-        }
+    const int N = p.N, rows_max = p.image_rows - 1;
+    const int a = cy - S, b = cy - S + K - 1; // raw rows
+    TileRanges tr;
+    tr.n = 0;
+    {
+        const int l = max(a, 0), h = min(min(b, N - 1), rows_max);
+        if (l <= h)
+            tr.add(l / TILE_R, h / TILE_R);
     }
-    int tc0 = -1, tc1 = -1, tc0e = -1, tc1e = -1;
-    for (int j = 0; j < K; j++) {
-        const int c = map_col(cx - S + j, p.N);
-        const int t = c / p.tile_c;
-        if (tc0 < 0) {
-            tc0 = tc0e = t;
-        } else if (t == tc0e + 1 || t == tc0e) {
-            tc0e = t;
-        } else if (tc1 < 0) {
-            tc1 = tc1e = t;
-        } else {
-            tc1e = t;
-        }
+    if (b >= N) {
+        const int l = max(a, N) - N, h = min(b - N, rows_max);
+        if (l <= h)
+            tr.add(l / TILE_R, h / TILE_R);
     }
-    if (tr0 < 0)
+    if (p.exact && a < 0) {
+        const int l = a + N, h = min(min(b, -1) + N, rows_max);
+        if (l <= h)
+            tr.add(l / TILE_R, h / TILE_R);
+    }
+    if (tr.n == 0)
         return;
-    for (int rr = 0; rr < 2; rr++) {
-        const int rlo = rr ? tr1 : tr0, rhi = rr ? tr1e : tr0e;
-        if (rlo < 0)
-            continue;
-        for (int tr = rlo; tr <= rhi; tr++) {
-            if (rr && tr >= tr0 && tr <= tr0e)
-                continue;
-            for (int cc = 0; cc < 2; cc++) {
-                const int clo = cc ? tc1 : tc0, chi = cc ? tc1e : tc0e;
-                if (clo < 0)
-                    continue;
-                for (int tc = clo; tc <= chi; tc++) {
-                    if (cc && tc >= tc0 && tc <= tc0e)
-                        continue;
-                    f(uint32_t(tc) * uint32_t(p.tiles_r) + uint32_t(tr));
-                }
-            }
-        }
+    const int c = cx - S, d = cx - S + K - 1; // raw columns
+    TileRanges tc;
+    tc.n = 0;
+    {
+        const int l = max(c, 0), h = min(d, N - 1);
+        if (l <= h)
+            tc.add(l / p.tile_c, h / p.tile_c);
     }
+    if (c < 0)
+        tc.add((c + N) / p.tile_c, (min(d, -1) + N) / p.tile_c);
+    if (d >= N)
+        tc.add((max(c, N) - N) / p.tile_c, (d - N) / p.tile_c);
+    tr.merge();
+    tc.merge();
+    for (int r = 0; r < tr.n; r++)
+        for (int t_r = tr.lo[r]; t_r <= tr.hi[r]; t_r++)
+            for (int q = 0; q < tc.n; q++)
+                for (int t_c = tc.lo[q]; t_c <= tc.hi[q]; t_c++)
+                    f(uint32_t(t_c) * uint32_t(p.tiles_r) + uint32_t(t_r));
 }
 
 // W-plane of sorted position k: the last plane whose first position <= k.
@@ -923,6 +948,57 @@ __global__ void __launch_bounds__(256) k_normalise(const RI* __restrict__ img, i
         const int ii = i < hs ? hp + i : hp - hs + (i - hs);
         const double v = double(src[oi]) * fj;
         dst[i] = RO(corr ? v * ginv[ii] : v);
+    }
+}
+
+// Same pass, four rows per thread with 16-byte loads and stores, for
+// image_size % 8 == 0 and padded % 4 == 0 (each group of four rows then lies
+// inside one crop segment and is 16-byte aligned).  blockIdx.y = column.
+template <typename RI, typename RO>
+__global__ void __launch_bounds__(256) k_normalise4(const RI* __restrict__ img, int padded, int image_size,
+    const double* total, const double* __restrict__ ginv, int corr, RO* __restrict__ out)
+{
+    const int j = blockIdx.y;
+    const double tot = total[0];
+    const double nf = tot > 0.0 ? 1.0 / tot : 0.0;
+    const int hp = padded / 2, hs = image_size / 2;
+    const int oj = j < hs ? j : padded + j - image_size;
+    const int jj = j < hs ? j + hp : hp + j - image_size;
+    const double fj = corr ? nf * ginv[jj] : nf;
+    const RI* src = img + size_t(oj) * padded;
+    RO* dst = out + size_t(j) * image_size;
+    const int groups = image_size / 4;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x) {
+        const int i = g * 4;
+        const int oi = i < hs ? i : padded - hs + (i - hs);
+        const int ii = i < hs ? hp + i : hp - hs + (i - hs);
+        double v[4];
+        if constexpr (sizeof(RI) == 4) {
+            const float4 x = *reinterpret_cast<const float4*>(src + oi);
+            v[0] = x.x;
+            v[1] = x.y;
+            v[2] = x.z;
+            v[3] = x.w;
+        } else {
+            const double2 a = *reinterpret_cast<const double2*>(src + oi);
+            const double2 b = *reinterpret_cast<const double2*>(src + oi + 2);
+            v[0] = a.x;
+            v[1] = a.y;
+            v[2] = b.x;
+            v[3] = b.y;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            v[k] *= fj;
+            if (corr)
+                v[k] *= ginv[ii + k];
+        }
+        if constexpr (sizeof(RO) == 4) {
+            *reinterpret_cast<float4*>(dst + i) = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
+        } else {
+            *reinterpret_cast<double2*>(dst + i) = make_double2(v[0], v[1]);
+            *reinterpret_cast<double2*>(dst + i + 2) = make_double2(v[2], v[3]);
+        }
     }
 }
 
