@@ -596,8 +596,6 @@ __device__ __forceinline__ void tap_value(const GridParams<R>& p, const R* tab, 
         kr = cv.x;
         ki = t.conj_k ? -cv.y : cv.y;
     }
-    kr = kr * t.wt;
-    ki = ki * t.wt;
 }
 
 template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
@@ -715,7 +713,46 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
             int kmax = mine ? t.K : 0;
             for (int o = 16; o > 0; o >>= 1)
                 kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-            if (KMODE != KM_EXACT) {
+            const bool anywrap = __any_sync(0xffffffffu, mine && cwrap);
+            if (KMODE != KM_EXACT && !anywrap && !BEAM) {
+                // common case: no footprint of the round crosses the grid's
+                // column edge, so each lane's in-tile columns are the window
+                // [jl, jh) and tap (i, j) sits at a fixed slot stride; the
+                // weight is folded into the visibility once per item
+                const int jl = mine ? jlo : 0;
+                const int jh = mine ? min(jhi, t.K) : 0;
+                const R vrw = vr * t.wt, viw = vim * t.wt;
+                for (int i = 0; i < kmax; i++) {
+                    const int rm = (mine && i < t.K) ? map_row(rb + i, gN, grows, wrap_neg) : -1;
+                    const int rl = rm - r0;
+                    const bool rok = rm >= 0 && rl >= 0 && rl < TILE_R;
+                    const int jhi_r = rok ? jh : 0;
+                    const int slot0 = cbase * TILE_R + rl;
+                    for (int j0 = 0; j0 < kmax; j0 += 8) {
+                        R kr[8], ki[8];
+#pragma unroll
+                        for (int jj = 0; jj < 8; jj++) {
+                            const int j = j0 + jj;
+                            kr[jj] = R(0);
+                            ki[jj] = R(0);
+                            if (j >= jl && j < jhi_r)
+                                tap_value<R, KMODE>(p, tab, t, i, j, kr[jj], ki[jj]);
+                        }
+#pragma unroll
+                        for (int jj = 0; jj < 8; jj++) {
+                            const int j = j0 + jj;
+                            if (j < kmax) {
+                                if (j >= jl && j < jhi_r) {
+                                    const R re = vrw * kr[jj] - viw * ki[jj];
+                                    const R im = vrw * ki[jj] + viw * kr[jj];
+                                    acc_rmw(&acc[slot0 + j * TILE_R], re, im);
+                                }
+                                __syncwarp();
+                            }
+                        }
+                    }
+                }
+            } else if (KMODE != KM_EXACT) {
                 // tabulated kernels: the lane's kernel row is fetched into
                 // registers eight taps at a time, so the loads are in flight
                 // together, then accumulated tap by tap in lockstep
@@ -730,8 +767,11 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
                             const int j = j0 + jj;
                             kr[jj] = R(0);
                             ki[jj] = R(0);
-                            if (rok && j < t.K && j >= jlo && j < jhi)
+                            if (rok && j < t.K && j >= jlo && j < jhi) {
                                 tap_value<R, KMODE>(p, tab, t, i, j, kr[jj], ki[jj]);
+                                kr[jj] = kr[jj] * t.wt;
+                                ki[jj] = ki[jj] * t.wt;
+                            }
                         }
 #pragma unroll
                         for (int jj = 0; jj < 8; jj++) {
@@ -763,6 +803,8 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
                             if (cl >= 0 && cl < TILE_C) {
                                 R kr, ki;
                                 tap_value<R, KMODE>(p, tab, t, i, j, kr, ki);
+                                kr = kr * t.wt;
+                                ki = ki * t.wt;
                                 const R re = vr * kr - vim * ki;
                                 const R im = vr * ki + vim * kr;
                                 acc_rmw(&acc[cl * TILE_R + rl], re, im);
