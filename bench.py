@@ -302,6 +302,7 @@ def run_gpu(args):
         "clocks": clocks,
     }
     if ws == 1 and not args.headline_only:
+        line.update(run_config1_and_source_finder(ctx))
         line["batched"] = run_batched(ctx, min(args.steps, 10), args.warmup)
         line["precision_study"] = run_precision(ctx)
         line["serving"] = run_serving()
@@ -432,6 +433,70 @@ def run_serving(rates=(10.0, 50.0, 100.0, 200.0), seconds=3.0, slots=4):
                     "p99_ms": round(float(np.percentile(lat, 99)), 2), "mean_ms": round(float(np.mean(lat)), 2),
                     "Mvis_per_s": round(nvis / wall / 1e6, 1), "islands_per_request": round(nisl / len(tickets), 1),
                     "peak_in_flight": int(st.peak_in_flight), "slots": slots})
+    return out
+
+
+def run_config1_and_source_finder(ctx):
+    """The reference's CPU-runnable plain imager (2048^2, 100k complex128 visibilities, w = 0, GaussianSinc
+    S=3 os=8, FP64) on the GPU against the CPU oracle; then the source finder (5 sigma detection, 3 sigma
+    analysis, BINAPPROX, 8-connectivity) on that image and on the 4096^2 headline image, device-resident."""
+    import numpy as np
+    import torch
+
+    from fastimaging_b200 import capi
+    from fastimaging_b200.synthetic import CONFIG1_IMAGER, CONFIG2_IMAGER, config1, config2
+    from oracle import stp_oracle as orc
+
+    s = config1()
+    N = s.image_size
+    dv = torch.from_numpy(s.vis).cuda()
+    dw = torch.from_numpy(s.weights).cuda()
+    duvw = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+    o64 = torch.empty(N * N, dtype=torch.float64, device="cuda")
+    st = torch.cuda.ExternalStream(ctx.stream)
+
+    def timed(fn, reps=5):
+        for _ in range(2):
+            fn()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    img = lambda: ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=capi.FP64, out_dtype=capi.F64,
+                                         device_ptrs=True, image_out=o64, **CONFIG1_IMAGER)
+    t1 = timed(img)
+    img()
+    torch.cuda.synchronize()
+    gpu = o64.cpu().numpy().reshape(N, N).T
+    ref, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, N, s.cell_size, threads=len(os.sched_getaffinity(0)),
+                                    fast=False, **CONFIG1_IMAGER)
+    err = float(np.max(np.abs(gpu - ref)) / np.max(np.abs(ref)))
+    out = {"config1": {"workload": "plain imager 2048^2, 100k complex128 visibilities, w = 0, GaussianSinc S=3 "
+                                   "os=8, FP64", "ms": round(t1, 4),
+                       "Mvis_per_s": round(s.vis.size / (t1 / 1e3) / 1e6, 1),
+                       "peak_rel_err_vs_oracle": err, "tolerance": 1e-10}}
+    res = []
+    s2 = config2()
+    N2 = s2.image_size
+    o2 = torch.empty(N2 * N2, dtype=torch.float32, device="cuda")
+    ctx.image_visibilities(torch.from_numpy(s2.vis).cuda(), torch.from_numpy(s2.weights).cuda(),
+                           torch.from_numpy(np.ascontiguousarray(s2.uvw.T)).cuda(), N2, s2.cell_size,
+                           precision=capi.FP32C, out_dtype=capi.F32, device_ptrs=True, image_out=o2,
+                           **CONFIG2_IMAGER)
+    torch.cuda.synchronize()
+    for name, im, n in (("2048^2 FP64 image", o64, N), ("4096^2 FP32 image", o2, N2)):
+        lab = torch.empty(n * n, dtype=torch.int32, device="cuda")
+        call = lambda: ctx.source_find(im, 5.0, 3.0, device_ptrs=True, rows=n, cols=n, label_out=lab)
+        t = timed(call, 5)
+        isl, _, info = call()
+        res.append({"image": name, "ms": round(t, 3), "Mpix_per_s": round(n * n / (t / 1e3) / 1e6, 1),
+                    "islands": len(isl), "labels_pos": int(info.n_labels_pos), "labels_neg": int(info.n_labels_neg)})
+    out["source_finder"] = res
     return out
 
 
