@@ -114,6 +114,22 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def job_rates(local_ms, units_per_rank_step, steps, device=None):
+    """Whole-job throughput of replicas: every rank processed `units_per_rank_step` units per step for
+    `steps` steps in local_ms[k] milliseconds (one entry per timed arm); the job's time is the MAX over
+    ranks (all ranks take this collective in the same order), and the rate counts the units of all ranks.
+    Returns (rates in M units/s, max times in ms)."""
+    import torch
+
+    ws = 1
+    tt = torch.tensor([float(x) for x in local_ms], dtype=torch.float64, device=device)
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        ws = torch.distributed.get_world_size()
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+    mx = [float(x) for x in tt.cpu()]
+    return [ws * units_per_rank_step * steps / (m / 1e3) / 1e6 for m in mx], mx
+
+
 def run_gpu(args):
     import numpy as np
     import torch
@@ -190,16 +206,7 @@ def run_gpu(args):
     clocks = clk.summary()
     _, ph, _, _ = timed(capi.FP32C, max(3, min(args.steps, 10)), 1, phases=True)
 
-    tot32 = sum(t32)
-    tot64 = sum(t64)
-    if ws > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([tot32, tot64], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        tot32, tot64 = float(tt[0]), float(tt[1])
-    value = ws * n * args.steps / (tot32 / 1e3) / 1e6
-    value64 = ws * n * args.steps / (tot64 / 1e3) / 1e6
+    (value, value64), (tot32, tot64) = job_rates([sum(t32), sum(t64)], n, args.steps, device=dev)
 
     # ---- e2e: host buffers (pinned), H2D + image D2H inside the timed region
     pv = torch.from_numpy(snap.vis).pin_memory()
@@ -233,14 +240,7 @@ def run_gpu(args):
         flush.zero_()
         torch.cuda.synchronize(dev)
         e2e_ms.append(e2e_step())  # device events around H2D .. D2H on the library stream
-    e2e_tot = sum(e2e_ms)
-    if ws > 1:
-        import torch.distributed as dist
-
-        tt = torch.tensor([e2e_tot], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_tot = float(tt[0])
-    e2e_value = ws * n * args.steps / (e2e_tot / 1e3) / 1e6
+    (e2e_value,), _ = job_rates([sum(e2e_ms)], n, args.steps, device=dev)
     h2d = snap.vis.nbytes + snap.weights.nbytes + snap.uvw.nbytes
     d2h = N * N * 4
     assert abs(float(pimg.double().max()) - float(out32.double().max())) <= 1e-6 * peak
