@@ -36,6 +36,20 @@ struct DevBuf {
     void* p = nullptr;
     size_t cap = 0;
 };
+
+// Device outputs of one gridding pass (context buffers).
+struct GridOut {
+    void* grid = nullptr;
+    void* beam = nullptr;
+    int image_rows = 0;
+    double* d_total = nullptr;             // [0] sample_grid_total
+    unsigned long long* d_ngood = nullptr; // [0] good visibilities
+    uint32_t* d_nitems = nullptr;          // tile-list entries
+    unsigned int* d_err = nullptr;
+    int* d_plane_support = nullptr;
+    int nplanes = 0;
+};
+
 } // namespace
 
 struct stpgpu_context {
@@ -71,6 +85,23 @@ struct stpgpu_context {
     cudaEvent_t tev[2] = { nullptr, nullptr };
     void* batch_host = nullptr;
     size_t batch_host_cap = 0;
+
+    // single-call path: graph of the last device-pointer call (see run_imager)
+    std::string single_sig;
+    cudaGraph_t single_graph = nullptr;
+    cudaGraphExec_t single_exec = nullptr;
+    GridOut single_g {};
+
+    void drop_single()
+    {
+        if (single_exec)
+            cudaGraphExecDestroy(single_exec);
+        if (single_graph)
+            cudaGraphDestroy(single_graph);
+        single_exec = nullptr;
+        single_graph = nullptr;
+        single_sig.clear();
+    }
 
     void drop_graph()
     {
@@ -160,6 +191,7 @@ struct stpgpu_context {
         for (auto w : wstreams)
             cudaStreamSynchronize(w);
         drop_graph();
+        drop_single();
         batch_sig.clear();
         batch_calls = 0;
         for (auto& kv : plans)
@@ -223,18 +255,6 @@ struct ImagerSetup {
     int nplanes = 0, max_support = 0, undersampling = 1, wmedian = 0;
     double trunc_perc = 0.0;
     int full_wsort = 0; // |w| order from the 64-bit sort (fallback of the 32-bit sort + run fix-up)
-};
-
-struct GridOut {
-    void* grid = nullptr;
-    void* beam = nullptr;
-    int image_rows = 0;
-    double* d_total = nullptr;             // [0] sample_grid_total
-    unsigned long long* d_ngood = nullptr; // [0] good visibilities
-    uint32_t* d_nitems = nullptr;          // tile-list entries
-    unsigned int* d_err = nullptr;
-    int* d_plane_support = nullptr;
-    int nplanes = 0;
 };
 
 void check_pars(const ImagerSetup& s)
@@ -498,7 +518,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         wq.invd = c->buf<double>("wkinv", size_t(P) * cs * cs);
         plane_support = c->buf<int>("psupport", P);
         wq.support = plane_support;
-        k_wkernel_plane<<<P, 256, 0, st>>>(wq);
+        k_wkernel_plane<<<P, 1024, 0, st>>>(wq);
         STPGPU_CHECK_LAUNCH();
         // per-offset K x K tables in the gridder's precision (worst-case
         // capacity: every plane at the maximum support)
@@ -762,7 +782,7 @@ void finish_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int 
 template <typename R, int COMP>
 void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const void* d_vis,
     int vis_c64, const double* d_wts, const double* d_uvw, int64_t n, void* d_image, void* d_beam, int out_f32,
-    stpgpu_imager_info* info)
+    stpgpu_imager_info* info, bool graphable = false)
 {
     if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
         fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
@@ -773,7 +793,47 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     const std::string cls = size_class(s, precision);
     GridOut g;
     auto it = c->tune.find(cls);
-    if (it != c->tune.end() || c->timing) {
+    // Device-pointer calls that repeat the previous call exactly (parameters,
+    // sizes, buffers) replay a CUDA graph of the gridding, FFT and
+    // normalisation kernels, captured on the first repeat; any other call
+    // drops it.  The data in the buffers may change between calls.
+    std::string sig;
+    if (graphable && !c->timing) {
+        auto put = [&](const void* q, size_t nb) { sig.append(reinterpret_cast<const char*>(q), nb); };
+        put(&precision, sizeof(precision));
+        put(&s, sizeof(s));
+        put(&image_size, sizeof(image_size));
+        put(&correction, sizeof(correction));
+        put(&vis_c64, sizeof(vis_c64));
+        put(&n, sizeof(n));
+        put(&out_f32, sizeof(out_f32));
+        const void* ptrs[6] = { d_vis, d_wts, d_uvw, d_image, d_beam, reinterpret_cast<const void*>(c->stream) };
+        put(ptrs, sizeof(ptrs));
+    }
+    const bool repeat = !sig.empty() && sig == c->single_sig;
+    if (!repeat)
+        c->drop_single();
+    if (repeat && c->single_exec) {
+        STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
+        g = c->single_g;
+    } else if (repeat && it != c->tune.end()) {
+        STPGPU_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, it->second & 0xff);
+            finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+        } catch (...) {
+            cudaGraph_t dead = nullptr;
+            cudaStreamEndCapture(c->stream, &dead);
+            if (dead)
+                cudaGraphDestroy(dead);
+            c->drop_single();
+            throw;
+        }
+        STPGPU_CUDA_TRY(cudaStreamEndCapture(c->stream, &c->single_graph));
+        STPGPU_CUDA_TRY(cudaGraphInstantiate(&c->single_exec, c->single_graph, 0));
+        STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
+        c->single_g = g;
+    } else if (it != c->tune.end() || c->timing) {
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n,
             it != c->tune.end() ? (it->second & 0xff) : TILE_C_DEFAULT);
     } else {
@@ -797,7 +857,10 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
             std::fprintf(stderr, "stpgpu tile tuner: %s  32 cols %.3f ms  16 cols %.3f ms  -> %d (single call)\n",
                 cls.c_str(), double(ms[0]), double(ms[1]), c->tune[cls]);
     }
-    finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+    if (!(repeat && c->single_exec))
+        finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+    if (!sig.empty())
+        c->single_sig = sig;
     const int N = s.N;
     ScalarsBack sb = read_back(c, g);
     if ((sb.err & 4u) && !s.full_wsort) {
@@ -1093,6 +1156,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
     stpgpu_imager_info* infos, stpgpu_batch_info* bi)
 {
     batch_streams(c);
+    c->drop_single();
     std::vector<BatchSnap> B(nb);
     std::string sig;
     auto put = [&](const void* p, size_t n) { sig.append(reinterpret_cast<const char*>(p), n); };
@@ -1808,15 +1872,15 @@ stpgpu_status stpgpu_image_visibilities_ex(stpgpu_context* c, const void* vis, i
         switch (precision) {
         case STPGPU_FP64:
             run_imager<double, 0>(c, s, image_size, pars->gridding_correction, dv, vc64, dw, duvw, n_vis, dimg, dbeam,
-                f32, inf);
+                f32, inf, device_ptrs != 0);
             break;
         case STPGPU_FP32:
             run_imager<float, 0>(c, s, image_size, pars->gridding_correction, dv, vc64, dw, duvw, n_vis, dimg, dbeam,
-                f32, inf);
+                f32, inf, device_ptrs != 0);
             break;
         case STPGPU_FP32C:
             run_imager<float, 1>(c, s, image_size, pars->gridding_correction, dv, vc64, dw, duvw, n_vis, dimg, dbeam,
-                f32, inf);
+                f32, inf, device_ptrs != 0);
             break;
         default:
             fail(STPGPU_ERR_INVALID_ARG, "precision");
@@ -1930,6 +1994,7 @@ stpgpu_status stpgpu_convolve_to_grid(stpgpu_context* c, int kernel_function, do
         }
         const double* dvis = to_device<double>(c, "in_vis", vis, 2 * size_t(n_vis));
         const double* dw = to_device<double>(c, "in_w", weights, size_t(n_vis));
+        c->drop_single(); // this call reuses the imager's buffers
         GridOut g = run_gridder<double, 0>(c, s, dvis, 0, dw, duv, 1, n_vis);
         ScalarsBack sb = read_back(c, g);
         if (sb.err & 4u) { // redo with the 64-bit |w| sort

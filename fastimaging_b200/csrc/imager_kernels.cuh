@@ -1332,7 +1332,7 @@ __device__ __forceinline__ double2 wk_value(const WkParams& q, double w, int px,
     return make_double2(re * q.aa[half + py], im * q.aa[half + py]);
 }
 
-__global__ void __launch_bounds__(256) k_wkernel_plane(WkParams q)
+__global__ void __launch_bounds__(1024) k_wkernel_plane(WkParams q)
 {
     const int p = blockIdx.x;
     const int half = q.half, arr = q.arr, os = q.os, lh = q.lh_max;

@@ -192,3 +192,35 @@ def test_imager_repeatable(ctx):
     a, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, kernel_exact=False)
     b, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, kernel_exact=False)
     assert peak_rel(a, b) < 1e-13
+
+
+def test_repeated_device_calls_replay_graph_with_new_data(ctx):
+    """Device-pointer calls that repeat the previous call are replayed from a
+    captured CUDA graph: the replay must read the buffers' current contents."""
+    import torch
+
+    s = _imager_case(51, 256, 5000, w_range=(-300.0, 300.0))
+    s2 = _imager_case(52, 256, 5000, w_range=(-300.0, 300.0))
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              num_wplanes=4, max_wpconv_support=8, kernel_trunc_perc=1.0)
+    c2 = capi.Context(0)
+    try:
+        dv = torch.from_numpy(s.vis).cuda()
+        dw = torch.from_numpy(s.weights).cuda()
+        duvw = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+        out = torch.empty(256 * 256, dtype=torch.float64, device="cuda")
+        ref1, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+        ref2, _, _ = ctx.image_visibilities(s2.vis, s2.weights, s2.uvw, 256, s2.cell_size, **kw)
+        for call in range(5):
+            if call == 3:  # new data in the same buffers
+                dv.copy_(torch.from_numpy(s2.vis))
+                dw.copy_(torch.from_numpy(s2.weights))
+                duvw.copy_(torch.from_numpy(np.ascontiguousarray(s2.uvw.T)))
+            out.fill_(-1.0)
+            _, _, info = c2.image_visibilities(dv, dw, duvw, 256, s.cell_size, device_ptrs=True, image_out=out, **kw)
+            got = out.cpu().numpy().reshape(256, 256).T
+            ref = ref1 if call < 3 else ref2
+            assert info.image_size == 256
+            assert peak_rel(got, ref) < 1e-12, call
+    finally:
+        c2.close()
