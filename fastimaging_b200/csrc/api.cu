@@ -1059,6 +1059,35 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
     std::vector<GridLaunch<R>> L(nb);
     std::vector<GridOut> G(nb);
     std::vector<void*> dimg(nb);
+    if (!device_ptrs && !class_ms) {
+        // host buffers: each snapshot runs its whole pipeline on its worker
+        // stream (H2D, preparation, gridder, c2r, normalisation, D2H), so the
+        // transfers of one snapshot overlap the compute of the others
+        batch_fork(c, main);
+        for (int i = 0; i < nb; i++) {
+            c->stream = c->wstreams[i % K];
+            c->ns = "b" + std::to_string(i) + "/";
+            BatchSnap& b = B[i];
+            const void* dv = to_device<unsigned char>(c, "in_vis", b.vis, (b.c64 ? 8 : vb) * size_t(b.n));
+            const double* dw = to_device<double>(c, "in_w", b.wts, size_t(b.n));
+            const double* duvw = to_device<double>(c, "in_uvw", b.uvw, 3 * size_t(b.n));
+            const size_t ob = (out_f32 ? 4 : 8) * size_t(b.image_size) * b.image_size;
+            void* di = c->buf<unsigned char>("out_img", ob);
+            GridOut g = run_gridder<R, COMP>(c, b.s, dv, b.c64, dw, duvw, 0, b.n, b.tile_c);
+            finish_imager<R>(c, b.s, b.image_size, b.correction, g, di, nullptr, out_f32);
+            BatchScalars* ds = c->buf<BatchScalars>("scal", 1);
+            k_collect_scalars<<<1, 1, 0, c->stream>>>(g.d_total, g.d_ngood, g.d_nitems, g.d_err,
+                g.d_plane_support ? g.d_plane_support : reinterpret_cast<const int*>(g.d_err),
+                g.d_plane_support ? g.nplanes : 0, ds);
+            STPGPU_CHECK_LAUNCH();
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(&scal[i], ds, sizeof(BatchScalars), cudaMemcpyDeviceToHost, c->stream));
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(b.image, di, ob, cudaMemcpyDeviceToHost, c->stream));
+        }
+        c->stream = main;
+        c->ns = "";
+        batch_join(c, main);
+        return nb;
+    }
     batch_fork(c, main);
     for (int i = 0; i < nb; i++) {
         c->stream = c->wstreams[i % K];
