@@ -135,7 +135,7 @@ class ServerStats(ctypes.Structure):
 
 EXPORTED = ["stpgpu_abi_version", "stpgpu_create", "stpgpu_destroy", "stpgpu_last_error", "stpgpu_stream",
             "stpgpu_set_timing", "stpgpu_trim", "stpgpu_image_visibilities", "stpgpu_image_visibilities_ex", "stpgpu_convolve_to_grid",
-            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_image_batch", "stpgpu_server_create",
+            "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_model_visibilities", "stpgpu_image_batch", "stpgpu_server_create",
             "stpgpu_server_destroy", "stpgpu_server_submit", "stpgpu_server_wait", "stpgpu_server_stats_get",
             "stpgpu_label_noalloc"]
 NOALLOC_MAX_PIXELS = 1024 * 1024
@@ -179,6 +179,7 @@ def load():
         L.stpgpu_source_find_ex.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(SfPars), vp, ctypes.c_int, vp, ctypes.c_int32,
                                             ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(SfInfo)]
+        L.stpgpu_model_visibilities.argtypes = [vp, vp, ctypes.c_int32, vp, ctypes.c_int64, vp, vp, ctypes.c_int]
         L.stpgpu_image_batch.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp,
                                          ctypes.POINTER(BatchInfo)]
         L.stpgpu_server_create.argtypes = [ctypes.POINTER(ServerPars), ctypes.POINTER(vp)]
@@ -280,6 +281,18 @@ class Context:
         if info.image_size == 0:
             return np.zeros((0, 0)), np.zeros((0, 0)), info
         return img, (beam if beam is not None else np.zeros((0, 0))), info
+
+    def model_visibilities(self, skymodel, uvw, vis=None):
+        """stp::generate_visibilities_from_local_skymodel on the GPU (host arrays): skymodel (n_src, 3) rows
+        (l, m, flux), uvw (n, 3).  With vis: returns vis - model (residual visibilities)."""
+        sky = np.asfortranarray(np.asarray(skymodel, dtype=np.float64).reshape(-1, 3))
+        uvwF = np.asfortranarray(np.asarray(uvw, dtype=np.float64).reshape(-1, 3))
+        n = uvwF.shape[0]
+        out = np.empty(n, dtype=np.complex128)
+        vin = None if vis is None else np.ascontiguousarray(vis, dtype=np.complex128).reshape(-1)
+        self._check(self.L.stpgpu_model_visibilities(self.h, _ptr(sky), sky.shape[0], _ptr(uvwF), n, _ptr(vin),
+                                                     _ptr(out), 0))
+        return out
 
     def image_batch(self, snapshots, precision=FP32C, out_dtype=F32, device_ptrs=True):
         """stpgpu_image_batch over a list of dicts, one per snapshot:

@@ -28,6 +28,7 @@
 #include "common.cuh"
 #include "imager_kernels.cuh"
 #include "sourcefind_kernels.cuh"
+#include "visibility_kernels.cuh"
 
 using namespace stpgpu;
 
@@ -1953,6 +1954,35 @@ stpgpu_status stpgpu_image_batch(stpgpu_context* c, const stpgpu_snapshot* snaps
         default:
             fail(STPGPU_ERR_INVALID_ARG, "precision");
         }
+    });
+}
+
+stpgpu_status stpgpu_model_visibilities(stpgpu_context* c, const double* skymodel, int32_t n_src, const double* uvw,
+    int64_t n_vis, const double* vis_in, double* vis_out, int device_ptrs)
+{
+    return guard(c, [&] {
+        if (n_src < 0 || n_vis < 0 || (n_vis > 0 && (!uvw || !vis_out)) || (n_src > 0 && !skymodel))
+            fail(STPGPU_ERR_INVALID_ARG, "null buffer or negative size");
+        if (n_vis == 0)
+            return;
+        cudaStream_t st = c->stream;
+        const double* dsky = skymodel;
+        const double* duvw = uvw;
+        const double* dvin = vis_in;
+        double* dout = vis_out;
+        if (!device_ptrs) {
+            dsky = to_device<double>(c, "mv_sky", skymodel, 3 * size_t(n_src));
+            duvw = to_device<double>(c, "mv_uvw", uvw, 3 * size_t(n_vis));
+            if (vis_in)
+                dvin = to_device<double>(c, "mv_in", vis_in, 2 * size_t(n_vis));
+            dout = c->buf<double>("mv_out", 2 * size_t(n_vis));
+        }
+        k_model_vis<<<grid1d(n_vis, VIS_THREADS), VIS_THREADS, 0, st>>>(dsky, n_src, duvw, n_vis, dvin,
+            vis_in != nullptr, dout);
+        STPGPU_CHECK_LAUNCH();
+        if (!device_ptrs)
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(vis_out, dout, 2 * sizeof(double) * size_t(n_vis), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
     });
 }
 

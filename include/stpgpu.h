@@ -228,6 +228,16 @@ STPGPU_API stpgpu_status stpgpu_source_find_ex(stpgpu_context* ctx, const void* 
     const stpgpu_sf_pars* pars, int32_t* label_map, int device_ptrs, stpgpu_island* islands, int32_t capacity,
     int32_t* n_islands, stpgpu_sf_info* info);
 
+/* stp::generate_visibilities_from_local_skymodel (src/stp/visibility/visibility.cpp:30-40,
+ * visibilities_for_point_source :15-28): model visibilities of a point-source
+ * sky model, FP64.  skymodel: n_src x 3 column-major (l[], m[], flux[]);
+ * uvw: n_vis x 3 column-major (lambda); vis_out: n_vis complex128
+ * (interleaved).  vis_in non-null: vis_out = vis_in - model (the residual
+ * visibilities of reduce.cpp:113-122; vis_in may equal vis_out).  Device
+ * pointers when device_ptrs != 0. */
+STPGPU_API stpgpu_status stpgpu_model_visibilities(stpgpu_context* ctx, const double* skymodel, int32_t n_src,
+    const double* uvw, int64_t n_vis, const double* vis_in, double* vis_out, int device_ptrs);
+
 /* One snapshot of a batch (stpgpu_image_batch).  Pointers are device
  * pointers when the batch call's device_ptrs != 0, else host pointers.
  * vis_dtype: STPGPU_C128 / STPGPU_C64; uvw n_vis x 3 column-major; image:

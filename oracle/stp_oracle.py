@@ -568,3 +568,22 @@ def source_find(image, detection_n_sigma, analysis_n_sigma, rms_est=0.0, find_ne
                 g = moments_fit(sign, float(ev[i]), m[0], m[1], m[2], m[3], m[4], rms, analysis_n_sigma)
                 islands.append((sign, float(ev[i]), x, y, int(ns[i]), g, Gaussian2dParams(), ""))
     return SourceFindResult(islands, L.reshape((rows, cols), order="F"), bg, rms, npos, nneg, va_p, va_n)
+
+
+def visibilities_for_point_source(uvw, l, m, flux):
+    """visibility.cpp:15-28: flux * n * exp(cx(0, -2 pi) * (dist_uvw * -(l, m, n - 1)))."""
+    src_n = math.sqrt(1 - l * l - m * m)
+    off = -np.array([l, m, src_n - 1.0])
+    uvw = np.asarray(uvw, dtype=np.float64).reshape(-1, 3)
+    dot = (uvw[:, 0] * off[0] + uvw[:, 1] * off[1]) + uvw[:, 2] * off[2]
+    theta = (-2.0 * math.pi) * dot
+    return flux * src_n * (np.cos(theta) + 1j * np.sin(theta))
+
+
+def generate_visibilities_from_local_skymodel(skymodel, uvw):
+    """visibility.cpp:30-40: model visibilities summed over the sky-model rows in order."""
+    uvw = np.asarray(uvw, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros(uvw.shape[0], dtype=np.complex128)
+    for l, m, f in np.asarray(skymodel, dtype=np.float64).reshape(-1, 3):
+        out += visibilities_for_point_source(uvw, l, m, f)
+    return out
