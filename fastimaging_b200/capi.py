@@ -65,7 +65,8 @@ class Island(ctypes.Structure):
                 ("extremum_y_idx", ctypes.c_int32), ("extremum_x_idx", ctypes.c_int32),
                 ("num_samples", ctypes.c_int32), ("bbox_top", ctypes.c_int32), ("bbox_bottom", ctypes.c_int32),
                 ("bbox_left", ctypes.c_int32), ("bbox_right", ctypes.c_int32),
-                ("moments_fit", ctypes.c_double * 6), ("leastsq_fit", ctypes.c_double * 6)]
+                ("moments_fit", ctypes.c_double * 6), ("leastsq_fit", ctypes.c_double * 6),
+                ("fit_iterations", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class SfPars(ctypes.Structure):

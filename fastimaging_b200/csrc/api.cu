@@ -1581,8 +1581,6 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         fail(STPGPU_ERR_INVALID_ARG, "image dimensions must be positive and even (ccl.h:116-117)");
     if (rows > 65536 || cols > 65536 || int64_t(rows) * cols >= (int64_t(1) << 32))
         fail(STPGPU_ERR_INVALID_ARG, "image too large for the labeler (ccl.h:118-119)");
-    if (p.gaussian_fitting)
-        fail(STPGPU_ERR_UNSUPPORTED, "Gaussian least-squares fitting (Ceres) is outside the GPU path");
     cudaStream_t st = c->stream;
     const int64_t n = int64_t(rows) * cols;
     double mean = 0.0, sigma = 0.0, median = 0.0;
@@ -1698,6 +1696,9 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     STPGPU_CHECK_LAUNCH();
     k_extrema_idx<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg, kpos, kneg, eidx, eidx + np);
     STPGPU_CHECK_LAUNCH();
+    const uint32_t* fit_pix = nullptr; // pixels sorted by label, and each label's segment
+    const uint32_t* fit_sb = nullptr;
+    const uint32_t* fit_se = nullptr;
     {
         // ordered (deterministic) moments: compact -> stable sort by label -> per-label sums
         uint32_t* fcnt = c->buf<uint32_t>("fg_cnt", nchunks + 1);
@@ -1733,7 +1734,10 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
                 fail(STPGPU_ERR_CUDA, "label sort failed");
             k_seg_bounds<<<grid1d(nk, 256), 256, 0, st>>>(k1, nk, sb, se);
             STPGPU_CHECK_LAUNCH();
+            fit_pix = v1;
         }
+        fit_sb = sb;
+        fit_se = se;
         k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, mom, ns);
         STPGPU_CHECK_LAUNCH();
     }
@@ -1778,6 +1782,49 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         mb[3] = a[3] / a[5] - mb[1] * mb[1];
         mb[4] = a[4] / a[5] - mb[0] * mb[1];
         moments_fit(o.sign, o.extremum_val, mb, rms, p.analysis_n_sigma, o.moments_fit);
+    }
+    if (p.gaussian_fitting && nis > 0) {
+        // least-squares 2-D Gaussian per island (sourcefind.cpp:719-866): islands of one or two pixels keep
+        // (extremum, 0, ...); the others start from the moments fit, unset widths as 1
+        std::vector<int> keys, which;
+        std::vector<double> init;
+        for (int i = 0; i < nis; i++) {
+            stpgpu_island& o = islands[i];
+            if (o.num_samples < 3) {
+                o.leastsq_fit[0] = o.extremum_val;
+                continue;
+            }
+            const int l = o.label_idx;
+            keys.push_back(l > 0 ? l - 1 : np + (-l - 1));
+            which.push_back(i);
+            const double* m = o.moments_fit;
+            const double g[6] = { m[0], m[1], m[2], m[3] > 0.0 ? m[3] : 1.0, m[4] > 0.0 ? m[4] : 1.0, m[5] };
+            init.insert(init.end(), g, g + 6);
+        }
+        const int nfit = int(keys.size());
+        if (nfit > 0 && fit_pix) {
+            int* dkeys = c->buf<int>("fit_keys", nfit);
+            double* dinit = c->buf<double>("fit_init", 6 * size_t(nfit));
+            double* dout = c->buf<double>("fit_out", 6 * size_t(nfit));
+            int* dit = c->buf<int>("fit_iter", nfit);
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(dkeys, keys.data(), sizeof(int) * nfit, cudaMemcpyHostToDevice, st));
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(dinit, init.data(), sizeof(double) * 6 * nfit, cudaMemcpyHostToDevice, st));
+            k_gauss_fit<T><<<nfit, 32, 0, st>>>(d_img, rows, cols, fit_pix, fit_sb, fit_se, dkeys, dinit, nfit, dout,
+                dit);
+            STPGPU_CHECK_LAUNCH();
+            std::vector<double> out(6 * size_t(nfit));
+            std::vector<int> its(nfit);
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(out.data(), dout, sizeof(double) * 6 * nfit, cudaMemcpyDeviceToHost, st));
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(its.data(), dit, sizeof(int) * nfit, cudaMemcpyDeviceToHost, st));
+            STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+            for (int k = 0; k < nfit; k++) {
+                stpgpu_island& o = islands[which[k]];
+                for (int q = 0; q < 6; q++)
+                    o.leastsq_fit[q] = out[6 * size_t(k) + q];
+                constrain(o.leastsq_fit); // fitting.cpp:32-57
+                o.fit_iterations = its[k];
+            }
+        }
     }
 }
 

@@ -660,3 +660,214 @@ __global__ void k_island_scatter(int np, int nn, const uint32_t* flags, const ui
 }
 
 } // namespace stpgpu
+
+namespace stpgpu {
+
+// ---------------------------------------------------------------- 2-D Gaussian fit
+//
+// Least-squares fit of A exp(-(a dx^2 + b dx dy + c dy^2)) to the pixels of
+// each island (the model and residual of GaussianResidual,
+// src/stp/sourcefind/fitting.h:183-210; a, b, c from the standard deviations
+// and theta as there), starting from the moments fit
+// (sourcefind.cpp:719-760).  The reference minimises with Ceres; here a
+// Levenberg-Marquardt iteration with analytic derivatives: one warp per
+// island, lanes over the island's pixels, the 6x6 normal equations reduced
+// with shuffles and solved by every lane (Cholesky).
+constexpr int FIT_MAX_ITER = 100;
+
+struct GaussTerms {
+    double a, b, c, da_dsx, db_dsx, dc_dsx, da_dsy, db_dsy, dc_dsy, da_dt, db_dt, dc_dt;
+};
+
+__device__ __forceinline__ GaussTerms gauss_terms(const double* p)
+{
+    GaussTerms g;
+    const double ct = cos(p[5]), st = sin(p[5]), s2t = sin(2.0 * p[5]), c2t = cos(2.0 * p[5]);
+    const double ct2 = ct * ct, st2 = st * st;
+    const double ix2 = 1.0 / (p[3] * p[3]), iy2 = 1.0 / (p[4] * p[4]);
+    const double ix3 = ix2 / p[3], iy3 = iy2 / p[4];
+    g.a = 0.5 * (ct2 * ix2 + st2 * iy2);
+    g.b = 0.5 * (s2t * ix2 - s2t * iy2);
+    g.c = 0.5 * (st2 * ix2 + ct2 * iy2);
+    g.da_dsx = -ct2 * ix3;
+    g.db_dsx = -s2t * ix3;
+    g.dc_dsx = -st2 * ix3;
+    g.da_dsy = -st2 * iy3;
+    g.db_dsy = s2t * iy3;
+    g.dc_dsy = -ct2 * iy3;
+    g.da_dt = 0.5 * s2t * (iy2 - ix2);
+    g.db_dt = c2t * (ix2 - iy2);
+    g.dc_dt = 0.5 * s2t * (ix2 - iy2);
+    return g;
+}
+
+// Sum over the warp, broadcast from lane 0 so that every lane holds the same
+// bits (the butterfly adds in a different order on each lane).
+__device__ __forceinline__ double warp_sum_bcast(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Cholesky solve of the 6x6 SPD system m x = r (m: 21 packed lower entries).
+__device__ __forceinline__ bool solve6(const double* m, const double* r, double* x)
+{
+    double L[6][6];
+    int t = 0;
+    for (int i = 0; i < 6; i++)
+        for (int j = 0; j <= i; j++)
+            L[i][j] = m[t++];
+    for (int j = 0; j < 6; j++) {
+        double d = L[j][j];
+        for (int k = 0; k < j; k++)
+            d -= L[j][k] * L[j][k];
+        if (!(d > 0.0))
+            return false;
+        d = sqrt(d);
+        L[j][j] = d;
+        for (int i = j + 1; i < 6; i++) {
+            double v = L[i][j];
+            for (int k = 0; k < j; k++)
+                v -= L[i][k] * L[j][k];
+            L[i][j] = v / d;
+        }
+    }
+    double y[6];
+    for (int i = 0; i < 6; i++) {
+        double v = r[i];
+        for (int k = 0; k < i; k++)
+            v -= L[i][k] * y[k];
+        y[i] = v / L[i][i];
+    }
+    for (int i = 5; i >= 0; i--) {
+        double v = y[i];
+        for (int k = i + 1; k < 6; k++)
+            v -= L[k][i] * x[k];
+        x[i] = v / L[i][i];
+    }
+    return true;
+}
+
+// pix[sb[key] .. se[key]) are the island's pixels (memory indices of the
+// column-major rows x cols image); x, y are display coordinates (the image is
+// unshifted: display = memory index shifted by half, sourcefind.cpp:230-245).
+template <typename T>
+__global__ void __launch_bounds__(32) k_gauss_fit(const T* __restrict__ img, int rows, int cols,
+    const uint32_t* __restrict__ pix, const uint32_t* __restrict__ sb, const uint32_t* __restrict__ se,
+    const int* __restrict__ keys, const double* __restrict__ init, int nis, double* outp, int* iters)
+{
+    const int isl = blockIdx.x;
+    if (isl >= nis)
+        return;
+    const int lane = threadIdx.x;
+    const int key = keys[isl];
+    const uint32_t b = sb[key], e = se[key];
+    const int hs = cols / 2, vs = rows / 2;
+    double p[6];
+    for (int k = 0; k < 6; k++)
+        p[k] = init[6 * isl + k];
+
+    // cost (and optionally the normal equations) at parameters q
+    auto pass = [&](const double* q, bool normal, double* JtJ, double* Jtr) -> double {
+        const GaussTerms g = gauss_terms(q);
+        double cost = 0.0;
+        double jj[21], jr[6];
+        if (normal) {
+            for (int k = 0; k < 21; k++)
+                jj[k] = 0.0;
+            for (int k = 0; k < 6; k++)
+                jr[k] = 0.0;
+        }
+        for (uint32_t t = b + lane; t < e; t += 32) {
+            const uint32_t m = pix[t];
+            const int rm = int(m % uint32_t(rows)), cm = int(m / uint32_t(rows));
+            const double x = double(cm < hs ? cm + hs : cm - hs);
+            const double y = double(rm < vs ? rm + vs : rm - vs);
+            const double dx = x - q[1], dy = y - q[2];
+            const double quad = g.a * dx * dx + g.b * dx * dy + g.c * dy * dy;
+            const double ex = exp(-quad);
+            const double r = q[0] * ex - double(img[m]);
+            cost += r * r;
+            if (normal) {
+                const double ae = q[0] * ex;
+                double J[6];
+                J[0] = ex;
+                J[1] = ae * (2.0 * g.a * dx + g.b * dy);
+                J[2] = ae * (g.b * dx + 2.0 * g.c * dy);
+                J[3] = -ae * (g.da_dsx * dx * dx + g.db_dsx * dx * dy + g.dc_dsx * dy * dy);
+                J[4] = -ae * (g.da_dsy * dx * dx + g.db_dsy * dx * dy + g.dc_dsy * dy * dy);
+                J[5] = -ae * (g.da_dt * dx * dx + g.db_dt * dx * dy + g.dc_dt * dy * dy);
+                int u = 0;
+                for (int i = 0; i < 6; i++) {
+                    jr[i] += J[i] * r;
+                    for (int j = 0; j <= i; j++)
+                        jj[u++] += J[i] * J[j];
+                }
+            }
+        }
+        if (normal) {
+            for (int k = 0; k < 21; k++)
+                JtJ[k] = warp_sum_bcast(jj[k]);
+            for (int k = 0; k < 6; k++)
+                Jtr[k] = warp_sum_bcast(jr[k]);
+        }
+        return warp_sum_bcast(cost);
+    };
+
+    double JtJ[21], Jtr[6];
+    double cost = pass(p, true, JtJ, Jtr);
+    double lambda = 1e-3;
+    int it = 0;
+    while (it < FIT_MAX_ITER) {
+        it++;
+        // (J^T J + lambda D) delta = -J^T r, D = diag(J^T J) floored at 1e-12 of its
+        // largest entry (a parameter the residuals do not depend on, such as
+        // theta of a circular Gaussian, then gets a zero step)
+        double m[21], rhs[6], d[6], q[6];
+        double dmax = 0.0;
+        for (int i = 0; i < 6; i++)
+            dmax = fmax(dmax, JtJ[i * (i + 1) / 2 + i]);
+        int u = 0;
+        for (int i = 0; i < 6; i++) {
+            rhs[i] = -Jtr[i];
+            for (int j = 0; j <= i; j++, u++)
+                m[u] = (i == j) ? JtJ[u] + lambda * fmax(JtJ[u], 1e-12 * dmax + 1e-300) : JtJ[u];
+        }
+        bool ok = solve6(m, rhs, d);
+        double cnew = 0.0;
+        if (ok) {
+            for (int k = 0; k < 6; k++)
+                q[k] = p[k] + d[k];
+            ok = q[3] != 0.0 && q[4] != 0.0;
+        }
+        if (ok) {
+            double dummy1[21], dummy2[6];
+            cnew = pass(q, false, dummy1, dummy2);
+            ok = cnew == cnew && cnew < cost; // NaN-safe
+        }
+        if (ok) {
+            double step = 0.0;
+            for (int k = 0; k < 6; k++)
+                step = fmax(step, fabs(d[k]) / (fabs(p[k]) + 1e-10));
+            const bool small = (cost - cnew) <= 1e-12 * cost || step <= 1e-10;
+            for (int k = 0; k < 6; k++)
+                p[k] = q[k];
+            cost = pass(p, true, JtJ, Jtr);
+            lambda = fmax(lambda * 0.1, 1e-15);
+            if (small)
+                break;
+        } else {
+            lambda *= 10.0;
+            if (lambda > 1e16)
+                break;
+        }
+    }
+    if (lane == 0) {
+        for (int k = 0; k < 6; k++)
+            outp[6 * isl + k] = p[k];
+        iters[isl] = it;
+    }
+}
+
+} // namespace stpgpu

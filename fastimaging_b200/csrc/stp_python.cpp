@@ -215,8 +215,17 @@ source_find_wrapper(np_double_array image_data, double detection_n_sigma, double
         m.semimajor = r.moments_fit[3];
         m.semiminor = r.moments_fit[4];
         m.theta = r.moments_fit[5];
-        out.emplace_back(r.sign, r.extremum_val, r.extremum_x_idx, r.extremum_y_idx, r.num_samples, m, l,
-            std::string());
+        l.amplitude = r.leastsq_fit[0];
+        l.x_centre = r.leastsq_fit[1];
+        l.y_centre = r.leastsq_fit[2];
+        l.semimajor = r.leastsq_fit[3];
+        l.semiminor = r.leastsq_fit[4];
+        l.theta = r.leastsq_fit[5];
+        std::string report;
+        if (gaussian_fitting)
+            report = r.num_samples < 3 ? "least-squares fit not run: source of one or two pixels"
+                                       : "Levenberg-Marquardt fit, " + std::to_string(r.fit_iterations) + " iterations";
+        out.emplace_back(r.sign, r.extremum_val, r.extremum_x_idx, r.extremum_y_idx, r.num_samples, m, l, report);
     }
     return out;
 }

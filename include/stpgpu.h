@@ -129,7 +129,9 @@ typedef struct {
     int32_t num_samples;
     int32_t bbox_top, bbox_bottom, bbox_left, bbox_right;
     double moments_fit[6];
-    double leastsq_fit[6];
+    double leastsq_fit[6]; /* with gaussian_fitting: least-squares 2-D Gaussian, else zeros */
+    int32_t fit_iterations; /* Levenberg-Marquardt iterations of the fit (0: not fitted) */
+    int32_t reserved;
 } stpgpu_island;
 
 /* SourceFindImage ctor arguments, src/stp/sourcefind/sourcefind.h:188-201.
@@ -143,7 +145,7 @@ typedef struct {
     int32_t find_negative_sources;
     int32_t sigma_clip_iters;
     int32_t median_method; /* stpgpu_median_method */
-    int32_t gaussian_fitting; /* must be 0 (Ceres fit outside the GPU path) */
+    int32_t gaussian_fitting; /* least-squares 2-D Gaussian per island (Levenberg-Marquardt in place of Ceres) */
     int32_t ccl_4connectivity;
     int32_t generate_labelmap;
     int32_t source_min_area;

@@ -512,8 +512,6 @@ def source_find(image, detection_n_sigma, analysis_n_sigma, rms_est=0.0, find_ne
     """SourceFindImage ctor, sourcefind.cpp:156-292 (+ the python tuple layout,
     stp_python.cpp:142-179).  Islands: (sign, extremum_val, x_idx, y_idx,
     num_samples, moments_fit, leastsq_fit, ceres_report)."""
-    if gaussian_fitting:
-        raise NotImplementedError("Gaussian fitting (Ceres) is not restated")
     data = np.asfortranarray(image, dtype=np.float64)
     rows, cols = data.shape
     mean = sigma = None
@@ -566,7 +564,10 @@ def source_find(image, detection_n_sigma, analysis_n_sigma, rms_est=0.0, find_ne
             if ns[i] >= source_min_area:
                 m = mo[5 * i:5 * i + 5]
                 g = moments_fit(sign, float(ev[i]), m[0], m[1], m[2], m[3], m[4], rms, analysis_n_sigma)
-                islands.append((sign, float(ev[i]), x, y, int(ns[i]), g, Gaussian2dParams(), ""))
+                fit = Gaussian2dParams()
+                if gaussian_fitting:
+                    fit = leastsq_fit_gaussian_2d(dataflat, L, rows, cols, sign * (i + 1), int(ns[i]), float(ev[i]), g)
+                islands.append((sign, float(ev[i]), x, y, int(ns[i]), g, fit, ""))
     return SourceFindResult(islands, L.reshape((rows, cols), order="F"), bg, rms, npos, nneg, va_p, va_n)
 
 
@@ -586,4 +587,96 @@ def generate_visibilities_from_local_skymodel(skymodel, uvw):
     out = np.zeros(uvw.shape[0], dtype=np.complex128)
     for l, m, f in np.asarray(skymodel, dtype=np.float64).reshape(-1, 3):
         out += visibilities_for_point_source(uvw, l, m, f)
+    return out
+
+
+FIT_MAX_ITER = 100
+
+
+def _gauss_terms(p):
+    """a, b, c of GaussianResidual (fitting.h:183-210) and their derivatives in (sx, sy, theta)."""
+    ct, st, s2t, c2t = math.cos(p[5]), math.sin(p[5]), math.sin(2.0 * p[5]), math.cos(2.0 * p[5])
+    ct2, st2 = ct * ct, st * st
+    ix2, iy2 = 1.0 / (p[3] * p[3]), 1.0 / (p[4] * p[4])
+    ix3, iy3 = ix2 / p[3], iy2 / p[4]
+    return dict(a=0.5 * (ct2 * ix2 + st2 * iy2), b=0.5 * (s2t * ix2 - s2t * iy2), c=0.5 * (st2 * ix2 + ct2 * iy2),
+                dsx=(-ct2 * ix3, -s2t * ix3, -st2 * ix3), dsy=(-st2 * iy3, s2t * iy3, -ct2 * iy3),
+                dt=(0.5 * s2t * (iy2 - ix2), c2t * (ix2 - iy2), 0.5 * s2t * (ix2 - iy2)))
+
+
+def gauss_fit_lm(vals, xs, ys, p0):
+    """Least-squares 2-D Gaussian (the residual of fitting.h:183-210) by Levenberg-Marquardt with analytic
+    derivatives; the algorithm the GPU runs (the reference uses Ceres, sourcefind.cpp:719-866).
+    Returns (params, iterations)."""
+    p = np.array(p0, dtype=np.float64)
+
+    def evaluate(q, normal):
+        g = _gauss_terms(q)
+        dx, dy = xs - q[1], ys - q[2]
+        ex = np.exp(-(g["a"] * dx * dx + g["b"] * dx * dy + g["c"] * dy * dy))
+        r = q[0] * ex - vals
+        cost = float(np.dot(r, r))
+        if not normal:
+            return cost, None, None
+        ae = q[0] * ex
+        J = np.empty((vals.size, 6))
+        J[:, 0] = ex
+        J[:, 1] = ae * (2.0 * g["a"] * dx + g["b"] * dy)
+        J[:, 2] = ae * (g["b"] * dx + 2.0 * g["c"] * dy)
+        for k, key in ((3, "dsx"), (4, "dsy"), (5, "dt")):
+            da, db, dc = g[key]
+            J[:, k] = -ae * (da * dx * dx + db * dx * dy + dc * dy * dy)
+        return cost, J.T @ J, J.T @ r
+
+    cost, JtJ, Jtr = evaluate(p, True)
+    lam = 1e-3
+    it = 0
+    while it < FIT_MAX_ITER:
+        it += 1
+        M = JtJ.copy()
+        dg = np.diag(JtJ)
+        M[np.diag_indices(6)] += lam * np.maximum(dg, 1e-12 * dg.max() + 1e-300)
+        ok = True
+        try:
+            Lc = np.linalg.cholesky(M)
+            d = np.linalg.solve(Lc.T, np.linalg.solve(Lc, -Jtr))
+            q = p + d
+            ok = q[3] != 0.0 and q[4] != 0.0
+        except np.linalg.LinAlgError:
+            ok = False
+        if ok:
+            cnew, _, _ = evaluate(q, False)
+            ok = cnew == cnew and cnew < cost
+        if ok:
+            step = float(np.max(np.abs(d) / (np.abs(p) + 1e-10)))
+            small = (cost - cnew) <= 1e-12 * cost or step <= 1e-10
+            p = q
+            cost, JtJ, Jtr = evaluate(p, True)
+            lam = max(lam * 0.1, 1e-15)
+            if small:
+                break
+        else:
+            lam *= 10.0
+            if lam > 1e16:
+                break
+    return p, it
+
+
+def leastsq_fit_gaussian_2d(dataflat, L, rows, cols, label, num_samples, extremum_val, moments):
+    """IslandParams::leastsq_fit_gaussian_2d (sourcefind.cpp:719-866) with the LM minimiser above: pixels of the
+    island in display coordinates, start at the moments fit (unset widths 1.0), result constrained
+    (fitting.cpp:32-57); islands of one or two pixels keep (extremum, 0, ...)."""
+    if num_samples < 3:
+        return Gaussian2dParams(extremum_val, 0.0, 0.0, 0.0, 0.0, 0.0)
+    m = np.nonzero(L == label)[0]
+    r, c = m % rows, m // rows
+    vs, hs = rows // 2, cols // 2
+    ys = np.where(r < vs, r + vs, r - vs).astype(np.float64)
+    xs = np.where(c < hs, c + hs, c - hs).astype(np.float64)
+    g = moments
+    p0 = [g.amplitude, g.x_centre, g.y_centre, g.semimajor if g.semimajor > 0 else 1.0,
+          g.semiminor if g.semiminor > 0 else 1.0, g.theta]
+    p, _ = gauss_fit_lm(dataflat[m], xs, ys, p0)
+    out = Gaussian2dParams(*[float(v) for v in p])
+    out.convert_to_constrained_parameters()
     return out
