@@ -258,6 +258,12 @@ struct ImagerSetup {
     int full_wsort = 0; // |w| order from the 64-bit sort (fallback of the 32-bit sort + run fix-up)
 };
 
+// W-projection with a maximum support above 32: the W-kernel tables and tile
+// lists are sized from the measured plane supports and list length (two
+// host round trips) instead of from the worst case, so such calls are not
+// captured into CUDA graphs.
+bool large_support(const ImagerSetup& s) { return s.nplanes > 0 && s.max_support > 32; }
+
 void check_pars(const ImagerSetup& s)
 {
     if (s.N <= 0 || (s.N % 2) != 0)
@@ -268,8 +274,8 @@ void check_pars(const ImagerSetup& s)
         fail(STPGPU_ERR_INVALID_ARG, "max_wpconv_support must be > 0 with W-projection");
     if (s.nplanes > 65535)
         fail(STPGPU_ERR_INVALID_ARG, "num_wplanes too large");
-    if (s.nplanes > 0 && s.max_support > 32)
-        fail(STPGPU_ERR_UNSUPPORTED, "max_wpconv_support > 32 is outside the GPU path");
+    if (s.nplanes > 0 && s.max_support > 127)
+        fail(STPGPU_ERR_UNSUPPORTED, "max_wpconv_support > 127 is outside the GPU path");
     if (s.nplanes == 0 && s.support > 32)
         fail(STPGPU_ERR_UNSUPPORTED, "kernel_support > 32 is outside the GPU path");
     if (s.os > 4096)
@@ -521,11 +527,21 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         wq.support = plane_support;
         k_wkernel_plane<<<P, 1024, 0, st>>>(wq);
         STPGPU_CHECK_LAUNCH();
-        // per-offset K x K tables in the gridder's precision (worst-case
-        // capacity: every plane at the maximum support)
-        const uint64_t cap_wk = uint64_t(P) * cs * cs * uint64_t(K) * K;
-        if (cap_wk * sizeof(C2) > (uint64_t(2) << 30) || cap_wk > 0xffffffffull)
-            fail(STPGPU_ERR_UNSUPPORTED, "W-kernel tables exceed 2 GB (planes x oversampling^2 x support^2)");
+        // per-offset K x K tables in the gridder's precision: worst-case
+        // capacity (every plane at the maximum support), or with large
+        // supports the sum over the measured plane supports
+        uint64_t cap_wk = uint64_t(P) * cs * cs * uint64_t(K) * K;
+        if (large_support(s)) {
+            std::vector<int> sup(P);
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(sup.data(), plane_support, sizeof(int) * P, cudaMemcpyDeviceToHost, st));
+            STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+            cap_wk = 0;
+            for (int v : sup)
+                cap_wk += uint64_t(cs) * cs * uint64_t(2 * v + 1) * uint64_t(2 * v + 1);
+            cap_wk = std::max<uint64_t>(cap_wk, 1);
+        }
+        if (cap_wk * sizeof(C2) > (uint64_t(16) << 30) || cap_wk > 0xffffffffull)
+            fail(STPGPU_ERR_UNSUPPORTED, "W-kernel tables exceed 16 GB (planes x oversampling^2 x support^2)");
         wk = c->buf<C2>("wkexp", cap_wk);
         wk_off = c->buf<uint32_t>("wkoff", P);
         k_wk_expand<R><<<dim3(P, cs * cs), 64, 0, st>>>(wq.convd, wq.invd, plane_support, P, cs, os, Lh, wk, wk_off);
@@ -544,10 +560,10 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     uint32_t* tcur = c->buf<uint32_t>("tcur", ntiles + 1);
     const int Kx = 2 * conv_support + 1;
     const uint64_t per_dim = uint64_t(ceil_div(Kx - 1, std::min(TILE_R, tile_c))) + 2;
-    const uint64_t cap = std::max<uint64_t>(1, uint64_t(nn) * 2 * per_dim * per_dim);
-    if (cap > 0xffffffffull)
+    uint64_t cap = std::max<uint64_t>(1, uint64_t(nn) * 2 * per_dim * per_dim);
+    if (!large_support(s) && cap > 0xffffffffull)
         fail(STPGPU_ERR_INVALID_ARG, "too many visibilities for one snapshot");
-    uint32_t* list = c->buf<uint32_t>("tlist", cap);
+    uint32_t* list = large_support(s) ? nullptr : c->buf<uint32_t>("tlist", cap);
     BinParams bp {};
     bp.N = N;
     bp.image_rows = image_rows;
@@ -572,6 +588,15 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     }
     k_scan_single<<<1, 1024, 0, st>>>(tcount, toff, ntiles);
     STPGPU_CHECK_LAUNCH();
+    if (large_support(s)) { // size the list from the counted entries
+        uint32_t total = 0;
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(&total, toff + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+        cap = std::max<uint64_t>(total, 1);
+        list = c->buf<uint32_t>("tlist", cap);
+        bp.list = list;
+        bp.list_capacity = cap;
+    }
     if (n > 0) {
         k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
@@ -609,8 +634,8 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     size_t smem = size_t(TILE_R) * tile_c * sizeof(A) * (s.beam ? 2 : 1);
     if (!wproj && !kernel_exact)
         smem += sizeof(R) * size_t(cs) * (2 * s.support + 1);
-    if (2 * conv_support + 1 > 65)
-        fail(STPGPU_ERR_UNSUPPORTED, "kernel support > 32 is outside the GPU path");
+    if (2 * conv_support + 1 > 255)
+        fail(STPGPU_ERR_UNSUPPORTED, "kernel support > 127 is outside the GPU path");
     const int kind = (wproj && n > 0) ? GK_WPROJ : (kernel_exact ? GK_EXACT : (!wproj ? GK_SEP : GK_NONE));
     if (kind == GK_NONE) {
         STPGPU_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(C2) * size_t(image_rows) * N, st));
@@ -799,7 +824,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     // normalisation kernels, captured on the first repeat; any other call
     // drops it.  The data in the buffers may change between calls.
     std::string sig;
-    if (graphable && !c->timing) {
+    if (graphable && !c->timing && !large_support(s)) {
         auto put = [&](const void* q, size_t nb) { sig.append(reinterpret_cast<const char*>(q), nb); };
         put(&precision, sizeof(precision));
         put(&s, sizeof(s));
@@ -1311,7 +1336,10 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             b.tile_c = c->tune[b.cls] & 0xff;
             b.persist = (c->tune[b.cls] & kLayoutPersist) ? 1 : 0;
         }
-        if (device_ptrs && c->batch_calls >= 2 && tuned == 0) {
+        bool capturable = true;
+        for (auto& b : B)
+            capturable = capturable && !large_support(b.s);
+        if (device_ptrs && capturable && c->batch_calls >= 2 && tuned == 0) {
             // capture the batch (buffers, plans and tables exist from the previous call)
             STPGPU_CUDA_TRY(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
             try {

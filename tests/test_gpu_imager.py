@@ -119,6 +119,21 @@ def test_imager_wproj_untruncated(ctx):
     assert peak_rel(img, ri) < TOL64
 
 
+@pytest.mark.parametrize("trunc", [0.0, 1.0])
+def test_imager_wproj_large_support(ctx, trunc):
+    """W-kernel supports above 32 (the reference's W-projection configurations use up to 127): tables and tile
+    lists sized from the measured supports."""
+    s = _imager_case(37, 256, 1500, w_range=(-4000.0, 4000.0))
+    kw = dict(kernel_func=5, kernel_support=3, kernel_exact=False, oversampling=4, analytic_gcf=True,
+              num_wplanes=3, max_wpconv_support=40, kernel_trunc_perc=trunc)
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    ri, _, g = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, return_grid=True, **kw)
+    assert info.max_plane_support == max(g.plane_supports)
+    if trunc == 0.0:
+        assert info.max_plane_support == 40
+    assert peak_rel(img, ri) < TOL64
+
+
 @pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal"])
 def test_imager_wproj_near_tied_w(ctx, pattern):
     """|w| values that are equal in single precision but distinct in double
