@@ -307,9 +307,14 @@ struct GridLaunch {
 // and "beamgrid" of precision R (complex), image_rows x N column-major.
 // tile_c: grid columns per tile (32 or 16).  With `defer` the gridder kernel
 // is not launched: its parameters are returned there instead.
+// Autotuned gridder layout bits beside the tile width (low 8 bits).
+constexpr int kLayoutPersist = 1 << 8; // batch: persistent work queue
+constexpr int kLayoutCols = 1 << 9;    // column-packed tile gridder (grid_tile_cols)
+
 template <typename R, int COMP>
 GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, int vis_c64, const double* d_wts,
-    const double* d_uv, int uv_is_pixels, int64_t n, int tile_c = TILE_C_DEFAULT, GridLaunch<R>* defer = nullptr)
+    const double* d_uv, int uv_is_pixels, int64_t n, int tile_c = TILE_C_DEFAULT, GridLaunch<R>* defer = nullptr,
+    bool cols = false)
 {
     if (tile_c != 32 && tile_c != 16)
         fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32");
@@ -660,7 +665,15 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         };
         const bool b = s.beam != 0;
         const bool t32 = tile_c == 32;
-        if (kind == GK_WPROJ)
+        // the column-packed gridder needs one footprint segment per axis and tile
+        const bool use_cols = cols && kind != GK_EXACT && N >= 2 * (2 * conv_support + 1 + 32) + 2;
+        if (use_cols && kind == GK_WPROJ)
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32, true>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16, true>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32, true>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16, true>));
+        else if (use_cols)
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, true, 32, true>) : launch(k_grid_tiles<R, COMP, KM_SEP, true, 16, true>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, false, 32, true>) : launch(k_grid_tiles<R, COMP, KM_SEP, false, 16, true>));
+        else if (kind == GK_WPROJ)
             b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16>))
               : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16>));
         else if (kind == GK_EXACT)
@@ -818,6 +831,13 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     const int precision = sizeof(R) == 8 ? STPGPU_FP64 : (COMP ? STPGPU_FP32C : STPGPU_FP32);
     const std::string cls = size_class(s, precision);
     GridOut g;
+    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c pins the tile width and gridder
+    // form (c: column-packed) instead of the autotuner's choice
+    if (const char* pin = std::getenv("STPGPU_GRIDDER_LAYOUT")) {
+        const int w = std::atoi(pin);
+        if (w == 16 || w == 32)
+            c->tune[cls] = w | (std::strchr(pin, 'c') ? kLayoutCols : 0);
+    }
     auto it = c->tune.find(cls);
     // Device-pointer calls that repeat the previous call exactly (parameters,
     // sizes, buffers) replay a CUDA graph of the gridding, FFT and
@@ -845,7 +865,8 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     } else if (repeat && it != c->tune.end()) {
         STPGPU_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, it->second & 0xff);
+            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, it->second & 0xff, nullptr,
+                (it->second & kLayoutCols) != 0);
             finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
         } catch (...) {
             cudaGraph_t dead = nullptr;
@@ -860,28 +881,40 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
         c->single_g = g;
     } else if (it != c->tune.end() || c->timing) {
-        g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n,
-            it != c->tune.end() ? (it->second & 0xff) : TILE_C_DEFAULT);
+        const int lay = it != c->tune.end() ? it->second : TILE_C_DEFAULT;
+        g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
+            (lay & kLayoutCols) != 0);
     } else {
         for (auto& e : c->tev)
             if (!e)
                 STPGPU_CUDA_TRY(cudaEventCreate(&e));
         // an untimed pass first grows every buffer (16 columns: the most
-        // tiles) and fills the cached tables, so neither timed pass pays that
-        float ms[2] = { 0.f, 0.f };
-        const int widths[2] = { 32, 16 };
+        // tiles) and fills the cached tables, so no timed pass pays that
+        // the column-packed form is a candidate for large kernels only (with
+        // K <= 17 the lane-per-item form is faster on every measured workload)
+        const int lays[4] = { 32, 16, 32 | kLayoutCols, 16 | kLayoutCols };
+        float ms[4] = { 0.f, 0.f, 1e30f, 1e30f };
+        const int ncand = (2 * (s.nplanes > 0 ? s.max_support : s.support) + 1) > 17 ? 4 : 2;
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, 16);
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < ncand; k++) {
             STPGPU_CUDA_TRY(cudaEventRecord(c->tev[0], c->stream));
-            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, widths[k]);
+            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lays[k] & 0xff, nullptr,
+                (lays[k] & kLayoutCols) != 0);
             STPGPU_CUDA_TRY(cudaEventRecord(c->tev[1], c->stream));
             STPGPU_CUDA_TRY(cudaEventSynchronize(c->tev[1]));
             STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms[k], c->tev[0], c->tev[1]));
         }
-        c->tune[cls] = ms[1] < ms[0] ? 16 : 32;
+        int best = 0;
+        for (int k = 1; k < ncand; k++)
+            if (ms[k] < ms[best])
+                best = k;
+        c->tune[cls] = lays[best];
         if (std::getenv("STPGPU_LOG_TUNING"))
-            std::fprintf(stderr, "stpgpu tile tuner: %s  32 cols %.3f ms  16 cols %.3f ms  -> %d (single call)\n",
-                cls.c_str(), double(ms[0]), double(ms[1]), c->tune[cls]);
+            std::fprintf(stderr,
+                "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, column-packed 32/16 %.3f/%.3f ms"
+                " -> %d%s (single call)\n",
+                cls.c_str(), double(ms[0]), double(ms[1]), double(ms[2]), double(ms[3]), lays[best] & 0xff,
+                (lays[best] & kLayoutCols) ? " column-packed" : "");
     }
     if (!(repeat && c->single_exec))
         finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
@@ -894,8 +927,9 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         ImagerSetup s64 = s;
         s64.full_wsort = 1;
         auto t = c->tune.find(cls);
-        g = run_gridder<R, COMP>(c, s64, d_vis, vis_c64, d_wts, d_uvw, 0, n,
-            t != c->tune.end() ? (t->second & 0xff) : TILE_C_DEFAULT);
+        const int lay = t != c->tune.end() ? t->second : TILE_C_DEFAULT;
+        g = run_gridder<R, COMP>(c, s64, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
+            (lay & kLayoutCols) != 0);
         finish_imager<R>(c, s64, image_size, correction, g, d_image, d_beam, out_f32);
         sb = read_back(c, g);
     }
@@ -1041,9 +1075,6 @@ void launch_grid_batch(cudaStream_t st, size_t smem, const BatchGridParams<R>& P
     STPGPU_CHECK_LAUNCH();
 }
 
-// Tuned gridder layout: tile width (32 or 16 grid columns) and whether the
-// batch gridder is persistent, packed as width | persistent << 8.
-constexpr int kLayoutPersist = 1 << 8;
 
 template <typename R, int COMP, int KMODE>
 void launch_mode(cudaStream_t st, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total, bool cap)

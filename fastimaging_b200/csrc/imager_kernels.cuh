@@ -832,14 +832,210 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
     }
 }
 
+// In-tile part of one footprint axis: taps t in [lo, hi) of raw index
+// base + t land on tile positions base + t + shift - origin.  `wrap_pos`:
+// raw indices >= N map to raw - N; `wrap_neg`: raw < 0 map to raw + N (else
+// they are dropped); only positions < limit exist.  Assumes N is large
+// against K + the tile size, so that at most one of the three candidate
+// segments meets the tile.
+__device__ __forceinline__ void tile_span(int base, int K, int N, int origin, int width, int limit, bool wrap_neg,
+    int& lo, int& hi, int& shift)
+{
+    const int top = min(origin + width, limit); // tile positions [origin, top)
+    // non-wrapped raw in [0, N)
+    lo = max(max(origin - base, -base), 0);
+    hi = min(min(top - base, N - base), K);
+    shift = 0;
+    if (lo < hi)
+        return;
+    // raw >= N -> raw - N
+    lo = max(max(origin + N - base, N - base), 0);
+    hi = min(top + N - base, K);
+    shift = -N;
+    if (lo < hi)
+        return;
+    if (wrap_neg) { // raw < 0 -> raw + N
+        lo = max(origin - N - base, 0);
+        hi = min(min(top - N - base, -base), K);
+        shift = N;
+        if (lo < hi)
+            return;
+    }
+    lo = hi = 0;
+}
+
+// Column-packed tile gridder (tabulated kernels).  One warp per tile.  Each
+// list entry (item, mirrored bit) is clipped to the tile: in-tile taps rows
+// [ilo, ihi) x columns [jlo, jhi).  A round packs the in-tile columns of
+// several entries side by side into the 32 lanes (lane = one column of one
+// entry) and walks their rows in lock-step, so lanes are spent on in-tile taps
+// only.  Lanes whose cells coincide in one step (two entries of a round
+// overlapping) are serialised by __match_any_sync; consecutive steps are
+// ordered by __syncwarp.  Requires N >= 2 (Kmax + tile) + 2 (one segment per
+// axis and tile); smaller grids use grid_tile.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
+__device__ __forceinline__ void grid_tile_cols(const GridParams<R>& p, int tile, unsigned char* smem_raw)
+{
+    using A = Acc<R, COMP>;
+    using C2 = typename Cplx<R>::T;
+    A* acc = reinterpret_cast<A*>(smem_raw);
+    A* bacc = acc + (BEAM ? TILE_R * TILE_C : 0);
+    R* tab = reinterpret_cast<R*>(acc + (BEAM ? 2 : 1) * TILE_R * TILE_C);
+    __shared__ int owner[32];
+    const int lane = threadIdx.x;
+    const int gN = p.N, grows = p.image_rows, gos = p.os;
+    const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
+    const int r0 = tr * TILE_R, c0 = tc * TILE_C;
+
+    for (int t = lane; t < TILE_R * TILE_C; t += 32) {
+        acc_zero(&acc[t]);
+        if (BEAM)
+            acc_zero(&bacc[t]);
+    }
+    if (KMODE == KM_SEP) {
+        const int K = 2 * p.support + 1;
+        for (int t = lane; t < p.cs * K; t += 32)
+            tab[t] = p.k1d[t];
+    }
+    __syncwarp();
+
+    const uint32_t beg = p.tile_off[tile], end = p.tile_off[tile + 1];
+    for (uint32_t base = beg; base < end; base += 32) {
+        // this lane's entry, clipped to the tile
+        const uint32_t e = base + lane;
+        int K = 1, ilo = 0, nrows = 0, jlo = 0, ncols = 0, rowb = 0, colb = 0;
+        uint32_t koff = 0; // W-proj: table offset of the item's K x K kernel; separable: cpy*K << 16 | cpx*K
+        R vr = R(0), vi = R(0), wt = R(0);
+        int conj = 0;
+        if (e < end) {
+            const uint32_t code = p.list[e];
+            const uint32_t idx = code >> 1;
+            const int mir = int(code & 1u);
+            const Item<R> it = p.items[idx];
+            int cx, cy;
+            item_centre(it, mir, gN, cx, cy);
+            const int S = (KMODE == KM_WPROJ) ? p.plane_support[it.plane] : p.support;
+            K = 2 * S + 1;
+            int cpx = it.cpx, cpy = it.cpy;
+            if (mir && gos > 1) {
+                cpx = gos - cpx;
+                cpy = gos - cpy;
+            }
+            const int rb = cy - S, cb = cx - S;
+            int ihi, jhi, rsh, csh;
+            tile_span(rb, K, gN, r0, TILE_R, grows, false, ilo, ihi, rsh);
+            tile_span(cb, K, gN, c0, TILE_C, gN, true, jlo, jhi, csh);
+            nrows = max(ihi - ilo, 0);
+            ncols = nrows > 0 ? max(jhi - jlo, 0) : 0;
+            rowb = rb + rsh - r0; // local row of tap i: rowb + i
+            colb = cb + csh - c0; // local column of tap j: colb + j
+            vr = it.vr;
+            vi = mir ? -it.vi : it.vi;
+            wt = it.w;
+            if (KMODE == KM_WPROJ) {
+                conj = (it.flags >> (mir ? 1 : 0)) & 1u;
+                koff = p.wk_off[it.plane] + uint32_t((cpy * p.cs + cpx) * K * K);
+            } else {
+                koff = (uint32_t(cpy * K) << 16) | uint32_t(cpx * K);
+            }
+        }
+        const R vrw = vr * wt, viw = vi * wt;
+        bool pending = ncols > 0;
+        while (__any_sync(0xffffffffu, pending)) {
+            // pack a prefix of the pending entries into the lanes
+            const int x = pending ? ncols : 0;
+            int incl = x;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += y;
+            }
+            const bool take = pending && incl <= 32;
+            const int off = incl - x;
+            if (take)
+                for (int t = 0; t < ncols; t++)
+                    owner[off + t] = lane;
+            int total = take ? incl : 0, steps = take ? nrows : 0;
+            for (int o = 16; o > 0; o >>= 1) {
+                total = max(total, __shfl_xor_sync(0xffffffffu, total, o));
+                steps = max(steps, __shfl_xor_sync(0xffffffffu, steps, o));
+            }
+            __syncwarp();
+            const int own = lane < total ? owner[lane] : lane;
+            __syncwarp();
+            const bool mine = lane < total;
+            // the owner entry's parameters
+            const int o_ilo = __shfl_sync(0xffffffffu, ilo, own);
+            const int o_nrows = __shfl_sync(0xffffffffu, nrows, own);
+            const int o_jlo = __shfl_sync(0xffffffffu, jlo, own);
+            const int o_off = __shfl_sync(0xffffffffu, off, own);
+            const int o_rowb = __shfl_sync(0xffffffffu, rowb, own);
+            const int o_colb = __shfl_sync(0xffffffffu, colb, own);
+            const int o_K = __shfl_sync(0xffffffffu, K, own);
+            const uint32_t o_koff = __shfl_sync(0xffffffffu, koff, own);
+            const R o_vr = __shfl_sync(0xffffffffu, vrw, own);
+            const R o_vi = __shfl_sync(0xffffffffu, viw, own);
+            const R o_wt = BEAM ? __shfl_sync(0xffffffffu, wt, own) : R(0);
+            const int o_conj = __shfl_sync(0xffffffffu, conj, own);
+            const int j = o_jlo + (lane - o_off);
+            const int col = o_colb + j;
+            for (int st = 0; st < steps; st++) {
+                const bool act = mine && st < o_nrows;
+                const int i = o_ilo + st;
+                R kr = R(0), ki = R(0);
+                if (act) {
+                    if (KMODE == KM_WPROJ) {
+                        const C2 v = p.wk[o_koff + uint32_t(i * o_K + j)];
+                        kr = v.x;
+                        ki = o_conj ? -v.y : v.y;
+                    } else {
+                        kr = tab[(o_koff >> 16) + uint32_t(i)] * tab[(o_koff & 0xffffu) + uint32_t(j)];
+                    }
+                }
+                const int slot = col * TILE_R + (o_rowb + i);
+                bool todo = act;
+                while (__any_sync(0xffffffffu, todo)) {
+                    const unsigned peers = __match_any_sync(0xffffffffu, todo ? slot : -1 - lane);
+                    const bool lead = todo && (__ffs(peers) - 1 == lane);
+                    if (lead) {
+                        const R re = o_vr * kr - o_vi * ki;
+                        const R im = o_vr * ki + o_vi * kr;
+                        acc_rmw(&acc[slot], re, im);
+                        if (BEAM)
+                            acc_rmw(&bacc[slot], kr * o_wt, ki * o_wt);
+                    }
+                    todo = todo && !lead;
+                    __syncwarp();
+                }
+            }
+            pending = pending && !take;
+        }
+    }
+    __syncwarp();
+    const int nr = min(TILE_R, grows - r0);
+    const int nc = min(TILE_C, gN - c0);
+    for (int q = lane; q < TILE_R * TILE_C; q += 32) {
+        const int rl = q % TILE_R, cl = q / TILE_R;
+        if (rl < nr && cl < nc) {
+            const size_t g = size_t(c0 + cl) * grows + (r0 + rl);
+            p.grid[g] = acc_value(acc[q]);
+            if (BEAM)
+                p.beam[g] = acc_value(bacc[q]);
+        }
+    }
+}
+
 // One CTA (one warp) per tile of one snapshot.
 // Residency target: the shared-memory tile allows ~28 CTAs per SM at 16
 // columns (8 KB FP32/FP32C cell tile) and ~14 at 32; registers are capped to match.
-template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, bool COLS = false>
 __global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) : 14) k_grid_tiles(GridParams<R> p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    grid_tile<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
+    if constexpr (COLS && KMODE != KM_EXACT)
+        grid_tile_cols<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
+    else
+        grid_tile<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
 }
 
 // Parameters of one persistent gridder launch: up to kBatchGrid snapshots,

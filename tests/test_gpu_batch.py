@@ -99,8 +99,9 @@ def test_batch_fp32c_host_buffers_against_oracle(ctx):
         ref, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, kw["image_size"], kw["cell_size"], **okw)
         single, _ = _single(ctx, s, kw, precision=capi.FP32C)
         img = img.astype(np.float64)
-        # same arithmetic as the single-snapshot call (accumulation order may differ)
-        assert peak_rel(img, single.astype(np.float64)) < 1e-6
+        # the single-snapshot call's image up to FP32 rounding (the two paths may pick different gridder
+        # forms, so the order of the FP32 accumulations differs)
+        assert peak_rel(img, single.astype(np.float64)) < 5e-6
         # FP32 against the FP64 oracle: 1e-5, except where the analytic PSWF
         # grid correction divides the field corners by gcf(1)^2 ~ 1.6e-5,
         # which magnifies single-precision rounding of the uncorrected image

@@ -239,3 +239,28 @@ def test_repeated_device_calls_replay_graph_with_new_data(ctx):
             assert peak_rel(got, ref) < 1e-12, call
     finally:
         c2.close()
+
+
+@pytest.mark.parametrize("layout", ["32", "16", "32c", "16c"])
+@pytest.mark.parametrize("wproj", [False, True])
+def test_imager_every_gridder_layout_vs_oracle(layout, wproj, monkeypatch):
+    """Each tile width and gridder form the autotuner may pick gives the oracle's image (FP64 1e-10,
+    FP32C 1e-5); the image spans the grid edges (items near the uv origin wrap after the shift)."""
+    monkeypatch.setenv("STPGPU_GRIDDER_LAYOUT", layout)
+    s = _imager_case(61, 256, 8000, w_range=(-600.0, 600.0) if wproj else (0.0, 0.0))
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              generate_beam=not wproj)
+    if wproj:
+        kw.update(num_wplanes=5, max_wpconv_support=8, kernel_trunc_perc=1.0)
+    ref, rbeam = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    c = capi.Context(0)
+    try:
+        img, beam, _ = c.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+        assert peak_rel(img, ref) < TOL64
+        if not wproj:
+            assert peak_rel(beam, rbeam) < TOL64
+        img32, _, _ = c.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, precision=capi.FP32C,
+                                           out_dtype=capi.F32, **kw)
+        assert peak_rel(img32.astype(np.float64), ref) < TOL32
+    finally:
+        c.close()
