@@ -82,7 +82,27 @@ struct stpgpu_context {
     int batch_calls = 0;
     cudaGraph_t batch_graph = nullptr;
     cudaGraphExec_t batch_exec = nullptr;
-    std::map<std::string, int> tune;
+    // gridder layouts chosen by the autotuner, per size class; shared by the
+    // slot contexts of a server so that a class is tuned once
+    struct TuneTable {
+        std::mutex mu;
+        std::map<std::string, int> m;
+    };
+    std::shared_ptr<TuneTable> tunes = std::make_shared<TuneTable>();
+    bool tune_get(const std::string& k, int& v)
+    {
+        std::lock_guard<std::mutex> lk(tunes->mu);
+        auto it = tunes->m.find(k);
+        if (it == tunes->m.end())
+            return false;
+        v = it->second;
+        return true;
+    }
+    void tune_set(const std::string& k, int v)
+    {
+        std::lock_guard<std::mutex> lk(tunes->mu);
+        tunes->m[k] = v;
+    }
     cudaEvent_t tev[2] = { nullptr, nullptr };
     void* batch_host = nullptr;
     size_t batch_host_cap = 0;
@@ -128,6 +148,18 @@ struct stpgpu_context {
         return false;
     }
 
+    // STPGPU_LOG_ALLOC=1: one line per allocation or plan creation with its
+    // host time (allocations after warm-up are what stall a serving loop)
+    static void log_alloc(const char* what, const std::string& name, size_t bytes,
+        std::chrono::steady_clock::time_point t0)
+    {
+        static const bool on = std::getenv("STPGPU_LOG_ALLOC") != nullptr;
+        if (!on)
+            return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "stpgpu alloc: %s %s %zu bytes %.3f ms\n", what, name.c_str(), bytes, ms);
+    }
+
     // Named scratch buffer, grown on demand (steady state allocates nothing).
     template <typename T>
     T* buf(const std::string& name, size_t count)
@@ -142,7 +174,9 @@ struct stpgpu_context {
                 b.cap = 0;
             }
             const size_t want = bytes + bytes / 8;
+            const auto t0 = std::chrono::steady_clock::now();
             STPGPU_CUDA_TRY(cudaMalloc(&b.p, want));
+            log_alloc("device buffer", ns + name, want, t0);
             b.cap = want;
             memo_keys.erase(ns + name);
         }
@@ -160,7 +194,9 @@ struct stpgpu_context {
             }
             pinned = nullptr;
             pinned_cap = 0;
+            const auto t0 = std::chrono::steady_clock::now();
             STPGPU_CUDA_TRY(cudaMallocHost(&pinned, bytes));
+            log_alloc("page-locked stage", ns, bytes, t0);
             pinned_cap = bytes;
         }
         return reinterpret_cast<T*>(pinned);
@@ -175,7 +211,9 @@ struct stpgpu_context {
         if (it != plans.end())
             return it->second;
         cufftHandle h;
+        const auto t0 = std::chrono::steady_clock::now();
         cufftResult r = cufftPlan2d(&h, N, N, type);
+        log_alloc("cuFFT plan", ns + "N" + std::to_string(N), 0, t0);
         if (r != CUFFT_SUCCESS)
             fail(STPGPU_ERR_CUFFT, "cufftPlan2d failed (" + std::to_string(int(r)) + ") for N=" + std::to_string(N));
         r = cufftSetStream(h, stream);
@@ -836,9 +874,10 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     if (const char* pin = std::getenv("STPGPU_GRIDDER_LAYOUT")) {
         const int w = std::atoi(pin);
         if (w == 16 || w == 32)
-            c->tune[cls] = w | (std::strchr(pin, 'c') ? kLayoutCols : 0);
+            c->tune_set(cls, w | (std::strchr(pin, 'c') ? kLayoutCols : 0));
     }
-    auto it = c->tune.find(cls);
+    int tuned_lay = 0;
+    const bool have_tune = c->tune_get(cls, tuned_lay);
     // Device-pointer calls that repeat the previous call exactly (parameters,
     // sizes, buffers) replay a CUDA graph of the gridding, FFT and
     // normalisation kernels, captured on the first repeat; any other call
@@ -862,11 +901,11 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     if (repeat && c->single_exec) {
         STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
         g = c->single_g;
-    } else if (repeat && it != c->tune.end()) {
+    } else if (repeat && have_tune) {
         STPGPU_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         try {
-            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, it->second & 0xff, nullptr,
-                (it->second & kLayoutCols) != 0);
+            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, tuned_lay & 0xff, nullptr,
+                (tuned_lay & kLayoutCols) != 0);
             finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
         } catch (...) {
             cudaGraph_t dead = nullptr;
@@ -880,8 +919,8 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         STPGPU_CUDA_TRY(cudaGraphInstantiate(&c->single_exec, c->single_graph, 0));
         STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
         c->single_g = g;
-    } else if (it != c->tune.end() || c->timing) {
-        const int lay = it != c->tune.end() ? it->second : TILE_C_DEFAULT;
+    } else if (have_tune || c->timing) {
+        const int lay = have_tune ? tuned_lay : TILE_C_DEFAULT;
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
             (lay & kLayoutCols) != 0);
     } else {
@@ -894,8 +933,11 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         // K <= 17 the lane-per-item form is faster on every measured workload)
         const int lays[4] = { 32, 16, 32 | kLayoutCols, 16 | kLayoutCols };
         float ms[4] = { 0.f, 0.f, 1e30f, 1e30f };
-        const int ncand = (2 * (s.nplanes > 0 ? s.max_support : s.support) + 1) > 17 ? 4 : 2;
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, 16);
+        // the widest kernel the data actually uses (W-planes are truncated
+        // below the maximum support), read back from the untimed pass
+        const int used_support = s.nplanes > 0 ? std::max(read_back(c, g).max_support, 0) : s.support;
+        const int ncand = (2 * used_support + 1) > 17 ? 4 : 2;
         for (int k = 0; k < ncand; k++) {
             STPGPU_CUDA_TRY(cudaEventRecord(c->tev[0], c->stream));
             g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lays[k] & 0xff, nullptr,
@@ -908,7 +950,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         for (int k = 1; k < ncand; k++)
             if (ms[k] < ms[best])
                 best = k;
-        c->tune[cls] = lays[best];
+        c->tune_set(cls, lays[best]);
         if (std::getenv("STPGPU_LOG_TUNING"))
             std::fprintf(stderr,
                 "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, column-packed 32/16 %.3f/%.3f ms"
@@ -926,8 +968,8 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         // rare data (many distinct |w| within one single-precision step): redo with the 64-bit |w| sort
         ImagerSetup s64 = s;
         s64.full_wsort = 1;
-        auto t = c->tune.find(cls);
-        const int lay = t != c->tune.end() ? t->second : TILE_C_DEFAULT;
+        int lay = TILE_C_DEFAULT;
+        c->tune_get(cls, lay);
         g = run_gridder<R, COMP>(c, s64, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
             (lay & kLayoutCols) != 0);
         finish_imager<R>(c, s64, image_size, correction, g, d_image, d_beam, out_f32);
@@ -1331,7 +1373,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         // tile autotuner: time both tile widths for classes not seen before
         std::vector<std::string> fresh;
         for (auto& b : B)
-            if (!c->tune.count(b.cls) && std::find(fresh.begin(), fresh.end(), b.cls) == fresh.end())
+            if (int v; !c->tune_get(b.cls, v) && std::find(fresh.begin(), fresh.end(), b.cls) == fresh.end())
                 fresh.push_back(b.cls);
         if (!fresh.empty()) {
             const int layouts[4] = { 32, 16, 32 | kLayoutPersist, 16 | kLayoutPersist };
@@ -1341,7 +1383,8 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
                     STPGPU_CUDA_TRY(cudaEventCreate(&c->pev[k]));
             for (int cand = 0; cand < 4; cand++) {
                 for (auto& b : B) {
-                    const int lay = c->tune.count(b.cls) ? c->tune[b.cls] : layouts[cand];
+                    int lay = layouts[cand];
+                    c->tune_get(b.cls, lay);
                     b.tile_c = lay & 0xff;
                     b.persist = (lay & kLayoutPersist) ? 1 : 0;
                 }
@@ -1354,7 +1397,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
                 for (int cand = 1; cand < 4; cand++)
                     if (t[cand][cls] < t[best][cls])
                         best = cand;
-                c->tune[cls] = layouts[best];
+                c->tune_set(cls, layouts[best]);
                 if (log_tuning)
                     std::fprintf(stderr,
                         "stpgpu gridder tuner: %s  32/16 cols %.3f/%.3f ms, persistent %.3f/%.3f ms -> %d%s\n",
@@ -1364,8 +1407,10 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             tuned = int(fresh.size());
         }
         for (auto& b : B) {
-            b.tile_c = c->tune[b.cls] & 0xff;
-            b.persist = (c->tune[b.cls] & kLayoutPersist) ? 1 : 0;
+            int lay = TILE_C_DEFAULT;
+            c->tune_get(b.cls, lay);
+            b.tile_c = lay & 0xff;
+            b.persist = (lay & kLayoutPersist) ? 1 : 0;
         }
         bool capturable = true;
         for (auto& b : B)
@@ -2282,8 +2327,10 @@ void serve_request(stpgpu_context* c, const stpgpu_request& r, stpgpu_result& re
     const int64_t npix = int64_t(image_size) * image_size;
     const size_t ob = f32 ? 4 : 8;
     void* dimg = c->buf<unsigned char>("srv_img", ob * size_t(std::max<int64_t>(npix, 1)));
+    const auto t_in = std::chrono::steady_clock::now();
     run_imager<R, COMP>(c, s, image_size, r.pars.gridding_correction, dv, c64, dw, duvw, n, dimg, nullptr, f32,
         &res.imager);
+    const auto t_img = std::chrono::steady_clock::now();
     if (res.imager.image_size > 0) {
         if (r.image)
             STPGPU_CUDA_TRY(cudaMemcpyAsync(r.image, dimg, ob * npix, cudaMemcpyDeviceToHost, c->stream));
@@ -2306,6 +2353,15 @@ void serve_request(stpgpu_context* c, const stpgpu_request& r, stpgpu_result& re
         }
     }
     STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    // STPGPU_LOG_SLOW=<ms>: host-side phase times of requests slower than that
+    static const char* slow = std::getenv("STPGPU_LOG_SLOW");
+    if (slow) {
+        const auto t_end = std::chrono::steady_clock::now();
+        auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+        if (ms(t_in, t_end) > std::atof(slow))
+            std::fprintf(stderr, "stpgpu slow request: N=%d n_vis=%lld imager %.3f ms, source finder %.3f ms\n",
+                image_size, (long long)n, ms(t_in, t_img), ms(t_img, t_end));
+    }
 }
 
 } // namespace
@@ -2414,6 +2470,8 @@ stpgpu_status stpgpu_server_create(const stpgpu_server_pars* pars, stpgpu_server
             delete sv;
             return s;
         }
+        if (!sv->slots.empty())
+            c->tunes = sv->slots[0]->tunes; // a size class is tuned once for all slots
         sv->slots.push_back(c);
     }
     for (int k = 0; k < pars->slots; k++)
