@@ -424,16 +424,10 @@ def run_serving(rates=(10.0, 50.0, 100.0, 200.0), seconds=3.0, slots=4):
     for rate in rates:
         srv = capi.Server(slots=slots, hbm_budget_bytes=64 << 30, precision=capi.FP32C)
         try:
-            # warm-up: one request per template alone (the slots share the gridder tuning of each size
-            # class), then the pool a few times concurrently so that every slot has grown its plans, tables
-            # and buffers before the arrivals start
+            # warm-up: every template once on every slot (buffers, cuFFT plans, gridder tuning), so that
+            # the timed arrivals allocate nothing
             for (v, w, uvw), kw, _ in pool:
-                srv.wait(srv.submit(v, w, uvw, find_sources=True, want_image=False, **kw))
-            for _ in range(slots):
-                warm = [srv.submit(v, w, uvw, find_sources=True, want_image=False, **kw)
-                        for (v, w, uvw), kw, _ in pool]
-                for t in warm:
-                    srv.wait(t)
+                srv.prepare(v, w, uvw, find_sources=True, want_image=False, **kw)
             n_req = max(4, int(rate * seconds))
             gaps = rng.exponential(1.0 / rate, size=n_req)
             picks = rng.integers(0, len(pool), size=n_req)

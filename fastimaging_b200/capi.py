@@ -137,7 +137,7 @@ class ServerStats(ctypes.Structure):
 EXPORTED = ["stpgpu_abi_version", "stpgpu_create", "stpgpu_destroy", "stpgpu_last_error", "stpgpu_stream",
             "stpgpu_set_timing", "stpgpu_trim", "stpgpu_image_visibilities", "stpgpu_image_visibilities_ex", "stpgpu_convolve_to_grid",
             "stpgpu_source_find", "stpgpu_source_find_ex", "stpgpu_model_visibilities", "stpgpu_image_batch", "stpgpu_server_create",
-            "stpgpu_server_destroy", "stpgpu_server_submit", "stpgpu_server_wait", "stpgpu_server_stats_get",
+            "stpgpu_server_destroy", "stpgpu_server_submit", "stpgpu_server_prepare", "stpgpu_server_wait", "stpgpu_server_stats_get",
             "stpgpu_label_noalloc"]
 NOALLOC_MAX_PIXELS = 1024 * 1024
 
@@ -186,6 +186,7 @@ def load():
         L.stpgpu_server_create.argtypes = [ctypes.POINTER(ServerPars), ctypes.POINTER(vp)]
         L.stpgpu_server_destroy.argtypes = [vp]
         L.stpgpu_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]
+        L.stpgpu_server_prepare.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(Result)]
         L.stpgpu_server_wait.argtypes = [vp, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(Result)]
         L.stpgpu_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
         L.stpgpu_label_noalloc.argtypes = [ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
@@ -426,6 +427,31 @@ class Server:
         sf: dict of source_find keywords (detection_n_sigma, analysis_n_sigma, ...).
         Inputs: numpy arrays (uvw (n, 3)), or page-locked torch CPU tensors
         (vis complex (n,), weights (n,), uvw (3, n) contiguous).  Returns a ticket."""
+        req, keep = self._request(vis, weights, uvw, find_sources, out_dtype, sf, want_labels, island_capacity,
+                                  want_image, imager_kw)
+        t = ctypes.c_int64()
+        st = self.L.stpgpu_server_submit(self.h, ctypes.byref(req), ctypes.byref(t))
+        if st != 0:
+            raise StpGpuError(st, "submit")
+        self._keep[t.value] = keep
+        return t.value
+
+    def prepare(self, vis, weights, uvw, find_sources=False, out_dtype=F32, sf=None, want_labels=False,
+                island_capacity=4096, want_image=True, **imager_kw):
+        """Run a request (the arguments of submit) once on every slot while
+        admission is held, so that requests of its size class admitted later
+        allocate, plan and tune nothing.  -> Result of the last slot."""
+        req, _keep = self._request(vis, weights, uvw, find_sources, out_dtype, sf, want_labels, island_capacity,
+                                    want_image, imager_kw)
+        res = Result()
+        st = self.L.stpgpu_server_prepare(self.h, ctypes.byref(req), ctypes.byref(res))
+        if st != 0:
+            raise StpGpuError(st, res.error.decode(errors="replace"))
+        return res
+
+    @staticmethod
+    def _request(vis, weights, uvw, find_sources, out_dtype, sf, want_labels, island_capacity, want_image,
+                 imager_kw):
         if hasattr(vis, "data_ptr"):
             n = int(weights.numel())
             vdt = C64 if str(vis.dtype).endswith("complex64") else C128
@@ -455,12 +481,7 @@ class Server:
         req = Request(_ptr(vis), vdt, int(out_dtype), _ptr(w), _ptr(uvwF), n,
                       ip, wp, _ptr(img), int(bool(find_sources)), int(island_capacity), sp, _ptr(labels),
                       ctypes.cast(isl, ctypes.c_void_p))
-        t = ctypes.c_int64()
-        st = self.L.stpgpu_server_submit(self.h, ctypes.byref(req), ctypes.byref(t))
-        if st != 0:
-            raise StpGpuError(st, "submit")
-        self._keep[t.value] = (vis, w, uvwF, img, labels, isl, req)
-        return t.value
+        return req, (vis, w, uvwF, img, labels, isl, req)
 
     def wait(self, ticket, timeout_s=-1.0):
         """-> (image, label_map or None, [Island], Result); raises on failure."""

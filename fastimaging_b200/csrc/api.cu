@@ -2377,6 +2377,7 @@ struct stpgpu_server {
     int64_t next_ticket = 1;
     int64_t inflight = 0, inflight_bytes = 0;
     bool stop = false;
+    int paused = 0; // stpgpu_server_prepare holds the slots: no admission
     std::chrono::steady_clock::time_point t0;
     std::vector<double> latency_ms;
     double first_submit = -1.0, last_done = 0.0;
@@ -2396,13 +2397,14 @@ struct stpgpu_server {
             {
                 std::unique_lock<std::mutex> lk(mu);
                 // first-in first-out: the head starts once its working set fits
-                cv_work.wait(lk, [&] {
-                    return stop
-                        || (!queue.empty() && inflight_bytes + queue.front()->res.est_bytes <= pars.hbm_budget_bytes);
-                });
+                auto admissible = [&] {
+                    return !paused && !queue.empty()
+                        && inflight_bytes + queue.front()->res.est_bytes <= pars.hbm_budget_bytes;
+                };
+                cv_work.wait(lk, [&] { return stop || admissible(); });
                 if (queue.empty() && stop)
                     return;
-                if (queue.empty() || inflight_bytes + queue.front()->res.est_bytes > pars.hbm_budget_bytes)
+                if (!admissible())
                     continue;
                 job = queue.front();
                 queue.pop_front();
@@ -2498,11 +2500,12 @@ stpgpu_status stpgpu_server_destroy(stpgpu_server* sv)
     return STPGPU_OK;
 }
 
-stpgpu_status stpgpu_server_submit(stpgpu_server* sv, const stpgpu_request* r, int64_t* ticket)
+namespace {
+
+// Parameter checks of a request and its working-set estimate.
+stpgpu_status check_request(const stpgpu_server* sv, const stpgpu_request* r, int64_t& est)
 {
-    if (!sv || !r || !ticket)
-        return STPGPU_ERR_INVALID_ARG;
-    int64_t est = 0;
+    est = 0;
     try {
         int image_size = 0;
         ImagerSetup s = setup_from(&r->pars, &r->wproj, nullptr, image_size);
@@ -2523,6 +2526,18 @@ stpgpu_status stpgpu_server_submit(stpgpu_server* sv, const stpgpu_request* r, i
     }
     if (est > sv->pars.hbm_budget_bytes)
         return STPGPU_ERR_OOM;
+    return STPGPU_OK;
+}
+
+} // namespace
+
+stpgpu_status stpgpu_server_submit(stpgpu_server* sv, const stpgpu_request* r, int64_t* ticket)
+{
+    if (!sv || !r || !ticket)
+        return STPGPU_ERR_INVALID_ARG;
+    int64_t est = 0;
+    if (const stpgpu_status bad = check_request(sv, r, est))
+        return bad;
     auto job = std::make_unique<ServerJob>();
     job->req = *r;
     job->res.est_bytes = est;
@@ -2539,6 +2554,53 @@ stpgpu_status stpgpu_server_submit(stpgpu_server* sv, const stpgpu_request* r, i
     }
     sv->cv_work.notify_all();
     return STPGPU_OK;
+}
+
+stpgpu_status stpgpu_server_prepare(stpgpu_server* sv, const stpgpu_request* r, stpgpu_result* out)
+{
+    if (!sv || !r)
+        return STPGPU_ERR_INVALID_ARG;
+    stpgpu_result res {};
+    if (const stpgpu_status bad = check_request(sv, r, res.est_bytes))
+        return bad;
+    {
+        // hold admission and let the requests in flight finish: the slots'
+        // contexts are then free for this thread
+        std::unique_lock<std::mutex> lk(sv->mu);
+        sv->paused++;
+        sv->cv_done.wait(lk, [&] { return sv->inflight == 0; });
+    }
+    stpgpu_status status = STPGPU_OK;
+    for (stpgpu_context* c : sv->slots) {
+        cudaSetDevice(c->device);
+        res = stpgpu_result {};
+        status = guard(c, [&] {
+            switch (sv->pars.precision) {
+            case STPGPU_FP64:
+                serve_request<double, 0>(c, *r, res);
+                break;
+            case STPGPU_FP32:
+                serve_request<float, 0>(c, *r, res);
+                break;
+            default:
+                serve_request<float, 1>(c, *r, res);
+                break;
+            }
+        });
+        if (status != STPGPU_OK) {
+            std::snprintf(res.error, sizeof(res.error), "%s", c->err.c_str());
+            break;
+        }
+    }
+    res.status = status;
+    if (out)
+        *out = res;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->paused--;
+    }
+    sv->cv_work.notify_all();
+    return status;
 }
 
 stpgpu_status stpgpu_server_wait(stpgpu_server* sv, int64_t ticket, double timeout_s, stpgpu_result* out)

@@ -343,6 +343,15 @@ STPGPU_API stpgpu_status stpgpu_server_destroy(stpgpu_server* server);
 /* Queue a request; *ticket identifies it.  STPGPU_ERR_OOM when its working
  * set alone exceeds the budget; STPGPU_ERR_INVALID_ARG for bad parameters. */
 STPGPU_API stpgpu_status stpgpu_server_submit(stpgpu_server* server, const stpgpu_request* request, int64_t* ticket);
+/* Run a request once on every slot, in the calling thread, while admission
+ * is held (queued requests wait; the requests in flight finish first).  Each
+ * slot then holds the buffers, cuFFT plans and tuned gridder layout of the
+ * request's size class, so requests of that class admitted later pay no
+ * allocation, plan creation or tuning (which can stall every slot on the
+ * device for up to a second).  Outputs go to the request's buffers; *result
+ * (nullable) holds the last slot's outcome.  Not counted in the statistics. */
+STPGPU_API stpgpu_status stpgpu_server_prepare(stpgpu_server* server, const stpgpu_request* request,
+    stpgpu_result* result);
 /* Wait up to timeout_s (< 0: forever) for a ticket; STPGPU_ERR_TIMEOUT if it
  * is not done by then (the ticket stays valid).  On success *result holds
  * the request's outcome and the ticket is released. */

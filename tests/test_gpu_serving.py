@@ -144,3 +144,26 @@ def test_request_larger_than_budget_is_rejected():
         assert e.value.status == 5
     finally:
         srv.close()
+
+
+def test_prepare_warms_every_slot_and_is_not_counted():
+    reqs = _requests()
+    srv = capi.Server(slots=3, precision=capi.FP64)
+    try:
+        # a request in flight while prepare holds admission
+        s0, kw0 = reqs[0]
+        t0 = srv.submit(s0.vis, s0.weights, s0.uvw, find_sources=True, out_dtype=capi.F64, **kw0)
+        s, kw = reqs[3]
+        res = srv.prepare(s.vis, s.weights, s.uvw, find_sources=True, out_dtype=capi.F64, **kw)
+        assert res.status == 0 and res.imager.image_size == kw["image_size"]
+        img, _, isl, r = srv.wait(t0)
+        assert r.status == 0
+        t = srv.submit(s.vis, s.weights, s.uvw, find_sources=True, out_dtype=capi.F64, **kw)
+        _, _, isl3, r3 = srv.wait(t)
+        st = srv.stats()
+    finally:
+        srv.close()
+    assert st.submitted == 2 and st.completed == 2
+    # the prepared request's outcome is the served one's
+    assert r3.n_islands == res.n_islands and r3.sf.n_labels_pos == res.sf.n_labels_pos
+    assert r3.imager.n_good_vis == res.imager.n_good_vis
