@@ -18,6 +18,7 @@ LIB_PATH = os.path.join(PKG, "libstpgpu.so")
 # enums (src/stp/types.h:32-89)
 TopHat, Triangle, Sinc, Gaussian, GaussianSinc, PSWF = range(6)
 ZEROMEDIAN, BINMEDIAN, BINAPPROX, NTHELEMENT = range(4)
+LINEAR, CUBIC, COSINE = range(3)  # InterpType of the Hankel-transform W-kernels
 FP64, FP32, FP32C = 0, 1, 2
 C128, C64 = 0, 1
 F64, F32 = 0, 1
@@ -98,13 +99,13 @@ class BatchInfo(ctypes.Structure):
 def imager_pars(image_size, cell_size, padding_factor=1.0, kernel_func=PSWF, kernel_support=3, kernel_exact=True,
                 oversampling=8, generate_beam=False, gridding_correction=True, analytic_gcf=False, num_wplanes=0,
                 wplanes_median=False, max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0,
-                padded_image_size=0, **_):
+                padded_image_size=0, hankel_opt=False, hankel_proj_slice=False, interp_type=LINEAR, **_):
     """(ImagerPars, WProjPars) from image_visibilities-style keywords."""
     ip = ImagerPars(int(image_size), int(padded_image_size), float(cell_size), float(padding_factor),
                     int(kernel_func), int(kernel_support), int(bool(kernel_exact)), int(oversampling),
                     int(bool(generate_beam)), int(bool(gridding_correction)), int(bool(analytic_gcf)), 0)
-    wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc), 0, 0,
-                   0, int(bool(wplanes_median)))
+    wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc),
+                   int(bool(hankel_opt)), int(bool(hankel_proj_slice)), int(interp_type), int(bool(wplanes_median)))
     return ip, wp
 
 
@@ -242,8 +243,8 @@ class Context:
                            kernel_support=3, kernel_exact=True, oversampling=8, generate_beam=False,
                            gridding_correction=True, analytic_gcf=False, num_wplanes=0, wplanes_median=False,
                            max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, hankel_opt=False,
-                           aproj_numtimesteps=0, precision=FP64, out_dtype=F64, padded_image_size=0,
-                           device_ptrs=False, image_out=None, beam_out=None):
+                           hankel_proj_slice=False, interp_type=LINEAR, aproj_numtimesteps=0, precision=FP64,
+                           out_dtype=F64, padded_image_size=0, device_ptrs=False, image_out=None, beam_out=None):
         """stp::image_visibilities semantics (sizes used as given).
 
         Host mode: numpy inputs (vis complex128/complex64 (n,), weights (n,),
@@ -255,7 +256,8 @@ class Context:
                         int(kernel_func), int(kernel_support), int(bool(kernel_exact)), int(oversampling),
                         int(bool(generate_beam)), int(bool(gridding_correction)), int(bool(analytic_gcf)), 0)
         wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc),
-                       int(bool(hankel_opt)), 0, 0, int(bool(wplanes_median)))
+                       int(bool(hankel_opt)), int(bool(hankel_proj_slice)), int(interp_type),
+                       int(bool(wplanes_median)))
         ap = AProjPars(int(aproj_numtimesteps), 0.0, 0.0, 0, 0.0)
         info = ImagerInfo()
         if device_ptrs:

@@ -294,6 +294,7 @@ struct ImagerSetup {
     int nplanes = 0, max_support = 0, undersampling = 1, wmedian = 0;
     double trunc_perc = 0.0;
     int full_wsort = 0; // |w| order from the 64-bit sort (fallback of the 32-bit sort + run fix-up)
+    int hankel = 0, proj_slice = 0, cubic = 0; // Hankel-transform W-kernels (hankel_opt)
 };
 
 // W-projection with a maximum support above 32: the W-kernel tables and tile
@@ -562,13 +563,29 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         // WideFieldImaging gets real_t(arc_sec_to_rad(cell)), scaled by N/workarea
         wq.scaled_cell = arc_sec_to_rad(s.cell_size) * scaling;
         wq.trunc_perc = s.trunc_perc;
-        wq.Qs = c->buf<double2>("wkQ", size_t(P) * half * half);
-        wq.Ts = c->buf<double2>("wkT", size_t(P) * Lh * half);
+        if (!s.hankel) {
+            wq.Qs = c->buf<double2>("wkQ", size_t(P) * half * half);
+            wq.Ts = c->buf<double2>("wkT", size_t(P) * Lh * half);
+        }
         wq.convd = c->buf<double2>("wkconv", size_t(P) * Lh * Lh);
         wq.invd = c->buf<double>("wkinv", size_t(P) * cs * cs);
         plane_support = c->buf<int>("psupport", P);
         wq.support = plane_support;
-        k_wkernel_plane<<<P, 1024, 0, st>>>(wq);
+        if (s.hankel) {
+            HankelParams hq {};
+            hq.n = s.proj_slice ? arr : arr / 2;
+            if (hq.n < 3)
+                fail(STPGPU_ERR_INVALID_ARG, "Hankel transform needs more than 2 radial samples");
+            hq.proj_slice = s.proj_slice;
+            hq.cubic = s.cubic;
+            hq.R = c->buf<double2>("hkR", size_t(P) * half);
+            hq.Y = c->buf<double2>("hkY", size_t(P) * hq.n);
+            hq.B = c->buf<double2>("hkB", size_t(P) * hq.n);
+            hq.Cp = c->buf<double>("hkC", size_t(P) * 2 * hq.n);
+            k_hankel_plane<<<P, 1024, 0, st>>>(wq, hq);
+        } else {
+            k_wkernel_plane<<<P, 1024, 0, st>>>(wq);
+        }
         STPGPU_CHECK_LAUNCH();
         // per-offset K x K tables in the gridder's precision: worst-case
         // capacity (every plane at the maximum support), or with large
@@ -1000,8 +1017,6 @@ ImagerSetup setup_from(const stpgpu_imager_pars* p, const stpgpu_wproj_pars* w, 
         fail(STPGPU_ERR_INVALID_ARG, "null imager parameters");
     if (a && a->num_timesteps > 0)
         fail(STPGPU_ERR_UNSUPPORTED, "A-projection is outside the GPU path");
-    if (w && w->num_wplanes > 0 && w->hankel_opt)
-        fail(STPGPU_ERR_UNSUPPORTED, "Hankel-transform W-kernels are outside the GPU path");
     if (p->kernel_function < 0 || p->kernel_function > 5)
         fail(STPGPU_ERR_INVALID_ARG, "unknown kernel function");
     if (!(p->cell_size > 0.0))
@@ -1029,6 +1044,15 @@ ImagerSetup setup_from(const stpgpu_imager_pars* p, const stpgpu_wproj_pars* w, 
         s.undersampling = w->undersampling_opt;
         s.trunc_perc = w->kernel_trunc_perc;
         s.wmedian = w->wplanes_median;
+        if (w->hankel_opt) {
+            // InterpType (types.h:55-59): LINEAR 0, CUBIC 1, COSINE 2 (interpolated linearly,
+            // aw_projection.cpp:263-266)
+            if (w->interp_type < 0 || w->interp_type > 2)
+                fail(STPGPU_ERR_INVALID_ARG, "unknown interp_type");
+            s.hankel = 1;
+            s.proj_slice = w->hankel_proj_slice ? 1 : 0;
+            s.cubic = w->interp_type == 1;
+        }
     }
     if (!p->kernel_exact && p->oversampling < 1)
         fail(STPGPU_ERR_INVALID_ARG, "oversampling must be >= 1 when kernel_exact is false");
@@ -2182,8 +2206,6 @@ stpgpu_status stpgpu_convolve_to_grid(stpgpu_context* c, int kernel_function, do
         if (wp) {
             if (!w)
                 fail(STPGPU_ERR_INVALID_ARG, "W-projection needs w");
-            if (wproj->hankel_opt)
-                fail(STPGPU_ERR_UNSUPPORTED, "Hankel-transform W-kernels are outside the GPU path");
             if (!(cell_size > 0.0))
                 fail(STPGPU_ERR_INVALID_ARG, "W-projection needs cell_size > 0");
             s.nplanes = wproj->num_wplanes;
@@ -2191,6 +2213,13 @@ stpgpu_status stpgpu_convolve_to_grid(stpgpu_context* c, int kernel_function, do
             s.undersampling = wproj->undersampling_opt;
             s.trunc_perc = wproj->kernel_trunc_perc;
             s.wmedian = wproj->wplanes_median;
+            if (wproj->hankel_opt) {
+                if (wproj->interp_type < 0 || wproj->interp_type > 2)
+                    fail(STPGPU_ERR_INVALID_ARG, "unknown interp_type");
+                s.hankel = 1;
+                s.proj_slice = wproj->hankel_proj_slice ? 1 : 0;
+                s.cubic = wproj->interp_type == 1;
+            }
         }
         if (!kernel_exact && !wp && oversampling < 1)
             fail(STPGPU_ERR_INVALID_ARG, "oversampling must be >= 1");

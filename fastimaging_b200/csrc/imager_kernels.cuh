@@ -1528,6 +1528,29 @@ __device__ __forceinline__ double2 wk_value(const WkParams& q, double w, int px,
     return make_double2(re * q.aa[half + py], im * q.aa[half + py]);
 }
 
+// 1/sum(Re) of each oversampled sub-kernel of plane p (ty outer, tx inner as
+// in generate_kernel_cache, aw_projection.cpp:383-448); conv is the plane's
+// quadrant conv[|dy| * lh + |dx|].
+__device__ void wk_inverse_sums(const WkParams& q, int p, const double2* conv, int S)
+{
+    const int cs = q.cs, os = q.os, lh = q.lh_max;
+    const int K = 2 * S + 1;
+    for (int t = threadIdx.x; t < cs * cs; t += blockDim.x) {
+        const int x = t % cs, y = t / cs;
+        double ks = 0.0;
+        for (int j = 0; j < K; j++) {
+            int ox = (j - S) * os + os / 2 - x;
+            ox = ox < 0 ? -ox : ox;
+            for (int i = 0; i < K; i++) {
+                int oy = (i - S) * os + os / 2 - y;
+                oy = oy < 0 ? -oy : oy;
+                ks += conv[size_t(oy) * lh + ox].x;
+            }
+        }
+        q.invd[(size_t(p) * cs + y) * cs + x] = 1 / ks;
+    }
+}
+
 __global__ void __launch_bounds__(1024) k_wkernel_plane(WkParams q)
 {
     const int p = blockIdx.x;
@@ -1598,7 +1621,6 @@ __global__ void __launch_bounds__(1024) k_wkernel_plane(WkParams q)
     }
     __syncthreads();
     const int S = s_support;
-    const int K = 2 * S + 1;
     const int L = min(S * os + os / 2 + 1, (arr >> 1) + 1);
     // 4. T[l][a] for l < L
     for (int t = threadIdx.x; t < L * half; t += blockDim.x) {
@@ -1626,22 +1648,188 @@ __global__ void __launch_bounds__(1024) k_wkernel_plane(WkParams q)
         conv[size_t(l) * lh + k] = make_double2(re, im);
     }
     __syncthreads();
-    // 6. 1/sum(Re) of each sub-kernel (ty outer, tx inner as in the reference)
-    const int cs = q.cs;
-    for (int t = threadIdx.x; t < cs * cs; t += blockDim.x) {
-        const int x = t % cs, y = t / cs;
-        double ks = 0.0;
-        for (int j = 0; j < K; j++) {
-            int ox = (j - S) * os + os / 2 - x;
-            ox = ox < 0 ? -ox : ox;
-            for (int i = 0; i < K; i++) {
-                int oy = (i - S) * os + os / 2 - y;
-                oy = oy < 0 ? -oy : oy;
-                ks += conv[size_t(oy) * lh + ox].x;
+    wk_inverse_sums(q, p, conv, S);
+}
+
+// Hankel-transform W-kernels (hankel_opt, aw_projection.cpp:211-287 and
+// RadialInterpolate, aw_projection.h:126-214): the radially symmetric W-kernel
+// comes from a 1-D transform of the image-domain kernel's radial profile,
+// interpolated at the radius of every kernel offset.
+struct HankelParams {
+    int n;          // radial samples: arr/2 (discrete Hankel transform) or arr (projection slice)
+    int proj_slice; // hankel_proj_slice: 1-D DFT of the kernel's projection onto one axis
+    int cubic;      // InterpType::CUBIC: natural cubic spline; otherwise linear
+    double2* R;     // scratch [P][half]: radial profile or projection
+    double2* Y;     // scratch [P][n]: transform at radii 0..n-1 (oversampled uv pixels)
+    double2* B;     // scratch [P][n]: spline quadratic coefficients
+    double* Cp;     // scratch [P][2][n]: forward-sweep factors of the spline solve
+};
+
+// Cubic (natural boundary, tk::spline semantics) or linear interpolation of
+// the unit-spaced samples Y at radius r; k = min(floor(r), n - 1), beyond the
+// last sample the end segment extrapolates linearly.
+__device__ __forceinline__ double2 hankel_interp(const HankelParams& h, const double2* Y, const double2* B, double r)
+{
+    const int n = h.n;
+    const int k = min(int(r), n - 1);
+    const double t = r - double(k);
+    const double2 y = Y[k];
+    if (!h.cubic) {
+        const double2 y0 = k < n - 1 ? y : Y[n - 2];
+        const double2 y1 = k < n - 1 ? Y[k + 1] : Y[n - 1];
+        return make_double2((y1.x - y0.x) * t + y.x, (y1.y - y0.y) * t + y.y);
+    }
+    auto coef = [&](int i, double2& a, double2& b, double2& c) { // segment i < n - 1
+        const double2 b0 = B[i], b1 = B[i + 1], y0 = Y[i], y1 = Y[i + 1];
+        a = make_double2(1.0 / 3.0 * (b1.x - b0.x), 1.0 / 3.0 * (b1.y - b0.y));
+        b = b0;
+        c = make_double2((y1.x - y0.x) - 1.0 / 3.0 * (2.0 * b0.x + b1.x),
+                         (y1.y - y0.y) - 1.0 / 3.0 * (2.0 * b0.y + b1.y));
+    };
+    double2 a, b, c;
+    if (k < n - 1) {
+        coef(k, a, b, c);
+    } else {
+        // end segment: a = 0, b = b[n-1] (0 for the natural spline), c = derivative at the last node
+        double2 a2, b2, c2;
+        coef(n - 2, a2, b2, c2);
+        a = make_double2(0.0, 0.0);
+        b = B[n - 1];
+        c = make_double2(3.0 * a2.x + 2.0 * b2.x + c2.x, 3.0 * a2.y + 2.0 * b2.y + c2.y);
+    }
+    return make_double2(((a.x * t + b.x) * t + c.x) * t + y.x, ((a.y * t + b.y) * t + c.y) * t + y.y);
+}
+
+// One block per W-plane.  Writes the plane's support, its quadrant
+// conv[|dy| * lh + |dx|] = f(sqrt(dx^2 + dy^2)) and the sub-kernel
+// normalisations, the same outputs as k_wkernel_plane.
+__global__ void __launch_bounds__(1024) k_hankel_plane(WkParams q, HankelParams h)
+{
+    const int p = blockIdx.x;
+    const int half = q.half, arr = q.arr, os = q.os, lh = q.lh_max, n = h.n;
+    const double w = q.w_avg[p];
+    double2* R = h.R + size_t(p) * half;
+    double2* Y = h.Y + size_t(p) * n;
+    double2* B = h.B + size_t(p) * n;
+    double2* conv = q.convd + size_t(p) * lh * lh;
+    __shared__ int s_support;
+    constexpr double kPi = 3.141592653589793238462643383279502884;
+    // 1. radial profile (aw_projection.cpp:226-240) or projection (:113-170)
+    for (int j = threadIdx.x; j < half; j += blockDim.x) {
+        double2 v;
+        if (!h.proj_slice) {
+            const double dx = double(j) * q.scaled_cell;
+            const double r2 = dx * dx;
+            if (r2 >= 1.0) {
+                v = make_double2(q.aa[half + j], 0.0);
+            } else {
+                const double nn = sqrt(1.0 - r2);
+                double sn, cn;
+                sincos((-2.0 * kPi) * w * (nn - 1.0), &sn, &cn);
+                v = make_double2((cn / nn) * q.aa[half + j], (sn / nn) * q.aa[half + j]);
+            }
+        } else if (j == 0) {
+            double re = 0.0, im = 0.0;
+            for (int i = 1; i < half; i++) {
+                const double2 e = wk_value(q, w, i, 0);
+                re += e.x;
+                im += e.y;
+            }
+            v = make_double2(re * 2.0 + q.aa[half] * q.aa[half], im * 2.0);
+        } else {
+            v = wk_value(q, w, j, 0);
+            for (int i = 1; i < half; i++) {
+                const double2 e = wk_value(q, w, i, j);
+                v.x += e.x * 2.0;
+                v.y += e.y * 2.0;
             }
         }
-        q.invd[(size_t(p) * cs + y) * cs + x] = 1 / ks;
+        R[j] = v;
     }
+    __syncthreads();
+    // 2. transform at radii k < n
+    const int jmax = min(half, n);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double re = 0.0, im = 0.0;
+        if (!h.proj_slice) {
+            // DHT column k (aw_projection.cpp:532-596): annulus j spans
+            // [rn_{j-1}, rn_j], rn_j = j + 1/2 except rn_{n-1} = n - 1
+            const double kk = (kPi / double(n)) * double(k);
+            const double kn = (2.0 * kPi) / kk;
+            double prev = 0.0;
+            for (int j = 0; j < jmax; j++) {
+                const double rn = j == n - 1 ? double(n - 1) : double(j) + 0.5;
+                const double F = k == 0 ? kPi * rn * rn : kn * rn * j1(kk * rn);
+                const double d = j == 0 ? F : F - prev;
+                prev = F;
+                re += d * R[j].x;
+                im += d * R[j].y;
+            }
+        } else {
+            // length-arr DFT of the even projection (fft_fftw_dft_c2c_1d)
+            re = R[0].x;
+            im = R[0].y;
+            for (int t = 1; t < half; t++) {
+                const double c = 2.0 * q.ctab[(k * t) % arr];
+                re += R[t].x * c;
+                im += R[t].y * c;
+            }
+        }
+        Y[k] = make_double2(re, im);
+    }
+    __syncthreads();
+    // 3. truncation (aw_projection.h:135-148)
+    if (threadIdx.x == 0) {
+        int S = q.max_support;
+        if (q.trunc_perc > 0.0) {
+            const double minv = hypot(Y[0].x, Y[0].y) * (q.trunc_perc / 100.0);
+            int t = q.max_support * os;
+            while (t > n - 1)
+                t -= os;
+            while (t > os) {
+                if (hypot(Y[t].x, Y[t].y) > minv)
+                    break;
+                t -= os;
+            }
+            S = min(int(ceil(double(t) * (1.0 / double(os)))), q.max_support);
+        }
+        s_support = S;
+        q.support[p] = S;
+    }
+    // 4. natural cubic spline: b_0 = b_{n-1} = 0 and, for 0 < i < n-1,
+    //    b_{i-1}/3 + 4 b_i/3 + b_{i+1}/3 = y_{i+1} - 2 y_i + y_{i-1}
+    //    (tridiagonal, forward elimination and back substitution; real and
+    //    imaginary parts in two threads)
+    if (h.cubic && threadIdx.x < 2) {
+        const int comp = threadIdx.x;
+        const double* y = reinterpret_cast<const double*>(Y) + comp;
+        double* b = reinterpret_cast<double*>(B) + comp;
+        double* cp = h.Cp + (size_t(p) * 2 + comp) * n;
+        b[0] = 0.0;
+        b[2 * (n - 1)] = 0.0;
+        double cprev = 0.0, dprev = 0.0;
+        for (int i = 1; i <= n - 2; i++) {
+            const double rhs = (y[2 * (i + 1)] - y[2 * i]) - (y[2 * i] - y[2 * (i - 1)]);
+            const double m = 4.0 / 3.0 - (1.0 / 3.0) * cprev;
+            cprev = (1.0 / 3.0) / m;
+            dprev = (rhs - (1.0 / 3.0) * dprev) / m;
+            cp[i] = cprev;
+            b[2 * i] = dprev;
+        }
+        for (int i = n - 3; i >= 1; i--)
+            b[2 * i] -= cp[i] * b[2 * (i + 1)];
+    }
+    __syncthreads();
+    // 5. kernel quadrant at the radius of each offset
+    const int S = s_support;
+    const int L = min(S * os + os / 2 + 1, lh);
+    for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
+        const int dx = t % L, dy = t / L;
+        const double r = dy == 0 ? double(dx) : (dx == 0 ? double(dy) : sqrt(double(dx * dx + dy * dy)));
+        conv[size_t(dy) * lh + dx] = hankel_interp(h, Y, B, r);
+    }
+    __syncthreads();
+    wk_inverse_sums(q, p, conv, S);
 }
 
 __global__ void k_cos_table(int arr, double* c)

@@ -33,7 +33,7 @@ using np_double_array = py::array_t<double, py::array::f_style | py::array::forc
 // Enumerations with the reference's names and values (src/stp/types.h).
 enum class KernelFunction { TopHat = 0, Triangle, Sinc, Gaussian, GaussianSinc, PSWF };
 enum class FFTRoutine { FFTW_ESTIMATE_FFT = 0, FFTW_MEASURE_FFT, FFTW_PATIENT_FFT, FFTW_WISDOM_FFT, FFTW_WISDOM_INPLACE_FFT };
-enum class InterpType { LINEAR = 0, COSINE, CUBIC };
+enum class InterpType { LINEAR = 0, CUBIC = 1, COSINE = 2 }; // stp::InterpType, src/stp/types.h:55-59
 enum class MedianMethod { ZEROMEDIAN = 0, BINMEDIAN, BINAPPROX, NTHELEMENT };
 enum class CeresDiffMethod { AutoDiff = 0, AutoDiff_SingleResBlk, AnalyticDiff, AnalyticDiff_SingleResBlk };
 enum class CeresSolverType { LinearSearch_BFGS = 0, LinearSearch_LBFGS, TrustRegion_DenseQR };

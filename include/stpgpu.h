@@ -76,7 +76,12 @@ typedef struct {
     int32_t r_fft;
 } stpgpu_imager_pars;
 
-/* stp::W_ProjectionPars, src/stp/types.h:182-250.  hankel_opt must be 0. */
+/* stp::W_ProjectionPars, src/stp/types.h:182-250.  With hankel_opt the
+ * W-kernels come from the Hankel transform of the radial profile
+ * (hankel_proj_slice = 0) or from the 1-D transform of the kernel's
+ * projection (hankel_proj_slice = 1), interpolated with interp_type
+ * (stp::InterpType: 0 LINEAR, 1 CUBIC, 2 COSINE = linear), as in
+ * generate_convolution_kernel_wproj, src/stp/gridder/aw_projection.cpp:211-287. */
 typedef struct {
     int32_t num_wplanes;
     int32_t max_wpconv_support;

@@ -35,6 +35,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # Enum values, same order as src/stp/types.h:32-89.
 TopHat, Triangle, Sinc, Gaussian, GaussianSinc, PSWF = range(6)
 ZEROMEDIAN, BINMEDIAN, BINAPPROX, NTHELEMENT = range(4)
+LINEAR, CUBIC, COSINE = range(3)
 
 _lib_lock = threading.Lock()
 _libs: dict = {}
@@ -176,6 +177,9 @@ class WProj:
     undersampling_opt: int = 1
     kernel_trunc_perc: float = 0.0
     wplanes_median: bool = False
+    hankel_opt: bool = False
+    hankel_proj_slice: bool = False
+    interp_type: int = LINEAR
 
     @property
     def enabled(self):
@@ -226,6 +230,166 @@ def wkernel_plane(w_value, aa, workarea, oversampling, cell_size_arcsec, scaling
     cache = np.empty(2 * cs * cs * K * K)
     L.orc_wkernel_cache(_d(convF), ctypes.c_int64(arr), ctypes.c_int(support), ctypes.c_int(oversampling), _d(cache))
     return support, cache
+
+
+def dht_matrix(n):
+    """Discrete Hankel transform matrix, stored transposed: D[j, i] is the
+    weight of radial sample j in output i (WideFieldImaging::dht,
+    aw_projection.cpp:532-596).  Sample j covers the annulus [rn_{j-1}, rn_j]
+    with rn_j = j + 1/2 (rn_{n-1} = n - 1); output i is the order-0 Hankel
+    transform at k_i = pi i / n of the piecewise-constant profile:
+    D[j, 0] = pi (rn_j^2 - rn_{j-1}^2), D[j, i] = F_i(j) - F_i(j-1) with
+    F_i(j) = (2 pi / k_i) rn_j J1(k_i rn_j).  J1 is scipy's Bessel function
+    (the reference evaluates a rational approximation good to about 1e-8)."""
+    from scipy.special import j1
+
+    idx = np.arange(n, dtype=np.float64)
+    k = (np.pi / n) * idx
+    rn = idx + 0.5
+    rn[n - 1] = n - 1
+    D = np.empty((n, n))
+    area = np.pi * rn * rn
+    D[0, 0] = area[0]
+    D[1:, 0] = area[1:] - area[:-1]
+    kn = (2.0 * np.pi) / k[1:]
+    F = kn[None, :] * rn[:, None] * j1(k[None, 1:] * rn[:, None])
+    D[0, 1:] = F[0]
+    D[1:, 1:] = F[1:] - F[:-1]
+    return D
+
+
+def spline_coefficients(y, cubic):
+    """tk::spline over unit-spaced nodes x_i = i (aw_projection.h:154-160 ->
+    spline.h set_points with the default natural boundary, f'' = 0 at both
+    ends).  Returns (a, b, c) with f(x_k + t) = ((a_k t + b_k) t + c_k) t + y_k
+    for k < n-1 and the end segment k = n-1 extrapolating (a = 0, b = b_{n-1},
+    c = f'(x_{n-1})); linear: a = b = 0, c_k = y_{k+1} - y_k, c_{n-1} = c_{n-2}."""
+    from scipy.linalg import solve_banded
+
+    y = np.asarray(y, dtype=np.float64)
+    n = y.size
+    a = np.zeros(n)
+    b = np.zeros(n)
+    c = np.zeros(n)
+    if not cubic:
+        c[:-1] = y[1:] - y[:-1]
+        c[-1] = c[-2]
+        return a, b, c
+    ab = np.zeros((3, n))
+    ab[0, 2:] = 1.0 / 3.0   # A(i, i+1), rows 1..n-2
+    ab[1, :] = 4.0 / 3.0    # A(i, i)
+    ab[2, :-2] = 1.0 / 3.0  # A(i, i-1), rows 1..n-2
+    ab[1, 0] = 2.0          # 2 b_0 = f''(x_0) = 0
+    ab[0, 1] = 0.0
+    ab[1, n - 1] = 2.0      # 2 b_{n-1} = 0
+    ab[2, n - 2] = 0.0
+    rhs = np.zeros(n)
+    rhs[1:-1] = (y[2:] - y[1:-1]) - (y[1:-1] - y[:-2])
+    b = solve_banded((1, 1), ab, rhs)
+    a[:-1] = 1.0 / 3.0 * (b[1:] - b[:-1])
+    c[:-1] = (y[1:] - y[:-1]) - 1.0 / 3.0 * (2.0 * b[:-1] + b[1:])
+    a[-1] = 0.0
+    c[-1] = 3.0 * a[-2] + 2.0 * b[-2] + c[-2]
+    return a, b, c
+
+
+def hankel_wkernel_plane(w_value, aa, workarea, oversampling, cell_size_arcsec, scaling, max_support, trunc_perc,
+                         current_support, proj_slice=False, interp_type=LINEAR):
+    """One W-plane with hankel_opt: generate_convolution_kernel_wproj's
+    Hankel branch (aw_projection.cpp:211-287), RadialInterpolate
+    (aw_projection.h:126-214) and the Hankel branch of generate_kernel_cache
+    (aw_projection.cpp:378-412).  Same return layout as wkernel_plane."""
+    os_ = int(oversampling)
+    arr = workarea * os_
+    half = workarea // 2
+    scaled = arc_sec_to_rad(cell_size_arcsec) * scaling
+    aa = np.asarray(aa, dtype=np.float64)
+
+    def value(px, py):  # combine_2d_kernel_value, aw_projection.cpp:455-474
+        dx = px * scaled
+        dy = py * scaled
+        r2 = dx * dx + dy * dy
+        a = aa[half + px] * aa[half + py]
+        with np.errstate(invalid="ignore"):
+            nn = np.sqrt(1.0 - np.minimum(r2, 1.0))
+            v = (np.exp(1j * ((-2.0 * np.pi) * w_value * (nn - 1.0))) / np.where(nn > 0, nn, 1.0)) * a
+        return np.where(r2 >= 1.0, a + 0j, v)
+
+    if not proj_slice:
+        j = np.arange(half)
+        dx = j * scaled
+        r2 = dx * dx
+        with np.errstate(invalid="ignore"):
+            nn = np.sqrt(1.0 - np.minimum(r2, 1.0))
+            tmp = np.exp(1j * ((-2.0 * np.pi) * w_value * (nn - 1.0))) / np.where(nn > 0, nn, 1.0)
+        tmp = np.where(r2 >= 1.0, 1.0 + 0j, tmp)
+        radial = tmp * aa[half + j]
+        n = arr // 2
+        D = dht_matrix(n)
+        Y = D[:half, :].T @ radial
+    else:
+        # projection onto one axis (generate_projected_image_domain_kernel, aw_projection.cpp:113-170)
+        ii, jj = np.meshgrid(np.arange(half), np.arange(half), indexing="ij")
+        V = value(ii, jj)  # V[i, j] = value(i, j)
+        P = np.empty(half, dtype=np.complex128)
+        P[0] = 2.0 * V[1:, 0].sum() + aa[half] * aa[half]
+        P[1:] = V[1:, 0] + 2.0 * V[1:, 1:].sum(axis=0)
+        out = np.zeros(arr, dtype=np.complex128)
+        out[:half] = P
+        out[arr - np.arange(1, half)] = P[1:]
+        Y = np.fft.fft(out)
+        n = arr
+    # truncation (aw_projection.h:135-148)
+    S = int(current_support)
+    if trunc_perc > 0.0:
+        minv = abs(Y[0]) * (trunc_perc / 100.0)
+        t = int(max_support) * os_
+        while t > os_:
+            if abs(Y[t]) > minv:
+                break
+            t -= os_
+        S = min(int(math.ceil(float(t) * (1.0 / os_))), int(max_support))
+    cubic = interp_type == CUBIC
+    ar, br, cr = spline_coefficients(Y.real, cubic)
+    ai, bi, ci = spline_coefficients(Y.imag, cubic)
+    ko = (S * 2 + 2) * os_ // 2
+    size = ko + ko * (ko - 1) // 2
+    hq = np.empty(size, dtype=np.complex128)
+    i = 0
+    for row in range(ko):  # half quadrant, row `row` holds columns row..ko-1
+        for col in range(row, ko):
+            if col == 0:
+                x = float(row)
+            elif row == 0:
+                x = float(col)
+            else:
+                x = math.sqrt(float(row * row + col * col))
+            k = min(int(x), n - 1)
+            t = x - k
+            hq[i] = complex(((ar[k] * t + br[k]) * t + cr[k]) * t + Y.real[k],
+                            ((ai[k] * t + bi[k]) * t + ci[k]) * t + Y.imag[k])
+            i += 1
+    cs = (os_ // 2) * 2 + 1
+    K = 2 * S + 1
+    cache = np.empty((cs * cs, K * K), dtype=np.complex128)
+    for x in range(cs):
+        for y in range(cs):
+            tmp = np.empty((K, K), dtype=np.complex128)  # tmp[tx, ty]
+            ksum = 0.0
+            for ty in range(K):
+                cx = (ty - S) * os_ + os_ // 2 - x
+                dcx = abs(cx)
+                for tx in range(K):
+                    cy = (tx - S) * os_ + os_ // 2 - y
+                    dcy = abs(cy)
+                    if dcx > dcy:
+                        vi = dcy * ko - ((dcy * (dcy + 1)) >> 1) + dcx
+                    else:
+                        vi = dcx * ko - ((dcx * (dcx + 1)) >> 1) + dcy
+                    tmp[tx, ty] = hq[vi]
+                    ksum += hq[vi].real
+            cache[y * cs + x] = (tmp / ksum).reshape(-1, order="F")
+    return S, cache.reshape(-1).view(np.float64).copy()
 
 
 def convolve_to_grid(kf, support, image_size, uv, vis, weights, kernel_exact=True, oversampling=1, shift_uv=True,
@@ -296,8 +460,13 @@ def convolve_to_grid(kf, support, image_size, uv, vis, weights, kernel_exact=Tru
         for p in range(nplanes):
             b = int(first[p])
             e = n if p == nplanes - 1 else int(first[p + 1])
-            cur, cache = wkernel_plane(float(w_avg[p]), aa, workarea, oversampling, cell_size, scaling,
-                                       int(wproj.max_wpconv_support), float(wproj.kernel_trunc_perc), cur)
+            if wproj.hankel_opt:
+                cur, cache = hankel_wkernel_plane(float(w_avg[p]), aa, workarea, oversampling, cell_size, scaling,
+                                                  int(wproj.max_wpconv_support), float(wproj.kernel_trunc_perc), cur,
+                                                  bool(wproj.hankel_proj_slice), int(wproj.interp_type))
+            else:
+                cur, cache = wkernel_plane(float(w_avg[p]), aa, workarea, oversampling, cell_size, scaling,
+                                           int(wproj.max_wpconv_support), float(wproj.kernel_trunc_perc), cur)
             res.plane_supports.append(cur)
             res.plane_w.append(float(w_avg[p]))
             accumulate(2, empty, cache, cur, b, e)
@@ -345,8 +514,8 @@ def normalise(img, padded, image_size, normalization_factor, gcf, grid_correctio
 def image_visibilities(vis, weights, uvw, image_size, cell_size, padding_factor=1.0, kernel_func=PSWF,
                        kernel_support=3, kernel_exact=True, oversampling=8, generate_beam=False,
                        gridding_correction=True, analytic_gcf=False, num_wplanes=0, wplanes_median=False,
-                       max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, threads=1, fast=False,
-                       return_grid=False):
+                       max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, hankel_opt=False,
+                       hankel_proj_slice=False, interp_type=LINEAR, threads=1, fast=False, return_grid=False):
     """stp_python.image_visibilities_wrapper (stp-python/stp_python.cpp:17-140)
     -> ImageVisibilities (stp/imager/imager.cpp:12-68) -> image_visibilities
     (stp/imager/imager.h:233-376).  Returns (image, beam)."""
@@ -361,7 +530,8 @@ def image_visibilities(vis, weights, uvw, image_size, cell_size, padding_factor=
     uv = np.empty((uvw.shape[0], 2))
     uv[:, 0] = uvw[:, 0] * inv
     uv[:, 1] = uvw[:, 1] * inv
-    wp = WProj(num_wplanes, max_wpconv_support, undersampling_opt, kernel_trunc_perc, wplanes_median)
+    wp = WProj(num_wplanes, max_wpconv_support, undersampling_opt, kernel_trunc_perc, wplanes_median, hankel_opt,
+               hankel_proj_slice, interp_type)
     g = convolve_to_grid(kernel_func, kernel_support, padded, uv, vis, weights, kernel_exact, oversampling, True,
                          True, generate_beam, wp, uvw[:, 2], cell_size, analytic_gcf, threads, fast)
     img = c2r(g.vis_grid, padded, threads)

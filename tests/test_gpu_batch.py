@@ -24,7 +24,7 @@ def peak_rel(a, b):
 
 
 def _cases():
-    """(snapshot, keywords) of uneven sizes, kernels and W-projection."""
+    """(snapshot, keywords) of uneven sizes, kernels, W-projection and Hankel-transform W-kernels."""
     out = []
     s = make_snapshot(41, 3000, 256, 2.0, n_src=3)
     out.append((s, dict(image_size=256, cell_size=s.cell_size, kernel_func=capi.GaussianSinc, kernel_support=3,
@@ -39,6 +39,10 @@ def _cases():
     s = make_snapshot(44, 4000, 384, 2.0, n_src=3)
     out.append((s, dict(image_size=384, padded_image_size=576, padding_factor=1.5, cell_size=s.cell_size,
                         kernel_func=capi.GaussianSinc, kernel_support=3, kernel_exact=False, oversampling=8)))
+    s = make_snapshot(46, 3000, 256, 2.0, n_src=3, w_range=(-900.0, 900.0))
+    out.append((s, dict(image_size=256, cell_size=s.cell_size, kernel_func=capi.PSWF, kernel_support=3,
+                        kernel_exact=False, oversampling=8, num_wplanes=3, max_wpconv_support=6,
+                        kernel_trunc_perc=1.0, hankel_opt=True, interp_type=capi.CUBIC)))
     s = make_snapshot(45, 300, 128, 2.0, n_src=1)
     s.uvw[:, :2] *= 1e6  # every visibility out of bounds: empty result
     out.append((s, dict(image_size=128, cell_size=s.cell_size, kernel_func=capi.GaussianSinc, kernel_support=3,

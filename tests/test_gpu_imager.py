@@ -134,6 +134,48 @@ def test_imager_wproj_large_support(ctx, trunc):
     assert peak_rel(img, ri) < TOL64
 
 
+@pytest.mark.parametrize("proj_slice,interp", [(False, capi.LINEAR), (False, capi.CUBIC), (True, capi.LINEAR),
+                                               (True, capi.CUBIC), (False, capi.COSINE)])
+def test_imager_hankel_fp64_vs_oracle(ctx, proj_slice, interp):
+    """Hankel-transform W-kernels (hankel_opt): discrete Hankel transform or projection slice, linear or
+    cubic radial interpolation, truncated at 1 %."""
+    s = _imager_case(35, 256, 5000, w_range=(-1500.0, 1500.0))
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              num_wplanes=5, max_wpconv_support=8, undersampling_opt=1, kernel_trunc_perc=1.0, hankel_opt=True,
+              hankel_proj_slice=proj_slice, interp_type=interp)
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    ri, _, g = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, return_grid=True, **kw)
+    assert info.max_plane_support == max(g.plane_supports)
+    assert peak_rel(img, ri) < TOL64
+
+
+def test_imager_hankel_large_support_and_fp32c(ctx):
+    s = _imager_case(36, 256, 2000, w_range=(-4000.0, 4000.0))
+    kw = dict(kernel_func=5, kernel_support=3, kernel_exact=False, oversampling=4, analytic_gcf=False,
+              num_wplanes=3, max_wpconv_support=40, kernel_trunc_perc=0.0, hankel_opt=True, interp_type=capi.CUBIC)
+    ri, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    assert info.max_plane_support == 40
+    assert peak_rel(img, ri) < TOL64
+    img32, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, precision=capi.FP32C,
+                                         out_dtype=capi.F32, **kw)
+    # 81 x 81 untruncated W-kernels in single precision: rounding the oracle's own kernel tables to FP32
+    # alone moves this image by 6.6e-6 of its peak (9.5e-6 for the FFT W-kernels of the same case), so the
+    # FP32 gridder + FP32 FFT are held to 1e-4 here; the small-support case below keeps 1e-5
+    assert peak_rel(img32.astype(np.float64), ri) < 1e-4
+
+
+def test_imager_hankel_fp32c_vs_oracle(ctx):
+    s = _imager_case(38, 256, 5000, w_range=(-1500.0, 1500.0))
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+              num_wplanes=5, max_wpconv_support=8, kernel_trunc_perc=1.0, hankel_opt=True,
+              hankel_proj_slice=True, interp_type=capi.CUBIC)
+    ri, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    img32, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, precision=capi.FP32C,
+                                         out_dtype=capi.F32, **kw)
+    assert peak_rel(img32.astype(np.float64), ri) < 1e-5
+
+
 @pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal"])
 def test_imager_wproj_near_tied_w(ctx, pattern):
     """|w| values that are equal in single precision but distinct in double
@@ -191,8 +233,8 @@ def test_imager_rejects_unsupported(ctx):
     s = _imager_case(1, 64, 100)
     with pytest.raises(capi.StpGpuError) as e:
         ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, num_wplanes=2, max_wpconv_support=4,
-                               kernel_exact=False, hankel_opt=True)
-    assert e.value.status == 2
+                               kernel_exact=False, hankel_opt=True, interp_type=7)
+    assert e.value.status == 1
     with pytest.raises(capi.StpGpuError) as e:
         ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, aproj_numtimesteps=2, kernel_exact=False)
     assert e.value.status == 2
