@@ -50,7 +50,8 @@ class WProjPars(ctypes.Structure):
 
 class AProjPars(ctypes.Structure):
     _fields_ = [("num_timesteps", ctypes.c_int32), ("obs_dec", ctypes.c_double), ("obs_ra", ctypes.c_double),
-                ("aproj_opt", ctypes.c_int32), ("aproj_mask_perc", ctypes.c_double)]
+                ("aproj_opt", ctypes.c_int32), ("aproj_mask_perc", ctypes.c_double), ("lha", ctypes.c_void_p),
+                ("pbeam_coefs", ctypes.c_void_p), ("n_pbeam_coefs", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class ImagerInfo(ctypes.Structure):
@@ -243,14 +244,19 @@ class Context:
                            kernel_support=3, kernel_exact=True, oversampling=8, generate_beam=False,
                            gridding_correction=True, analytic_gcf=False, num_wplanes=0, wplanes_median=False,
                            max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, hankel_opt=False,
-                           hankel_proj_slice=False, interp_type=LINEAR, aproj_numtimesteps=0, precision=FP64,
-                           out_dtype=F64, padded_image_size=0, device_ptrs=False, image_out=None, beam_out=None):
+                           hankel_proj_slice=False, interp_type=LINEAR, aproj_numtimesteps=0, obs_dec=0.0,
+                           obs_ra=0.0, aproj_opt=False, aproj_mask_perc=0.0, lha=None, pbeam_coefs=None,
+                           precision=FP64, out_dtype=F64, padded_image_size=0, device_ptrs=False, image_out=None,
+                           beam_out=None):
         """stp::image_visibilities semantics (sizes used as given).
 
         Host mode: numpy inputs (vis complex128/complex64 (n,), weights (n,),
         uvw (n, 3)); returns (image, beam, info) as F-ordered arrays.
         Device mode: torch CUDA tensors; uvw must be (3, n) contiguous (the
         column-major n x 3 layout); outputs written into image_out/beam_out.
+        A-projection (aproj_numtimesteps > 0): lha (n,) local hour angles in
+        hours (a CUDA tensor in device mode), pbeam_coefs the beam's
+        spherical-harmonic coefficients (host).
         """
         ip = ImagerPars(int(image_size), int(padded_image_size), float(cell_size), float(padding_factor),
                         int(kernel_func), int(kernel_support), int(bool(kernel_exact)), int(oversampling),
@@ -258,7 +264,12 @@ class Context:
         wp = WProjPars(int(num_wplanes), int(max_wpconv_support), int(undersampling_opt), float(kernel_trunc_perc),
                        int(bool(hankel_opt)), int(bool(hankel_proj_slice)), int(interp_type),
                        int(bool(wplanes_median)))
-        ap = AProjPars(int(aproj_numtimesteps), 0.0, 0.0, 0, 0.0)
+        coefs = np.ascontiguousarray(np.asarray(pbeam_coefs if pbeam_coefs is not None else [], dtype=np.float64))
+        if lha is not None and not hasattr(lha, "data_ptr"):
+            lha = np.ascontiguousarray(np.asarray(lha, dtype=np.float64).reshape(-1))
+        ap = AProjPars(int(aproj_numtimesteps), float(obs_dec), float(obs_ra), int(bool(aproj_opt)),
+                       float(aproj_mask_perc), _ptr(lha) if lha is not None else None,
+                       _ptr(coefs) if coefs.size else None, int(coefs.size), 0)
         info = ImagerInfo()
         if device_ptrs:
             n = int(weights.numel())

@@ -29,6 +29,7 @@
 #include "imager_kernels.cuh"
 #include "sourcefind_kernels.cuh"
 #include "visibility_kernels.cuh"
+#include "aproj_kernels.cuh"
 
 using namespace stpgpu;
 
@@ -68,6 +69,7 @@ struct stpgpu_context {
     }
     std::map<std::string, DevBuf> bufs;
     std::map<std::tuple<int, int, cudaStream_t>, cufftHandle> plans; // (N, cufftType, stream)
+    std::map<std::tuple<int, int, int, cudaStream_t>, cufftHandle> plans_many; // (N, type, batch, stream)
     // Prefix of buffer and memo names: the batch path gives every snapshot
     // slot its own buffers ("b<i>/"); single calls use "".
     std::string ns;
@@ -223,6 +225,27 @@ struct stpgpu_context {
         return h;
     }
 
+    // Batched N x N transforms (A-projection kernels), cached like plan().
+    cufftHandle plan_many(int N, cufftType type, int batch)
+    {
+        const auto key = std::make_tuple(N, int(type), batch, stream);
+        auto it = plans_many.find(key);
+        if (it != plans_many.end())
+            return it->second;
+        cufftHandle h;
+        int dims[2] = { N, N };
+        const auto t0 = std::chrono::steady_clock::now();
+        cufftResult r = cufftPlanMany(&h, 2, dims, nullptr, 1, N * N, nullptr, 1, N * N, type, batch);
+        log_alloc("cuFFT plan", ns + "N" + std::to_string(N) + "x" + std::to_string(batch), 0, t0);
+        if (r != CUFFT_SUCCESS)
+            fail(STPGPU_ERR_CUFFT, "cufftPlanMany failed (" + std::to_string(int(r)) + ") for N=" + std::to_string(N));
+        r = cufftSetStream(h, stream);
+        if (r != CUFFT_SUCCESS)
+            fail(STPGPU_ERR_CUFFT, "cufftSetStream failed");
+        plans_many[key] = h;
+        return h;
+    }
+
     void release()
     {
         if (stream)
@@ -236,6 +259,9 @@ struct stpgpu_context {
         for (auto& kv : plans)
             cufftDestroy(kv.second);
         plans.clear();
+        for (auto& kv : plans_many)
+            cufftDestroy(kv.second);
+        plans_many.clear();
         for (auto& kv : bufs)
             if (kv.second.p)
                 cudaFree(kv.second.p);
@@ -295,6 +321,14 @@ struct ImagerSetup {
     double trunc_perc = 0.0;
     int full_wsort = 0; // |w| order from the 64-bit sort (fallback of the 32-bit sort + run fix-up)
     int hankel = 0, proj_slice = 0, cubic = 0; // Hankel-transform W-kernels (hankel_opt)
+    // A-projection: time steps, rotated-kernel option, pointing (radians),
+    // per-visibility hour angles (device pointer once the call has staged
+    // them) and the beam's spherical-harmonic coefficients (host)
+    int ntimesteps = 0, aproj_opt = 0;
+    double obs_dec = 0.0, obs_ra = 0.0;
+    const double* lha = nullptr;
+    const double* pbcoefs = nullptr;
+    int npbcoefs = 0;
 };
 
 // W-projection with a maximum support above 32: the W-kernel tables and tile
@@ -427,6 +461,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     int lh = 0;
     C2* wk = nullptr;
     uint32_t* wk_off = nullptr;
+    uint8_t* ts_of = nullptr; // A-projection time step per visibility
     int* plane_support = nullptr;
     if (!wproj && !kernel_exact) {
         // populate_kernel_cache (gridder.h:73-105) as a 1-D table, FP64 on the device
@@ -569,9 +604,70 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         }
         wq.convd = c->buf<double2>("wkconv", size_t(P) * Lh * Lh);
         wq.invd = c->buf<double>("wkinv", size_t(P) * cs * cs);
-        plane_support = c->buf<int>("psupport", P);
+        const int T = std::max(s.ntimesteps, 1);
+        const int PT = P * T;
+        plane_support = c->buf<int>("psupport", PT);
         wq.support = plane_support;
-        if (s.hankel) {
+        const double2* aconv = nullptr; // A-projection: transformed kernels [P*T][arr][arr]
+        if (s.ntimesteps > 0) {
+            // time steps and their parallactic angles (gridder.h:507-520, gridder.cpp:148-200)
+            double* iv = c->buf<double>("ap_iv", T + 1);
+            double* lmean = c->buf<double>("ap_lmean", T);
+            double* angle = c->buf<double>("ap_angle", T);
+            ts_of = c->buf<uint8_t>("ap_ts", nn);
+            k_lha_intervals<<<1, 1024, 0, st>>>(s.lha, n, T, iv);
+            STPGPU_CHECK_LAUNCH();
+            k_lha_steps<R><<<grid1d(n, 256), 256, 0, st>>>(s.lha, items, n, T, iv, ts_of);
+            STPGPU_CHECK_LAUNCH();
+            k_lha_means<R><<<T, 256, 0, st>>>(s.lha, items, ts_of, n, lmean);
+            STPGPU_CHECK_LAUNCH();
+            k_parangle<<<1, 256, 0, st>>>(lmean, T, s.obs_dec, s.obs_ra, angle);
+            STPGPU_CHECK_LAUNCH();
+            // inverse primary beam per step (one unrotated beam with aproj_opt)
+            double* coefs = c->buf<double>("ap_coefs", s.npbcoefs);
+            STPGPU_CUDA_TRY(
+                cudaMemcpyAsync(coefs, s.pbcoefs, sizeof(double) * s.npbcoefs, cudaMemcpyHostToDevice, st));
+            const int deg = (s.npbcoefs - 1) / 2;
+            const double fov = arc_sec_to_rad(s.cell_size) * double(N);
+            const int nA = s.aproj_opt ? 1 : T;
+            double* Abeam = c->buf<double>("ap_beam", size_t(nA) * workarea * workarea);
+            k_aproj_beam<<<grid1d(int64_t(nA) * workarea * workarea, 256), 256, 0, st>>>(nA, workarea, fov, coefs, deg,
+                s.aproj_opt ? nullptr : angle, Abeam);
+            STPGPU_CHECK_LAUNCH();
+            // W-screen x beam, 2-D FFT per (plane, step) or per plane
+            const int G = P * nA;
+            const size_t img = size_t(arr) * arr;
+            const size_t nimg = size_t(G) + (s.aproj_opt ? size_t(PT) : 0);
+            if (nimg * img * sizeof(double2) > (uint64_t(8) << 30))
+                fail(STPGPU_ERR_UNSUPPORTED,
+                    "A-projection kernels exceed 8 GB (planes x time steps x (workarea x oversampling)^2)");
+            double2* abuf = c->buf<double2>("ap_fft", nimg * img);
+            STPGPU_CUDA_TRY(cudaMemsetAsync(abuf, 0, sizeof(double2) * size_t(G) * img, st));
+            const int span = 2 * half - 1;
+            k_aproj_screen<<<grid1d(int64_t(G) * span * span, 256), 256, 0, st>>>(wq, P, nA, Abeam, abuf);
+            STPGPU_CHECK_LAUNCH();
+            if (cufftExecZ2Z(c->plan_many(arr, CUFFT_Z2Z, G), reinterpret_cast<cufftDoubleComplex*>(abuf),
+                    reinterpret_cast<cufftDoubleComplex*>(abuf), CUFFT_FORWARD)
+                != CUFFT_SUCCESS)
+                fail(STPGPU_ERR_CUFFT, "A-projection kernel FFT failed");
+            k_aproj_support<<<grid1d(G, 128), 128, 0, st>>>(abuf, G, arr, os, s.max_support, s.trunc_perc,
+                s.aproj_opt ? T : 1, plane_support);
+            STPGPU_CHECK_LAUNCH();
+            aconv = abuf;
+            if (s.aproj_opt) {
+                // rotate each plane's kernel by the step's angle, step after
+                // step on the previous step's result (gridder.h:732-737)
+                double2* rot = abuf + size_t(G) * img; // [P][T][arr][arr]
+                for (int t = 0; t < T; t++) {
+                    const double2* src = t == 0 ? abuf : rot + size_t(t - 1) * img;
+                    const int64_t src_stride = t == 0 ? int64_t(img) : int64_t(T) * int64_t(img);
+                    k_aproj_rotate<<<grid1d(int64_t(P) * int64_t(img), 256), 256, 0, st>>>(src, src_stride,
+                        rot + size_t(t) * img, int64_t(T) * int64_t(img), P, arr, angle, t);
+                    STPGPU_CHECK_LAUNCH();
+                }
+                aconv = rot;
+            }
+        } else if (s.hankel) {
             HankelParams hq {};
             hq.n = s.proj_slice ? arr : arr / 2;
             if (hq.n < 3)
@@ -590,10 +686,10 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         // per-offset K x K tables in the gridder's precision: worst-case
         // capacity (every plane at the maximum support), or with large
         // supports the sum over the measured plane supports
-        uint64_t cap_wk = uint64_t(P) * cs * cs * uint64_t(K) * K;
+        uint64_t cap_wk = uint64_t(PT) * cs * cs * uint64_t(K) * K;
         if (large_support(s)) {
-            std::vector<int> sup(P);
-            STPGPU_CUDA_TRY(cudaMemcpyAsync(sup.data(), plane_support, sizeof(int) * P, cudaMemcpyDeviceToHost, st));
+            std::vector<int> sup(PT);
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(sup.data(), plane_support, sizeof(int) * PT, cudaMemcpyDeviceToHost, st));
             STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
             cap_wk = 0;
             for (int v : sup)
@@ -603,12 +699,16 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         if (cap_wk * sizeof(C2) > (uint64_t(16) << 30) || cap_wk > 0xffffffffull)
             fail(STPGPU_ERR_UNSUPPORTED, "W-kernel tables exceed 16 GB (planes x oversampling^2 x support^2)");
         wk = c->buf<C2>("wkexp", cap_wk);
-        wk_off = c->buf<uint32_t>("wkoff", P);
-        k_wk_expand<R><<<dim3(P, cs * cs), 64, 0, st>>>(wq.convd, wq.invd, plane_support, P, cs, os, Lh, wk, wk_off);
+        wk_off = c->buf<uint32_t>("wkoff", PT);
+        if (aconv)
+            k_aproj_expand<R><<<dim3(PT, cs * cs), 256, 0, st>>>(aconv, arr, plane_support, cs, os, wk, wk_off);
+        else
+            k_wk_expand<R><<<dim3(P, cs * cs), 64, 0, st>>>(wq.convd, wq.invd, plane_support, P, cs, os, Lh, wk,
+                wk_off);
         STPGPU_CHECK_LAUNCH();
         lh = Lh;
         g.d_plane_support = plane_support;
-        g.nplanes = P;
+        g.nplanes = PT;
     }
 
     // ---- binning into 32x32 uv tiles
@@ -632,6 +732,8 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     bp.tile_c = tile_c;
     bp.support = s.support;
     bp.plane_support = plane_support;
+    bp.ts_of = ts_of;
+    bp.ntimesteps = std::max(s.ntimesteps, 1);
     bp.exact = kernel_exact;
     bp.n = n;
     bp.tile_count = tcount;
@@ -900,7 +1002,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     // normalisation kernels, captured on the first repeat; any other call
     // drops it.  The data in the buffers may change between calls.
     std::string sig;
-    if (graphable && !c->timing && !large_support(s)) {
+    if (graphable && !c->timing && !large_support(s) && s.ntimesteps == 0) {
         auto put = [&](const void* q, size_t nb) { sig.append(reinterpret_cast<const char*>(q), nb); };
         put(&precision, sizeof(precision));
         put(&s, sizeof(s));
@@ -1015,8 +1117,6 @@ ImagerSetup setup_from(const stpgpu_imager_pars* p, const stpgpu_wproj_pars* w, 
 {
     if (!p)
         fail(STPGPU_ERR_INVALID_ARG, "null imager parameters");
-    if (a && a->num_timesteps > 0)
-        fail(STPGPU_ERR_UNSUPPORTED, "A-projection is outside the GPU path");
     if (p->kernel_function < 0 || p->kernel_function > 5)
         fail(STPGPU_ERR_INVALID_ARG, "unknown kernel function");
     if (!(p->cell_size > 0.0))
@@ -1056,6 +1156,24 @@ ImagerSetup setup_from(const stpgpu_imager_pars* p, const stpgpu_wproj_pars* w, 
     }
     if (!p->kernel_exact && p->oversampling < 1)
         fail(STPGPU_ERR_INVALID_ARG, "oversampling must be >= 1 when kernel_exact is false");
+    if (a && a->num_timesteps > 0) {
+        // imager.h:274-283
+        if (s.nplanes <= 0)
+            fail(STPGPU_ERR_INVALID_ARG, "W-projection must be used when A-projection is enabled.");
+        if (s.hankel)
+            fail(STPGPU_ERR_INVALID_ARG, "Hankel transform cannot be used when A-projection is enabled.");
+        if (a->num_timesteps > 255 || int64_t(a->num_timesteps) * s.nplanes > 65535)
+            fail(STPGPU_ERR_UNSUPPORTED, "A-projection supports at most 255 time steps and 65535 planes x steps");
+        if (a->n_pbeam_coefs < 1 || !a->pbeam_coefs)
+            fail(STPGPU_ERR_INVALID_ARG, "A-projection needs the primary beam coefficients");
+        s.ntimesteps = a->num_timesteps;
+        s.aproj_opt = a->aproj_opt ? 1 : 0;
+        s.obs_dec = (a->obs_dec * M_PI) / 180.0; // deg2rad, global_macros.h:40
+        s.obs_ra = (a->obs_ra * M_PI) / 180.0;
+        s.lha = a->lha;
+        s.pbcoefs = a->pbeam_coefs;
+        s.npbcoefs = a->n_pbeam_coefs;
+    }
     return s;
 }
 
@@ -2054,10 +2172,14 @@ stpgpu_status stpgpu_image_visibilities_ex(stpgpu_context* c, const void* vis, i
         const bool timed = !device_ptrs;
         if (timed)
             STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+        if (s.ntimesteps > 0 && n_vis > 0 && !s.lha)
+            fail(STPGPU_ERR_INVALID_ARG, "A-projection needs the hour angle of every visibility (lha)");
         if (!device_ptrs) {
             dv = to_device<unsigned char>(c, "in_vis", vis, vbytes * size_t(n_vis));
             dw = to_device<double>(c, "in_w", weights, size_t(n_vis));
             duvw = to_device<double>(c, "in_uvw", uvw, 3 * size_t(n_vis));
+            if (s.ntimesteps > 0)
+                s.lha = to_device<double>(c, "in_lha", s.lha, size_t(n_vis));
         }
         const int64_t npix = int64_t(image_size) * image_size;
         const size_t obytes = out_dtype == STPGPU_F32 ? 4 : 8;

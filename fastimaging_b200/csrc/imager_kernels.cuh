@@ -235,6 +235,8 @@ struct BinParams {
     int tile_c;              // tile width in grid columns (TILE_R rows per tile)
     int support;             // non-W-proj support
     const int* plane_support; // W-proj truncated support per plane (nullable)
+    const uint8_t* ts_of;     // A-projection: time step per visibility (nullable)
+    int ntimesteps;           // planes are indexed plane * ntimesteps + step
     int exact;               // rows wrap negative (exact gridder)
     int64_t n;
     uint32_t* tile_count;
@@ -368,7 +370,13 @@ __global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t*
     const Item<R> it = items[i];
     if (!it.good)
         return;
-    const int S = order ? p.plane_support[plane_of(first, P, k)] : p.support;
+    int S = p.support;
+    if (order) {
+        int plane = plane_of(first, P, k);
+        if (p.ts_of)
+            plane = plane * p.ntimesteps + p.ts_of[i];
+        S = p.plane_support[plane];
+    }
     for (int mir = 0; mir < int(it.good); mir++)
         for_item_tiles(it, mir, S, p, [&](uint32_t t) { atomicAdd(&p.tile_count[t], 1u); });
 }
@@ -387,7 +395,9 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
         return;
     int S = p.support;
     if (order) {
-        const int plane = plane_of(first, P, k);
+        int plane = plane_of(first, P, k);
+        if (p.ts_of)
+            plane = plane * p.ntimesteps + p.ts_of[i];
         S = p.plane_support[plane];
         items[i].plane = uint16_t(plane);
     }

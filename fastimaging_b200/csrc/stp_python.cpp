@@ -90,13 +90,13 @@ py::tuple image_visibilities_wrapper(np_complex_double_array vis, np_double_arra
     np_double_array pbeam_coefs)
 {
     (void)fft_wisdom_filename;
-    (void)lha;
-    (void)pbeam_coefs;
     if (uvw_lambda.ndim() != 2 || uvw_lambda.shape(1) != 3)
         throw std::runtime_error("stp_python: uvw_lambda must have shape (n_vis, 3)");
     const int64_t n = int64_t(uvw_lambda.shape(0));
     if (int64_t(vis.size()) < n || int64_t(snr_weights.size()) < n)
         throw std::runtime_error("stp_python: vis and snr_weights need n_vis entries");
+    if (aproj_numtimesteps > 0 && int64_t(lha.size()) < n)
+        throw std::runtime_error("stp_python: lha needs n_vis entries");
 
     // image sizes rounded up to multiples of 4 (stp_python.cpp:60-67)
     while (image_size % 4)
@@ -133,6 +133,9 @@ py::tuple image_visibilities_wrapper(np_complex_double_array vis, np_double_arra
     ap.obs_ra = obs_ra;
     ap.aproj_opt = aproj_opt;
     ap.aproj_mask_perc = aproj_mask_perc;
+    ap.lha = aproj_numtimesteps > 0 ? lha.data() : nullptr;
+    ap.pbeam_coefs = pbeam_coefs.size() ? pbeam_coefs.data() : nullptr;
+    ap.n_pbeam_coefs = int32_t(pbeam_coefs.size());
 
     auto image = f_matrix(image_size, image_size);
     auto beam = f_matrix(generate_beam ? image_size : 0, generate_beam ? image_size : 0);

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define STPGPU_ABI_VERSION 1
+#define STPGPU_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define STPGPU_API __attribute__((visibility("default")))
@@ -93,14 +93,23 @@ typedef struct {
     int32_t wplanes_median;
 } stpgpu_wproj_pars;
 
-/* stp::A_ProjectionPars, src/stp/types.h:255-316.  num_timesteps must be 0
- * (A-projection is outside the GPU path). */
+/* stp::A_ProjectionPars, src/stp/types.h:255-316 (the reference's
+ * experimental ENABLE_APROJECTION build).  num_timesteps > 0 enables it
+ * (needs W-projection, no Hankel option): lha holds each visibility's local
+ * hour angle in hours (n_vis values; a device pointer when the call takes
+ * device pointers), pbeam_coefs the 2*degree+1 spherical-harmonic
+ * coefficients of the primary beam (host memory).  aproj_mask_perc is
+ * accepted and unused, as in the reference. */
 typedef struct {
     int32_t num_timesteps;
-    double obs_dec;
-    double obs_ra;
-    int32_t aproj_opt;
+    double obs_dec;           /* degrees */
+    double obs_ra;            /* degrees */
+    int32_t aproj_opt;        /* rotate the convolution kernel instead of the beam */
     double aproj_mask_perc;
+    const double* lha;
+    const double* pbeam_coefs;
+    int32_t n_pbeam_coefs;
+    int32_t reserved;
 } stpgpu_aproj_pars;
 
 /* Per-call imaging report. */

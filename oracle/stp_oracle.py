@@ -392,9 +392,199 @@ def hankel_wkernel_plane(w_value, aa, workarea, oversampling, cell_size_arcsec, 
     return S, cache.reshape(-1).view(np.float64).copy()
 
 
+@dataclass
+class AProj:
+    """stp::A_ProjectionPars (types.h:255-316): num_timesteps > 0 enables it."""
+    num_timesteps: int = 0
+    obs_dec: float = 0.0
+    obs_ra: float = 0.0
+    aproj_opt: bool = False
+    lha: np.ndarray | None = None
+    pbeam_coefs: list | None = None
+
+    @property
+    def enabled(self):
+        return self.num_timesteps > 0
+
+
+def _linspace(start, end, num):
+    """arma::linspace: start + i * delta for i < num - 1, the last point = end."""
+    delta = (end - start) / float(num - 1)
+    out = start + np.arange(num, dtype=np.float64) * delta
+    out[num - 1] = end
+    return out
+
+
+def average_lha_planes(lha, good, num_timesteps):
+    """gridder.cpp:148-200.  lha in the gridder's (|w|-sorted) order; returns
+    (mean hour angle per step, step of each visibility; 0 where not good)."""
+    lha = np.asarray(lha, dtype=np.float64)
+    T = int(num_timesteps)
+    lo, hi = float(lha.min()), float(lha.max())
+    step = (hi - lo) / T
+    iv = _linspace(lo - step / 2, hi + step / 2, T + 1)
+    ts = np.zeros(lha.size, dtype=np.int64)
+    planes = np.zeros(T)
+    count = np.zeros(T, dtype=np.int64)
+    for i in np.nonzero(np.asarray(good) != 0)[0]:
+        t = lha[i]
+        k = 1
+        v = iv[1]
+        while t > v:
+            k += 1
+            if k < T + 1:
+                v = iv[k]
+            else:
+                break
+        sel = k - 1
+        ts[i] = sel
+        planes[sel] += t
+        count[sel] += 1
+    planes = np.where(count > 0, planes / np.maximum(count, 1), 0.0)
+    return planes, ts
+
+
+def parangle(ha, dec_rad, ra_rad):
+    """aw_projection.cpp:599-608 (the pointing RA where a latitude would stand)."""
+    h = ha * (15.0 * math.pi / 180.0)
+    s_ = math.cos(ra_rad) * math.sin(h)
+    c_ = math.sin(ra_rad) * math.cos(dec_rad) - math.cos(ra_rad) * math.sin(dec_rad) * math.cos(h)
+    return math.atan2(s_, c_)
+
+
+def sh_abs(l, m, phi, theta):
+    """|real spherical harmonic Y_l^m(theta, phi)| (orthonormal; the
+    reference's sh::EvalSH from google/spherical-harmonics, un-vendored
+    submodule, restated from the definition): sqrt2 K |P_l^|m|(cos theta)|
+    |cos(m phi)| for m > 0, |sin(|m| phi)| for m < 0, K |P_l^0| for m = 0."""
+    phi = np.asarray(phi, dtype=np.float64)
+    theta = np.asarray(theta, dtype=np.float64)
+    am = abs(m)
+    x = np.cos(theta)
+    sn = np.abs(np.sin(theta))
+    pmm = np.ones_like(x)
+    f = 1.0
+    for _ in range(am):
+        pmm = pmm * (f * sn)
+        f += 2.0
+    p = pmm
+    if l > am:
+        pm2 = pmm
+        pm1 = x * (2.0 * am + 1.0) * pmm
+        p = pm1
+        for ll in range(am + 2, l + 1):
+            p = ((2.0 * ll - 1.0) * x * pm1 - (ll + am - 1.0) * pm2) / float(ll - am)
+            pm2, pm1 = pm1, p
+    ratio = 1.0
+    for k in range(l - am + 1, l + am + 1):
+        ratio /= float(k)
+    v = math.sqrt((2.0 * l + 1.0) / (4.0 * math.pi) * ratio) * p
+    if m > 0:
+        v = v * (math.sqrt(2.0) * np.cos(float(m) * phi))
+    elif m < 0:
+        v = v * (math.sqrt(2.0) * np.sin(float(am) * phi))
+    return np.abs(v)
+
+
+def generate_a_kernel(coefs, fov, workarea, rot_angle=0.0):
+    """gridder.cpp:243-275: A[j + c, i + c] = 1 / sum_m |Y_deg^m(phi + rot,
+    theta) c_m| with theta = |(j, i)| fov / workarea, phi = atan(i / j)
+    (pi/2 for j = 0)."""
+    coefs = np.asarray(coefs, dtype=np.float64)
+    deg = int((coefs.size - 1) // 2)
+    c = workarea // 2
+    j = np.arange(-c, c, dtype=np.float64)[:, None]
+    i = np.arange(-c, c, dtype=np.float64)[None, :]
+    j_rad = j * fov / float(workarea)
+    i_rad = i * fov / float(workarea)
+    theta = np.sqrt(j_rad * j_rad + i_rad * i_rad)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        phi = np.where(j != 0, np.arctan(i_rad / np.where(j != 0, j_rad, 1.0)), math.pi / 2.0)
+    acc = np.zeros((workarea, workarea))
+    for m in range(-deg, deg + 1):
+        acc = acc + np.abs(sh_abs(deg, m, phi + rot_angle, theta) * coefs[deg + m])
+    return 1.0 / acc
+
+
+def rotate_matrix_cx(m, angle, cval):
+    """matrix_math.cpp:715-733 (complex rotate_matrix, out_size = in_size):
+    bilinear rotation about (n/2 - 0.5, n/2 - 0.5) with the reference's edge
+    rules; samples that fall outside take cval."""
+    n = m.shape[1]
+    tol = 10e-8
+    cosa = math.cos(angle)
+    sina = math.sin(angle)
+    ctr = float(n) / 2 - 0.5
+    idx = np.arange(n, dtype=np.float64)
+    sa = sina * (idx - ctr)
+    ca = cosa * (idx - ctr)
+    V = (ca[:, None] + sa[None, :]) + ctr   # out(j, i): row j, column i
+    H = (-sa[:, None] + ca[None, :]) + ctr
+    top = V.astype(np.int64)
+    left = H.astype(np.int64)
+    bottom = top + 1
+    right = left + 1
+
+    def cround(x):
+        return np.where(x >= 0, np.floor(x + 0.5), np.ceil(x - 0.5)).astype(np.int64)
+
+    negv = V < -tol
+    top = np.where(negv, top - 1, top)
+    rv = cround(V)
+    edge = (~negv) & (rv == n - 1) & ((V - rv) < tol)
+    top = np.where(edge, rv, top)
+    bottom = np.where(edge, rv, bottom)
+    negh = H < -tol
+    left = np.where(negh, left - 1, left)
+    rh = cround(H)
+    edgeh = (~negh) & (rh == n - 1) & ((H - rh) < tol)
+    left = np.where(edgeh, rh, left)
+    right = np.where(edgeh, rh, right)
+    ok = (top >= 0) & (bottom < n) & (left >= 0) & (right < n)
+    t_, b_ = np.clip(top, 0, n - 1), np.clip(bottom, 0, n - 1)
+    l_, r_ = np.clip(left, 0, n - 1), np.clip(right, 0, n - 1)
+    tl, tr, bl, br = m[t_, l_], m[t_, r_], m[b_, l_], m[b_, r_]
+    hd = H - left
+    vd = V - top
+    tb = tl + hd * (tr - tl)
+    bb = bl + hd * (br - bl)
+    out = tb + vd * (bb - tb)
+    return np.where(ok, out, cval)
+
+
+def _aproj_conv(comb, A, workarea, oversampling):
+    """generate_convolution_kernel_aproj before the truncation
+    (aw_projection.cpp:290-348): the W-screen times the beam on the
+    workarea's corners, then the forward 2-D FFT."""
+    arr = workarea * oversampling
+    half = workarea // 2
+    rows = np.concatenate([np.arange(0, half), np.arange(arr - half, arr)])
+    offs = np.concatenate([np.arange(0, half), np.arange(-half, 0)])
+    tmp = np.zeros((arr, arr), dtype=np.complex128)
+    tmp[np.ix_(rows, rows)] = comb[np.ix_(rows, rows)] * A[np.ix_(half + offs, half + offs)]
+    return scipy.fft.fft2(tmp)
+
+
+def _conv_truncate_and_cache(conv, arr, max_support, oversampling, trunc_perc, current):
+    L = lib()
+    convF = np.asfortranarray(conv).reshape(-1, order="F").view(np.float64).copy()
+    support = L.orc_wkernel_truncate(_d(convF), ctypes.c_int64(arr), ctypes.c_int(max_support),
+                                     ctypes.c_int(oversampling), ctypes.c_double(trunc_perc), ctypes.c_int(current))
+    return support, convF
+
+
+def _conv_cache(convF, arr, support, oversampling):
+    L = lib()
+    cs = (oversampling // 2) * 2 + 1
+    K = 2 * support + 1
+    cache = np.empty(2 * cs * cs * K * K)
+    L.orc_wkernel_cache(_d(convF), ctypes.c_int64(arr), ctypes.c_int(support), ctypes.c_int(oversampling), _d(cache))
+    return cache
+
+
 def convolve_to_grid(kf, support, image_size, uv, vis, weights, kernel_exact=True, oversampling=1, shift_uv=True,
                      halfplane=True, generate_beam=True, wproj: WProj | None = None, w=None, cell_size=0.0,
-                     analytic_gcf=True, threads=1, fast=False, trunc=None):
+                     analytic_gcf=True, threads=1, fast=False, trunc=None, aproj: AProj | None = None):
     """stp::convolve_to_grid, gridder.h:240-997.  uv in pixels (n x 2).
 
     ``trunc`` is the kernel functor's own parameter (truncation radius or
@@ -457,6 +647,50 @@ def convolve_to_grid(kf, support, image_size, uv, vis, weights, kernel_exact=Tru
         scaling = float(image_size) / float(workarea)
         aa = img_dom_kernel(kf, trunc, workarea, analytic_gcf)
         cur = int(wproj.max_wpconv_support)
+        if aproj is not None and aproj.enabled:
+            # A-projection (gridder.h:507-520,686-745): per plane and time step
+            order = np.argsort(np.abs(np.ascontiguousarray(np.asarray(w, dtype=np.float64).reshape(-1))),
+                               kind="stable")
+            slha = np.asarray(aproj.lha, dtype=np.float64).reshape(-1)[order]
+            T = int(aproj.num_timesteps)
+            lha_planes, ts_of = average_lha_planes(slha, good, T)
+            dec = (aproj.obs_dec * math.pi) / 180.0
+            ra = (aproj.obs_ra * math.pi) / 180.0
+            fov = arc_sec_to_rad(cell_size) * float(image_size)
+            arr = workarea * oversampling
+            angles = [parangle(float(lha_planes[t]), dec, ra) for t in range(T)]
+            A0 = generate_a_kernel(aproj.pbeam_coefs, fov, workarea) if aproj.aproj_opt else None
+            good_all = good.copy()
+            for p in range(nplanes):
+                b = int(first[p])
+                e = n if p == nplanes - 1 else int(first[p + 1])
+                comb = np.empty(2 * arr * arr)
+                L.orc_wkernel_image_domain(ctypes.c_double(float(w_avg[p])), _d(np.ascontiguousarray(aa)),
+                                           ctypes.c_int(workarea), ctypes.c_int(oversampling),
+                                           ctypes.c_double(arc_sec_to_rad(cell_size)), ctypes.c_double(scaling),
+                                           _d(comb))
+                M = comb.view(np.complex128).reshape((arr, arr), order="F")
+                if aproj.aproj_opt:
+                    conv = _aproj_conv(M, A0, workarea, oversampling)
+                    cur, _ = _conv_truncate_and_cache(conv, arr, int(wproj.max_wpconv_support), oversampling,
+                                                      float(wproj.kernel_trunc_perc), cur)
+                for t in range(T):
+                    if aproj.aproj_opt:
+                        sh = np.fft.fftshift(conv)
+                        conv = np.fft.fftshift(rotate_matrix_cx(sh, angles[t], sh[0, 0]))
+                        convF = np.asfortranarray(conv).reshape(-1, order="F").view(np.float64).copy()
+                    else:
+                        A = generate_a_kernel(aproj.pbeam_coefs, fov, workarea, angles[t])
+                        conv = _aproj_conv(M, A, workarea, oversampling)
+                        cur, convF = _conv_truncate_and_cache(conv, arr, int(wproj.max_wpconv_support),
+                                                              oversampling, float(wproj.kernel_trunc_perc), cur)
+                    cache = _conv_cache(convF, arr, cur, oversampling)
+                    res.plane_supports.append(cur)
+                    res.plane_w.append(float(w_avg[p]))
+                    good[:] = np.where(ts_of == t, good_all, 0)
+                    accumulate(2, empty, cache, cur, b, e)
+            good[:] = good_all
+            nplanes = 0
         for p in range(nplanes):
             b = int(first[p])
             e = n if p == nplanes - 1 else int(first[p + 1])
@@ -515,7 +749,9 @@ def image_visibilities(vis, weights, uvw, image_size, cell_size, padding_factor=
                        kernel_support=3, kernel_exact=True, oversampling=8, generate_beam=False,
                        gridding_correction=True, analytic_gcf=False, num_wplanes=0, wplanes_median=False,
                        max_wpconv_support=0, undersampling_opt=1, kernel_trunc_perc=0.0, hankel_opt=False,
-                       hankel_proj_slice=False, interp_type=LINEAR, threads=1, fast=False, return_grid=False):
+                       hankel_proj_slice=False, interp_type=LINEAR, aproj_numtimesteps=0, obs_dec=0.0, obs_ra=0.0,
+                       aproj_opt=False, aproj_mask_perc=0.0, lha=None, pbeam_coefs=None, threads=1, fast=False,
+                       return_grid=False):
     """stp_python.image_visibilities_wrapper (stp-python/stp_python.cpp:17-140)
     -> ImageVisibilities (stp/imager/imager.cpp:12-68) -> image_visibilities
     (stp/imager/imager.h:233-376).  Returns (image, beam)."""
@@ -532,8 +768,9 @@ def image_visibilities(vis, weights, uvw, image_size, cell_size, padding_factor=
     uv[:, 1] = uvw[:, 1] * inv
     wp = WProj(num_wplanes, max_wpconv_support, undersampling_opt, kernel_trunc_perc, wplanes_median, hankel_opt,
                hankel_proj_slice, interp_type)
+    ap = AProj(int(aproj_numtimesteps), float(obs_dec), float(obs_ra), bool(aproj_opt), lha, pbeam_coefs)
     g = convolve_to_grid(kernel_func, kernel_support, padded, uv, vis, weights, kernel_exact, oversampling, True,
-                         True, generate_beam, wp, uvw[:, 2], cell_size, analytic_gcf, threads, fast)
+                         True, generate_beam, wp, uvw[:, 2], cell_size, analytic_gcf, threads, fast, aproj=ap)
     img = c2r(g.vis_grid, padded, threads)
     beam = c2r(g.sampling_grid, padded, threads) if generate_beam else None
     out_img = np.zeros((0, 0))

@@ -29,7 +29,7 @@ def test_library_exports_all_symbols():
     L = ctypes.CDLL(capi.LIB_PATH)
     for name in _declared():
         assert hasattr(L, name), name
-    assert L.stpgpu_abi_version() == 1
+    assert L.stpgpu_abi_version() == 2
 
 
 def test_struct_sizes_match_header():

@@ -176,6 +176,49 @@ def test_imager_hankel_fp32c_vs_oracle(ctx):
     assert peak_rel(img32.astype(np.float64), ri) < 1e-5
 
 
+def _aproj_case(seed):
+    s = make_snapshot(seed, 4000, 256, 20.0, n_src=4, flux=(1.0, 5.0), noise_sigma=0.05, w_range=(-600.0, 600.0))
+    lha = np.random.default_rng(seed).uniform(-3.0, 2.0, s.vis.size)
+    kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=4, analytic_gcf=False,
+              num_wplanes=3, max_wpconv_support=8, kernel_trunc_perc=1.0, aproj_numtimesteps=3, obs_dec=-40.0,
+              obs_ra=25.0, lha=lha, pbeam_coefs=[0.3, 0.8, 1.0, 0.5, 0.2])
+    return s, kw
+
+
+@pytest.mark.parametrize("opt", [False, True])
+def test_imager_aproj_fp64_vs_oracle(ctx, opt):
+    """A-projection: kernels per W-plane and hour-angle step, the beam rotated per step (or, with aproj_opt,
+    the convolution kernel rotated step after step)."""
+    s, kw = _aproj_case(61)
+    kw["aproj_opt"] = opt
+    img, _, info = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    ri, _, g = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, return_grid=True, **kw)
+    assert info.max_plane_support == max(g.plane_supports)
+    assert peak_rel(img, ri) < TOL64
+    # the beam changed the image (against plain W-projection)
+    wkw = {k: v for k, v in kw.items() if k not in ("aproj_numtimesteps", "obs_dec", "obs_ra", "lha", "pbeam_coefs",
+                                                    "aproj_opt")}
+    wimg, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **wkw)
+    assert peak_rel(img, wimg) > 1e-6
+
+
+def test_imager_aproj_device_pointers_and_fp32c(ctx):
+    import torch
+
+    s, kw = _aproj_case(62)
+    ri, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, **kw)
+    dkw = dict(kw, lha=torch.from_numpy(kw["lha"]).cuda())
+    out = torch.empty(256 * 256, dtype=torch.float64, device="cuda")
+    ctx.image_visibilities(torch.from_numpy(s.vis).cuda(), torch.from_numpy(s.weights).cuda(),
+                           torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda(), 256, s.cell_size,
+                           device_ptrs=True, image_out=out, **dkw)
+    torch.cuda.synchronize()
+    assert peak_rel(out.cpu().numpy().reshape(256, 256).T, ri) < TOL64
+    img32, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 256, s.cell_size, precision=capi.FP32C,
+                                         out_dtype=capi.F32, **kw)
+    assert peak_rel(img32.astype(np.float64), ri) < 1e-5
+
+
 @pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal"])
 def test_imager_wproj_near_tied_w(ctx, pattern):
     """|w| values that are equal in single precision but distinct in double
@@ -235,9 +278,14 @@ def test_imager_rejects_unsupported(ctx):
         ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, num_wplanes=2, max_wpconv_support=4,
                                kernel_exact=False, hankel_opt=True, interp_type=7)
     assert e.value.status == 1
-    with pytest.raises(capi.StpGpuError) as e:
-        ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, aproj_numtimesteps=2, kernel_exact=False)
-    assert e.value.status == 2
+    # A-projection needs W-projection, no Hankel option, hour angles and beam coefficients (imager.h:274-283)
+    lha = np.zeros(s.vis.size)
+    for extra in (dict(), dict(num_wplanes=2, max_wpconv_support=4, hankel_opt=True, pbeam_coefs=[1.0], lha=lha),
+                  dict(num_wplanes=2, max_wpconv_support=4, lha=lha)):
+        with pytest.raises(capi.StpGpuError) as e:
+            ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, 1.0, aproj_numtimesteps=2, kernel_exact=False,
+                                   **extra)
+        assert e.value.status == 1
     with pytest.raises(capi.StpGpuError) as e:
         ctx.image_visibilities(s.vis, s.weights, s.uvw, 64, -1.0)
     assert e.value.status == 1
