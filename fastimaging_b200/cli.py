@@ -8,7 +8,8 @@ array names, run on the GPU through the C ABI.
     python -m fastimaging_b200.cli run_sourcefind CONFIG.json INPUT.npz [-s OUT.json] [-o OUT.npz] [-l] [-n] [-b]
 
 Input NPZ arrays: uvw_lambda (n x 3), vis (n, complex), snr_weights (n),
-skymodel (k x 3: l, m, flux; with -d the model visibilities are subtracted);
+skymodel (k x 3: l, m, flux; with -d the model visibilities are subtracted),
+lha (n, hours; read when aprojection_settings enable A-projection);
 run_sourcefind reads image.  Outputs: islands as JSON
 ({"Islands": [{"sign", "val", "x_idx", "y_idx", "MomentsFit", "GaussianFit"}]},
 save_json_sf_output.cpp), label_map / image and beam as NPZ.
@@ -78,10 +79,16 @@ def load_config(path):
                max_wpconv_support=int(wp.get("max_wpconv_support", 0)), hankel_opt=bool(wp.get("hankel_opt", False)),
                undersampling_opt=int(wp.get("undersampling_opt", 1)),
                kernel_trunc_perc=float(wp.get("kernel_trunc_perc", 0.0)))
+    cfg["hankel_proj_slice"] = bool(wp.get("hankel_proj_slice", False))
+    cfg["interp_type"] = capi.LINEAR
     if "interp_type" in wp:
         pick(INTERP, wp["interp_type"], "interp_type")
+        cfg["interp_type"] = {"linear": capi.LINEAR, "cosine": capi.COSINE, "cubic": capi.CUBIC}[wp["interp_type"]]
     ap = doc.get("aprojection_settings", {})
-    cfg["aproj_numtimesteps"] = int(ap.get("aproj_numtimesteps", 0))
+    cfg.update(aproj_numtimesteps=int(ap.get("aproj_numtimesteps", 0)), obs_dec=float(ap.get("obs_dec", 0.0)),
+               obs_ra=float(ap.get("obs_ra", 0.0)), aproj_opt=bool(ap.get("aproj_opt", False)),
+               aproj_mask_perc=float(ap.get("aproj_mask_perc", 0.0)),
+               pbeam_coefs=[float(v) for v in ap.get("pbeam_coefs", [])])
 
     sf = doc.get("sourcefind_settings", {})
     cfg.update(detection_n_sigma=float(sf.get("sourcefind_detection", 0.0)),
@@ -132,8 +139,12 @@ def islands_json(islands, gaussian_fitting):
 def _imager_kw(cfg):
     keys = ("padding_factor", "kernel_func", "kernel_support", "kernel_exact", "oversampling", "generate_beam",
             "gridding_correction", "analytic_gcf", "num_wplanes", "wplanes_median", "max_wpconv_support",
-            "undersampling_opt", "kernel_trunc_perc", "hankel_opt", "aproj_numtimesteps", "padded_image_size")
-    return {k: cfg[k] for k in keys}
+            "undersampling_opt", "kernel_trunc_perc", "hankel_opt", "hankel_proj_slice", "interp_type",
+            "aproj_numtimesteps", "padded_image_size")
+    kw = {k: cfg[k] for k in keys}
+    if cfg["aproj_numtimesteps"] > 0:
+        kw.update({k: cfg[k] for k in ("obs_dec", "obs_ra", "aproj_opt", "aproj_mask_perc", "pbeam_coefs")})
+    return kw
 
 
 def _sf_args(cfg, swapped=False):
@@ -170,8 +181,11 @@ def _run_imager(ctx, cfg, npz, diff, log):
     if diff:
         vis = ctx.model_visibilities(np.asarray(npz["skymodel"], dtype=np.float64), uvw, vis=vis)
         log("Use residual visibilities - input visibilities subtracted from model visibilities")
+    kw = _imager_kw(cfg)
+    if cfg["aproj_numtimesteps"] > 0:
+        kw["lha"] = np.asarray(npz["lha"], dtype=np.float64).reshape(-1)  # reduce.cpp:107-111
     t0 = time.perf_counter()
-    img, beam, info = ctx.image_visibilities(vis, w, uvw, cfg["image_size"], cfg["cell_size"], **_imager_kw(cfg))
+    img, beam, info = ctx.image_visibilities(vis, w, uvw, cfg["image_size"], cfg["cell_size"], **kw)
     return img, beam, info, time.perf_counter() - t0
 
 

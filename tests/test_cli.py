@@ -39,6 +39,15 @@ def test_config_keys_and_defaults(tmp_path):
     p.write_text(json.dumps({"imager_settings": {"kernel_function": "Bessel"}}))
     with pytest.raises(ValueError):
         cli.load_config(str(p))
+    # Hankel and A-projection settings (load_json_config.cpp: wprojection_settings, aprojection_settings)
+    p.write_text(json.dumps({"wprojection_settings": {"num_wplanes": 4, "hankel_opt": True, "hankel_proj_slice": True,
+                                                      "interp_type": "cubic"},
+                             "aprojection_settings": {"aproj_numtimesteps": 3, "obs_dec": -30.0, "obs_ra": 20.0,
+                                                      "pbeam_coefs": [0.5, 1.0, 0.5], "aproj_opt": True}}))
+    h = cli.load_config(str(p))
+    assert h["hankel_opt"] and h["hankel_proj_slice"] and h["interp_type"] == capi.CUBIC
+    assert h["aproj_numtimesteps"] == 3 and h["pbeam_coefs"] == [0.5, 1.0, 0.5] and h["aproj_opt"]
+    assert h["obs_dec"] == -30.0 and h["obs_ra"] == 20.0
     empty = tmp_path / "e.json"
     empty.write_text("")
     with pytest.raises(RuntimeError):

@@ -57,10 +57,28 @@ def test_image_visibilities_wrapper_empty_result():
     assert img.shape == (0, 0) and bm.shape == (0, 0)
 
 
-def test_image_visibilities_wrapper_rejects_aprojection():
-    s = make_snapshot(24, 100, 64, 1.0, n_src=1)
+def test_image_visibilities_wrapper_aprojection_and_hankel():
+    s = make_snapshot(24, 3000, 128, 10.0, n_src=2, w_range=(-500.0, 500.0))
+    # A-projection without W-projection is an error (imager.h:279-280)
     with pytest.raises(RuntimeError):
-        stp_python.image_visibilities_wrapper(s.vis, s.weights, s.uvw, 64, s.cell_size, aproj_numtimesteps=2)
+        stp_python.image_visibilities_wrapper(s.vis, s.weights, s.uvw, 128, s.cell_size, aproj_numtimesteps=2)
+    lha = np.linspace(-2.0, 2.0, s.vis.size)
+    kw = dict(kernel_func=stp_python.KernelFunction.GaussianSinc, kernel_exact=False, kernel_oversampling=4,
+              num_wplanes=2, max_wpconv_support=6, kernel_trunc_perc=1.0)
+    img, _ = stp_python.image_visibilities_wrapper(s.vis, s.weights, s.uvw, 128, s.cell_size, aproj_numtimesteps=2,
+                                                   obs_dec=-30.0, obs_ra=10.0, lha=lha,
+                                                   pbeam_coefs=np.array([0.2, 1.0, 0.4]), **kw)
+    ref, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 128, s.cell_size, kernel_func=orc.GaussianSinc,
+                                    kernel_exact=False, oversampling=4, num_wplanes=2, max_wpconv_support=6,
+                                    kernel_trunc_perc=1.0, aproj_numtimesteps=2, obs_dec=-30.0, obs_ra=10.0, lha=lha,
+                                    pbeam_coefs=[0.2, 1.0, 0.4])
+    assert np.max(np.abs(img - ref)) < 1e-10 * np.max(np.abs(ref))
+    img, _ = stp_python.image_visibilities_wrapper(s.vis, s.weights, s.uvw, 128, s.cell_size, hankel_opt=True,
+                                                   interp_type=stp_python.InterpType.CUBIC, **kw)
+    ref, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, 128, s.cell_size, kernel_func=orc.GaussianSinc,
+                                    kernel_exact=False, oversampling=4, num_wplanes=2, max_wpconv_support=6,
+                                    kernel_trunc_perc=1.0, hankel_opt=True, interp_type=orc.CUBIC)
+    assert np.max(np.abs(img - ref)) < 1e-10 * np.max(np.abs(ref))
 
 
 def test_source_find_wrapper_matches_oracle():
