@@ -383,11 +383,14 @@ struct GridLaunch {
 // Autotuned gridder layout bits beside the tile width (low 8 bits).
 constexpr int kLayoutPersist = 1 << 8; // batch: persistent work queue
 constexpr int kLayoutCols = 1 << 9;    // column-packed tile gridder (grid_tile_cols)
+constexpr int kLayoutTaps = 1 << 10;   // lane-per-tap tile gridder (grid_tile_taps)
+// gridder form of a layout: 0 lanes-per-item, 1 column-packed, 2 lane-per-tap
+inline int form_of(int lay) { return (lay & kLayoutCols) ? 1 : ((lay & kLayoutTaps) ? 2 : 0); }
 
 template <typename R, int COMP>
 GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, int vis_c64, const double* d_wts,
     const double* d_uv, int uv_is_pixels, int64_t n, int tile_c = TILE_C_DEFAULT, GridLaunch<R>* defer = nullptr,
-    bool cols = false)
+    int form = 0)
 {
     if (tile_c != 32 && tile_c != 16)
         fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32");
@@ -453,6 +456,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
 
     // ---- kernels
     const uint32_t* sorted_perm = nullptr;
+    Item<R>* items_sorted = nullptr; // W-projection: the items in |w| order
     const int64_t* plane_first = nullptr;
     int nplanes = 0;
     const R* k1d = nullptr;
@@ -516,7 +520,11 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         uint32_t* gflag = c->buf<uint32_t>("gflag", nn + 1);
         uint32_t* cgood = c->buf<uint32_t>("cgood", nn + 1);
         double* absw_sorted = c->buf<double>("absw_sorted", nn);
-        k_gather_good<R><<<grid1d(n, 256), 256, 0, st>>>(perm, items, pp.absw_key, n, good_sorted, gflag, absw_sorted);
+        // binning and gridding read the items in |w| order (sequential
+        // passes instead of gathers through the permutation)
+        items_sorted = c->buf<Item<R>>("items_sorted", nn);
+        k_gather_good<R><<<grid1d(n, 256), 256, 0, st>>>(perm, items, pp.absw_key, n, good_sorted, gflag, absw_sorted,
+            items_sorted);
         STPGPU_CHECK_LAUNCH();
         STPGPU_CUDA_TRY(cudaMemsetAsync(gflag + n, 0, sizeof(uint32_t), st));
         size_t tb2 = 0;
@@ -680,7 +688,9 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
             hq.Cp = c->buf<double>("hkC", size_t(P) * 2 * hq.n);
             k_hankel_plane<<<P, 1024, 0, st>>>(wq, hq);
         } else {
-            k_wkernel_plane<<<P, 1024, 0, st>>>(wq);
+            const size_t ct_bytes = sizeof(double) * size_t(arr);
+            wq.ctab_in_smem = ct_bytes <= 24 * 1024;
+            k_wkernel_plane<<<P, 1024, wq.ctab_in_smem ? ct_bytes : 0, st>>>(wq);
         }
         STPGPU_CHECK_LAUNCH();
         // per-offset K x K tables in the gridder's precision: worst-case
@@ -724,6 +734,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     if (!large_support(s) && cap > 0xffffffffull)
         fail(STPGPU_ERR_INVALID_ARG, "too many visibilities for one snapshot");
     uint32_t* list = large_support(s) ? nullptr : c->buf<uint32_t>("tlist", cap);
+    Item<R>* bin_items = items_sorted ? items_sorted : items;
     BinParams bp {};
     bp.N = N;
     bp.image_rows = image_rows;
@@ -732,6 +743,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     bp.tile_c = tile_c;
     bp.support = s.support;
     bp.plane_support = plane_support;
+    bp.presorted = items_sorted != nullptr;
     bp.ts_of = ts_of;
     bp.ntimesteps = std::max(s.ntimesteps, 1);
     bp.exact = kernel_exact;
@@ -745,7 +757,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     STPGPU_CUDA_TRY(cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (ntiles + 1), st));
     STPGPU_CUDA_TRY(cudaMemsetAsync(tcur, 0, sizeof(uint32_t) * (ntiles + 1), st));
     if (n > 0) {
-        k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, sorted_perm, plane_first, nplanes);
+        k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
     }
     k_scan_single<<<1, 1024, 0, st>>>(tcount, toff, ntiles);
@@ -760,7 +772,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         bp.list_capacity = cap;
     }
     if (n > 0) {
-        k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, items, sorted_perm, plane_first, nplanes);
+        k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
     }
     g.d_nitems = toff + ntiles;
@@ -776,7 +788,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     gp.os = os;
     gp.cs = cs;
     gp.exact_wrap = kernel_exact;
-    gp.items = items;
+    gp.items = bin_items;
     gp.tile_off = toff;
     gp.list = list;
     gp.k1d = k1d;
@@ -822,14 +834,22 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         };
         const bool b = s.beam != 0;
         const bool t32 = tile_c == 32;
-        // the column-packed gridder needs one footprint segment per axis and tile
-        const bool use_cols = cols && kind != GK_EXACT && N >= 2 * (2 * conv_support + 1 + 32) + 2;
+        // the column-packed and lane-per-tap gridders need one footprint
+        // segment per axis and tile
+        const bool clip_ok = kind != GK_EXACT && N >= 2 * (2 * conv_support + 1 + 32) + 2;
+        const bool use_cols = form == 1 && clip_ok, use_taps = form == 2 && clip_ok;
         if (use_cols && kind == GK_WPROJ)
-            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32, true>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16, true>))
-              : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32, true>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16, true>));
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16, 1>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16, 1>));
         else if (use_cols)
-            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, true, 32, true>) : launch(k_grid_tiles<R, COMP, KM_SEP, true, 16, true>))
-              : (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, false, 32, true>) : launch(k_grid_tiles<R, COMP, KM_SEP, false, 16, true>));
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, true, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_SEP, true, 16, 1>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, false, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_SEP, false, 16, 1>));
+        else if (use_taps && kind == GK_WPROJ)
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32, 2>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16, 2>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32, 2>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16, 2>));
+        else if (use_taps)
+            b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, true, 32, 2>) : launch(k_grid_tiles<R, COMP, KM_SEP, true, 16, 2>))
+              : (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, false, 32, 2>) : launch(k_grid_tiles<R, COMP, KM_SEP, false, 16, 2>));
         else if (kind == GK_WPROJ)
             b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16>))
               : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16>));
@@ -988,12 +1008,14 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     const int precision = sizeof(R) == 8 ? STPGPU_FP64 : (COMP ? STPGPU_FP32C : STPGPU_FP32);
     const std::string cls = size_class(s, precision);
     GridOut g;
-    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c pins the tile width and gridder
-    // form (c: column-packed) instead of the autotuner's choice
+    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c|32t|16t pins the tile width and
+    // gridder form (c: column-packed, t: lane-per-tap) instead of the
+    // autotuner's choice
     if (const char* pin = std::getenv("STPGPU_GRIDDER_LAYOUT")) {
         const int w = std::atoi(pin);
         if (w == 16 || w == 32)
-            c->tune_set(cls, w | (std::strchr(pin, 'c') ? kLayoutCols : 0));
+            c->tune_set(cls,
+                w | (std::strchr(pin, 'c') ? kLayoutCols : 0) | (std::strchr(pin, 't') ? kLayoutTaps : 0));
     }
     int tuned_lay = 0;
     const bool have_tune = c->tune_get(cls, tuned_lay);
@@ -1024,7 +1046,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         STPGPU_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         try {
             g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, tuned_lay & 0xff, nullptr,
-                (tuned_lay & kLayoutCols) != 0);
+                form_of(tuned_lay));
             finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
         } catch (...) {
             cudaGraph_t dead = nullptr;
@@ -1041,7 +1063,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     } else if (have_tune || c->timing) {
         const int lay = have_tune ? tuned_lay : TILE_C_DEFAULT;
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
-            (lay & kLayoutCols) != 0);
+            form_of(lay));
     } else {
         for (auto& e : c->tev)
             if (!e)
@@ -1050,21 +1072,28 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         // tiles) and fills the cached tables, so no timed pass pays that
         // the column-packed form is a candidate for large kernels only (with
         // K <= 17 the lane-per-item form is faster on every measured workload)
-        const int lays[4] = { 32, 16, 32 | kLayoutCols, 16 | kLayoutCols };
-        float ms[4] = { 0.f, 0.f, 1e30f, 1e30f };
+        const int lays[6] = { 32, 16, 32 | kLayoutTaps, 16 | kLayoutTaps, 32 | kLayoutCols, 16 | kLayoutCols };
+        float ms[6] = { 0.f, 0.f, 1e30f, 1e30f, 1e30f, 1e30f };
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, 16);
         // the widest kernel the data actually uses (W-planes are truncated
         // below the maximum support), read back from the untimed pass
         const int used_support = s.nplanes > 0 ? std::max(read_back(c, g).max_support, 0) : s.support;
-        const int ncand = (2 * used_support + 1) > 17 ? 4 : 2;
-        for (int k = 0; k < ncand; k++) {
-            STPGPU_CUDA_TRY(cudaEventRecord(c->tev[0], c->stream));
-            g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lays[k] & 0xff, nullptr,
-                (lays[k] & kLayoutCols) != 0);
-            STPGPU_CUDA_TRY(cudaEventRecord(c->tev[1], c->stream));
-            STPGPU_CUDA_TRY(cudaEventSynchronize(c->tev[1]));
-            STPGPU_CUDA_TRY(cudaEventElapsedTime(&ms[k], c->tev[0], c->tev[1]));
-        }
+        // the clipped forms need one footprint segment per axis and tile
+        const bool clip_ok = !s.kernel_exact && s.N >= 2 * (2 * (s.nplanes > 0 ? s.max_support : s.support) + 33) + 2;
+        const int ncand = !clip_ok ? 2 : ((2 * used_support + 1) > 17 ? 6 : 4);
+        // each candidate timed twice, the faster pass kept (single passes
+        // of close candidates swap order from run to run)
+        for (int rep = 0; rep < 2; rep++)
+            for (int k = 0; k < ncand; k++) {
+                STPGPU_CUDA_TRY(cudaEventRecord(c->tev[0], c->stream));
+                g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lays[k] & 0xff, nullptr,
+                    form_of(lays[k]));
+                STPGPU_CUDA_TRY(cudaEventRecord(c->tev[1], c->stream));
+                STPGPU_CUDA_TRY(cudaEventSynchronize(c->tev[1]));
+                float t = 0.f;
+                STPGPU_CUDA_TRY(cudaEventElapsedTime(&t, c->tev[0], c->tev[1]));
+                ms[k] = rep == 0 ? t : std::min(ms[k], t);
+            }
         int best = 0;
         for (int k = 1; k < ncand; k++)
             if (ms[k] < ms[best])
@@ -1072,10 +1101,11 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         c->tune_set(cls, lays[best]);
         if (std::getenv("STPGPU_LOG_TUNING"))
             std::fprintf(stderr,
-                "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, column-packed 32/16 %.3f/%.3f ms"
-                " -> %d%s (single call)\n",
-                cls.c_str(), double(ms[0]), double(ms[1]), double(ms[2]), double(ms[3]), lays[best] & 0xff,
-                (lays[best] & kLayoutCols) ? " column-packed" : "");
+                "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, lane-per-tap 32/16 %.3f/%.3f ms,"
+                " column-packed 32/16 %.3f/%.3f ms -> %d%s (single call)\n",
+                cls.c_str(), double(ms[0]), double(ms[1]), double(ms[2]), double(ms[3]), double(ms[4]),
+                double(ms[5]), lays[best] & 0xff,
+                (lays[best] & kLayoutCols) ? " column-packed" : ((lays[best] & kLayoutTaps) ? " lane-per-tap" : ""));
     }
     if (!(repeat && c->single_exec))
         finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
@@ -1090,7 +1120,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         int lay = TILE_C_DEFAULT;
         c->tune_get(cls, lay);
         g = run_gridder<R, COMP>(c, s64, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
-            (lay & kLayoutCols) != 0);
+            form_of(lay));
         finish_imager<R>(c, s64, image_size, correction, g, d_image, d_beam, out_f32);
         sb = read_back(c, g);
     }

@@ -235,6 +235,7 @@ struct BinParams {
     int tile_c;              // tile width in grid columns (TILE_R rows per tile)
     int support;             // non-W-proj support
     const int* plane_support; // W-proj truncated support per plane (nullable)
+    int presorted;            // W-proj: `items` already permuted into |w| order
     const uint8_t* ts_of;     // A-projection: time step per visibility (nullable)
     int ntimesteps;           // planes are indexed plane * ntimesteps + step
     int exact;               // rows wrap negative (exact gridder)
@@ -303,6 +304,22 @@ __device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, int S
     item_centre(it, mir, p.N, cx, cy);
     const int N = p.N, rows_max = p.image_rows - 1;
     const int a = cy - S, b = cy - S + K - 1; // raw rows
+    {
+        // common case: the footprint wraps on neither axis, so it covers one
+        // range of tile rows and one of tile columns (tile sizes are powers
+        // of two; every index here is non-negative)
+        const int c = cx - S, d = cx - S + K - 1;
+        if (a >= 0 && b < N && c >= 0 && d < N) {
+            const int h = min(b, rows_max);
+            if (a > h)
+                return;
+            const int cshift = p.tile_c == 32 ? 5 : 4;
+            for (int t_r = a / TILE_R; t_r <= h / TILE_R; t_r++)
+                for (int t_c = c >> cshift; t_c <= (d >> cshift); t_c++)
+                    f(uint32_t(t_c) * uint32_t(p.tiles_r) + uint32_t(t_r));
+            return;
+        }
+    }
     TileRanges tr;
     tr.n = 0;
     {
@@ -359,14 +376,16 @@ __device__ __forceinline__ int plane_of(const int64_t* first, int P, int64_t k)
 
 // With W-projection (`order` = the |w| permutation, `first` = plane starts)
 // items are visited in |w| order and take the plane of their sorted
-// position; the fill pass records it in the item for the gridder.
+// position k; the fill pass records it in the item for the gridder.  With
+// p.presorted the items array is already in |w| order (item k is sorted
+// position k), else item order[k] is visited.
 template <typename R>
 __global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t* order, const int64_t* first, int P)
 {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= p.n)
         return;
-    const int64_t i = order ? int64_t(order[k]) : k;
+    const int64_t i = (order && !p.presorted) ? int64_t(order[k]) : k;
     const Item<R> it = items[i];
     if (!it.good)
         return;
@@ -374,7 +393,7 @@ __global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t*
     if (order) {
         int plane = plane_of(first, P, k);
         if (p.ts_of)
-            plane = plane * p.ntimesteps + p.ts_of[i];
+            plane = plane * p.ntimesteps + p.ts_of[order[k]];
         S = p.plane_support[plane];
     }
     for (int mir = 0; mir < int(it.good); mir++)
@@ -389,7 +408,7 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= p.n)
         return;
-    const int64_t i = order ? int64_t(order[k]) : k;
+    const int64_t i = (order && !p.presorted) ? int64_t(order[k]) : k;
     const Item<R> it = items[i];
     if (!it.good)
         return;
@@ -397,7 +416,7 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
     if (order) {
         int plane = plane_of(first, P, k);
         if (p.ts_of)
-            plane = plane * p.ntimesteps + p.ts_of[i];
+            plane = plane * p.ntimesteps + p.ts_of[order[k]];
         S = p.plane_support[plane];
         items[i].plane = uint16_t(plane);
     }
@@ -1038,12 +1057,165 @@ __device__ __forceinline__ void grid_tile_cols(const GridParams<R>& p, int tile,
 // One CTA (one warp) per tile of one snapshot.
 // Residency target: the shared-memory tile allows ~28 CTAs per SM at 16
 // columns (8 KB FP32/FP32C cell tile) and ~14 at 32; registers are capped to match.
-template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, bool COLS = false>
+// Lane-per-tap tile gridder (tabulated kernels).  One warp per tile; the
+// 32 list entries of a batch are clipped to the tile by their own lanes
+// (window rows [ilo, ihi) x columns [jlo, jhi)), then taken one at a time:
+// the entry's parameters are broadcast and its in-tile taps are spread over
+// the lanes, 32 per pass (lane = tap, column-major in the window, so that
+// consecutive lanes touch consecutive accumulator cells).  All taps of one
+// pass hit distinct cells, so there are no conflicts; consecutive passes are
+// ordered by __syncwarp.  Every lane does useful work on windows of 32 taps
+// or more; small kernels (K = 5 or 7 at one tile per footprint) fill most of
+// a pass.  Requires N >= 2 (Kmax + tile) + 2, as grid_tile_cols.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C>
+__device__ __forceinline__ void grid_tile_taps(const GridParams<R>& p, int tile, unsigned char* smem_raw)
+{
+    using A = Acc<R, COMP>;
+    using C2 = typename Cplx<R>::T;
+    A* acc = reinterpret_cast<A*>(smem_raw);
+    A* bacc = acc + (BEAM ? TILE_R * TILE_C : 0);
+    R* tab = reinterpret_cast<R*>(acc + (BEAM ? 2 : 1) * TILE_R * TILE_C);
+    const int lane = threadIdx.x;
+    const int gN = p.N, grows = p.image_rows, gos = p.os;
+    const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
+    const int r0 = tr * TILE_R, c0 = tc * TILE_C;
+
+    for (int t = lane; t < TILE_R * TILE_C; t += 32) {
+        acc_zero(&acc[t]);
+        if (BEAM)
+            acc_zero(&bacc[t]);
+    }
+    if (KMODE == KM_SEP) {
+        const int K = 2 * p.support + 1;
+        for (int t = lane; t < p.cs * K; t += 32)
+            tab[t] = p.k1d[t];
+    }
+    __syncwarp();
+
+    const uint32_t beg = p.tile_off[tile], end = p.tile_off[tile + 1];
+    for (uint32_t base = beg; base < end; base += 32) {
+        // this lane's entry, clipped to the tile
+        const uint32_t e = base + lane;
+        int K = 1, ilo = 0, nrows = 0, jlo = 0, ncols = 0, rowb = 0, colb = 0;
+        uint32_t koff = 0; // W-proj: table offset of the item's K x K kernel; separable: cpy*K << 16 | cpx*K
+        R vr = R(0), vi = R(0), wt = R(0);
+        int conj = 0;
+        if (e < end) {
+            const uint32_t code = p.list[e];
+            const uint32_t idx = code >> 1;
+            const int mir = int(code & 1u);
+            const Item<R> it = p.items[idx];
+            int cx, cy;
+            item_centre(it, mir, gN, cx, cy);
+            const int S = (KMODE == KM_WPROJ) ? p.plane_support[it.plane] : p.support;
+            K = 2 * S + 1;
+            int cpx = it.cpx, cpy = it.cpy;
+            if (mir && gos > 1) {
+                cpx = gos - cpx;
+                cpy = gos - cpy;
+            }
+            const int rb = cy - S, cb = cx - S;
+            int ihi, jhi, rsh, csh;
+            tile_span(rb, K, gN, r0, TILE_R, grows, false, ilo, ihi, rsh);
+            tile_span(cb, K, gN, c0, TILE_C, gN, true, jlo, jhi, csh);
+            nrows = max(ihi - ilo, 0);
+            ncols = nrows > 0 ? max(jhi - jlo, 0) : 0;
+            if (ncols == 0)
+                nrows = 0;
+            rowb = rb + rsh - r0; // local row of tap i: rowb + i
+            colb = cb + csh - c0; // local column of tap j: colb + j
+            vr = it.vr;
+            vi = mir ? -it.vi : it.vi;
+            wt = it.w;
+            if (KMODE == KM_WPROJ) {
+                conj = (it.flags >> (mir ? 1 : 0)) & 1u;
+                koff = p.wk_off[it.plane] + uint32_t((cpy * p.cs + cpx) * K * K);
+            } else {
+                koff = (uint32_t(cpy * K) << 16) | uint32_t(cpx * K);
+            }
+        }
+        const R vrw = vr * wt, viw = vi * wt;
+        const int nt = nrows * ncols;
+        const int np = (nt + 31) >> 5;
+        // passes of the batch: unit u belongs to the last lane whose start <= u
+        int incl = np;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        const int start = incl - np;
+        const int units = __shfl_sync(0xffffffffu, incl, 31);
+        // packed per-entry words for the broadcasts
+        const int geo = (ilo & 0xff) | ((jlo & 0xff) << 8) | ((nrows & 0xff) << 16) | ((conj & 1) << 24);
+        const int loc = (rowb & 0xffff) | int(unsigned(colb) << 16);
+        const int kn = (K & 0xffff) | (nt << 16);
+        const float rcp = nrows > 0 ? 1.0f / float(nrows) : 0.0f;
+        for (int u = 0; u < units; u++) {
+            const unsigned le = __ballot_sync(0xffffffffu, np > 0 && start <= u);
+            const int own = 31 - __clz(le);
+            const int pass = u - __shfl_sync(0xffffffffu, start, own);
+            const int o_geo = __shfl_sync(0xffffffffu, geo, own);
+            const int o_loc = __shfl_sync(0xffffffffu, loc, own);
+            const int o_kn = __shfl_sync(0xffffffffu, kn, own);
+            const uint32_t o_koff = __shfl_sync(0xffffffffu, koff, own);
+            const float o_rcp = __shfl_sync(0xffffffffu, rcp, own);
+            const R o_vr = __shfl_sync(0xffffffffu, vrw, own);
+            const R o_vi = __shfl_sync(0xffffffffu, viw, own);
+            const R o_wt = BEAM ? __shfl_sync(0xffffffffu, wt, own) : R(0);
+            const int o_nt = o_kn >> 16, o_K = o_kn & 0xffff;
+            const int t = pass * 32 + lane;
+            if (t < o_nt) {
+                // window column-major: consecutive lanes take consecutive rows,
+                // i.e. consecutive accumulator cells
+                const int o_nrows = (o_geo >> 16) & 0xff;
+                const int dj = int((float(t) + 0.5f) * o_rcp);
+                const int di = t - dj * o_nrows;
+                const int i = (o_geo & 0xff) + di, j = ((o_geo >> 8) & 0xff) + dj;
+                R kr, ki;
+                if (KMODE == KM_WPROJ) {
+                    const C2 v = p.wk[o_koff + uint32_t(i * o_K + j)];
+                    kr = v.x;
+                    ki = ((o_geo >> 24) & 1) ? -v.y : v.y;
+                } else {
+                    kr = tab[(o_koff >> 16) + uint32_t(i)] * tab[(o_koff & 0xffffu) + uint32_t(j)];
+                    ki = R(0);
+                }
+                const int row = int(short(o_loc & 0xffff)) + i, col = (o_loc >> 16) + j;
+                const int slot = col * TILE_R + row;
+                const R re = o_vr * kr - o_vi * ki;
+                const R im = o_vr * ki + o_vi * kr;
+                acc_rmw(&acc[slot], re, im);
+                if (BEAM)
+                    acc_rmw(&bacc[slot], kr * o_wt, ki * o_wt);
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    const int nr = min(TILE_R, grows - r0);
+    const int nc = min(TILE_C, gN - c0);
+    for (int q = lane; q < TILE_R * TILE_C; q += 32) {
+        const int rl = q % TILE_R, cl = q / TILE_R;
+        if (rl < nr && cl < nc) {
+            const size_t g = size_t(c0 + cl) * grows + (r0 + rl);
+            p.grid[g] = acc_value(acc[q]);
+            if (BEAM)
+                p.beam[g] = acc_value(bacc[q]);
+        }
+    }
+}
+
+// FORM: 0 lanes-per-item (grid_tile), 1 column-packed (grid_tile_cols),
+// 2 lane-per-tap (grid_tile_taps); the exact gridder always uses grid_tile.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, int FORM = 0>
 __global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) : 14) k_grid_tiles(GridParams<R> p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    if constexpr (COLS && KMODE != KM_EXACT)
+    if constexpr (FORM == 1 && KMODE != KM_EXACT)
         grid_tile_cols<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
+    else if constexpr (FORM == 2 && KMODE != KM_EXACT)
+        grid_tile_taps<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
     else
         grid_tile<R, COMP, KMODE, BEAM, TILE_C>(p, int(blockIdx.x), smem_raw);
 }
@@ -1429,17 +1601,20 @@ __global__ void __launch_bounds__(256) k_wplane_finish(const double* partial, co
 
 template <typename R>
 __global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, const double* absw, int64_t n,
-    uint8_t* good_sorted, uint32_t* gflag, double* absw_sorted)
+    uint8_t* good_sorted, uint32_t* gflag, double* absw_sorted, Item<R>* items_sorted)
 {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= n)
         return;
     const uint32_t i = perm[k];
-    uint8_t g = items[i].good != 0;
+    const Item<R> it = items[i];
+    uint8_t g = it.good != 0;
     good_sorted[k] = g;
     gflag[k] = g;
     if (absw_sorted)
         absw_sorted[k] = absw[i];
+    if (items_sorted)
+        items_sorted[k] = it; // binning and gridding read the items in |w| order
 }
 
 // The |w| order from a stable sort on 32-bit keys (float(|w|) rounded down)
@@ -1514,6 +1689,7 @@ struct WkParams {
     const double* aa; // image-domain AA kernel over the workarea
     const double* ctab; // cos(2 pi t / arr), t < arr
     int half, arr, os, cs, max_support, lh_max;
+    int ctab_in_smem; // k_wkernel_plane: launched with arr doubles of dynamic shared memory
     double scaled_cell, trunc_perc;
     double2* Qs;   // scratch [P][half][half]
     double2* Ts;   // scratch [P][lh_max][half]
@@ -1571,7 +1747,15 @@ __global__ void __launch_bounds__(1024) k_wkernel_plane(WkParams q)
     double2* conv = q.convd + size_t(p) * lh * lh;
     __shared__ double2 row0[1024];
     __shared__ int s_support;
-    auto C = [&](int t) { return q.ctab[t % arr]; };
+    // the cosine table in shared memory when the launch gave room for it
+    extern __shared__ double sct[];
+    const double* ct = q.ctab;
+    if (q.ctab_in_smem) {
+        for (int t = threadIdx.x; t < arr; t += blockDim.x)
+            sct[t] = q.ctab[t];
+        ct = sct;
+    }
+    auto C = [&](int t) { return ct[t % arr]; };
     // 1. image-domain quadrant Q[a][b] (row a, column b)
     for (int t = threadIdx.x; t < half * half; t += blockDim.x) {
         const int a = t % half, b = t / half;
