@@ -114,6 +114,8 @@ struct stpgpu_context {
     cudaGraph_t single_graph = nullptr;
     cudaGraphExec_t single_exec = nullptr;
     GridOut single_g {};
+    int single_launches = 0; // our kernels in single_graph (counted at capture)
+    int batch_launches = 0;  // our kernels in batch_graph
 
     void drop_single()
     {
@@ -1041,8 +1043,10 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         c->drop_single();
     if (repeat && c->single_exec) {
         STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
+        g_launches += c->single_launches; // the replay runs the captured kernels
         g = c->single_g;
     } else if (repeat && have_tune) {
+        const int before = g_launches;
         STPGPU_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         try {
             g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, tuned_lay & 0xff, nullptr,
@@ -1060,6 +1064,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         STPGPU_CUDA_TRY(cudaGraphInstantiate(&c->single_exec, c->single_graph, 0));
         STPGPU_CUDA_TRY(cudaGraphLaunch(c->single_exec, c->stream));
         c->single_g = g;
+        c->single_launches = g_launches - before;
     } else if (have_tune || c->timing) {
         const int lay = have_tune ? tuned_lay : TILE_C_DEFAULT;
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr,
@@ -1540,6 +1545,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
         STPGPU_CUDA_TRY(cudaGraphLaunch(c->batch_exec, main));
         STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, main));
+        g_launches = c->batch_launches; // the replay runs the captured kernels
         graph = 1;
     } else {
         // tile autotuner: time both tile widths for classes not seen before
@@ -1600,6 +1606,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
                 throw;
             }
             STPGPU_CUDA_TRY(cudaStreamEndCapture(main, &c->batch_graph));
+            c->batch_launches = g_launches;
             STPGPU_CUDA_TRY(cudaGraphInstantiate(&c->batch_exec, c->batch_graph, 0));
             STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
             STPGPU_CUDA_TRY(cudaGraphLaunch(c->batch_exec, main));

@@ -127,7 +127,7 @@ typedef struct {
      * [0] grid init (prepass, W-planes and W-kernels, binning),
      * [1] grid loop (the tile gridder kernel), [2] FFT, [3] normalise. */
     double phase_ms[4];
-    int32_t n_launches; /* kernels this library launched (cuFFT's excluded) */
+    int32_t n_launches; /* kernels of this library the call ran, graph replays included (cuFFT's excluded) */
     int32_t reserved;
 } stpgpu_imager_info;
 
@@ -276,7 +276,7 @@ typedef struct {
     int32_t graph;           /* 1: ran as a replay of a captured CUDA graph */
     int32_t gridder_launches; /* persistent gridder launches (one per kernel variant) */
     int32_t tuned_classes;   /* size classes the tile autotuner measured in this call */
-    int32_t n_launches;      /* kernels this library launched when not replayed (cuFFT's excluded) */
+    int32_t n_launches;      /* kernels of this library the call ran, graph replays included (cuFFT's excluded) */
 } stpgpu_batch_info;
 
 /* Many snapshots of uneven sizes in one call: per-snapshot preparation on

@@ -77,6 +77,7 @@ def test_batch_device_eager_graph_and_replay_match_single(ctx):
         torch.cuda.synchronize()
         outs, infos, bi = ctx.image_batch(snaps, precision=capi.FP64, out_dtype=capi.F64, device_ptrs=True)
         graphs.append(bi.graph)
+        assert bi.n_launches > len(snaps), call  # graph replays run the captured kernels
         for (s, kw), out, info, (ref, rinfo) in zip(cases, outs, infos, refs):
             n = kw["image_size"]
             assert info.sample_grid_total == rinfo.sample_grid_total

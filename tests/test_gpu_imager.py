@@ -327,6 +327,8 @@ def test_repeated_device_calls_replay_graph_with_new_data(ctx):
             ref = ref1 if call < 3 else ref2
             assert info.image_size == 256
             assert peak_rel(got, ref) < 1e-12, call
+            # every call, replays included, reports the kernels of ours it ran
+            assert info.n_launches > 5, call
     finally:
         c2.close()
 
