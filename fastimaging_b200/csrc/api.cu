@@ -394,8 +394,8 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     const double* d_uv, int uv_is_pixels, int64_t n, int tile_c = TILE_C_DEFAULT, GridLaunch<R>* defer = nullptr,
     int form = 0)
 {
-    if (tile_c != 32 && tile_c != 16)
-        fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32");
+    if (tile_c != 32 && tile_c != 16 && !(tile_c == 8 && form == 2))
+        fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32 (8 with the lane-per-tap gridder)");
     using C2 = typename Cplx<R>::T;
     check_pars(s);
     cudaStream_t st = c->stream;
@@ -846,7 +846,25 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         else if (use_cols)
             b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, true, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_SEP, true, 16, 1>))
               : (t32 ? launch(k_grid_tiles<R, COMP, KM_SEP, false, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_SEP, false, 16, 1>));
-        else if (use_taps && kind == GK_WPROJ)
+        else if (use_taps && tile_c == 8) {
+            // four 8-column tiles per block (k_grid_tiles_mw)
+            const int tb = int((smem + 15) / 16 * 16);
+            auto launch_mw = [&](auto kern) {
+                const size_t bs = size_t(4) * size_t(tb);
+                if (bs > 48 * 1024)
+                    STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bs)));
+                c->mark(1);
+                kern<<<unsigned((ntiles + 3) / 4), 128, bs, st>>>(gp, ntiles, tb);
+                STPGPU_CHECK_LAUNCH();
+                c->mark(2);
+            };
+            if (kind == GK_WPROJ)
+                b ? launch_mw(k_grid_tiles_mw<R, COMP, KM_WPROJ, true, 8, 4>)
+                  : launch_mw(k_grid_tiles_mw<R, COMP, KM_WPROJ, false, 8, 4>);
+            else
+                b ? launch_mw(k_grid_tiles_mw<R, COMP, KM_SEP, true, 8, 4>)
+                  : launch_mw(k_grid_tiles_mw<R, COMP, KM_SEP, false, 8, 4>);
+        } else if (use_taps && kind == GK_WPROJ)
             b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32, 2>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16, 2>))
               : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32, 2>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16, 2>));
         else if (use_taps)
@@ -1010,12 +1028,12 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
     const int precision = sizeof(R) == 8 ? STPGPU_FP64 : (COMP ? STPGPU_FP32C : STPGPU_FP32);
     const std::string cls = size_class(s, precision);
     GridOut g;
-    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c|32t|16t pins the tile width and
+    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c|32t|16t|8t pins the tile width and
     // gridder form (c: column-packed, t: lane-per-tap) instead of the
     // autotuner's choice
     if (const char* pin = std::getenv("STPGPU_GRIDDER_LAYOUT")) {
         const int w = std::atoi(pin);
-        if (w == 16 || w == 32)
+        if (w == 16 || w == 32 || (w == 8 && std::strchr(pin, 't')))
             c->tune_set(cls,
                 w | (std::strchr(pin, 'c') ? kLayoutCols : 0) | (std::strchr(pin, 't') ? kLayoutTaps : 0));
     }
@@ -1077,15 +1095,16 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         // tiles) and fills the cached tables, so no timed pass pays that
         // the column-packed form is a candidate for large kernels only (with
         // K <= 17 the lane-per-item form is faster on every measured workload)
-        const int lays[6] = { 32, 16, 32 | kLayoutTaps, 16 | kLayoutTaps, 32 | kLayoutCols, 16 | kLayoutCols };
-        float ms[6] = { 0.f, 0.f, 1e30f, 1e30f, 1e30f, 1e30f };
+        const int lays[7] = { 32, 16, 32 | kLayoutTaps, 16 | kLayoutTaps, 8 | kLayoutTaps, 32 | kLayoutCols,
+            16 | kLayoutCols };
+        float ms[7] = { 0.f, 0.f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f };
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, 16);
         // the widest kernel the data actually uses (W-planes are truncated
         // below the maximum support), read back from the untimed pass
         const int used_support = s.nplanes > 0 ? std::max(read_back(c, g).max_support, 0) : s.support;
         // the clipped forms need one footprint segment per axis and tile
         const bool clip_ok = !s.kernel_exact && s.N >= 2 * (2 * (s.nplanes > 0 ? s.max_support : s.support) + 33) + 2;
-        const int ncand = !clip_ok ? 2 : ((2 * used_support + 1) > 17 ? 6 : 4);
+        const int ncand = !clip_ok ? 2 : ((2 * used_support + 1) > 17 ? 7 : 5);
         // each candidate timed twice, the faster pass kept (single passes
         // of close candidates swap order from run to run)
         for (int rep = 0; rep < 2; rep++)
@@ -1106,10 +1125,10 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         c->tune_set(cls, lays[best]);
         if (std::getenv("STPGPU_LOG_TUNING"))
             std::fprintf(stderr,
-                "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, lane-per-tap 32/16 %.3f/%.3f ms,"
-                " column-packed 32/16 %.3f/%.3f ms -> %d%s (single call)\n",
+                "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, lane-per-tap 32/16/8 %.3f/%.3f/%.3f"
+                " ms, column-packed 32/16 %.3f/%.3f ms -> %d%s (single call)\n",
                 cls.c_str(), double(ms[0]), double(ms[1]), double(ms[2]), double(ms[3]), double(ms[4]),
-                double(ms[5]), lays[best] & 0xff,
+                double(ms[5]), double(ms[6]), lays[best] & 0xff,
                 (lays[best] & kLayoutCols) ? " column-packed" : ((lays[best] & kLayoutTaps) ? " lane-per-tap" : ""));
     }
     if (!(repeat && c->single_exec))

@@ -313,7 +313,7 @@ __device__ __forceinline__ void for_item_tiles(const Item<R>& it, int mir, int S
             const int h = min(b, rows_max);
             if (a > h)
                 return;
-            const int cshift = p.tile_c == 32 ? 5 : 4;
+            const int cshift = p.tile_c == 32 ? 5 : (p.tile_c == 16 ? 4 : 3);
             for (int t_r = a / TILE_R; t_r <= h / TILE_R; t_r++)
                 for (int t_c = c >> cshift; t_c <= (d >> cshift); t_c++)
                     f(uint32_t(t_c) * uint32_t(p.tiles_r) + uint32_t(t_r));
@@ -1075,7 +1075,7 @@ __device__ __forceinline__ void grid_tile_taps(const GridParams<R>& p, int tile,
     A* acc = reinterpret_cast<A*>(smem_raw);
     A* bacc = acc + (BEAM ? TILE_R * TILE_C : 0);
     R* tab = reinterpret_cast<R*>(acc + (BEAM ? 2 : 1) * TILE_R * TILE_C);
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31;
     const int gN = p.N, grows = p.image_rows, gos = p.os;
     const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
     const int r0 = tr * TILE_R, c0 = tc * TILE_C;
@@ -1204,6 +1204,20 @@ __device__ __forceinline__ void grid_tile_taps(const GridParams<R>& p, int tile,
                 p.beam[g] = acc_value(bacc[q]);
         }
     }
+}
+
+// Lane-per-tap gridder with WPB warps per block, each on its own tile (tile
+// blockIdx.x * WPB + warp, its accumulators at warp * tile_bytes): narrow
+// tiles keep the shared memory per warp small, and several warps per block
+// raise the resident warps past the per-SM block limit.
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, int WPB>
+__global__ void __launch_bounds__(32 * WPB, 44 / WPB) k_grid_tiles_mw(GridParams<R> p, int ntiles, int tile_bytes)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5;
+    const int tile = int(blockIdx.x) * WPB + warp;
+    if (tile < ntiles)
+        grid_tile_taps<R, COMP, KMODE, BEAM, TILE_C>(p, tile, smem_raw + size_t(warp) * size_t(tile_bytes));
 }
 
 // FORM: 0 lanes-per-item (grid_tile), 1 column-packed (grid_tile_cols),

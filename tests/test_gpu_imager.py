@@ -333,7 +333,7 @@ def test_repeated_device_calls_replay_graph_with_new_data(ctx):
         c2.close()
 
 
-@pytest.mark.parametrize("layout", ["32", "16", "32c", "16c", "32t", "16t"])
+@pytest.mark.parametrize("layout", ["32", "16", "32c", "16c", "32t", "16t", "8t"])
 @pytest.mark.parametrize("wproj", [False, True])
 def test_imager_every_gridder_layout_vs_oracle(layout, wproj, monkeypatch):
     """Each tile width and gridder form the autotuner may pick gives the oracle's image (FP64 1e-10,
