@@ -1257,7 +1257,19 @@ struct BatchSnap {
     std::string cls; // size class of the tile autotuner
     int tile_c = TILE_C_DEFAULT;
     int persist = 0;
+    int form = 0; // gridder form: 0 lanes-per-item, 2 lane-per-tap
 };
+
+// Tuned layout of a batch snapshot.  The lane-per-tap form clips footprints
+// to tiles and needs one segment per axis and tile (as in run_gridder).
+void apply_layout(BatchSnap& b, int lay)
+{
+    b.tile_c = lay & 0xff;
+    b.persist = (lay & kLayoutPersist) ? 1 : 0;
+    const int conv = b.s.nplanes > 0 ? b.s.max_support : b.s.support;
+    const bool clip_ok = !b.s.kernel_exact && b.s.N >= 2 * (2 * conv + 1 + 32) + 2;
+    b.form = ((lay & kLayoutTaps) && clip_ok) ? 2 : 0;
+}
 
 void batch_streams(stpgpu_context* c)
 {
@@ -1291,10 +1303,10 @@ void batch_join(stpgpu_context* c, cudaStream_t main)
     }
 }
 
-template <typename R, int COMP, int KMODE, int TC, bool PERSIST>
+template <typename R, int COMP, int KMODE, int TC, bool PERSIST, int FORM>
 void launch_grid_batch(cudaStream_t st, size_t smem, const BatchGridParams<R>& P, uint32_t total_tiles, bool capturing)
 {
-    auto kern = k_grid_batch<R, COMP, KMODE, false, TC, PERSIST>;
+    auto kern = k_grid_batch<R, COMP, KMODE, false, TC, PERSIST, FORM>;
     if (!capturing && smem > 48 * 1024)
         STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     uint32_t blocks = std::max<uint32_t>(1, total_tiles);
@@ -1314,16 +1326,25 @@ void launch_grid_batch(cudaStream_t st, size_t smem, const BatchGridParams<R>& P
 }
 
 
-template <typename R, int COMP, int KMODE>
-void launch_mode(cudaStream_t st, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total, bool cap)
+template <typename R, int COMP, int KMODE, int FORM>
+void launch_mode_form(cudaStream_t st, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total, bool cap)
 {
     const bool t32 = (layout & 0xff) == 32;
     if (layout & kLayoutPersist)
-        t32 ? launch_grid_batch<R, COMP, KMODE, 32, true>(st, smem, P, total, cap)
-            : launch_grid_batch<R, COMP, KMODE, 16, true>(st, smem, P, total, cap);
+        t32 ? launch_grid_batch<R, COMP, KMODE, 32, true, FORM>(st, smem, P, total, cap)
+            : launch_grid_batch<R, COMP, KMODE, 16, true, FORM>(st, smem, P, total, cap);
     else
-        t32 ? launch_grid_batch<R, COMP, KMODE, 32, false>(st, smem, P, total, cap)
-            : launch_grid_batch<R, COMP, KMODE, 16, false>(st, smem, P, total, cap);
+        t32 ? launch_grid_batch<R, COMP, KMODE, 32, false, FORM>(st, smem, P, total, cap)
+            : launch_grid_batch<R, COMP, KMODE, 16, false, FORM>(st, smem, P, total, cap);
+}
+
+template <typename R, int COMP, int KMODE>
+void launch_mode(cudaStream_t st, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total, bool cap)
+{
+    if (KMODE != KM_EXACT && (layout & kLayoutTaps))
+        launch_mode_form<R, COMP, KMODE, 2>(st, layout, smem, P, total, cap);
+    else
+        launch_mode_form<R, COMP, KMODE, 0>(st, layout, smem, P, total, cap);
 }
 
 template <typename R, int COMP>
@@ -1411,7 +1432,7 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
         if (L[i].kind == GK_NONE || L[i].ntiles == 0)
             continue;
         std::string key = std::to_string(L[i].kind) + "/" + std::to_string(L[i].tile_c) + "/"
-            + std::to_string(B[i].persist);
+            + std::to_string(B[i].persist) + "/" + std::to_string(B[i].form);
         if (class_ms)
             key += "|" + B[i].cls;
         groups[key].push_back(i);
@@ -1438,8 +1459,9 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
             if (class_ms)
                 STPGPU_CUDA_TRY(cudaEventRecord(c->pev[0], main));
             const GridLaunch<R>& l0 = L[all[c0]];
-            launch_group<R, COMP>(main, l0.kind, l0.tile_c | (B[all[c0]].persist ? kLayoutPersist : 0), smem, *P,
-                tot, capturing);
+            launch_group<R, COMP>(main, l0.kind,
+                l0.tile_c | (B[all[c0]].persist ? kLayoutPersist : 0) | (B[all[c0]].form == 2 ? kLayoutTaps : 0),
+                smem, *P, tot, capturing);
             nlaunch++;
             if (class_ms) {
                 STPGPU_CUDA_TRY(cudaEventRecord(c->pev[1], main));
@@ -1573,17 +1595,18 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             if (int v; !c->tune_get(b.cls, v) && std::find(fresh.begin(), fresh.end(), b.cls) == fresh.end())
                 fresh.push_back(b.cls);
         if (!fresh.empty()) {
-            const int layouts[4] = { 32, 16, 32 | kLayoutPersist, 16 | kLayoutPersist };
-            std::map<std::string, float> t[4];
+            constexpr int NC = 8;
+            const int layouts[NC] = { 32, 16, 32 | kLayoutPersist, 16 | kLayoutPersist, 32 | kLayoutTaps,
+                16 | kLayoutTaps, 32 | kLayoutPersist | kLayoutTaps, 16 | kLayoutPersist | kLayoutTaps };
+            std::map<std::string, float> t[NC];
             for (int k = 0; k < 5; k++)
                 if (!c->pev[k])
                     STPGPU_CUDA_TRY(cudaEventCreate(&c->pev[k]));
-            for (int cand = 0; cand < 4; cand++) {
+            for (int cand = 0; cand < NC; cand++) {
                 for (auto& b : B) {
                     int lay = layouts[cand];
                     c->tune_get(b.cls, lay);
-                    b.tile_c = lay & 0xff;
-                    b.persist = (lay & kLayoutPersist) ? 1 : 0;
+                    apply_layout(b, lay);
                 }
                 batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, &t[cand]);
                 STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
@@ -1591,23 +1614,25 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             static const bool log_tuning = std::getenv("STPGPU_LOG_TUNING") != nullptr;
             for (auto& cls : fresh) {
                 int best = 0;
-                for (int cand = 1; cand < 4; cand++)
+                for (int cand = 1; cand < NC; cand++)
                     if (t[cand][cls] < t[best][cls])
                         best = cand;
                 c->tune_set(cls, layouts[best]);
                 if (log_tuning)
                     std::fprintf(stderr,
-                        "stpgpu gridder tuner: %s  32/16 cols %.3f/%.3f ms, persistent %.3f/%.3f ms -> %d%s\n",
+                        "stpgpu gridder tuner: %s  32/16 cols %.3f/%.3f ms, persistent %.3f/%.3f ms, lane-per-tap"
+                        " %.3f/%.3f ms, lane-per-tap persistent %.3f/%.3f ms -> %d%s%s\n",
                         cls.c_str(), double(t[0][cls]), double(t[1][cls]), double(t[2][cls]), double(t[3][cls]),
-                        layouts[best] & 0xff, (layouts[best] & kLayoutPersist) ? " persistent" : "");
+                        double(t[4][cls]), double(t[5][cls]), double(t[6][cls]), double(t[7][cls]),
+                        layouts[best] & 0xff, (layouts[best] & kLayoutPersist) ? " persistent" : "",
+                        (layouts[best] & kLayoutTaps) ? " lane-per-tap" : "");
             }
             tuned = int(fresh.size());
         }
         for (auto& b : B) {
             int lay = TILE_C_DEFAULT;
             c->tune_get(b.cls, lay);
-            b.tile_c = lay & 0xff;
-            b.persist = (lay & kLayoutPersist) ? 1 : 0;
+            apply_layout(b, lay);
         }
         bool capturable = true;
         for (auto& b : B)

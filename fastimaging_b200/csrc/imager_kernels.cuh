@@ -1252,7 +1252,7 @@ struct BatchGridParams {
 // counter (zeroed before the launch) until the queue is empty.
 // PERSIST = false: one CTA per work item (w = blockIdx.x), the hardware
 // block scheduler being the queue; the autotuner picks the faster form.
-template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, bool PERSIST>
+template <typename R, int COMP, int KMODE, bool BEAM, int TILE_C, bool PERSIST, int FORM = 0>
 __global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) : 14) k_grid_batch(const __grid_constant__ BatchGridParams<R> P)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1279,7 +1279,10 @@ __global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) 
                 hi = mid - 1;
         }
         __syncwarp();
-        grid_tile<R, COMP, KMODE, BEAM, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw);
+        if constexpr (FORM == 2 && KMODE != KM_EXACT)
+            grid_tile_taps<R, COMP, KMODE, BEAM, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw);
+        else
+            grid_tile<R, COMP, KMODE, BEAM, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw);
         __syncwarp();
     }
 }
