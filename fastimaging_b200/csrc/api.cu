@@ -745,7 +745,6 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     bp.tile_c = tile_c;
     bp.support = s.support;
     bp.plane_support = plane_support;
-    bp.presorted = items_sorted != nullptr;
     bp.ts_of = ts_of;
     bp.ntimesteps = std::max(s.ntimesteps, 1);
     bp.exact = kernel_exact;

@@ -235,7 +235,6 @@ struct BinParams {
     int tile_c;              // tile width in grid columns (TILE_R rows per tile)
     int support;             // non-W-proj support
     const int* plane_support; // W-proj truncated support per plane (nullable)
-    int presorted;            // W-proj: `items` already permuted into |w| order
     const uint8_t* ts_of;     // A-projection: time step per visibility (nullable)
     int ntimesteps;           // planes are indexed plane * ntimesteps + step
     int exact;               // rows wrap negative (exact gridder)
@@ -375,18 +374,17 @@ __device__ __forceinline__ int plane_of(const int64_t* first, int P, int64_t k)
 }
 
 // With W-projection (`order` = the |w| permutation, `first` = plane starts)
-// items are visited in |w| order and take the plane of their sorted
-// position k; the fill pass records it in the item for the gridder.  With
-// p.presorted the items array is already in |w| order (item k is sorted
-// position k), else item order[k] is visited.
+// `items` is already permuted into |w| order (item k is sorted position k);
+// each item takes the plane of its position, which the fill pass records in
+// the item for the gridder (order[k] is the item's input index, used for
+// per-visibility inputs such as the A-projection time step).
 template <typename R>
 __global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t* order, const int64_t* first, int P)
 {
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= p.n)
         return;
-    const int64_t i = (order && !p.presorted) ? int64_t(order[k]) : k;
-    const Item<R> it = items[i];
+    const Item<R> it = items[k];
     if (!it.good)
         return;
     int S = p.support;
@@ -408,8 +406,8 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
     const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (k >= p.n)
         return;
-    const int64_t i = (order && !p.presorted) ? int64_t(order[k]) : k;
-    const Item<R> it = items[i];
+    const int64_t i = k;
+    const Item<R> it = items[k];
     if (!it.good)
         return;
     int S = p.support;
@@ -418,7 +416,7 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
         if (p.ts_of)
             plane = plane * p.ntimesteps + p.ts_of[order[k]];
         S = p.plane_support[plane];
-        items[i].plane = uint16_t(plane);
+        items[k].plane = uint16_t(plane);
     }
     for (int mir = 0; mir < int(it.good); mir++)
         for_item_tiles(it, mir, S, p, [&](uint32_t t) {
