@@ -752,17 +752,32 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     bp.tile_count = tcount;
     bp.tile_off = toff;
     bp.tile_cursor = tcur;
+    // list slots kept by the count pass (the fill then needs no atomics)
+    bp.ranks = c->buf<uint32_t>("tranks", size_t(std::max<int64_t>(n, 1)) * 2 * kRankSlots);
+    bp.rank_overflow = c->buf<uint32_t>("trankovf", 1);
     bp.list = list;
     bp.list_capacity = cap;
     bp.err = g.d_err;
     STPGPU_CUDA_TRY(cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (ntiles + 1), st));
     STPGPU_CUDA_TRY(cudaMemsetAsync(tcur, 0, sizeof(uint32_t) * (ntiles + 1), st));
+    STPGPU_CUDA_TRY(cudaMemsetAsync(bp.rank_overflow, 0, sizeof(uint32_t), st));
     if (n > 0) {
         k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
     }
-    k_scan_single<<<1, 1024, 0, st>>>(tcount, toff, ntiles);
-    STPGPU_CHECK_LAUNCH();
+    if (ntiles <= 4096) {
+        k_scan_single<<<1, 1024, 0, st>>>(tcount, toff, ntiles);
+        STPGPU_CHECK_LAUNCH();
+    } else {
+        // many tiles: the multi-block scan (tcount[ntiles] is 0, so
+        // toff[ntiles] receives the total)
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, tcount, toff, ntiles + 1, st);
+        void* tmp = c->buf<unsigned char>("cubtmp_tiles", tb);
+        if (cub::DeviceScan::ExclusiveSum(tmp, tb, tcount, toff, ntiles + 1, st) != cudaSuccess)
+            fail(STPGPU_ERR_CUDA, "tile offset scan failed");
+        g_launches += 2;
+    }
     if (large_support(s)) { // size the list from the counted entries
         uint32_t total = 0;
         STPGPU_CUDA_TRY(cudaMemcpyAsync(&total, toff + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -2530,7 +2545,9 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
     int64_t b = n * ((vis_c64 ? 8 : 16) + 8 + 24) + n * (rb == 8 ? 40 : 28);
     const int64_t per_dim = ceil_div(2 * conv, 16) + 2;
     b += std::max<int64_t>(n, 1) * 2 * per_dim * per_dim * 4; // tile-list capacity
+    b += std::max<int64_t>(n, 1) * 2 * kRankSlots * 4;         // list slots kept by the count pass
     if (s.nplanes > 0) {
+        b += n * (rb == 8 ? 40 : 28); // items in |w| order
         const int64_t os = std::max(1, (s.os >> 1) << 1), cs = (os / 2) * 2 + 1, K = 2 * conv + 1;
         const int64_t lh = conv * os + os / 2 + 1;
         b += n * 41;                                                  // |w| sort, planes

@@ -230,6 +230,8 @@ __device__ __forceinline__ int map_row(int raw, int N, int rows, bool wrap_neg)
     return raw < rows ? raw : -1;
 }
 
+constexpr int kRankSlots = 4; // tiles per (item, mirror) whose list slots the count pass keeps
+
 struct BinParams {
     int N, image_rows, tiles_r, tiles_c;
     int tile_c;              // tile width in grid columns (TILE_R rows per tile)
@@ -242,6 +244,8 @@ struct BinParams {
     uint32_t* tile_count;
     const uint32_t* tile_off;
     uint32_t* tile_cursor;
+    uint32_t* ranks;          // nullable: [kRankSlots][2][n] list slots taken by the count pass
+    uint32_t* rank_overflow;  // set when some (item, mirror) touched more than kRankSlots tiles
     uint32_t* list;
     uint64_t list_capacity;
     unsigned int* err;
@@ -394,8 +398,21 @@ __global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t*
             plane = plane * p.ntimesteps + p.ts_of[order[k]];
         S = p.plane_support[plane];
     }
-    for (int mir = 0; mir < int(it.good); mir++)
-        for_item_tiles(it, mir, S, p, [&](uint32_t t) { atomicAdd(&p.tile_count[t], 1u); });
+    for (int mir = 0; mir < int(it.good); mir++) {
+        // the count's atomic returns the entry's slot in the tile list; up to
+        // kRankSlots of them per (item, mirror) are kept for the fill pass
+        int q = 0;
+        for_item_tiles(it, mir, S, p, [&](uint32_t t) {
+            const uint32_t r = atomicAdd(&p.tile_count[t], 1u);
+            if (p.ranks) {
+                if (q < kRankSlots)
+                    p.ranks[size_t(q * 2 + mir) * size_t(p.n) + size_t(k)] = r; // slot-major: coalesced
+                else
+                    *p.rank_overflow = 1u;
+            }
+            q++;
+        });
+    }
 }
 
 // Lists are filled in |w| order for W-projection, so that a warp's items
@@ -418,15 +435,22 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
         S = p.plane_support[plane];
         items[k].plane = uint16_t(plane);
     }
-    for (int mir = 0; mir < int(it.good); mir++)
+    // slots from the count pass when every (item, mirror) kept its slots
+    // (no footprint with more than kRankSlots tiles), else from cursors
+    const bool ranked = p.ranks && *p.rank_overflow == 0u;
+    for (int mir = 0; mir < int(it.good); mir++) {
+        int q = 0;
         for_item_tiles(it, mir, S, p, [&](uint32_t t) {
-            const uint32_t slot = atomicAdd(&p.tile_cursor[t], 1u);
+            const uint32_t slot = ranked ? p.ranks[size_t(q * 2 + mir) * size_t(p.n) + size_t(k)]
+                                         : atomicAdd(&p.tile_cursor[t], 1u);
+            q++;
             const uint64_t pos = uint64_t(p.tile_off[t]) + slot;
             if (pos < p.list_capacity)
                 p.list[pos] = uint32_t(i) * 2u + uint32_t(mir);
             else
                 atomicOr(p.err, 1u);
         });
+    }
 }
 
 // Exclusive scan of n counts into off[0..n] (single block of 1024 threads,
