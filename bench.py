@@ -281,7 +281,7 @@ def run_gpu(args):
         "grid_init": n * (16 + 24 + 8) + n * 28 + items * 4 * 2,
     }
     # the dominant kernel: the tile gridder is the single most expensive launch of a step (the
-    # grid-init phase is ~15 short kernels, the largest a 20 us radix-sort pass)
+    # grid-init phase is ~20 short kernels, none above ~45 us)
     dom = names.index("grid_loop")
     dom_name = names[dom]
     achieved = alg[dom_name] / (mean_ph[dom] / 1e3) / 1e9
@@ -295,7 +295,16 @@ def run_gpu(args):
     roofline = {"bound": "hbm", "kernel": "k_grid_tiles (grid_loop phase)", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
                 "phase_ms": {k: round(float(v), 4) for k, v in zip(names, mean_ph)},
-                "algorithmic_bytes": alg[dom_name]}
+                "algorithmic_bytes": alg[dom_name],
+                # every phase against the same HBM peak (algorithmic bytes / its phase time)
+                "phase_frac": {k: round(alg[k] / (float(v) / 1e3) / 1e9 / hbm, 4) for k, v in zip(names, mean_ph)
+                               if v > 0}}
+    # the whole snapshot: vis/uvw/weights in, the half-plane grid written and read once, the image written
+    # once (FP32), against the step time
+    snap_bytes = n * (16 + 24 + 8) + 2 * rows * N * 8 + N * N * 4
+    t_roof_ms = snap_bytes / (hbm * 1e9) * 1e3
+    roofline["snapshot"] = {"algorithmic_bytes": int(snap_bytes), "t_roof_ms": round(t_roof_ms, 4),
+                            "frac": round(t_roof_ms / (tot32 / args.steps), 4)}
 
     p50 = float(np.percentile(t32, 50))
     p99 = float(np.percentile(t32, 99))
