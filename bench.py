@@ -657,7 +657,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the batched, precision-study and serving sections")
+    ap.add_argument("--section", choices=["config1_sf"], default=None,
+                    help="run one section alone and print its JSON (config1_sf: the plain 2048^2 imager and the "
+                         "source finder), for profiling")
     args = ap.parse_args()
+    if args.section == "config1_sf":
+        from fastimaging_b200 import capi
+
+        ctx = capi.Context(0)
+        try:
+            print(json.dumps(run_config1_and_source_finder(ctx)), flush=True)
+        finally:
+            ctx.close()
+        return
     if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3
     if args.impl == "reference":
