@@ -16,6 +16,40 @@ __device__ __forceinline__ double ld(const T* p, int64_t i)
     return double(p[i]);
 }
 
+// Grid-stride visit of x[0..n) in 16-byte loads (four floats or two pairs of
+// doubles per step, when x is 16-byte aligned), then the tail; f(value) is
+// called once per element.  The wide loads keep enough bytes in flight per
+// thread for the streaming passes over an image.
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
+{
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    int64_t done = 0;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        const int64_t n4 = n / 4;
+        for (int64_t g = tid; g < n4; g += stride) {
+            if constexpr (sizeof(T) == 4) {
+                const float4 q = reinterpret_cast<const float4*>(x)[g];
+                f(double(q.x));
+                f(double(q.y));
+                f(double(q.z));
+                f(double(q.w));
+            } else {
+                const double2 a = reinterpret_cast<const double2*>(x)[2 * g];
+                const double2 b = reinterpret_cast<const double2*>(x)[2 * g + 1];
+                f(double(a.x));
+                f(double(a.y));
+                f(double(b.x));
+                f(double(b.y));
+            }
+        }
+        done = n4 * 4;
+    }
+    for (int64_t i = done + tid; i < n; i += stride)
+        f(double(x[i]));
+}
+
 // order-preserving 64-bit key of a double (non-NaN)
 __device__ __forceinline__ unsigned long long okey(double v)
 {
@@ -68,11 +102,10 @@ template <typename T>
 __global__ void __launch_bounds__(SF_THREADS) k_sum_sq(const T* x, int64_t n, double* part)
 {
     double v[2] = { 0.0, 0.0 };
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        double a = ld(x, i);
+    for_each_elem(x, n, [&](double a) {
         v[0] += a;
         v[1] += a * a;
-    }
+    });
     block_sums<2>(v, part + 2 * blockIdx.x);
 }
 
@@ -109,13 +142,13 @@ __global__ void __launch_bounds__(SF_THREADS) k_hist(const T* x, int64_t n, doub
     for (int k = threadIdx.x; k < BINS_N + 2; k += blockDim.x)
         h[k] = 0;
     __syncthreads();
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const int b = int_trunc_x86((ld(x, i) - leftend) * scale);
+    for_each_elem(x, n, [&](double a) {
+        const int b = int_trunc_x86((a - leftend) * scale);
         if (b < 0)
             atomicAdd(&h[BINS_N + 1], 1u);
         else if (b <= BINS_N)
             atomicAdd(&h[b], 1u);
-    }
+    });
     __syncthreads();
     for (int k = threadIdx.x; k < BINS_N + 2; k += blockDim.x)
         if (h[k])
@@ -130,11 +163,11 @@ template <typename T>
 __global__ void __launch_bounds__(SF_THREADS) k_radix_hist(const T* x, int64_t n, unsigned long long prefix,
     unsigned long long mask, int shift, unsigned int* hist /* 65536 */)
 {
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const unsigned long long k = okey(ld(x, i));
+    for_each_elem(x, n, [&](double a) {
+        const unsigned long long k = okey(a);
         if ((k & mask) == prefix)
             atomicAdd(&hist[(k >> shift) & 0xffffull], 1u);
-    }
+    });
 }
 
 // Single block: find the digit bucket containing rank `state[0]` (0-based
@@ -182,15 +215,15 @@ __global__ void __launch_bounds__(SF_THREADS) k_clip_pass(const T* x, int64_t n,
     double prev_upper, double* part)
 {
     double v[3] = { 0.0, 0.0, 0.0 };
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const double d = ld(x, i) - median;
+    for_each_elem(x, n, [&](double xv) {
+        const double d = xv - median;
         const double a = fabs(d);
         if (a > upper && !(a > prev_upper)) {
             v[0] += d;
             v[1] += d * d;
             v[2] += 1.0;
         }
-    }
+    });
     block_sums<3>(v, part + 3 * blockIdx.x);
 }
 
