@@ -233,9 +233,12 @@ __global__ void __launch_bounds__(SF_THREADS) k_clip_pass(const T* x, int64_t n,
 // c_i = (mc + cols/2) mod cols in order, rows in memory order (ccl.h:162-183).
 struct CclGeom {
     int rows, cols, rshift, cshift;
+    // images hold fewer than 2^32 pixels (checked by the callers), so the
+    // index arithmetic is 32-bit
     __device__ __forceinline__ int64_t mem_of_key(int64_t s) const
     {
-        const int ci = int(s / rows), r = int(s % rows);
+        const uint32_t su = uint32_t(s), ur = uint32_t(rows);
+        const int ci = int(su / ur), r = int(su - uint32_t(ci) * ur);
         const int mc = ci >= cshift ? ci - cshift : ci + cshift;
         return int64_t(mc) * rows + r;
     }
@@ -315,7 +318,7 @@ __global__ void k_ccl_union(const uint8_t* cls, CclGeom g, int conn4, int slice_
     if (!my)
         return;
     const int rows = g.rows;
-    const int ci = int(s / rows), r = int(s % rows);
+    const int ci = int(uint32_t(s) / uint32_t(rows)), r = int(uint32_t(s) - uint32_t(ci) * uint32_t(rows));
     auto link = [&](int64_t q) {
         if (cls[q] == my)
             uf_union(P, uint32_t(s), uint32_t(q), err);
@@ -583,7 +586,7 @@ __global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uin
     for (uint32_t t = b; t < e; t++) {
         const int64_t m = vals[t];
         const double val = ld(img, m);
-        const int r = int(m % rows), c = int(m / rows);
+        const int c = int(uint32_t(m) / uint32_t(rows)), r = int(uint32_t(m) - uint32_t(c) * uint32_t(rows));
         const double y = r < vs ? double(r + vs) : double(r - vs);
         const double x = c < hs ? double(c + hs) : double(c - hs);
         const double xb = __dmul_rn(x, val), yb = __dmul_rn(y, val);
@@ -627,7 +630,7 @@ __global__ void k_moments(const T* img, int32_t* L, int rows, int cols, unsigned
         return;
     }
     const double val = ld(img, m);
-    const int r = int(m % rows), c = int(m / rows);
+    const int c = int(uint32_t(m) / uint32_t(rows)), r = int(uint32_t(m) - uint32_t(c) * uint32_t(rows));
     const int vs = rows / 2, hs = cols / 2;
     const double y = r < vs ? double(r + vs) : double(r - vs);
     const double x = c < hs ? double(c + hs) : double(c - hs);
