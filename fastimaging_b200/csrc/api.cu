@@ -2017,26 +2017,39 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     unsigned long long* ext_pos = ext;
     unsigned long long* ext_neg = ext + np;
     const unsigned long long kpos = host_okey(d_pos), kneg = host_okey(d_neg);
-    {
-        std::vector<unsigned long long> init(nl);
-        for (int i = 0; i < np; i++)
-            init[i] = kpos;
-        for (int i = np; i < np + nneg; i++)
-            init[i] = kneg;
-        unsigned long long* hi = c->host_stage<unsigned long long>(nl);
-        std::memcpy(hi, init.data(), sizeof(unsigned long long) * nl);
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(ext, hi, sizeof(unsigned long long) * nl, cudaMemcpyHostToDevice, st));
-        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    }
-    hcnt = c->host_stage<uint32_t>(4); // the staging area may have been reallocated above
-    STPGPU_CUDA_TRY(cudaMemsetAsync(eidx, 0xff, sizeof(unsigned long long) * nl, st));
     STPGPU_CUDA_TRY(cudaMemsetAsync(mom, 0, sizeof(double) * 6 * nl, st));
     STPGPU_CUDA_TRY(cudaMemsetAsync(ns, 0, sizeof(int) * nl, st));
     STPGPU_CUDA_TRY(cudaMemsetAsync(nvalid, 0, sizeof(uint32_t), st));
-    k_extrema<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg);
-    STPGPU_CHECK_LAUNCH();
-    k_extrema_idx<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg, kpos, kneg, eidx, eidx + np);
-    STPGPU_CHECK_LAUNCH();
+    const bool packed = sizeof(T) == 4 && (n % 4) == 0 && (reinterpret_cast<uintptr_t>(d_img) % 16) == 0
+        && (reinterpret_cast<uintptr_t>(L) % 16) == 0 && n < (int64_t(1) << 32);
+    if (packed && nl > 0) {
+        // one pass: threshold rounded onto the float grid (largest float <=
+        // the positive threshold, smallest float >= the negative one)
+        float tf = float(d_pos);
+        if (double(tf) > d_pos)
+            tf = std::nextafter(tf, -HUGE_VALF);
+        float tc = float(d_neg);
+        if (double(tc) < d_neg)
+            tc = std::nextafter(tc, HUGE_VALF);
+        const uint32_t fpos = fkey32(tf), fneg = fkey32(tc);
+        unsigned long long* pk = c->buf<unsigned long long>("sf_pk", nl);
+        k_extrema_init<<<grid1d(nl, 256), 256, 0, st>>>(pk, np, nl, (unsigned long long)fpos << 32 | 0xffffffffull,
+            (unsigned long long)fneg << 32);
+        STPGPU_CHECK_LAUNCH();
+        k_extrema_packed4<<<grid1d(n / 4, 256), 256, 0, st>>>(reinterpret_cast<const float*>(d_img), L, n / 4, pk,
+            pk + np);
+        STPGPU_CHECK_LAUNCH();
+        k_extrema_unpack<<<grid1d(nl, 256), 256, 0, st>>>(pk, np, nl, fpos, fneg, kpos, kneg, ext, eidx);
+        STPGPU_CHECK_LAUNCH();
+    } else {
+        k_extrema_init<<<grid1d(std::max(nl, 1), 256), 256, 0, st>>>(ext, np, nl, kpos, kneg);
+        STPGPU_CHECK_LAUNCH();
+        STPGPU_CUDA_TRY(cudaMemsetAsync(eidx, 0xff, sizeof(unsigned long long) * nl, st));
+        k_extrema<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg);
+        STPGPU_CHECK_LAUNCH();
+        k_extrema_idx<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg, kpos, kneg, eidx, eidx + np);
+        STPGPU_CHECK_LAUNCH();
+    }
     const uint32_t* fit_pix = nullptr; // pixels sorted by label, and each label's segment
     const uint32_t* fit_sb = nullptr;
     const uint32_t* fit_se = nullptr;

@@ -457,6 +457,78 @@ __global__ void k_extrema(const T* img, const int32_t* L, int64_t n, unsigned lo
         atomicMin(&ext_neg[-l - 1], k);
 }
 
+// Single-precision images: extremum and its first memory index in one pass,
+// as one 64-bit key per label (the value's order key above the index;
+// positives keep the maximum with the lowest index through atomicMax on
+// ~index, negatives the minimum with the lowest index through atomicMin).
+// Starting keys hold the detection threshold rounded to the float grid
+// (largest float <= threshold for positives, smallest float >= threshold for
+// negatives), so only values strictly beyond the threshold replace them.
+__device__ __host__ inline uint32_t fkey32(float v)
+{
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    return (u >> 31) ? ~u : (u | 0x80000000u);
+}
+__device__ inline float fkey32_inv(uint32_t k)
+{
+    const uint32_t u = (k >> 31) ? (k & 0x7fffffffu) : ~k;
+    return __uint_as_float(u);
+}
+
+__global__ void k_extrema_init(unsigned long long* a, int np, int nl, unsigned long long vpos, unsigned long long vneg)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nl)
+        a[i] = i < np ? vpos : vneg;
+}
+
+// Four pixels per thread (n % 4 == 0, 16-byte aligned image and labels).
+__global__ void k_extrema_packed4(const float* img, const int32_t* L, int64_t n4, unsigned long long* pk_pos,
+    unsigned long long* pk_neg)
+{
+    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (g >= n4)
+        return;
+    const int4 l4 = reinterpret_cast<const int4*>(L)[g];
+    if ((l4.x | l4.y | l4.z | l4.w) == 0)
+        return;
+    const float4 v4 = reinterpret_cast<const float4*>(img)[g];
+    const int32_t ls[4] = { l4.x, l4.y, l4.z, l4.w };
+    const float vs[4] = { v4.x, v4.y, v4.z, v4.w };
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int32_t l = ls[q];
+        if (l == 0)
+            continue;
+        const uint32_t m = uint32_t(g * 4 + q);
+        const unsigned long long k = (unsigned long long)fkey32(vs[q]) << 32;
+        if (l > 0)
+            atomicMax(&pk_pos[l - 1], k | (0xffffffffu - m));
+        else
+            atomicMin(&pk_neg[-l - 1], k | m);
+    }
+}
+
+// Packed keys -> the order keys of the extrema (double) and their indices,
+// the layout the two-pass path produces.
+__global__ void k_extrema_unpack(const unsigned long long* pk, int np, int nl, uint32_t thr_pos, uint32_t thr_neg,
+    unsigned long long kpos, unsigned long long kneg, unsigned long long* ext, unsigned long long* eidx)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nl)
+        return;
+    const bool pos = i < np;
+    const uint32_t hi = uint32_t(pk[i] >> 32), lo = uint32_t(pk[i]);
+    if (hi != (pos ? thr_pos : thr_neg)) {
+        ext[i] = okey(double(fkey32_inv(hi)));
+        eidx[i] = pos ? (unsigned long long)(0xffffffffu - lo) : (unsigned long long)lo;
+    } else {
+        ext[i] = pos ? kpos : kneg;
+        eidx[i] = ~0ull;
+    }
+}
+
 // First memory index holding the extremum (the serial reference keeps the
 // first occurrence in memory order).
 template <typename T>

@@ -89,6 +89,24 @@ def test_source_find_float32_input(ctx):
     _compare(isl, ref, lab, ref.label_map)
 
 
+def test_source_find_float32_extremum_ties(ctx):
+    """Single-precision images take the one-pass extremum (value and first memory index in one 64-bit key):
+    equal maxima / minima inside one island resolve to the first pixel in memory order, as in the
+    reference's serial scan."""
+    rng = np.random.default_rng(10)
+    img = (0.5 * rng.normal(size=(160, 128))).astype(np.float32)
+    img[30:35, 40:46] += 6.0
+    img[31, 41] = img[33, 44] = np.float32(12.5)   # tied maxima, (31, 41) first in memory (column-major)
+    img[100:104, 20:25] -= 6.0
+    img[102, 21] = img[100, 23] = np.float32(-11.0)  # tied minima
+    img = np.asfortranarray(img)
+    ref = orc.source_find(img.astype(np.float64), 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5)
+    _compare(isl, ref, lab, ref.label_map)
+    got = {(i.sign, i.extremum_x_idx, i.extremum_y_idx) for i in isl}
+    assert len(got) == len(isl) >= 2
+
+
 def test_source_find_no_labelmap_cleanup(ctx):
     rng = np.random.default_rng(13)
     img = rng.normal(size=(64, 64))
