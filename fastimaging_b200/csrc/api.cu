@@ -1839,32 +1839,24 @@ double estimate_rms(stpgpu_context* c, const T* x, int64_t n, double num_sigma, 
 {
     cudaStream_t st = c->stream;
     const double m = mean - median;
-    double s = sigma;
-    double d1 = m * double(n), d2 = (s * s + m * m) * double(n);
-    unsigned long long valid = (unsigned long long)n;
-    double prev_upper = 1.7976931348623157e308;
     const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8);
     double* part = c->buf<double>("sf_part", 3 * size_t(nb));
-    double* out = c->buf<double>("sf_out", 4);
-    double* h = c->host_stage<double>(4);
+    ClipState* cs = c->buf<ClipState>("sf_clip", 1);
+    // every iteration is enqueued; the state on the device carries the
+    // bounds from one pass to the next and stops the passes once nothing
+    // is removed, so the host reads the result once
+    k_clip_init<<<1, 1, 0, st>>>(cs, sigma, m, double(n), num_sigma);
+    STPGPU_CHECK_LAUNCH();
     for (int it = 0; it < iters; it++) {
-        const double upper = num_sigma * s;
-        k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, median, upper, prev_upper, part);
+        k_clip_pass_dev<T><<<nb, SF_THREADS, 0, st>>>(x, n, median, cs, part);
         STPGPU_CHECK_LAUNCH();
-        k_finish_parts<3><<<1, 256, 0, st>>>(part, int(nb), out);
+        k_clip_finish<<<1, 256, 0, st>>>(part, int(nb), cs, num_sigma);
         STPGPU_CHECK_LAUNCH();
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(h, out, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-        const unsigned long long rem = (unsigned long long)(h[2] + 0.5);
-        if (rem == 0)
-            break;
-        valid -= rem;
-        d1 -= h[0];
-        d2 -= h[1];
-        s = std::sqrt(d2 / double(valid) - (d1 / double(valid)) * (d1 / double(valid)));
-        prev_upper = upper;
     }
-    return s;
+    ClipState* h = c->host_stage<ClipState>(1);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, cs, sizeof(ClipState), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    return h->s;
 }
 
 unsigned long long host_okey(double v)

@@ -208,12 +208,38 @@ __global__ void k_radix_pick(const unsigned int* hist, int shift, unsigned long 
 
 // -------------------------------------------------- sigma clip (estimate_rms)
 
-// One clipping pass (sourcefind.cpp:54-134): samples with
-// |x - median| > upper and not > prev_upper; sums of v, v^2 and the count.
-template <typename T>
-__global__ void __launch_bounds__(SF_THREADS) k_clip_pass(const T* x, int64_t n, double median, double upper,
-    double prev_upper, double* part)
+// estimate_rms (sourcefind.cpp:54-134) with the iteration state on the
+// device (no host round trip per iteration).  A clipping pass sums v, v^2
+// and the count of samples with |x - median| > upper and not > prev_upper;
+// the pass reads the current bounds, the finish step sums
+// the partials in a fixed order and updates the state exactly as the
+// reference's loop (sourcefind.cpp:82-134), with explicitly rounded
+// operations; once nothing is removed the remaining passes return at once.
+struct ClipState {
+    double s, d1, d2, valid, prev_upper, upper;
+    int done;
+};
+
+__global__ void k_clip_init(ClipState* cs, double sigma, double m, double n, double num_sigma)
 {
+    ClipState c;
+    c.s = sigma;
+    c.d1 = __dmul_rn(m, n);
+    c.d2 = __dmul_rn(__dadd_rn(__dmul_rn(sigma, sigma), __dmul_rn(m, m)), n);
+    c.valid = n;
+    c.prev_upper = 1.7976931348623157e308;
+    c.upper = __dmul_rn(num_sigma, sigma);
+    c.done = 0;
+    *cs = c;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(SF_THREADS) k_clip_pass_dev(const T* x, int64_t n, double median, const ClipState* cs,
+    double* part)
+{
+    if (cs->done)
+        return;
+    const double upper = cs->upper, prev_upper = cs->prev_upper;
     double v[3] = { 0.0, 0.0, 0.0 };
     for_each_elem(x, n, [&](double xv) {
         const double d = xv - median;
@@ -225,6 +251,42 @@ __global__ void __launch_bounds__(SF_THREADS) k_clip_pass(const T* x, int64_t n,
         }
     });
     block_sums<3>(v, part + 3 * blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_clip_finish(const double* part, int nb, ClipState* cs, double num_sigma)
+{
+    if (cs->done)
+        return;
+    __shared__ double sm[3][256];
+    for (int q = 0; q < 3; q++) {
+        double t = 0.0;
+        for (int k = threadIdx.x; k < nb; k += blockDim.x)
+            t += part[3 * k + q];
+        sm[q][threadIdx.x] = t;
+    }
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int q = 0; q < 3; q++)
+                sm[q][threadIdx.x] += sm[q][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0)
+        return;
+    ClipState c = *cs;
+    const unsigned long long rem = (unsigned long long)(sm[2][0] + 0.5);
+    if (rem == 0) {
+        c.done = 1;
+    } else {
+        c.valid = __dsub_rn(c.valid, double(rem));
+        c.d1 = __dsub_rn(c.d1, sm[0][0]);
+        c.d2 = __dsub_rn(c.d2, sm[1][0]);
+        const double a = __ddiv_rn(c.d2, c.valid), b = __ddiv_rn(c.d1, c.valid);
+        c.s = __dsqrt_rn(__dsub_rn(a, __dmul_rn(b, b)));
+        c.prev_upper = c.upper;
+        c.upper = __dmul_rn(num_sigma, c.s);
+    }
+    *cs = c;
 }
 
 // -------------------------------------------------- connected components
