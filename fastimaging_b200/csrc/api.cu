@@ -1906,9 +1906,65 @@ void moments_fit(int sign, double extremum, const double* mb, double rms, double
     constrain(g);
 }
 
+// Labeller buffers for n pixels in ccl_chunks(n) chunks.
+struct CclBufs {
+    uint8_t* cls; // ccl_chunks(n) * CCL_CHUNK bytes (background padding past n)
+    uint32_t* P; // n union-find parents (foreground keys only)
+    uint32_t* R; // n: label number of each root
+    uint32_t* cnt; // 3 rows of ccl_chunks(n) + 1: positive roots, negative roots, foreground keys per chunk
+    uint32_t* off; // their exclusive scans, same layout
+    uint32_t* misc; // [0..2] the three totals, [3] union-find step-bound flag (zero before the call)
+    uint32_t* fgl; // n: foreground keys in scan order, or null
+    int32_t* L; // n: label map in memory order, or null
+};
+
+inline int64_t ccl_chunks(int64_t n) { return (n + CCL_CHUNK - 1) / CCL_CHUNK; }
+
+// Enqueues the labeller (ccl.h:19-773 semantics, see the kernels) on st.
+// Counts its launches; makes no allocation and throws nothing.
+template <typename T>
+cudaError_t ccl_enqueue(cudaStream_t st, const T* img, const CclGeom& g, double tp, double tn, int findneg,
+    int conn4, int slice, const CclBufs& b)
+{
+    const int64_t n = int64_t(g.rows) * g.cols;
+    const int64_t nch = ccl_chunks(n), npad = nch * CCL_CHUNK;
+    const int stride = int(nch + 1);
+    unsigned* err = b.misc + 3;
+    if (g.rows % 4 == 0 && (reinterpret_cast<uintptr_t>(img) & 15) == 0) {
+        const int64_t ng = npad / 4;
+        k_ccl_init4<T><<<unsigned(std::min<int64_t>(ceil_div(ng, SF_THREADS), 148 * 8)), SF_THREADS, 0, st>>>(img,
+            g, tp, tn, findneg, n / 4, ng, reinterpret_cast<uint32_t*>(b.cls), reinterpret_cast<uint4*>(b.P));
+    } else {
+        if (npad > n) {
+            const cudaError_t e = cudaMemsetAsync(b.cls + n, 0, size_t(npad - n), st);
+            if (e != cudaSuccess)
+                return e;
+        }
+        k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(img, g, tp, tn, findneg, b.cls, b.P);
+    }
+    k_ccl_union<<<unsigned(nch), SF_THREADS, 0, st>>>(b.cls, g, conn4, slice, b.P, err);
+    k_ccl_flatten<<<unsigned(nch), SF_THREADS, 0, st>>>(b.cls, b.P, b.cnt, stride, err);
+    k_scan_rows<<<3, 1024, 0, st>>>(b.cnt, b.off, int(nch), stride, b.misc);
+    k_ccl_rank<<<unsigned(nch), SF_THREADS, 0, st>>>(b.cls, b.P, b.off, stride, b.R, b.fgl);
+    g_launches += 5;
+    if (b.L) {
+        if (g.rows % 4 == 0 && (reinterpret_cast<uintptr_t>(b.L) & 15) == 0) {
+            const int64_t ng = n / 4;
+            k_ccl_label4<<<unsigned(std::min<int64_t>(ceil_div(ng, SF_THREADS), 148 * 8)), SF_THREADS, 0, st>>>(
+                b.cls, b.P, b.R, g, ng, b.L);
+        } else {
+            k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(b.cls, b.P, b.R, g, b.L);
+        }
+        g_launches++;
+    }
+    return cudaGetLastError();
+}
+
+// write_labels: fill the label map (d_labels, or the context's "ccl_L"
+// buffer when d_labels is null).
 template <typename T>
 void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, const stpgpu_sf_pars& p, int32_t* d_labels,
-    std::vector<stpgpu_island>& islands, stpgpu_sf_info& info)
+    bool write_labels, std::vector<stpgpu_island>& islands, stpgpu_sf_info& info)
 {
     if (rows <= 0 || cols <= 0 || (rows % 2) || (cols % 2))
         fail(STPGPU_ERR_INVALID_ARG, "image dimensions must be positive and even (ccl.h:116-117)");
@@ -1958,46 +2014,32 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     const double d_neg = bg - p.detection_n_sigma * rms;
 
     // ---- connected components
-    CclGeom geom { rows, cols, rows / 2, cols / 2 };
-    uint8_t* cls = c->buf<uint8_t>("ccl_cls", n);
-    uint32_t* P = c->buf<uint32_t>("ccl_P", n);
-    uint32_t* R = c->buf<uint32_t>("ccl_R", n);
-    unsigned int* err = c->buf<unsigned int>("ccl_err", 2);
-    int32_t* L = d_labels ? d_labels : c->buf<int32_t>("ccl_L", n);
-    STPGPU_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), st));
+    const CclGeom geom { rows, cols, rows / 2, cols / 2 };
+    const int64_t nch = ccl_chunks(n);
+    CclBufs cb;
+    cb.cls = c->buf<uint8_t>("ccl_cls", size_t(nch) * CCL_CHUNK);
+    cb.P = c->buf<uint32_t>("ccl_P", n);
+    cb.R = c->buf<uint32_t>("ccl_R", n);
+    cb.cnt = c->buf<uint32_t>("ccl_cnt", 3 * size_t(nch + 1));
+    cb.off = c->buf<uint32_t>("ccl_off", 3 * size_t(nch + 1));
+    cb.misc = c->buf<uint32_t>("ccl_misc", 8);
+    cb.fgl = c->buf<uint32_t>("ccl_fgl", n);
+    cb.L = write_labels ? (d_labels ? d_labels : c->buf<int32_t>("ccl_L", n)) : nullptr;
+    STPGPU_CUDA_TRY(cudaMemsetAsync(cb.misc, 0, 8 * sizeof(uint32_t), st));
     const int slice = p.ccl_slice_cols > 0 ? p.ccl_slice_cols : std::max(2, cols / 8);
-    k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, geom, a_pos, a_neg, p.find_negative_sources, cls, P);
-    STPGPU_CHECK_LAUNCH();
-    k_ccl_union<<<grid1d(n, 256), 256, 0, st>>>(cls, geom, p.ccl_4connectivity, slice, P, err);
-    STPGPU_CHECK_LAUNCH();
-    k_ccl_flatten<<<grid1d(n, 256), 256, 0, st>>>(cls, n, P, err);
-    STPGPU_CHECK_LAUNCH();
-    const int nchunks = int(ceil_div(n, RANK_CHUNK));
-    uint32_t* cpos = c->buf<uint32_t>("ccl_cpos", nchunks + 1);
-    uint32_t* cneg = c->buf<uint32_t>("ccl_cneg", nchunks + 1);
-    uint32_t* opos = c->buf<uint32_t>("ccl_opos", nchunks + 1);
-    uint32_t* oneg = c->buf<uint32_t>("ccl_oneg", nchunks + 1);
-    k_ccl_rootcount<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, cpos, cneg);
-    STPGPU_CHECK_LAUNCH();
-    k_scan_single<<<1, 1024, 0, st>>>(cpos, opos, nchunks);
-    k_scan_single<<<1, 1024, 0, st>>>(cneg, oneg, nchunks);
-    STPGPU_CHECK_LAUNCH();
-    k_ccl_rank<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, opos, oneg, R);
-    STPGPU_CHECK_LAUNCH();
-    k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(cls, P, R, geom, L);
-    STPGPU_CHECK_LAUNCH();
-    uint32_t* hcnt = c->host_stage<uint32_t>(4);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[0], opos + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[1], oneg + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[2], err, sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, a_pos, a_neg, p.find_negative_sources, p.ccl_4connectivity, slice,
+        cb));
+    // label counts, foreground count and the union-find flag in one read-back
+    uint32_t* hcnt = c->host_stage<uint32_t>(8);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    if (hcnt[2])
+    if (hcnt[3])
         fail(STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)");
-    const int np = int(hcnt[0]), nneg = int(hcnt[1]);
+    const int np = int(hcnt[0]), nneg = int(hcnt[1]), nfg = int(hcnt[2]);
     info.n_labels_pos = np;
     info.n_labels_neg = nneg;
 
-    // ---- extrema, detection filter, moments (sourcefind.cpp:342-628)
+    // ---- extrema, detection filter, moments (sourcefind.cpp:342-628) over the foreground list
     const int nl = std::max(1, np + nneg);
     unsigned long long* ext = c->buf<unsigned long long>("sf_ext", nl);
     unsigned long long* eidx = c->buf<unsigned long long>("sf_eidx", nl);
@@ -2005,16 +2047,19 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     int* ns = c->buf<int>("sf_ns", nl);
     uint32_t* flags = c->buf<uint32_t>("sf_flags", nl + 1);
     uint32_t* foff = c->buf<uint32_t>("sf_foff", nl + 1);
-    uint32_t* nvalid = c->buf<uint32_t>("sf_nvalid", 2);
+    uint32_t* sb = c->buf<uint32_t>("fg_sb", nl);
+    uint32_t* se = c->buf<uint32_t>("fg_se", nl);
+    uint32_t* sp = c->buf<uint32_t>("fg_sp", nl);
+    uint32_t* nvalid = cb.misc + 4;
     unsigned long long* ext_pos = ext;
     unsigned long long* ext_neg = ext + np;
     const unsigned long long kpos = host_okey(d_pos), kneg = host_okey(d_neg);
-    STPGPU_CUDA_TRY(cudaMemsetAsync(mom, 0, sizeof(double) * 6 * nl, st));
-    STPGPU_CUDA_TRY(cudaMemsetAsync(ns, 0, sizeof(int) * nl, st));
-    STPGPU_CUDA_TRY(cudaMemsetAsync(nvalid, 0, sizeof(uint32_t), st));
-    const bool packed = sizeof(T) == 4 && (n % 4) == 0 && (reinterpret_cast<uintptr_t>(d_img) % 16) == 0
-        && (reinterpret_cast<uintptr_t>(L) % 16) == 0 && n < (int64_t(1) << 32);
-    if (packed && nl > 0) {
+    const int64_t nfk = std::max(nfg, 1);
+    uint32_t* fcode = c->buf<uint32_t>("fg_code", nfk);
+    uint32_t* fm = c->buf<uint32_t>("fg_m", nfk);
+    const unsigned gl = unsigned(ceil_div(std::max(nfg, 1), 256));
+    const bool packed = sizeof(T) == 4;
+    if (packed) {
         // one pass: threshold rounded onto the float grid (largest float <=
         // the positive threshold, smallest float >= the negative one)
         float tf = float(d_pos);
@@ -2025,82 +2070,62 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
             tc = std::nextafter(tc, HUGE_VALF);
         const uint32_t fpos = fkey32(tf), fneg = fkey32(tc);
         unsigned long long* pk = c->buf<unsigned long long>("sf_pk", nl);
-        k_extrema_init<<<grid1d(nl, 256), 256, 0, st>>>(pk, np, nl, (unsigned long long)fpos << 32 | 0xffffffffull,
-            (unsigned long long)fneg << 32);
+        k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(pk, nullptr, np, nl, (unsigned long long)fpos << 32 | 0xffffffffull,
+            (unsigned long long)fneg << 32, sb, se, sp, nvalid);
         STPGPU_CHECK_LAUNCH();
-        k_extrema_packed4<<<grid1d(n / 4, 256), 256, 0, st>>>(reinterpret_cast<const float*>(d_img), L, n / 4, pk,
-            pk + np);
+        k_fg_gather<T, true><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, pk);
         STPGPU_CHECK_LAUNCH();
         k_extrema_unpack<<<grid1d(nl, 256), 256, 0, st>>>(pk, np, nl, fpos, fneg, kpos, kneg, ext, eidx);
         STPGPU_CHECK_LAUNCH();
     } else {
-        k_extrema_init<<<grid1d(std::max(nl, 1), 256), 256, 0, st>>>(ext, np, nl, kpos, kneg);
+        k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(ext, eidx, np, nl, kpos, kneg, sb, se, sp, nvalid);
         STPGPU_CHECK_LAUNCH();
-        STPGPU_CUDA_TRY(cudaMemsetAsync(eidx, 0xff, sizeof(unsigned long long) * nl, st));
-        k_extrema<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg);
+        k_fg_gather<T, false><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, ext);
         STPGPU_CHECK_LAUNCH();
-        k_extrema_idx<T><<<grid1d(n, 256), 256, 0, st>>>(d_img, L, n, ext_pos, ext_neg, kpos, kneg, eidx, eidx + np);
-        STPGPU_CHECK_LAUNCH();
-    }
-    const uint32_t* fit_pix = nullptr; // pixels sorted by label, and each label's segment
-    const uint32_t* fit_sb = nullptr;
-    const uint32_t* fit_se = nullptr;
-    {
-        // ordered (deterministic) moments: compact -> stable sort by label -> per-label sums
-        uint32_t* fcnt = c->buf<uint32_t>("fg_cnt", nchunks + 1);
-        uint32_t* foffs = c->buf<uint32_t>("fg_off", nchunks + 1);
-        k_fg_count<<<nchunks, SF_THREADS, 0, st>>>(L, n, np, ext_pos, ext_neg, kpos, kneg, fcnt);
-        STPGPU_CHECK_LAUNCH();
-        k_scan_single<<<1, 1024, 0, st>>>(fcnt, foffs, nchunks);
-        STPGPU_CHECK_LAUNCH();
-        uint32_t* hk = c->host_stage<uint32_t>(4);
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hk, foffs + nchunks, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-        const int64_t nk = hk[0];
-        const int64_t nkk = std::max<int64_t>(nk, 1);
-        uint32_t* k0 = c->buf<uint32_t>("fg_k0", nkk);
-        uint32_t* v0 = c->buf<uint32_t>("fg_v0", nkk);
-        uint32_t* k1 = c->buf<uint32_t>("fg_k1", nkk);
-        uint32_t* v1 = c->buf<uint32_t>("fg_v1", nkk);
-        k_fg_compact<<<nchunks, SF_THREADS, 0, st>>>(L, n, np, ext_pos, ext_neg, kpos, kneg, p.generate_labelmap,
-            foffs, k0, v0);
-        STPGPU_CHECK_LAUNCH();
-        uint32_t* sb = c->buf<uint32_t>("fg_sb", nl);
-        uint32_t* se = c->buf<uint32_t>("fg_se", nl);
-        STPGPU_CUDA_TRY(cudaMemsetAsync(sb, 0, sizeof(uint32_t) * nl, st));
-        STPGPU_CUDA_TRY(cudaMemsetAsync(se, 0, sizeof(uint32_t) * nl, st));
-        if (nk > 0) {
-            int end_bit = 1;
-            while (end_bit < 32 && (uint64_t(1) << end_bit) < uint64_t(nl))
-                end_bit++;
-            size_t tb = 0;
-            cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, int(nk), 0, end_bit, st);
-            void* tmp = c->buf<unsigned char>("cubtmp_sf", tb);
-            if (cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, v0, v1, int(nk), 0, end_bit, st) != cudaSuccess)
-                fail(STPGPU_ERR_CUDA, "label sort failed");
-            k_seg_bounds<<<grid1d(nk, 256), 256, 0, st>>>(k1, nk, sb, se);
-            STPGPU_CHECK_LAUNCH();
-            fit_pix = v1;
-        }
-        fit_sb = sb;
-        fit_se = se;
-        k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, mom, ns);
+        k_fg_extrema_idx<T><<<gl, 256, 0, st>>>(d_img, fcode, fm, nfg, np, ext, kpos, kneg, eidx);
         STPGPU_CHECK_LAUNCH();
     }
+    // ordered (deterministic) moments: stable sort of the list by label
+    // (invalid labels last), segments, per-label sums in memory order
+    const uint32_t* fit_pix = nullptr;
+    uint32_t* k0 = c->buf<uint32_t>("fg_k0", nfk);
+    uint32_t* v0 = c->buf<uint32_t>("fg_v0", nfk);
+    uint32_t* k1 = c->buf<uint32_t>("fg_k1", nfk);
+    uint32_t* v1 = c->buf<uint32_t>("fg_v1", nfk);
+    int end_bit = 1;
+    while (end_bit < 32 && (uint64_t(1) << end_bit) <= uint64_t(nl))
+        end_bit++;
+    const uint32_t sentinel = uint32_t((uint64_t(1) << end_bit) - 1);
+    if (nfg > 0) {
+        k_fg_keys<<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, sentinel, k0, v0,
+            p.generate_labelmap ? cb.L : nullptr);
+        STPGPU_CHECK_LAUNCH();
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, nfg, 0, end_bit, st);
+        void* tmp = c->buf<unsigned char>("cubtmp_sf", tb);
+        if (cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, v0, v1, nfg, 0, end_bit, st) != cudaSuccess)
+            fail(STPGPU_ERR_CUDA, "label sort failed");
+        k_seg_bounds<<<gl, 256, 0, st>>>(k1, v1, nfg, uint32_t(np + nneg), uint32_t(cols / 2) * uint32_t(rows), sb, se,
+            sp);
+        STPGPU_CHECK_LAUNCH();
+        fit_pix = v1;
+    }
+    k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, sp, mom, ns);
+    STPGPU_CHECK_LAUNCH();
     k_island_flags<<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext_pos, ext_neg, kpos, kneg, ns, ns + np,
         p.source_min_area, flags, nvalid);
     STPGPU_CHECK_LAUNCH();
-    k_scan_single<<<1, 1024, 0, st>>>(flags, foff, np + nneg);
+    // island total next to the valid-label count (misc[4], misc[5]): one read-back
+    k_scan_rows<<<1, 1024, 0, st>>>(flags, foff, np + nneg, 0, cb.misc + 5);
     STPGPU_CHECK_LAUNCH();
     IslandRaw* raw = c->buf<IslandRaw>("sf_raw", nl);
     k_island_scatter<<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, flags, foff, ext_pos, ext_neg, eidx, eidx + np, ns,
         ns + np, mom, mom + 6 * size_t(np), raw);
     STPGPU_CHECK_LAUNCH();
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[0], foff + (np + nneg), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&hcnt[1], nvalid, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    const int nis = int(hcnt[0]);
-    info.n_valid_labels = int(hcnt[1]);
+    const int nis = int(hcnt[1]);
+    info.n_valid_labels = int(hcnt[0]);
     info.n_islands = nis;
     std::vector<IslandRaw> hr(nis);
     if (nis)
@@ -2155,8 +2180,7 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
             int* dit = c->buf<int>("fit_iter", nfit);
             STPGPU_CUDA_TRY(cudaMemcpyAsync(dkeys, keys.data(), sizeof(int) * nfit, cudaMemcpyHostToDevice, st));
             STPGPU_CUDA_TRY(cudaMemcpyAsync(dinit, init.data(), sizeof(double) * 6 * nfit, cudaMemcpyHostToDevice, st));
-            k_gauss_fit<T><<<nfit, 32, 0, st>>>(d_img, rows, cols, fit_pix, fit_sb, fit_se, dkeys, dinit, nfit, dout,
-                dit);
+            k_gauss_fit<T><<<nfit, 32, 0, st>>>(d_img, rows, cols, fit_pix, sb, se, sp, dkeys, dinit, nfit, dout, dit);
             STPGPU_CHECK_LAUNCH();
             std::vector<double> out(6 * size_t(nfit));
             std::vector<int> its(nfit);
@@ -2495,10 +2519,11 @@ stpgpu_status stpgpu_source_find_ex(stpgpu_context* c, const void* image, int im
         stpgpu_sf_info local {};
         stpgpu_sf_info* inf = info ? info : &local;
         std::memset(inf, 0, sizeof(*inf));
+        const bool want = label_map != nullptr;
         if (image_dtype == STPGPU_F32)
-            run_source_find<float>(c, reinterpret_cast<const float*>(dimg), rows, cols, *pars, dl, isl, *inf);
+            run_source_find<float>(c, reinterpret_cast<const float*>(dimg), rows, cols, *pars, dl, want, isl, *inf);
         else
-            run_source_find<double>(c, reinterpret_cast<const double*>(dimg), rows, cols, *pars, dl, isl, *inf);
+            run_source_find<double>(c, reinterpret_cast<const double*>(dimg), rows, cols, *pars, dl, want, isl, *inf);
         if (!device_ptrs && label_map) {
             const int32_t* src = c->buf<int32_t>("ccl_L", n);
             STPGPU_CUDA_TRY(cudaMemcpyAsync(label_map, src, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->stream));
@@ -2559,8 +2584,8 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += int64_t(s.nplanes) * (cs * cs * K * K * 2 * rb + lh * lh * 16 + 64 * 64 * 16);
     }
     b += rows * N * 2 * rb + N * N * rb + int64_t(image_size) * image_size * rb;
-    if (find_sources)
-        b += int64_t(image_size) * image_size * 29;
+    if (find_sources) // classes, parents, ranks, labels, foreground list; list arrays for every pixel at worst
+        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 24);
     return b + (int64_t(8) << 20);
 }
 
@@ -2591,10 +2616,10 @@ void serve_request(stpgpu_context* c, const stpgpu_request& r, stpgpu_result& re
             std::vector<stpgpu_island> isl;
             if (f32)
                 run_source_find<float>(c, reinterpret_cast<const float*>(dimg), image_size, image_size, r.sf, nullptr,
-                    isl, res.sf);
+                    r.label_map != nullptr, isl, res.sf);
             else
                 run_source_find<double>(c, reinterpret_cast<const double*>(dimg), image_size, image_size, r.sf,
-                    nullptr, isl, res.sf);
+                    nullptr, r.label_map != nullptr, isl, res.sf);
             if (r.label_map)
                 STPGPU_CUDA_TRY(cudaMemcpyAsync(r.label_map, c->buf<int32_t>("ccl_L", npix), sizeof(int32_t) * npix,
                     cudaMemcpyDeviceToHost, c->stream));
@@ -2926,14 +2951,17 @@ stpgpu_status stpgpu_server_stats_get(stpgpu_server* sv, stpgpu_server_stats* ou
 // host-side it uses no heap either (no exceptions, strings or containers).
 //
 // Scratch layout for n = rows * cols pixels (byte offsets, 256-aligned):
-//   cls  n bytes        pixel class (0 background, 1 positive, 2 negative)
+//   cls  nchunks * CCL_CHUNK bytes   pixel class (0 background, 1 positive,
+//                       2 negative), background padding past n
 //   P    n uint32       union-find parents
 //   R    n uint32       final label number of each root
-//   err  2 uint32       union-find step-bound flag; MUST start at zero, so
-//                       every call clears it before the first kernel
-//   cpos, cneg, opos, oneg   (nchunks + 1) uint32 each: roots per chunk of
-//                       RANK_CHUNK keys and their exclusive scans
-// Everything except err is fully written before it is read in each call.
+//   misc 8 uint32       row totals and the union-find step-bound flag; the
+//                       flag MUST start at zero, so every call clears misc
+//                       before the first kernel
+//   cnt, off            3 * (nchunks + 1) uint32 each: positive roots,
+//                       negative roots and foreground keys per chunk of
+//                       CCL_CHUNK keys, and their exclusive scans
+// Everything except misc is fully written before it is read in each call.
 // The array is shared by every call on a device: two calls whose kernels
 // overlap on the GPU (different streams, or different host threads) race on
 // it and give wrong labels.  The first call on a device resolves the array's
@@ -2943,10 +2971,11 @@ stpgpu_status stpgpu_server_stats_get(stpgpu_server* sv, stpgpu_server_stats* ou
 namespace stpgpu {
 
 constexpr size_t noalloc_align(size_t b) { return (b + 255) / 256 * 256; }
-constexpr size_t noalloc_chunks(size_t n) { return (n + RANK_CHUNK - 1) / RANK_CHUNK; }
+constexpr size_t noalloc_chunks(size_t n) { return (n + CCL_CHUNK - 1) / CCL_CHUNK; }
 constexpr size_t noalloc_bytes(size_t n)
 {
-    return noalloc_align(n) + 2 * noalloc_align(4 * n) + 256 + 4 * noalloc_align(4 * (noalloc_chunks(n) + 1));
+    return noalloc_align(noalloc_chunks(n) * CCL_CHUNK) + 2 * noalloc_align(4 * n) + 256
+        + 2 * noalloc_align(12 * (noalloc_chunks(n) + 1));
 }
 constexpr size_t kNoallocScratchBytes = noalloc_bytes(STPGPU_NOALLOC_MAX_PIXELS);
 
@@ -2971,41 +3000,28 @@ static cudaError_t noalloc_label_run(unsigned char* base, cudaStream_t st, const
     const int64_t n = int64_t(rows) * cols;
     const size_t nch = noalloc_chunks(size_t(n));
     size_t o = 0;
-    uint8_t* cls = base + o;
-    o += noalloc_align(size_t(n));
-    uint32_t* P = reinterpret_cast<uint32_t*>(base + o);
+    CclBufs b;
+    b.cls = base + o;
+    o += noalloc_align(nch * CCL_CHUNK);
+    b.P = reinterpret_cast<uint32_t*>(base + o);
     o += noalloc_align(4 * size_t(n));
-    uint32_t* R = reinterpret_cast<uint32_t*>(base + o);
+    b.R = reinterpret_cast<uint32_t*>(base + o);
     o += noalloc_align(4 * size_t(n));
-    unsigned int* err = reinterpret_cast<unsigned int*>(base + o);
+    b.misc = reinterpret_cast<uint32_t*>(base + o);
     o += 256;
-    uint32_t* cnt[4];
-    for (int k = 0; k < 4; k++) {
-        cnt[k] = reinterpret_cast<uint32_t*>(base + o);
-        o += noalloc_align(4 * (nch + 1));
-    }
-    cudaError_t e = cudaMemsetAsync(err, 0, 2 * sizeof(unsigned int), st);
+    b.cnt = reinterpret_cast<uint32_t*>(base + o);
+    o += noalloc_align(12 * (nch + 1));
+    b.off = reinterpret_cast<uint32_t*>(base + o);
+    b.fgl = nullptr;
+    b.L = L;
+    cudaError_t e = cudaMemsetAsync(b.misc, 0, 8 * sizeof(uint32_t), st);
     if (e != cudaSuccess)
         return e;
     const CclGeom geom { rows, cols, rows / 2, cols / 2 };
-    const int nchunks = int(nch);
-    k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(img, geom, tp, tn, findneg, cls, P);
-    k_ccl_union<<<grid1d(n, 256), 256, 0, st>>>(cls, geom, conn4, slice, P, err);
-    k_ccl_flatten<<<grid1d(n, 256), 256, 0, st>>>(cls, n, P, err);
-    k_ccl_rootcount<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, cnt[0], cnt[1]);
-    k_scan_single<<<1, 1024, 0, st>>>(cnt[0], cnt[2], nchunks);
-    k_scan_single<<<1, 1024, 0, st>>>(cnt[1], cnt[3], nchunks);
-    k_ccl_rank<<<nchunks, SF_THREADS, 0, st>>>(cls, P, n, cnt[2], cnt[3], R);
-    k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(cls, P, R, geom, L);
-    g_launches += 8;
-    if ((e = cudaGetLastError()) != cudaSuccess)
+    if ((e = ccl_enqueue<T>(st, img, geom, tp, tn, findneg, conn4, slice, b)) != cudaSuccess)
         return e;
-    // counts and the step-bound flag, read back into host stack memory
-    if ((e = cudaMemcpyAsync(&h[0], cnt[2] + nchunks, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-        return e;
-    if ((e = cudaMemcpyAsync(&h[1], cnt[3] + nchunks, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-        return e;
-    if ((e = cudaMemcpyAsync(&h[2], err, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+    // label counts and the step-bound flag, read back into host stack memory
+    if ((e = cudaMemcpyAsync(h, b.misc, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
         return e;
     return cudaStreamSynchronize(st);
 }
@@ -3059,7 +3075,7 @@ extern "C" stpgpu_status stpgpu_label_noalloc(int device, void* stream, const vo
     }
     const int slice = ccl_slice_cols > 0 ? ccl_slice_cols : std::max(2, cols / 8);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    uint32_t h[3] = { 0, 0, 0 }; // positive labels, negative labels, step-bound flag
+    uint32_t h[4] = { 0, 0, 0, 0 }; // positive labels, negative labels, foreground keys, step-bound flag
     if (image_dtype == STPGPU_F32)
         e = noalloc_label_run<float>(base, st, static_cast<const float*>(image), rows, cols, analysis_thresh_pos,
             analysis_thresh_neg, find_negative_sources, ccl_4connectivity, slice, label_map, h);
@@ -3069,7 +3085,7 @@ extern "C" stpgpu_status stpgpu_label_noalloc(int device, void* stream, const vo
     cudaSetDevice(prev);
     if (e != cudaSuccess)
         return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_CUDA, "labelling", e);
-    if (h[2])
+    if (h[3])
         return noalloc_msg(err_msg, err_msg_len, STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)",
             cudaSuccess);
     if (n_labels_pos)

@@ -457,7 +457,7 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
 // n up to a few hundred thousand).  off[n] = total.  Each thread first
 // loads 16 elements (16 coalesced rows of 1024), then the rows are scanned
 // in order with warp shuffles and one shared-memory step per row.
-__global__ void __launch_bounds__(1024) k_scan_single(const uint32_t* cnt, uint32_t* off, int n)
+__device__ __forceinline__ uint32_t scan_block_1024(const uint32_t* cnt, uint32_t* off, int n)
 {
     __shared__ uint32_t wsum[32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -503,6 +503,21 @@ __global__ void __launch_bounds__(1024) k_scan_single(const uint32_t* cnt, uint3
     }
     if (tid == 0)
         off[n] = carry;
+    return carry;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_single(const uint32_t* cnt, uint32_t* off, int n)
+{
+    scan_block_1024(cnt, off, n);
+}
+
+// One such scan per block: row blockIdx.x of cnt and off (row stride
+// `stride`); the totals also go to tot[row].
+__global__ void __launch_bounds__(1024) k_scan_rows(const uint32_t* cnt, uint32_t* off, int n, int stride, uint32_t* tot)
+{
+    const uint32_t t = scan_block_1024(cnt + int64_t(blockIdx.x) * stride, off + int64_t(blockIdx.x) * stride, n);
+    if (threadIdx.x == 0)
+        tot[blockIdx.x] = t;
 }
 
 // ---------------------------------------------------------------- accumulators

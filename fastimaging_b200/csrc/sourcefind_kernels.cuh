@@ -306,6 +306,79 @@ struct CclGeom {
     }
 };
 
+// The labelling passes after the first work on chunks of CCL_CHUNK scan keys,
+// one block of SF_THREADS threads per chunk, each thread reading the classes
+// of CCL_KPT consecutive keys with one 16-byte load.  The class array is
+// padded with background up to a whole number of chunks.
+constexpr int CCL_KPT = 16;
+constexpr int CCL_CHUNK = SF_THREADS * CCL_KPT;
+
+__device__ __forceinline__ uint32_t cls_at(const uint32_t (&w)[4], int k)
+{
+    return (w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+}
+
+__device__ __forceinline__ void load_cls16(const uint8_t* cls, uint32_t (&w)[4])
+{
+    const uint4 v = reinterpret_cast<const uint4*>(cls)[int64_t(blockIdx.x) * SF_THREADS + threadIdx.x];
+    w[0] = v.x;
+    w[1] = v.y;
+    w[2] = v.z;
+    w[3] = v.w;
+}
+
+// Exclusive scan of v over the block (SF_THREADS threads); *total = the sum.
+// Callers pack up to three 16-bit counts into v.
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* total)
+{
+    __shared__ unsigned long long ws[SF_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        ws[warp] = x;
+    __syncthreads();
+    unsigned long long before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < SF_THREADS / 32; w++) {
+        const unsigned long long t = ws[w];
+        if (w < warp)
+            before += t;
+        all += t;
+    }
+    *total = all;
+    __syncthreads();
+    return before + x - v;
+}
+
+// The chunk's foreground keys in scan order, compacted into q as
+// (offset in the chunk) | class << 12; returns their number.
+__device__ __forceinline__ int chunk_queue(const uint32_t (&w)[4], uint16_t* q)
+{
+    uint32_t mask = 0;
+#pragma unroll
+    for (int k = 0; k < CCL_KPT; k++)
+        if (cls_at(w, k))
+            mask |= 1u << k;
+    unsigned long long tot = 0;
+    int p = int(block_excl_scan(__popc(mask), &tot));
+    while (mask) {
+        const int k = __ffs(mask) - 1;
+        mask &= mask - 1;
+        q[p++] = uint16_t((threadIdx.x * CCL_KPT + k) | (cls_at(w, k) << 12));
+    }
+    __syncthreads();
+    return int(tot);
+}
+
+// Classes (0 background, 1 above the positive analysis threshold, 2 below
+// the negative one) and parents of foreground keys, one key per thread; the
+// general form, for any even image size.
 template <typename T>
 __global__ void k_ccl_init(const T* img, CclGeom g, double tp, double tn, int findneg, uint8_t* cls, uint32_t* P)
 {
@@ -320,7 +393,54 @@ __global__ void k_ccl_init(const T* img, CclGeom g, double tp, double tn, int fi
     else if (findneg && v < tn)
         c = 2;
     cls[s] = c;
-    P[s] = uint32_t(s);
+    if (c)
+        P[s] = uint32_t(s);
+}
+
+// The same for rows % 4 == 0 and a 16-byte aligned image: four keys of one
+// column per step (one 16-byte load or two), classes stored four at a time,
+// parents of groups holding foreground as one 16-byte store.  Groups from
+// ngroups to ngroups_pad are the background padding of the class array.
+template <typename T>
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_init4(const T* img, CclGeom g, double tp, double tn, int findneg,
+    int64_t ngroups, int64_t ngroups_pad, uint32_t* cls4, uint4* P4)
+{
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < ngroups_pad; q += stride) {
+        uint32_t packed = 0;
+        if (q < ngroups) {
+            const int64_t m = g.mem_of_key(4 * q);
+            double v[4];
+            if constexpr (sizeof(T) == 4) {
+                const float4 f = *reinterpret_cast<const float4*>(img + m);
+                v[0] = f.x;
+                v[1] = f.y;
+                v[2] = f.z;
+                v[3] = f.w;
+            } else {
+                const double2 a = *reinterpret_cast<const double2*>(img + m);
+                const double2 b = *reinterpret_cast<const double2*>(img + m + 2);
+                v[0] = a.x;
+                v[1] = a.y;
+                v[2] = b.x;
+                v[3] = b.y;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                uint32_t c = 0;
+                if (v[k] > tp)
+                    c = 1;
+                else if (findneg && v[k] < tn)
+                    c = 2;
+                packed |= c << (8 * k);
+            }
+            if (packed) {
+                const uint32_t s = uint32_t(4 * q);
+                P4[q] = make_uint4(s, s + 1, s + 2, s + 3);
+            }
+        }
+        cls4[q] = packed;
+    }
 }
 
 __device__ __forceinline__ uint32_t uf_find(const uint32_t* P, uint32_t x, unsigned* err)
@@ -370,120 +490,117 @@ __device__ __forceinline__ void uf_union(uint32_t* P, uint32_t a, uint32_t b, un
 //   bottom-left(c_i-1, r+1)                    c_i >= 1, r not in {rows/2-1, rows-1}
 //   wrap t-left(c_i-1, rows-1)                 c_i >= 1, r == 0
 //   slice link (c_i-1, 0)                      r == rows-1, c_i a slice start
-__global__ void k_ccl_union(const uint8_t* cls, CclGeom g, int conn4, int slice_cols, uint32_t* P, unsigned* err)
+// One thread per foreground key of the chunk (compacted first, so the
+// unions of a dense island run in parallel).
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_union(const uint8_t* cls, CclGeom g, int conn4, int slice_cols,
+    uint32_t* P, unsigned* err)
 {
-    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int64_t n = int64_t(g.rows) * g.cols;
-    if (s >= n)
-        return;
-    const uint8_t my = cls[s];
-    if (!my)
-        return;
+    __shared__ uint16_t q[CCL_CHUNK];
+    uint32_t w[4];
+    load_cls16(cls, w);
+    const int nq = chunk_queue(w, q);
+    const int64_t base = int64_t(blockIdx.x) * CCL_CHUNK;
     const int rows = g.rows;
-    const int ci = int(uint32_t(s) / uint32_t(rows)), r = int(uint32_t(s) - uint32_t(ci) * uint32_t(rows));
-    auto link = [&](int64_t q) {
-        if (cls[q] == my)
-            uf_union(P, uint32_t(s), uint32_t(q), err);
-    };
-    if (ci >= 1)
-        link(s - rows);
-    if (r != 0 && r != g.rshift)
-        link(s - 1);
-    if (r == 0)
-        link(s + rows - 1);
-    if (!conn4 && ci >= 1) {
+    for (int i = threadIdx.x; i < nq; i += SF_THREADS) {
+        const int64_t s = base + (q[i] & 0xfff);
+        const uint32_t my = q[i] >> 12;
+        const int ci = int(uint32_t(s) / uint32_t(rows)), r = int(uint32_t(s) - uint32_t(ci) * uint32_t(rows));
+        auto link = [&](int64_t t) {
+            if (cls[t] == my)
+                uf_union(P, uint32_t(s), uint32_t(t), err);
+        };
+        if (ci >= 1)
+            link(s - rows);
         if (r != 0 && r != g.rshift)
-            link(s - rows - 1);
-        if (r != g.rshift - 1 && r != rows - 1)
-            link(s - rows + 1);
-        if (r == 0)
             link(s - 1);
-        if (r == rows - 1 && (ci % slice_cols) == 0)
-            link(s - 2 * int64_t(rows) + 1);
-    }
-}
-
-__global__ void k_ccl_flatten(const uint8_t* cls, int64_t n, uint32_t* P, unsigned* err)
-{
-    const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (s >= n || !cls[s])
-        return;
-    P[s] = uf_find(P, uint32_t(s), err);
-}
-
-// Per block of SF_THREADS*8 keys: number of positive / negative roots.
-constexpr int RANK_CHUNK = SF_THREADS * 8;
-__global__ void __launch_bounds__(SF_THREADS) k_ccl_rootcount(const uint8_t* cls, const uint32_t* P, int64_t n,
-    uint32_t* cnt_pos, uint32_t* cnt_neg)
-{
-    __shared__ uint32_t sp, sn;
-    if (threadIdx.x == 0)
-        sp = sn = 0;
-    __syncthreads();
-    uint32_t lp = 0, ln = 0;
-    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
-    for (int k = threadIdx.x; k < RANK_CHUNK; k += blockDim.x) {
-        const int64_t s = b0 + k;
-        if (s < n && cls[s] && P[s] == uint32_t(s)) {
-            if (cls[s] == 1)
-                lp++;
-            else
-                ln++;
+        if (r == 0)
+            link(s + rows - 1);
+        if (!conn4 && ci >= 1) {
+            if (r != 0 && r != g.rshift)
+                link(s - rows - 1);
+            if (r != g.rshift - 1 && r != rows - 1)
+                link(s - rows + 1);
+            if (r == 0)
+                link(s - 1);
+            if (r == rows - 1 && (ci % slice_cols) == 0)
+                link(s - 2 * int64_t(rows) + 1);
         }
     }
-    atomicAdd(&sp, lp);
-    atomicAdd(&sn, ln);
-    __syncthreads();
+}
+
+// Path compression of every foreground key to its root, and per chunk the
+// number of positive roots, negative roots and foreground keys (rows 0, 1,
+// 2 of cnt, row stride `stride`).
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_flatten(const uint8_t* cls, uint32_t* P, uint32_t* cnt, int stride,
+    unsigned* err)
+{
+    __shared__ uint16_t q[CCL_CHUNK];
+    uint32_t w[4];
+    load_cls16(cls, w);
+    const int nq = chunk_queue(w, q);
+    const uint32_t base = uint32_t(blockIdx.x) * CCL_CHUNK;
+    uint32_t rp = 0, rn = 0;
+    for (int i = threadIdx.x; i < nq; i += SF_THREADS) {
+        const uint32_t s = base + (q[i] & 0xfff);
+        const uint32_t r = uf_find(P, s, err);
+        if (r == s) {
+            if ((q[i] >> 12) == 1)
+                rp++;
+            else
+                rn++;
+        } else {
+            P[s] = r;
+        }
+    }
+    unsigned long long tot = 0;
+    block_excl_scan(rp | (unsigned long long)rn << 16, &tot);
     if (threadIdx.x == 0) {
-        cnt_pos[blockIdx.x] = sp;
-        cnt_neg[blockIdx.x] = sn;
+        cnt[blockIdx.x] = uint32_t(tot & 0xffff);
+        cnt[stride + blockIdx.x] = uint32_t((tot >> 16) & 0xffff);
+        cnt[2 * stride + blockIdx.x] = uint32_t(nq);
     }
 }
 
 // Final label number of each root: 1 + its rank among roots of the same sign
 // in scan order (ccl.h:452-480 numbers roots in increasing provisional-label
-// order, which is scan order of each component's first pixel).
-__global__ void __launch_bounds__(SF_THREADS) k_ccl_rank(const uint8_t* cls, const uint32_t* P, int64_t n,
-    const uint32_t* off_pos, const uint32_t* off_neg, uint32_t* R)
+// order, which is scan order of each component's first pixel); off holds the
+// exclusive scans of k_ccl_flatten's counts.  With fgl, also the list of all
+// foreground keys in scan order.
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_rank(const uint8_t* cls, const uint32_t* P, const uint32_t* off,
+    int stride, uint32_t* R, uint32_t* fgl)
 {
-    __shared__ uint32_t wp[SF_THREADS / 32], wn[SF_THREADS / 32];
-    __shared__ uint32_t base_p, base_n;
-    if (threadIdx.x == 0) {
-        base_p = off_pos[blockIdx.x];
-        base_n = off_neg[blockIdx.x];
-    }
-    __syncthreads();
-    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int round = 0; round < RANK_CHUNK / SF_THREADS; round++) {
-        const int64_t s = b0 + int64_t(round) * SF_THREADS + threadIdx.x;
-        bool isroot = s < n && cls[s] && P[s] == uint32_t(s);
-        const bool pos = isroot && cls[s] == 1;
-        const bool neg = isroot && cls[s] == 2;
-        const unsigned bp = __ballot_sync(0xffffffffu, pos), bn = __ballot_sync(0xffffffffu, neg);
-        if (lane == 0) {
-            wp[warp] = __popc(bp);
-            wn[warp] = __popc(bn);
-        }
-        __syncthreads();
-        uint32_t ep = base_p, en = base_n;
-        for (int w = 0; w < warp; w++) {
-            ep += wp[w];
-            en += wn[w];
-        }
-        const unsigned lm = (1u << lane) - 1u;
-        if (pos)
-            R[s] = ep + __popc(bp & lm) + 1;
-        if (neg)
-            R[s] = en + __popc(bn & lm) + 1;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 0; w < SF_THREADS / 32; w++) {
-                base_p += wp[w];
-                base_n += wn[w];
+    uint32_t w[4];
+    load_cls16(cls, w);
+    const uint32_t s0 = uint32_t(blockIdx.x) * CCL_CHUNK + threadIdx.x * CCL_KPT;
+    uint32_t fgmask = 0, rootmask = 0, np = 0, nn = 0;
+#pragma unroll
+    for (int k = 0; k < CCL_KPT; k++) {
+        const uint32_t c = cls_at(w, k);
+        if (c) {
+            fgmask |= 1u << k;
+            if (P[s0 + k] == s0 + k) {
+                rootmask |= 1u << k;
+                if (c == 1)
+                    np++;
+                else
+                    nn++;
             }
         }
-        __syncthreads();
+    }
+    unsigned long long tot = 0;
+    const unsigned long long ex
+        = block_excl_scan(np | (unsigned long long)nn << 16 | (unsigned long long)__popc(fgmask) << 32, &tot);
+    uint32_t rp = off[blockIdx.x] + uint32_t(ex & 0xffff);
+    uint32_t rn = off[stride + blockIdx.x] + uint32_t((ex >> 16) & 0xffff);
+    uint32_t fp = off[2 * stride + blockIdx.x] + uint32_t(ex >> 32);
+    while (fgmask) {
+        const int k = __ffs(fgmask) - 1;
+        fgmask &= fgmask - 1;
+        const uint32_t s = s0 + k;
+        if (rootmask & (1u << k))
+            R[s] = cls_at(w, k) == 1 ? ++rp : ++rn;
+        if (fgl)
+            fgl[fp++] = s;
     }
 }
 
@@ -499,28 +616,38 @@ __global__ void k_ccl_label(const uint8_t* cls, const uint32_t* P, const uint32_
     L[m] = c == 0 ? 0 : (c == 1 ? int32_t(R[P[s]]) : -int32_t(R[P[s]]));
 }
 
-// -------------------------------------------------- label analysis
-
-// Extrema (sourcefind.cpp:342-378): init = detection threshold, strict compare.
-template <typename T>
-__global__ void k_extrema(const T* img, const int32_t* L, int64_t n, unsigned long long* ext_pos,
-    unsigned long long* ext_neg)
+// The same four keys of one column at a time (rows % 4 == 0, 16-byte aligned
+// label map): one 4-byte class load and one 16-byte store per step.
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_label4(const uint8_t* cls, const uint32_t* P, const uint32_t* R,
+    CclGeom g, int64_t ngroups, int32_t* L)
 {
-    const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (m >= n)
-        return;
-    const int32_t l = L[m];
-    if (l == 0)
-        return;
-    const unsigned long long k = okey(ld(img, m));
-    if (l > 0)
-        atomicMax(&ext_pos[l - 1], k);
-    else
-        atomicMin(&ext_neg[-l - 1], k);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < ngroups; q += stride) {
+        const uint32_t c4 = reinterpret_cast<const uint32_t*>(cls)[q];
+        int v[4] = { 0, 0, 0, 0 };
+        if (c4) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t c = (c4 >> (8 * k)) & 0xffu;
+                if (c) {
+                    const int r = int(R[P[4 * q + k]]);
+                    v[k] = c == 1 ? r : -r;
+                }
+            }
+        }
+        reinterpret_cast<int4*>(L)[g.mem_of_key(4 * q) >> 2] = make_int4(v[0], v[1], v[2], v[3]);
+    }
 }
 
-// Single-precision images: extremum and its first memory index in one pass,
-// as one 64-bit key per label (the value's order key above the index;
+// -------------------------------------------------- label analysis
+//
+// Everything after the labelling works on the list of foreground keys in
+// scan order (k_ccl_rank's fgl), not on the image: entry i has the label
+// code (positives 0..np-1, negatives np..np+nn-1) and the memory index of
+// its pixel.
+
+// Single-precision images keep the extremum and its first memory index as
+// one 64-bit key per label (the value's order key above the index;
 // positives keep the maximum with the lowest index through atomicMax on
 // ~index, negatives the minimum with the lowest index through atomicMin).
 // Starting keys hold the detection threshold rounded to the float grid
@@ -538,42 +665,59 @@ __device__ inline float fkey32_inv(uint32_t k)
     return __uint_as_float(u);
 }
 
-__global__ void k_extrema_init(unsigned long long* a, int np, int nl, unsigned long long vpos, unsigned long long vneg)
+// Per-label starting state: extremum keys at the detection threshold
+// (sourcefind.cpp:342-378 starts from it and compares strictly), first
+// indices unset (eidx, when given), empty segments.
+__global__ void k_fg_init(unsigned long long* ext, unsigned long long* eidx, int np, int nl, unsigned long long vpos,
+    unsigned long long vneg, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split, uint32_t* nvalid)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < nl)
-        a[i] = i < np ? vpos : vneg;
+    if (i == 0)
+        *nvalid = 0;
+    if (i >= nl)
+        return;
+    ext[i] = i < np ? vpos : vneg;
+    if (eidx)
+        eidx[i] = ~0ull;
+    seg_begin[i] = 0;
+    seg_end[i] = 0;
+    seg_split[i] = 0;
 }
 
-// Four pixels per thread (n % 4 == 0, 16-byte aligned image and labels).
-__global__ void k_extrema_packed4(const float* img, const int32_t* L, int64_t n4, unsigned long long* pk_pos,
-    unsigned long long* pk_neg)
+// Label code and memory index of each foreground key, and the extremum of
+// each label: PACKED (single precision) the 64-bit value-and-index keys
+// above, else the order key of the value (its first index follows in
+// k_fg_extrema_idx).
+template <typename T, bool PACKED>
+__global__ void k_fg_gather(const T* img, const uint8_t* cls, const uint32_t* P, const uint32_t* R, CclGeom g,
+    const uint32_t* fgl, int nfg, int np, uint32_t* fcode, uint32_t* fm, unsigned long long* ext)
 {
-    const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (g >= n4)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfg)
         return;
-    const int4 l4 = reinterpret_cast<const int4*>(L)[g];
-    if ((l4.x | l4.y | l4.z | l4.w) == 0)
-        return;
-    const float4 v4 = reinterpret_cast<const float4*>(img)[g];
-    const int32_t ls[4] = { l4.x, l4.y, l4.z, l4.w };
-    const float vs[4] = { v4.x, v4.y, v4.z, v4.w };
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int32_t l = ls[q];
-        if (l == 0)
-            continue;
-        const uint32_t m = uint32_t(g * 4 + q);
-        const unsigned long long k = (unsigned long long)fkey32(vs[q]) << 32;
-        if (l > 0)
-            atomicMax(&pk_pos[l - 1], k | (0xffffffffu - m));
+    const uint32_t s = fgl[i];
+    const bool pos = cls[s] == 1;
+    const uint32_t r = R[P[s]] - 1;
+    const uint32_t code = pos ? r : uint32_t(np) + r;
+    const uint32_t m = uint32_t(g.mem_of_key(s));
+    fcode[i] = code;
+    fm[i] = m;
+    if constexpr (PACKED) {
+        const unsigned long long k = (unsigned long long)fkey32(float(img[m])) << 32;
+        if (pos)
+            atomicMax(&ext[code], k | (0xffffffffu - m));
         else
-            atomicMin(&pk_neg[-l - 1], k | m);
+            atomicMin(&ext[code], k | m);
+    } else {
+        const unsigned long long k = okey(ld(img, m));
+        if (pos)
+            atomicMax(&ext[code], k);
+        else
+            atomicMin(&ext[code], k);
     }
 }
 
-// Packed keys -> the order keys of the extrema (double) and their indices,
-// the layout the two-pass path produces.
+// Packed keys -> the order keys of the extrema (double) and their indices.
 __global__ void k_extrema_unpack(const unsigned long long* pk, int np, int nl, uint32_t thr_pos, uint32_t thr_neg,
     unsigned long long kpos, unsigned long long kneg, unsigned long long* ext, unsigned long long* eidx)
 {
@@ -594,131 +738,88 @@ __global__ void k_extrema_unpack(const unsigned long long* pk, int np, int nl, u
 // First memory index holding the extremum (the serial reference keeps the
 // first occurrence in memory order).
 template <typename T>
-__global__ void k_extrema_idx(const T* img, const int32_t* L, int64_t n, const unsigned long long* ext_pos,
-    const unsigned long long* ext_neg, unsigned long long det_pos_key, unsigned long long det_neg_key,
-    unsigned long long* idx_pos, unsigned long long* idx_neg)
+__global__ void k_fg_extrema_idx(const T* img, const uint32_t* fcode, const uint32_t* fm, int nfg, int np,
+    const unsigned long long* ext, unsigned long long det_pos_key, unsigned long long det_neg_key,
+    unsigned long long* eidx)
 {
-    const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (m >= n)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfg)
         return;
-    const int32_t l = L[m];
-    if (l == 0)
-        return;
+    const uint32_t code = fcode[i], m = fm[i];
     const unsigned long long k = okey(ld(img, m));
-    if (l > 0) {
-        if (k > det_pos_key && k == ext_pos[l - 1])
-            atomicMin(&idx_pos[l - 1], (unsigned long long)m);
-    } else {
-        if (k < det_neg_key && k == ext_neg[-l - 1])
-            atomicMin(&idx_neg[-l - 1], (unsigned long long)m);
-    }
+    const bool hit = int(code) < np ? k > det_pos_key : k < det_neg_key;
+    if (hit && k == ext[code])
+        atomicMin(&eidx[code], (unsigned long long)m);
 }
 
-// Deterministic moments (sourcefind.cpp:457-569).  The foreground pixels of
-// valid labels are compacted in memory order, stably sorted by label, and
-// each label's sums are accumulated sequentially in memory order -- the
-// order of the reference's single-range loop -- with explicitly rounded
-// operations (no FMA contraction), so the sums are bit-identical to it.
-//
-// Pass 1: per chunk of RANK_CHUNK pixels, the number of kept pixels.
-__global__ void __launch_bounds__(SF_THREADS) k_fg_count(const int32_t* L, int64_t n, int np,
-    const unsigned long long* ext_pos, const unsigned long long* ext_neg, unsigned long long det_pos_key,
-    unsigned long long det_neg_key, uint32_t* cnt)
+// Sort keys of the list: the label code of labels whose extremum passes the
+// detection threshold, `sentinel` (above every code) for the others, whose
+// pixels are zeroed in the label map L when given (generate_labelmap).
+__global__ void k_fg_keys(const uint32_t* fcode, const uint32_t* fm, int nfg, int np, const unsigned long long* ext,
+    unsigned long long det_pos_key, unsigned long long det_neg_key, uint32_t sentinel, uint32_t* keys, uint32_t* vals,
+    int32_t* L)
 {
-    __shared__ uint32_t sc;
-    if (threadIdx.x == 0)
-        sc = 0;
-    __syncthreads();
-    uint32_t loc = 0;
-    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
-    for (int k = threadIdx.x; k < RANK_CHUNK; k += blockDim.x) {
-        const int64_t m = b0 + k;
-        if (m >= n)
-            break;
-        const int32_t l = L[m];
-        if (l > 0 ? ext_pos[l - 1] > det_pos_key : (l < 0 && ext_neg[-l - 1] < det_neg_key))
-            loc++;
-    }
-    atomicAdd(&sc, loc);
-    __syncthreads();
-    if (threadIdx.x == 0)
-        cnt[blockIdx.x] = sc;
-    (void)np;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfg)
+        return;
+    const uint32_t code = fcode[i], m = fm[i];
+    const bool valid = int(code) < np ? ext[code] > det_pos_key : ext[code] < det_neg_key;
+    keys[i] = valid ? code : sentinel;
+    vals[i] = m;
+    if (!valid && L)
+        L[m] = 0;
 }
 
-// Pass 2: ordered compaction; key = label code (positives 0..np-1, negatives
-// np..np+nn-1), value = memory index.  Invalid labels are zeroed in the map
-// when generate_labelmap.
-__global__ void __launch_bounds__(SF_THREADS) k_fg_compact(int32_t* L, int64_t n, int np,
-    const unsigned long long* ext_pos, const unsigned long long* ext_neg, unsigned long long det_pos_key,
-    unsigned long long det_neg_key, int generate_labelmap, const uint32_t* off, uint32_t* keys, uint32_t* vals)
-{
-    __shared__ uint32_t wc[SF_THREADS / 32];
-    __shared__ uint32_t base;
-    if (threadIdx.x == 0)
-        base = off[blockIdx.x];
-    __syncthreads();
-    const int64_t b0 = int64_t(blockIdx.x) * RANK_CHUNK;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int round = 0; round < RANK_CHUNK / SF_THREADS; round++) {
-        const int64_t m = b0 + int64_t(round) * SF_THREADS + threadIdx.x;
-        int32_t l = 0;
-        bool keep = false;
-        if (m < n) {
-            l = L[m];
-            if (l != 0) {
-                keep = l > 0 ? ext_pos[l - 1] > det_pos_key : ext_neg[-l - 1] < det_neg_key;
-                if (!keep && generate_labelmap)
-                    L[m] = 0;
-            }
-        }
-        const unsigned b = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0)
-            wc[warp] = __popc(b);
-        __syncthreads();
-        uint32_t e = base;
-        for (int w = 0; w < warp; w++)
-            e += wc[w];
-        if (keep) {
-            const uint32_t pos = e + __popc(b & ((1u << lane) - 1u));
-            keys[pos] = l > 0 ? uint32_t(l - 1) : uint32_t(np + (-l - 1));
-            vals[pos] = uint32_t(m);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0)
-            for (int w = 0; w < SF_THREADS / 32; w++)
-                base += wc[w];
-        __syncthreads();
-    }
-}
-
-// Segment starts of the label-sorted list.
-__global__ void k_seg_bounds(const uint32_t* keys, int64_t nk, uint32_t* seg_begin, uint32_t* seg_end)
+// Deterministic moments (sourcefind.cpp:457-569).  After a stable sort of
+// the list by key, each valid label's pixels form one segment in scan order.
+// Scan order visits the memory columns from cols/2 first, so a segment is
+// memory order rotated: its pixels in memory columns < cols/2 (memory index
+// < split_m) start at seg_split.  Memory order is [split, end) then
+// [begin, split) -- the order of the reference's single-range loop.
+__global__ void k_seg_bounds(const uint32_t* keys, const uint32_t* vals, int64_t nk, uint32_t nl, uint32_t split_m,
+    uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split)
 {
     const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= nk)
         return;
     const uint32_t k = keys[t];
-    if (t == 0 || keys[t - 1] != k)
+    if (k >= nl)
+        return;
+    const bool first = t == 0 || keys[t - 1] != k;
+    const bool last = t == nk - 1 || keys[t + 1] != k;
+    if (first)
         seg_begin[k] = uint32_t(t);
-    if (t == nk - 1 || keys[t + 1] != k)
+    if (last)
         seg_end[k] = uint32_t(t + 1);
+    const bool low = vals[t] < split_m;
+    if (low && (first || vals[t - 1] >= split_m))
+        seg_split[k] = uint32_t(t);
+    if (!low && last)
+        seg_split[k] = uint32_t(t + 1);
 }
 
-// One thread per label: ordered sums over its pixels.  mom: 6 doubles per
-// label code: sum x v, y v, x^2 v, y^2 v, x y v, v (display coordinates).
+// List position of the j-th pixel (memory order) of segment [b, e) split at sp.
+__device__ __forceinline__ uint32_t seg_at(uint32_t b, uint32_t sp, uint32_t e, uint32_t j)
+{
+    return j < e - sp ? sp + j : b + (j - (e - sp));
+}
+
+// One thread per label: ordered sums over its pixels, with explicitly
+// rounded operations (no FMA contraction), so the sums are bit-identical to
+// the reference's.  mom: 6 doubles per label code: sum x v, y v, x^2 v,
+// y^2 v, x y v, v (display coordinates).
 template <typename T>
 __global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uint32_t* vals,
-    const uint32_t* seg_begin, const uint32_t* seg_end, double* mom, int* ns)
+    const uint32_t* seg_begin, const uint32_t* seg_end, const uint32_t* seg_split, double* mom, int* ns)
 {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl)
         return;
-    const uint32_t b = seg_begin[l], e = seg_end[l];
+    const uint32_t b = seg_begin[l], e = seg_end[l], sp = seg_split[l];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
     const int vs = rows / 2, hs = cols / 2;
-    for (uint32_t t = b; t < e; t++) {
-        const int64_t m = vals[t];
+    for (uint32_t j = 0; j < e - b; j++) {
+        const int64_t m = vals[seg_at(b, sp, e, j)];
         const double val = ld(img, m);
         const int c = int(uint32_t(m) / uint32_t(rows)), r = int(uint32_t(m) - uint32_t(c) * uint32_t(rows));
         const double y = r < vs ? double(r + vs) : double(r - vs);
@@ -741,43 +842,6 @@ __global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uin
     ns[l] = int(e - b);
 }
 
-// Moments / sample counts over valid labels with atomics (unordered sums);
-// kept for reference, superseded by the ordered path above.
-template <typename T>
-__global__ void k_moments(const T* img, int32_t* L, int rows, int cols, unsigned long long det_pos_key,
-    unsigned long long det_neg_key, const unsigned long long* ext_pos, const unsigned long long* ext_neg,
-    int generate_labelmap, double* mom_pos, double* mom_neg, int* ns_pos, int* ns_neg)
-{
-    const int64_t m = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int64_t n = int64_t(rows) * cols;
-    if (m >= n)
-        return;
-    const int32_t l = L[m];
-    if (l == 0)
-        return;
-    const bool pos = l > 0;
-    const int idx = pos ? l - 1 : -l - 1;
-    const bool valid = pos ? (ext_pos[idx] > det_pos_key) : (ext_neg[idx] < det_neg_key);
-    if (!valid) {
-        if (generate_labelmap)
-            L[m] = 0;
-        return;
-    }
-    const double val = ld(img, m);
-    const int c = int(uint32_t(m) / uint32_t(rows)), r = int(uint32_t(m) - uint32_t(c) * uint32_t(rows));
-    const int vs = rows / 2, hs = cols / 2;
-    const double y = r < vs ? double(r + vs) : double(r - vs);
-    const double x = c < hs ? double(c + hs) : double(c - hs);
-    const double xb = x * val, yb = y * val;
-    double* mo = (pos ? mom_pos : mom_neg) + 6 * size_t(idx);
-    atomicAdd(pos ? &ns_pos[idx] : &ns_neg[idx], 1);
-    atomicAdd(&mo[0], xb);
-    atomicAdd(&mo[1], yb);
-    atomicAdd(&mo[2], xb * x);
-    atomicAdd(&mo[3], yb * y);
-    atomicAdd(&mo[4], xb * y);
-    atomicAdd(&mo[5], val);
-}
 
 struct IslandRaw {
     int32_t label;
@@ -920,19 +984,21 @@ __device__ __forceinline__ bool solve6(const double* m, const double* r, double*
 }
 
 // pix[sb[key] .. se[key]) are the island's pixels (memory indices of the
-// column-major rows x cols image); x, y are display coordinates (the image is
-// unshifted: display = memory index shifted by half, sourcefind.cpp:230-245).
+// column-major rows x cols image), in memory order from sp[key] (seg_at);
+// x, y are display coordinates (the image is unshifted: display = memory
+// index shifted by half, sourcefind.cpp:230-245).
 template <typename T>
 __global__ void __launch_bounds__(32) k_gauss_fit(const T* __restrict__ img, int rows, int cols,
     const uint32_t* __restrict__ pix, const uint32_t* __restrict__ sb, const uint32_t* __restrict__ se,
-    const int* __restrict__ keys, const double* __restrict__ init, int nis, double* outp, int* iters)
+    const uint32_t* __restrict__ sp, const int* __restrict__ keys, const double* __restrict__ init, int nis,
+    double* outp, int* iters)
 {
     const int isl = blockIdx.x;
     if (isl >= nis)
         return;
     const int lane = threadIdx.x;
     const int key = keys[isl];
-    const uint32_t b = sb[key], e = se[key];
+    const uint32_t b = sb[key], e = se[key], split = sp[key];
     const int hs = cols / 2, vs = rows / 2;
     double p[6];
     for (int k = 0; k < 6; k++)
@@ -949,8 +1015,8 @@ __global__ void __launch_bounds__(32) k_gauss_fit(const T* __restrict__ img, int
             for (int k = 0; k < 6; k++)
                 jr[k] = 0.0;
         }
-        for (uint32_t t = b + lane; t < e; t += 32) {
-            const uint32_t m = pix[t];
+        for (uint32_t j = lane; j < e - b; j += 32) {
+            const uint32_t m = pix[seg_at(b, split, e, j)];
             const int rm = int(m % uint32_t(rows)), cm = int(m / uint32_t(rows));
             const double x = double(cm < hs ? cm + hs : cm - hs);
             const double y = double(rm < vs ? rm + vs : rm - vs);
