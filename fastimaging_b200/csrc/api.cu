@@ -1766,99 +1766,6 @@ double median_exact(stpgpu_context* c, const T* x, int64_t n)
     return (v1 + v2) / 2;
 }
 
-template <typename T>
-void mean_sigma(stpgpu_context* c, const T* x, int64_t n, double& mean, double& sigma)
-{
-    cudaStream_t st = c->stream;
-    const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8);
-    double* part = c->buf<double>("sf_part", 3 * size_t(nb));
-    double* out = c->buf<double>("sf_out", 4);
-    k_sum_sq<T><<<nb, SF_THREADS, 0, st>>>(x, n, part);
-    STPGPU_CHECK_LAUNCH();
-    k_finish_parts<2><<<1, 256, 0, st>>>(part, int(nb), out);
-    STPGPU_CHECK_LAUNCH();
-    double* h = c->host_stage<double>(4);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    mean = h[0] / double(n);
-    sigma = std::sqrt(h[1] / double(n) - mean * mean);
-}
-
-// mat_median_binapprox (matrix_math.cpp:334-455)
-template <typename T>
-double median_binapprox(stpgpu_context* c, const T* x, int64_t n, double mean, double sigma)
-{
-    const int N = BINS_N;
-    if ((sigma * 2) < 0.0001)
-        return median_exact(c, x, n);
-    cudaStream_t st = c->stream;
-    const double scalefactor = double(N) / (2 * sigma);
-    const double leftend = mean - sigma;
-    unsigned long long* bins = c->buf<unsigned long long>("sf_bins", N + 2);
-    STPGPU_CUDA_TRY(cudaMemsetAsync(bins, 0, sizeof(unsigned long long) * (N + 2), st));
-    k_hist<T><<<std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8), SF_THREADS, 0, st>>>(x, n, leftend, scalefactor,
-        bins);
-    STPGPU_CHECK_LAUNCH();
-    unsigned long long* h = c->host_stage<unsigned long long>(N + 2);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, bins, sizeof(unsigned long long) * (N + 2), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<unsigned long long> b(h, h + N + 1);
-    const unsigned long long bottom = h[N + 1];
-    if (n & 1) {
-        const unsigned long long k = (unsigned long long)(n + 1) / 2;
-        unsigned long long count = bottom;
-        for (int i = 0; i < N + 1; i++) {
-            count += b[i];
-            if (count >= k)
-                return double(i + 0.5) / scalefactor + leftend;
-        }
-    } else {
-        const unsigned long long k = (unsigned long long)n / 2;
-        unsigned long long count = bottom;
-        for (int i = 0; i < N + 1; i++) {
-            count += b[i];
-            if (count >= k) {
-                int j = i;
-                while (count == k) {
-                    j++;
-                    count += b[j];
-                    if (j == N)
-                        break;
-                }
-                return double(i + j + 1) / (2 * scalefactor) + leftend;
-            }
-        }
-    }
-    return median_exact(c, x, n);
-}
-
-// estimate_rms (sourcefind.cpp:22-154), num_sigma = 3
-template <typename T>
-double estimate_rms(stpgpu_context* c, const T* x, int64_t n, double num_sigma, int iters, double mean, double sigma,
-    double median)
-{
-    cudaStream_t st = c->stream;
-    const double m = mean - median;
-    const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * 8);
-    double* part = c->buf<double>("sf_part", 3 * size_t(nb));
-    ClipState* cs = c->buf<ClipState>("sf_clip", 1);
-    // every iteration is enqueued; the state on the device carries the
-    // bounds from one pass to the next and stops the passes once nothing
-    // is removed, so the host reads the result once
-    k_clip_init<<<1, 1, 0, st>>>(cs, sigma, m, double(n), num_sigma);
-    STPGPU_CHECK_LAUNCH();
-    for (int it = 0; it < iters; it++) {
-        k_clip_pass_dev<T><<<nb, SF_THREADS, 0, st>>>(x, n, median, cs, part);
-        STPGPU_CHECK_LAUNCH();
-        k_clip_finish<<<1, 256, 0, st>>>(part, int(nb), cs, num_sigma);
-        STPGPU_CHECK_LAUNCH();
-    }
-    ClipState* h = c->host_stage<ClipState>(1);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, cs, sizeof(ClipState), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    return h->s;
-}
-
 unsigned long long host_okey(double v)
 {
     unsigned long long u;
@@ -1906,6 +1813,81 @@ void moments_fit(int sign, double extremum, const double* mb, double rms, double
     constrain(g);
 }
 
+// Device state of one source-finder call: labeller counters, pass tickets,
+// statistics and the clipping state, cleared by one memset per call.
+struct SfState {
+    uint32_t misc[8]; // CclBufs::misc, then the valid-label count [4] and the island count [5]
+    unsigned int tickets[4];
+    SfStats st;
+    ClipState cs;
+};
+
+// Statistics and thresholds (sourcefind.cpp:280-301) enqueued into s->st;
+// only the exact median (NTHELEMENT, BINMEDIAN, or exact = the binned
+// median's fallback) waits on the host.
+template <typename T>
+void enqueue_stats(stpgpu_context* c, const T* x, int64_t n, const stpgpu_sf_pars& p, SfState* s, bool exact)
+{
+    cudaStream_t st = c->stream;
+    const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * SF_STREAM_BLOCKS);
+    double* part = c->buf<double>("sf_part", 3 * size_t(nb));
+    unsigned long long* bins = c->buf<unsigned long long>("sf_bins", BINS_N + 2);
+    const bool est = !(std::fabs(p.rms_est) > 0.0);
+    auto sum_sq = [&](bool with_bins) {
+        k_sum_sq<T><<<nb, SF_THREADS, 0, st>>>(x, n, part, &s->tickets[0], &s->st, with_bins ? bins : nullptr);
+        STPGPU_CHECK_LAUNCH();
+    };
+    auto set_median = [&](double m) {
+        k_sf_set_median<<<1, 1, 0, st>>>(&s->st, m);
+        STPGPU_CHECK_LAUNCH();
+    };
+    switch (p.median_method) {
+    case STPGPU_ZEROMEDIAN: // the state starts at zero
+        if (est)
+            sum_sq(false);
+        break;
+    case STPGPU_BINAPPROX:
+        if (!exact) {
+            sum_sq(true);
+            k_hist<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, bins, &s->tickets[1]);
+            STPGPU_CHECK_LAUNCH();
+            break;
+        }
+        [[fallthrough]];
+    case STPGPU_BINMEDIAN: // successive binning ends in nth_element: the exact median
+        sum_sq(false);
+        set_median(median_exact(c, x, n));
+        break;
+    case STPGPU_NTHELEMENT:
+        set_median(median_exact(c, x, n));
+        if (est)
+            sum_sq(false);
+        break;
+    default:
+        fail(STPGPU_ERR_INVALID_ARG, "unknown median method");
+    }
+    if (est) {
+        k_clip_init<<<1, 1, 0, st>>>(&s->cs, &s->st, double(n), 3.0);
+        STPGPU_CHECK_LAUNCH();
+        // candidate regions of the second pass: per warp of the grid, its
+        // share of the image's 4-sample groups plus the tail
+        const bool cands = p.sigma_clip_iters > 2 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+        const int64_t nwarps = int64_t(nb) * (SF_THREADS / 32);
+        const int64_t cap_w = (ceil_div(n / 4, int64_t(nb) * SF_THREADS) + 1) * 128;
+        T* cand = cands ? c->buf<T>("sf_cand", size_t(nwarps * cap_w)) : nullptr;
+        uint32_t* cand_cnt = cands ? c->buf<uint32_t>("sf_cand_cnt", size_t(nwarps)) : nullptr;
+        for (int it = 0; it < p.sigma_clip_iters; it++) {
+            const int mode = !cands || it == 0 ? 0 : (it == 1 ? 1 : 2);
+            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0, mode, cand,
+                cand_cnt, cap_w);
+            STPGPU_CHECK_LAUNCH();
+        }
+    }
+    k_sf_thresholds<<<1, 1, 0, st>>>(&s->st, est ? &s->cs : nullptr, p.rms_est, p.analysis_n_sigma,
+        p.detection_n_sigma);
+    STPGPU_CHECK_LAUNCH();
+}
+
 // Labeller buffers for n pixels in ccl_chunks(n) chunks.
 struct CclBufs {
     uint8_t* cls; // ccl_chunks(n) * CCL_CHUNK bytes (background padding past n)
@@ -1923,24 +1905,24 @@ inline int64_t ccl_chunks(int64_t n) { return (n + CCL_CHUNK - 1) / CCL_CHUNK; }
 // Enqueues the labeller (ccl.h:19-773 semantics, see the kernels) on st.
 // Counts its launches; makes no allocation and throws nothing.
 template <typename T>
-cudaError_t ccl_enqueue(cudaStream_t st, const T* img, const CclGeom& g, double tp, double tn, int findneg,
-    int conn4, int slice, const CclBufs& b)
+cudaError_t ccl_enqueue(cudaStream_t st, const T* img, const CclGeom& g, const double* thr, double tp, double tn,
+    int findneg, int conn4, int slice, const CclBufs& b)
 {
     const int64_t n = int64_t(g.rows) * g.cols;
     const int64_t nch = ccl_chunks(n), npad = nch * CCL_CHUNK;
     const int stride = int(nch + 1);
     unsigned* err = b.misc + 3;
     if (g.rows % 4 == 0 && (reinterpret_cast<uintptr_t>(img) & 15) == 0) {
-        const int64_t ng = npad / 4;
-        k_ccl_init4<T><<<unsigned(std::min<int64_t>(ceil_div(ng, SF_THREADS), 148 * 8)), SF_THREADS, 0, st>>>(img,
-            g, tp, tn, findneg, n / 4, ng, reinterpret_cast<uint32_t*>(b.cls), reinterpret_cast<uint4*>(b.P));
+        const int64_t nu = npad / CCL_KPT;
+        k_ccl_init16<T><<<unsigned(std::min<int64_t>(ceil_div(nu, SF_THREADS), 148 * 4)), SF_THREADS, 0, st>>>(img,
+            g, thr, tp, tn, findneg, n / 4, nu, reinterpret_cast<uint4*>(b.cls), reinterpret_cast<uint4*>(b.P));
     } else {
         if (npad > n) {
             const cudaError_t e = cudaMemsetAsync(b.cls + n, 0, size_t(npad - n), st);
             if (e != cudaSuccess)
                 return e;
         }
-        k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(img, g, tp, tn, findneg, b.cls, b.P);
+        k_ccl_init<T><<<grid1d(n, 256), 256, 0, st>>>(img, g, thr, tp, tn, findneg, b.cls, b.P);
     }
     k_ccl_union<<<unsigned(nch), SF_THREADS, 0, st>>>(b.cls, g, conn4, slice, b.P, err);
     k_ccl_flatten<<<unsigned(nch), SF_THREADS, 0, st>>>(b.cls, b.P, b.cnt, stride, err);
@@ -1950,8 +1932,8 @@ cudaError_t ccl_enqueue(cudaStream_t st, const T* img, const CclGeom& g, double 
     if (b.L) {
         if (g.rows % 4 == 0 && (reinterpret_cast<uintptr_t>(b.L) & 15) == 0) {
             const int64_t ng = n / 4;
-            k_ccl_label4<<<unsigned(std::min<int64_t>(ceil_div(ng, SF_THREADS), 148 * 8)), SF_THREADS, 0, st>>>(
-                b.cls, b.P, b.R, g, ng, b.L);
+            k_ccl_label16<<<unsigned(std::min<int64_t>(ceil_div(ceil_div(ng, 4), SF_THREADS), 148 * 4)), SF_THREADS,
+                0, st>>>(b.cls, b.P, b.R, g, ng, b.L);
         } else {
             k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(b.cls, b.P, b.R, g, b.L);
         }
@@ -1972,47 +1954,6 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         fail(STPGPU_ERR_INVALID_ARG, "image too large for the labeler (ccl.h:118-119)");
     cudaStream_t st = c->stream;
     const int64_t n = int64_t(rows) * cols;
-    double mean = 0.0, sigma = 0.0, median = 0.0;
-    bool have_ms = false;
-    switch (p.median_method) {
-    case STPGPU_ZEROMEDIAN:
-        median = 0.0;
-        break;
-    case STPGPU_BINAPPROX:
-        mean_sigma(c, d_img, n, mean, sigma);
-        have_ms = true;
-        median = median_binapprox(c, d_img, n, mean, sigma);
-        break;
-    case STPGPU_BINMEDIAN: // successive binning ends in nth_element: the exact median
-        mean_sigma(c, d_img, n, mean, sigma);
-        have_ms = true;
-        median = median_exact(c, d_img, n);
-        break;
-    case STPGPU_NTHELEMENT:
-        median = median_exact(c, d_img, n);
-        break;
-    default:
-        fail(STPGPU_ERR_INVALID_ARG, "unknown median method");
-    }
-    const double bg = median;
-    double rms;
-    if (std::fabs(p.rms_est) > 0.0) {
-        rms = p.rms_est;
-    } else {
-        if (!have_ms)
-            mean_sigma(c, d_img, n, mean, sigma);
-        rms = estimate_rms(c, d_img, n, 3, p.sigma_clip_iters, mean, sigma, median);
-    }
-    info.bg_level = bg;
-    info.rms_est = rms;
-    info.mean = mean;
-    info.sigma = sigma;
-    // thresholds (sourcefind.cpp:298-301)
-    const double a_pos = bg + p.analysis_n_sigma * rms;
-    const double a_neg = bg - p.analysis_n_sigma * rms;
-    const double d_pos = bg + p.detection_n_sigma * rms;
-    const double d_neg = bg - p.detection_n_sigma * rms;
-
     // ---- connected components
     const CclGeom geom { rows, cols, rows / 2, cols / 2 };
     const int64_t nch = ccl_chunks(n);
@@ -2022,60 +1963,88 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     cb.R = c->buf<uint32_t>("ccl_R", n);
     cb.cnt = c->buf<uint32_t>("ccl_cnt", 3 * size_t(nch + 1));
     cb.off = c->buf<uint32_t>("ccl_off", 3 * size_t(nch + 1));
-    cb.misc = c->buf<uint32_t>("ccl_misc", 8);
     cb.fgl = c->buf<uint32_t>("ccl_fgl", n);
     cb.L = write_labels ? (d_labels ? d_labels : c->buf<int32_t>("ccl_L", n)) : nullptr;
-    STPGPU_CUDA_TRY(cudaMemsetAsync(cb.misc, 0, 8 * sizeof(uint32_t), st));
+    SfState* sfs = c->buf<SfState>("sf_state", 1);
+    cb.misc = sfs->misc;
     const int slice = p.ccl_slice_cols > 0 ? p.ccl_slice_cols : std::max(2, cols / 8);
-    STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, a_pos, a_neg, p.find_negative_sources, p.ccl_4connectivity, slice,
-        cb));
-    // label counts, foreground count and the union-find flag in one read-back
-    uint32_t* hcnt = c->host_stage<uint32_t>(8);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    if (hcnt[3])
+    // statistics, thresholds and labels with one read-back (label counts,
+    // foreground count, union-find flag, statistics); a second attempt only
+    // when the binned median does not apply
+    SfState h;
+    for (int attempt = 0;; attempt++) {
+        STPGPU_CUDA_TRY(cudaMemsetAsync(sfs, 0, sizeof(SfState), st));
+        enqueue_stats<T>(c, d_img, n, p, sfs, attempt > 0);
+        STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
+            p.ccl_4connectivity, slice, cb));
+        SfState* hs = c->host_stage<SfState>(1);
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hs, sfs, sizeof(SfState), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+        h = *hs;
+        if (!h.st.need_exact || attempt > 0)
+            break;
+    }
+    if (h.misc[3])
         fail(STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)");
-    const int np = int(hcnt[0]), nneg = int(hcnt[1]), nfg = int(hcnt[2]);
+    info.bg_level = h.st.median;
+    info.rms_est = h.st.rms;
+    info.mean = h.st.mean;
+    info.sigma = h.st.sigma;
+    const double d_pos = h.st.thr[2], d_neg = h.st.thr[3];
+    const double rms = h.st.rms;
+    const int np = int(h.misc[0]), nneg = int(h.misc[1]), nfg = int(h.misc[2]);
     info.n_labels_pos = np;
     info.n_labels_neg = nneg;
 
     // ---- extrema, detection filter, moments (sourcefind.cpp:342-628) over the foreground list
     const int nl = std::max(1, np + nneg);
+    // per label: extremum keys (single precision: value-and-index keys),
+    // first indices, moments, sample counts, list segments
     unsigned long long* ext = c->buf<unsigned long long>("sf_ext", nl);
     unsigned long long* eidx = c->buf<unsigned long long>("sf_eidx", nl);
     double* mom = c->buf<double>("sf_mom", 6 * size_t(nl));
     int* ns = c->buf<int>("sf_ns", nl);
-    uint32_t* flags = c->buf<uint32_t>("sf_flags", nl + 1);
-    uint32_t* foff = c->buf<uint32_t>("sf_foff", nl + 1);
     uint32_t* sb = c->buf<uint32_t>("fg_sb", nl);
     uint32_t* se = c->buf<uint32_t>("fg_se", nl);
     uint32_t* sp = c->buf<uint32_t>("fg_sp", nl);
     uint32_t* nvalid = cb.misc + 4;
-    unsigned long long* ext_pos = ext;
-    unsigned long long* ext_neg = ext + np;
+    uint32_t* nisl = cb.misc + 5;
     const unsigned long long kpos = host_okey(d_pos), kneg = host_okey(d_neg);
     const int64_t nfk = std::max(nfg, 1);
     uint32_t* fcode = c->buf<uint32_t>("fg_code", nfk);
     uint32_t* fm = c->buf<uint32_t>("fg_m", nfk);
+    uint32_t* k0 = c->buf<uint32_t>("fg_k0", nfk);
+    uint32_t* v0 = c->buf<uint32_t>("fg_v0", nfk);
+    uint32_t* k1 = c->buf<uint32_t>("fg_k1", nfk);
+    uint32_t* v1 = c->buf<uint32_t>("fg_v1", nfk);
+    IslandRaw* raw = c->buf<IslandRaw>("sf_raw", nl);
     const unsigned gl = unsigned(ceil_div(std::max(nfg, 1), 256));
-    const bool packed = sizeof(T) == 4;
-    if (packed) {
-        // one pass: threshold rounded onto the float grid (largest float <=
-        // the positive threshold, smallest float >= the negative one)
+    int end_bit = 1;
+    while (end_bit < 32 && (uint64_t(1) << end_bit) <= uint64_t(nl))
+        end_bit++;
+    const uint32_t sentinel = uint32_t((uint64_t(1) << end_bit) - 1);
+    int32_t* zero_map = p.generate_labelmap ? cb.L : nullptr;
+    constexpr bool packed = sizeof(T) == 4;
+    uint32_t fpos = 0, fneg = 0;
+    if constexpr (packed) {
+        // extremum and first index in one pass: threshold rounded onto the
+        // float grid (largest float <= the positive threshold, smallest
+        // float >= the negative one)
         float tf = float(d_pos);
         if (double(tf) > d_pos)
             tf = std::nextafter(tf, -HUGE_VALF);
         float tc = float(d_neg);
         if (double(tc) < d_neg)
             tc = std::nextafter(tc, HUGE_VALF);
-        const uint32_t fpos = fkey32(tf), fneg = fkey32(tc);
-        unsigned long long* pk = c->buf<unsigned long long>("sf_pk", nl);
-        k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(pk, nullptr, np, nl, (unsigned long long)fpos << 32 | 0xffffffffull,
+        fpos = fkey32(tf);
+        fneg = fkey32(tc);
+        k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(ext, nullptr, np, nl, (unsigned long long)fpos << 32 | 0xffffffffull,
             (unsigned long long)fneg << 32, sb, se, sp, nvalid);
         STPGPU_CHECK_LAUNCH();
-        k_fg_gather<T, true><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, pk);
+        k_fg_gather<T, true><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, ext);
         STPGPU_CHECK_LAUNCH();
-        k_extrema_unpack<<<grid1d(nl, 256), 256, 0, st>>>(pk, np, nl, fpos, fneg, kpos, kneg, ext, eidx);
+        k_fg_keys<true><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, fpos, fneg, sentinel, k0, v0,
+            zero_map);
         STPGPU_CHECK_LAUNCH();
     } else {
         k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(ext, eidx, np, nl, kpos, kneg, sb, se, sp, nvalid);
@@ -2084,22 +2053,13 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         STPGPU_CHECK_LAUNCH();
         k_fg_extrema_idx<T><<<gl, 256, 0, st>>>(d_img, fcode, fm, nfg, np, ext, kpos, kneg, eidx);
         STPGPU_CHECK_LAUNCH();
+        k_fg_keys<false><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, 0u, 0u, sentinel, k0, v0, zero_map);
+        STPGPU_CHECK_LAUNCH();
     }
     // ordered (deterministic) moments: stable sort of the list by label
     // (invalid labels last), segments, per-label sums in memory order
     const uint32_t* fit_pix = nullptr;
-    uint32_t* k0 = c->buf<uint32_t>("fg_k0", nfk);
-    uint32_t* v0 = c->buf<uint32_t>("fg_v0", nfk);
-    uint32_t* k1 = c->buf<uint32_t>("fg_k1", nfk);
-    uint32_t* v1 = c->buf<uint32_t>("fg_v1", nfk);
-    int end_bit = 1;
-    while (end_bit < 32 && (uint64_t(1) << end_bit) <= uint64_t(nl))
-        end_bit++;
-    const uint32_t sentinel = uint32_t((uint64_t(1) << end_bit) - 1);
     if (nfg > 0) {
-        k_fg_keys<<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, sentinel, k0, v0,
-            p.generate_labelmap ? cb.L : nullptr);
-        STPGPU_CHECK_LAUNCH();
         size_t tb = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, nfg, 0, end_bit, st);
         void* tmp = c->buf<unsigned char>("cubtmp_sf", tb);
@@ -2112,25 +2072,36 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     }
     k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, sp, mom, ns);
     STPGPU_CHECK_LAUNCH();
-    k_island_flags<<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext_pos, ext_neg, kpos, kneg, ns, ns + np,
-        p.source_min_area, flags, nvalid);
+    // islands appended in any order; the valid-label and island counts and
+    // the first records come back in one read (a second only for more)
+    k_islands<packed><<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext, eidx, fpos, fneg, kpos, kneg, ns, mom,
+        p.source_min_area, nvalid, nisl, raw);
     STPGPU_CHECK_LAUNCH();
-    // island total next to the valid-label count (misc[4], misc[5]): one read-back
-    k_scan_rows<<<1, 1024, 0, st>>>(flags, foff, np + nneg, 0, cb.misc + 5);
-    STPGPU_CHECK_LAUNCH();
-    IslandRaw* raw = c->buf<IslandRaw>("sf_raw", nl);
-    k_island_scatter<<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, flags, foff, ext_pos, ext_neg, eidx, eidx + np, ns,
-        ns + np, mom, mom + 6 * size_t(np), raw);
-    STPGPU_CHECK_LAUNCH();
+    constexpr int kFirst = 512;
+    const int first = std::min(nl, kFirst);
+    unsigned char* hb = c->host_stage<unsigned char>(64 + sizeof(IslandRaw) * size_t(kFirst));
+    uint32_t* hcnt = reinterpret_cast<uint32_t*>(hb);
+    IslandRaw* hfirst = reinterpret_cast<IslandRaw*>(hb + 64);
     STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * first, cudaMemcpyDeviceToHost, st));
     STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
     const int nis = int(hcnt[1]);
     info.n_valid_labels = int(hcnt[0]);
     info.n_islands = nis;
     std::vector<IslandRaw> hr(nis);
-    if (nis)
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hr.data(), raw, sizeof(IslandRaw) * nis, cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    std::copy(hfirst, hfirst + std::min(nis, first), hr.begin());
+    if (nis > first) {
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hr.data() + first, raw + first, sizeof(IslandRaw) * (nis - first),
+            cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    // label order: positives by label, then negatives
+    std::sort(hr.begin(), hr.end(), [](const IslandRaw& a, const IslandRaw& b) {
+        const bool na = a.label < 0, nb = b.label < 0;
+        if (na != nb)
+            return nb;
+        return std::abs(a.label) < std::abs(b.label);
+    });
     islands.resize(nis);
     const int vs = rows / 2, hs = cols / 2;
     for (int i = 0; i < nis; i++) {
@@ -2584,8 +2555,9 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += int64_t(s.nplanes) * (cs * cs * K * K * 2 * rb + lh * lh * 16 + 64 * 64 * 16);
     }
     b += rows * N * 2 * rb + N * N * rb + int64_t(image_size) * image_size * rb;
-    if (find_sources) // classes, parents, ranks, labels, foreground list; list arrays for every pixel at worst
-        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 24);
+    if (find_sources) // classes, parents, ranks, labels, foreground list, clipping candidates; list arrays for
+                      // every pixel at worst
+        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 24 + 9);
     return b + (int64_t(8) << 20);
 }
 
@@ -3018,7 +2990,7 @@ static cudaError_t noalloc_label_run(unsigned char* base, cudaStream_t st, const
     if (e != cudaSuccess)
         return e;
     const CclGeom geom { rows, cols, rows / 2, cols / 2 };
-    if ((e = ccl_enqueue<T>(st, img, geom, tp, tn, findneg, conn4, slice, b)) != cudaSuccess)
+    if ((e = ccl_enqueue<T>(st, img, geom, nullptr, tp, tn, findneg, conn4, slice, b)) != cudaSuccess)
         return e;
     // label counts and the step-bound flag, read back into host stack memory
     if ((e = cudaMemcpyAsync(h, b.misc, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st)) != cudaSuccess)

@@ -7,6 +7,9 @@
 namespace stpgpu {
 
 constexpr int SF_THREADS = 256;
+// Resident blocks per SM that the streaming statistics passes are built for
+// (<= 32 registers a thread) and launched with: one wave of 148 * 8 blocks.
+constexpr int SF_STREAM_BLOCKS = 8;
 constexpr int BINS_N = 1000; // binapprox / binmedian bin count (matrix_math.cpp:54,339)
 constexpr uint32_t UF_MAX_STEPS = 1u << 26; // bound on union-find loops
 
@@ -14,6 +17,26 @@ template <typename T>
 __device__ __forceinline__ double ld(const T* p, int64_t i)
 {
     return double(p[i]);
+}
+
+// Four consecutive samples x[4g .. 4g+3] (x 16-byte aligned).
+template <typename T>
+__device__ __forceinline__ void load4(const T* x, int64_t g, T (&v)[4])
+{
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = reinterpret_cast<const float4*>(x)[g];
+        v[0] = q.x;
+        v[1] = q.y;
+        v[2] = q.z;
+        v[3] = q.w;
+    } else {
+        const double2 a = reinterpret_cast<const double2*>(x)[2 * g];
+        const double2 b = reinterpret_cast<const double2*>(x)[2 * g + 1];
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = b.x;
+        v[3] = b.y;
+    }
 }
 
 // Grid-stride visit of x[0..n) in 16-byte loads (four floats or two pairs of
@@ -29,20 +52,11 @@ __device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
     if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
         const int64_t n4 = n / 4;
         for (int64_t g = tid; g < n4; g += stride) {
-            if constexpr (sizeof(T) == 4) {
-                const float4 q = reinterpret_cast<const float4*>(x)[g];
-                f(double(q.x));
-                f(double(q.y));
-                f(double(q.z));
-                f(double(q.w));
-            } else {
-                const double2 a = reinterpret_cast<const double2*>(x)[2 * g];
-                const double2 b = reinterpret_cast<const double2*>(x)[2 * g + 1];
-                f(double(a.x));
-                f(double(a.y));
-                f(double(b.x));
-                f(double(b.y));
-            }
+            T a[4];
+            load4(x, g, a);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                f(double(a[k]));
         }
         done = n4 * 4;
     }
@@ -97,9 +111,102 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* out_part)
     }
 }
 
-// sum x, sum x^2 (mat_mean_and_stddev, matrix_math.cpp:457-499)
+// Exclusive scan of v over the block (SF_THREADS threads); *total = the sum.
+// Callers pack up to three 16-bit counts into v.
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* total)
+{
+    __shared__ unsigned long long ws[SF_THREADS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        ws[warp] = x;
+    __syncthreads();
+    unsigned long long before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < SF_THREADS / 32; w++) {
+        const unsigned long long t = ws[w];
+        if (w < warp)
+            before += t;
+        all += t;
+    }
+    *total = all;
+    __syncthreads();
+    return before + x - v;
+}
+
+// -------------------------------------------------- statistics on the device
+//
+// The statistics of the image and the thresholds derived from them stay on
+// the device from the first pass to the labeller, so the host waits only
+// once, for the label counts.  A pass ends with its last block (the last to
+// take a ticket) reducing every block's partials in a fixed order, so the
+// results do not depend on block scheduling.
+
+struct SfStats {
+    double mean, sigma, median, rms;
+    double thr[4]; // analysis +, analysis -, detection +, detection -
+    unsigned int need_exact; // the binned median does not apply: the exact path must run
+    unsigned int pad;
+};
+
+// True in exactly one block, the last to finish the pass; every other
+// block's writes before the call are visible to it (the barrier, then one
+// fenced ticket per block, as in a grid-wide barrier).  Resets the ticket
+// for the next pass.
+__device__ __forceinline__ bool last_block(unsigned int* ticket)
+{
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned int t = atomicAdd(ticket, 1u);
+        last = t == gridDim.x - 1;
+        if (last) {
+            *ticket = 0;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return last;
+}
+
+// Sum NV-wide partials of nb blocks in a fixed order (one block of
+// SF_THREADS threads: strided sums, warp trees, warps in order); the result
+// is valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void reduce_parts(const double* part, int nb, double (&out)[NV])
+{
+    __shared__ double s[NV][SF_THREADS / 32];
+    for (int q = 0; q < NV; q++) {
+        double t = 0.0;
+        for (int k = threadIdx.x; k < nb; k += SF_THREADS)
+            t += __ldcg(part + NV * k + q);
+        t = warp_sum(t);
+        if ((threadIdx.x & 31) == 0)
+            s[q][threadIdx.x >> 5] = t;
+    }
+    __syncthreads();
+    for (int q = 0; q < NV; q++) {
+        double t = 0.0;
+        for (int w = 0; w < SF_THREADS / 32; w++)
+            t += s[q][w];
+        out[q] = t;
+    }
+}
+
+// mean and sigma (mat_mean_and_stddev, matrix_math.cpp:457-499):
+// sum x, sum x^2 per block, then mean = sum / n and
+// sigma = sqrt(sum x^2 / n - mean^2) in the last block.  Also clears the
+// histogram bins for the binned median (when given).
 template <typename T>
-__global__ void __launch_bounds__(SF_THREADS) k_sum_sq(const T* x, int64_t n, double* part)
+__global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_sum_sq(const T* x, int64_t n, double* part,
+    unsigned int* ticket, SfStats* st, unsigned long long* bins)
 {
     double v[2] = { 0.0, 0.0 };
     for_each_elem(x, n, [&](double a) {
@@ -107,43 +214,44 @@ __global__ void __launch_bounds__(SF_THREADS) k_sum_sq(const T* x, int64_t n, do
         v[1] += a * a;
     });
     block_sums<2>(v, part + 2 * blockIdx.x);
+    if (!last_block(ticket))
+        return;
+    double s[2];
+    reduce_parts<2>(part, gridDim.x, s);
+    if (bins)
+        for (int k = threadIdx.x; k < BINS_N + 2; k += SF_THREADS)
+            bins[k] = 0;
+    if (threadIdx.x == 0) {
+        const double dn = double(n);
+        const double mean = __ddiv_rn(s[0], dn);
+        st->mean = mean;
+        st->sigma = __dsqrt_rn(__dsub_rn(__ddiv_rn(s[1], dn), __dmul_rn(mean, mean)));
+    }
 }
 
-// Sum NV-wide partials of nb blocks in a fixed order (one block).
-template <int NV>
-__global__ void k_finish_parts(const double* part, int nb, double* out)
-{
-    __shared__ double s[NV][256];
-    for (int q = 0; q < NV; q++) {
-        double t = 0.0;
-        for (int k = threadIdx.x; k < nb; k += blockDim.x)
-            t += part[NV * k + q];
-        s[q][threadIdx.x] = t;
-    }
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o)
-            for (int q = 0; q < NV; q++)
-                s[q][threadIdx.x] += s[q][threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int q = 0; q < NV; q++)
-            out[q] = s[q][0];
-}
-
-// Histogram over [leftend, leftend + N/scale] with N+1 bins plus the
-// bottom count (matrix_math.cpp:358-401): bin = int((x - leftend) * scale).
+// mat_median_binapprox (matrix_math.cpp:334-455): N+1 bins over
+// [mean - sigma, mean + sigma] plus the count below, bin = int((x - leftend)
+// * scale), scale = N / (2 sigma); the last block walks the cumulative
+// counts to the median's bin.  sigma * 2 < 1e-4, or no bin reaching the
+// median's rank, set need_exact (the exact median is then taken instead).
 template <typename T>
-__global__ void __launch_bounds__(SF_THREADS) k_hist(const T* x, int64_t n, double leftend, double scale,
-    unsigned long long* bins /* BINS_N + 2: [0..N] bins, [N+1] bottom */)
+__global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_hist(const T* x, int64_t n, SfStats* st,
+    unsigned long long* bins /* BINS_N + 2: [0..N] bins, [N+1] bottom */, unsigned int* ticket)
 {
+    const double mean = st->mean, sigma = st->sigma;
+    if (__dmul_rn(sigma, 2.0) < 0.0001) {
+        if (blockIdx.x == 0 && threadIdx.x == 0)
+            st->need_exact = 1;
+        return;
+    }
+    const double scale = __ddiv_rn(double(BINS_N), __dmul_rn(2.0, sigma));
+    const double leftend = __dsub_rn(mean, sigma);
     __shared__ unsigned int h[BINS_N + 2];
     for (int k = threadIdx.x; k < BINS_N + 2; k += blockDim.x)
         h[k] = 0;
     __syncthreads();
     for_each_elem(x, n, [&](double a) {
-        const int b = int_trunc_x86((a - leftend) * scale);
+        const int b = int_trunc_x86(__dmul_rn(__dsub_rn(a, leftend), scale));
         if (b < 0)
             atomicAdd(&h[BINS_N + 1], 1u);
         else if (b <= BINS_N)
@@ -153,6 +261,60 @@ __global__ void __launch_bounds__(SF_THREADS) k_hist(const T* x, int64_t n, doub
     for (int k = threadIdx.x; k < BINS_N + 2; k += blockDim.x)
         if (h[k])
             atomicAdd(&bins[k], (unsigned long long)h[k]);
+    if (!last_block(ticket))
+        return;
+    // cumulative counts: 4 consecutive bins per thread (1024 >= N + 1)
+    static_assert(4 * SF_THREADS >= BINS_N + 1, "bins per thread");
+    __shared__ unsigned long long cum[4 * SF_THREADS];
+    __shared__ int hit;
+    unsigned long long b4[4], loc = 0;
+    for (int q = 0; q < 4; q++) {
+        const int i = 4 * threadIdx.x + q;
+        b4[q] = i <= BINS_N ? __ldcg(bins + i) : 0ull;
+        loc += b4[q];
+    }
+    if (threadIdx.x == 0)
+        hit = -1;
+    unsigned long long tot = 0;
+    unsigned long long c = __ldcg(bins + BINS_N + 1) + block_excl_scan(loc, &tot);
+    const unsigned long long k = (n & 1) ? (unsigned long long)(n + 1) / 2 : (unsigned long long)n / 2;
+    for (int q = 0; q < 4; q++) {
+        const unsigned long long prev = c;
+        c += b4[q];
+        cum[4 * threadIdx.x + q] = c;
+        const int i = 4 * threadIdx.x + q;
+        if (i <= BINS_N && c >= k && prev < k)
+            hit = i; // exactly one bin crosses the rank
+        if (i == 0 && prev >= k)
+            hit = 0; // the count below the range already reaches it
+    }
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    const int i = hit;
+    if (i < 0) {
+        st->need_exact = 1;
+        return;
+    }
+    if (n & 1) {
+        st->median = __dadd_rn(__ddiv_rn(double(i) + 0.5, scale), leftend);
+    } else {
+        unsigned long long count = cum[i];
+        int j = i;
+        while (count == k) {
+            j++;
+            count += __ldcg(bins + j);
+            if (j == BINS_N)
+                break;
+        }
+        st->median = __dadd_rn(__ddiv_rn(double(i + j + 1), __dmul_rn(2.0, scale)), leftend);
+    }
+}
+
+// Median from the exact (host-driven) selection.
+__global__ void k_sf_set_median(SfStats* st, double median)
+{
+    st->median = median;
 }
 
 // -------------------------------------------------- exact selection (nth_element)
@@ -209,19 +371,27 @@ __global__ void k_radix_pick(const unsigned int* hist, int shift, unsigned long 
 // -------------------------------------------------- sigma clip (estimate_rms)
 
 // estimate_rms (sourcefind.cpp:54-134) with the iteration state on the
-// device (no host round trip per iteration).  A clipping pass sums v, v^2
-// and the count of samples with |x - median| > upper and not > prev_upper;
-// the pass reads the current bounds, the finish step sums
-// the partials in a fixed order and updates the state exactly as the
+// device.  A clipping pass sums v, v^2 and the count of samples with
+// |x - median| > upper and not > prev_upper; its last block sums the
+// partials in a fixed order and updates the state exactly as the
 // reference's loop (sourcefind.cpp:82-134), with explicitly rounded
 // operations; once nothing is removed the remaining passes return at once.
+//
+// Later passes only need the samples between the shrinking bounds: the
+// second pass (mode 1) also keeps every sample with
+// 0.5 * upper < |x - median| <= upper in per-warp candidate regions (in
+// visiting order), and the passes after it (mode 2) read those regions
+// instead of the image while their band stays inside the candidates' (else
+// they read the image again).
 struct ClipState {
-    double s, d1, d2, valid, prev_upper, upper;
+    double s, d1, d2, valid, prev_upper, upper, cand_lo, cand_hi;
     int done;
 };
 
-__global__ void k_clip_init(ClipState* cs, double sigma, double m, double n, double num_sigma)
+// Starting state from the mean, sigma and median in st (m = mean - median).
+__global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double num_sigma)
 {
+    const double sigma = st->sigma, m = __dsub_rn(st->mean, st->median);
     ClipState c;
     c.s = sigma;
     c.d1 = __dmul_rn(m, n);
@@ -229,19 +399,27 @@ __global__ void k_clip_init(ClipState* cs, double sigma, double m, double n, dou
     c.valid = n;
     c.prev_upper = 1.7976931348623157e308;
     c.upper = __dmul_rn(num_sigma, sigma);
+    c.cand_lo = 1.7976931348623157e308;
+    c.cand_hi = 0.0;
     c.done = 0;
     *cs = c;
 }
 
+// mode 0: read the image; 1: read it and keep the candidates (x 16-byte
+// aligned; cand holds cap_w samples per warp of the grid, cand_cnt one count
+// per warp); 2: read the candidates when they cover the band.
 template <typename T>
-__global__ void __launch_bounds__(SF_THREADS) k_clip_pass_dev(const T* x, int64_t n, double median, const ClipState* cs,
-    double* part)
+__global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(const T* x, int64_t n, const SfStats* st,
+    ClipState* cs, double* part, unsigned int* ticket, double num_sigma, int mode, T* cand, uint32_t* cand_cnt,
+    int64_t cap_w)
 {
     if (cs->done)
         return;
+    const double median = st->median;
     const double upper = cs->upper, prev_upper = cs->prev_upper;
+    const double lo = __dmul_rn(0.5, upper);
     double v[3] = { 0.0, 0.0, 0.0 };
-    for_each_elem(x, n, [&](double xv) {
+    auto band = [&](double xv) {
         const double d = xv - median;
         const double a = fabs(d);
         if (a > upper && !(a > prev_upper)) {
@@ -249,44 +427,113 @@ __global__ void __launch_bounds__(SF_THREADS) k_clip_pass_dev(const T* x, int64_
             v[1] += d * d;
             v[2] += 1.0;
         }
-    });
+    };
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    if (mode == 2 && !(upper < cs->cand_lo) && !(prev_upper > cs->cand_hi)) {
+        const uint32_t cnt = cand_cnt[wid];
+        const T* r = cand + wid * cap_w;
+        for (uint32_t i = lane; i < cnt; i += 32)
+            band(double(r[i]));
+    } else if (mode == 1) {
+        T* r = cand + wid * cap_w;
+        uint32_t pos = 0;
+        // one warp-wide step: this lane's k values (k <= 4), band sums, and
+        // the candidates appended in lane order
+        auto step = [&](const T (&a)[4], int k) {
+            uint32_t m = 0;
+            for (int q = 0; q < k; q++) {
+                const double xv = double(a[q]);
+                band(xv);
+                const double ad = fabs(xv - median);
+                if (ad > lo && !(ad > upper))
+                    m |= 1u << q;
+            }
+            const int c = __popc(m);
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            uint32_t p = pos + uint32_t(incl - c);
+            while (m) {
+                const int q = __ffs(m) - 1;
+                m &= m - 1;
+                r[p++] = a[q];
+            }
+            pos += uint32_t(total);
+        };
+        const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+        const int64_t n4 = n / 4;
+        // the next step's load is issued before this step's scan and stores
+        T nxt[4];
+        if ((wid << 5) + lane < n4)
+            load4(x, (wid << 5) + lane, nxt);
+        for (int64_t g0 = wid << 5; g0 < n4; g0 += stride) {
+            T a[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                a[q] = nxt[q];
+            const int k = g0 + lane < n4 ? 4 : 0;
+            if (g0 + stride + lane < n4)
+                load4(x, g0 + stride + lane, nxt);
+            step(a, k);
+        }
+        if (wid == 0) { // the last n % 4 samples
+            const int64_t i = n4 * 4 + lane;
+            T a[4];
+            int k = 0;
+            if (i < n) {
+                a[0] = x[i];
+                k = 1;
+            }
+            step(a, k);
+        }
+        if (lane == 0)
+            cand_cnt[wid] = pos;
+    } else {
+        for_each_elem(x, n, band);
+    }
     block_sums<3>(v, part + 3 * blockIdx.x);
-}
-
-__global__ void __launch_bounds__(256) k_clip_finish(const double* part, int nb, ClipState* cs, double num_sigma)
-{
-    if (cs->done)
+    if (!last_block(ticket))
         return;
-    __shared__ double sm[3][256];
-    for (int q = 0; q < 3; q++) {
-        double t = 0.0;
-        for (int k = threadIdx.x; k < nb; k += blockDim.x)
-            t += part[3 * k + q];
-        sm[q][threadIdx.x] = t;
-    }
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o)
-            for (int q = 0; q < 3; q++)
-                sm[q][threadIdx.x] += sm[q][threadIdx.x + o];
-        __syncthreads();
-    }
+    double sm[3];
+    reduce_parts<3>(part, gridDim.x, sm);
     if (threadIdx.x != 0)
         return;
     ClipState c = *cs;
-    const unsigned long long rem = (unsigned long long)(sm[2][0] + 0.5);
+    if (mode == 1) {
+        c.cand_lo = lo;
+        c.cand_hi = upper;
+    }
+    const unsigned long long rem = (unsigned long long)(sm[2] + 0.5);
     if (rem == 0) {
         c.done = 1;
     } else {
         c.valid = __dsub_rn(c.valid, double(rem));
-        c.d1 = __dsub_rn(c.d1, sm[0][0]);
-        c.d2 = __dsub_rn(c.d2, sm[1][0]);
+        c.d1 = __dsub_rn(c.d1, sm[0]);
+        c.d2 = __dsub_rn(c.d2, sm[1]);
         const double a = __ddiv_rn(c.d2, c.valid), b = __ddiv_rn(c.d1, c.valid);
         c.s = __dsqrt_rn(__dsub_rn(a, __dmul_rn(b, b)));
         c.prev_upper = c.upper;
         c.upper = __dmul_rn(num_sigma, c.s);
     }
     *cs = c;
+}
+
+// rms (the clipped sigma, or the caller's estimate when cs is null) and the
+// thresholds bg +- n_sigma * rms with bg = the median (sourcefind.cpp:298-301).
+__global__ void k_sf_thresholds(SfStats* st, const ClipState* cs, double rms_fixed, double ana, double det)
+{
+    const double rms = cs ? cs->s : rms_fixed, bg = st->median;
+    st->rms = rms;
+    st->thr[0] = __dadd_rn(bg, __dmul_rn(ana, rms));
+    st->thr[1] = __dsub_rn(bg, __dmul_rn(ana, rms));
+    st->thr[2] = __dadd_rn(bg, __dmul_rn(det, rms));
+    st->thr[3] = __dsub_rn(bg, __dmul_rn(det, rms));
 }
 
 // -------------------------------------------------- connected components
@@ -327,35 +574,6 @@ __device__ __forceinline__ void load_cls16(const uint8_t* cls, uint32_t (&w)[4])
     w[3] = v.w;
 }
 
-// Exclusive scan of v over the block (SF_THREADS threads); *total = the sum.
-// Callers pack up to three 16-bit counts into v.
-__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* total)
-{
-    __shared__ unsigned long long ws[SF_THREADS / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= o)
-            x += y;
-    }
-    if (lane == 31)
-        ws[warp] = x;
-    __syncthreads();
-    unsigned long long before = 0, all = 0;
-#pragma unroll
-    for (int w = 0; w < SF_THREADS / 32; w++) {
-        const unsigned long long t = ws[w];
-        if (w < warp)
-            before += t;
-        all += t;
-    }
-    *total = all;
-    __syncthreads();
-    return before + x - v;
-}
-
 // The chunk's foreground keys in scan order, compacted into q as
 // (offset in the chunk) | class << 12; returns their number.
 __device__ __forceinline__ int chunk_queue(const uint32_t (&w)[4], uint16_t* q)
@@ -378,14 +596,20 @@ __device__ __forceinline__ int chunk_queue(const uint32_t (&w)[4], uint16_t* q)
 
 // Classes (0 background, 1 above the positive analysis threshold, 2 below
 // the negative one) and parents of foreground keys, one key per thread; the
-// general form, for any even image size.
+// general form, for any even image size.  The thresholds are thr[0], thr[1]
+// when thr is given (computed on the device), else tp, tn.
 template <typename T>
-__global__ void k_ccl_init(const T* img, CclGeom g, double tp, double tn, int findneg, uint8_t* cls, uint32_t* P)
+__global__ void k_ccl_init(const T* img, CclGeom g, const double* thr, double tp, double tn, int findneg, uint8_t* cls,
+    uint32_t* P)
 {
     const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t n = int64_t(g.rows) * g.cols;
     if (s >= n)
         return;
+    if (thr) {
+        tp = thr[0];
+        tn = thr[1];
+    }
     const double v = ld(img, g.mem_of_key(s));
     uint8_t c = 0;
     if (v > tp)
@@ -397,49 +621,61 @@ __global__ void k_ccl_init(const T* img, CclGeom g, double tp, double tn, int fi
         P[s] = uint32_t(s);
 }
 
-// The same for rows % 4 == 0 and a 16-byte aligned image: four keys of one
-// column per step (one 16-byte load or two), classes stored four at a time,
-// parents of groups holding foreground as one 16-byte store.  Groups from
-// ngroups to ngroups_pad are the background padding of the class array.
+// The same for rows % 4 == 0 and a 16-byte aligned image: CCL_KPT keys per
+// step in groups of four keys of one column (one 16-byte load each, or two
+// for doubles, all issued before the classes are formed), classes stored
+// as one 16-byte word, parents of groups holding foreground as one 16-byte
+// store.  Groups from ngroups on are the background padding of the class
+// array (nunits = its length in CCL_KPT keys).
 template <typename T>
-__global__ void __launch_bounds__(SF_THREADS) k_ccl_init4(const T* img, CclGeom g, double tp, double tn, int findneg,
-    int64_t ngroups, int64_t ngroups_pad, uint32_t* cls4, uint4* P4)
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_init16(const T* img, CclGeom g, const double* thr, double tp,
+    double tn, int findneg, int64_t ngroups, int64_t nunits, uint4* cls16, uint4* P4)
 {
+    if (thr) {
+        tp = thr[0];
+        tn = thr[1];
+    }
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < ngroups_pad; q += stride) {
-        uint32_t packed = 0;
-        if (q < ngroups) {
-            const int64_t m = g.mem_of_key(4 * q);
-            double v[4];
-            if constexpr (sizeof(T) == 4) {
-                const float4 f = *reinterpret_cast<const float4*>(img + m);
-                v[0] = f.x;
-                v[1] = f.y;
-                v[2] = f.z;
-                v[3] = f.w;
-            } else {
-                const double2 a = *reinterpret_cast<const double2*>(img + m);
-                const double2 b = *reinterpret_cast<const double2*>(img + m + 2);
-                v[0] = a.x;
-                v[1] = a.y;
-                v[2] = b.x;
-                v[3] = b.y;
-            }
+    for (int64_t u = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < nunits; u += stride) {
+        T v[16];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                uint32_t c = 0;
-                if (v[k] > tp)
-                    c = 1;
-                else if (findneg && v[k] < tn)
-                    c = 2;
-                packed |= c << (8 * k);
-            }
-            if (packed) {
-                const uint32_t s = uint32_t(4 * q);
-                P4[q] = make_uint4(s, s + 1, s + 2, s + 3);
+        for (int j = 0; j < 4; j++) {
+            const int64_t q = 4 * u + j;
+            if (q < ngroups) {
+                T a[4];
+                load4(img + g.mem_of_key(4 * q), 0, a);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    v[4 * j + k] = a[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    v[4 * j + k] = T(0);
             }
         }
-        cls4[q] = packed;
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            uint32_t packed = 0;
+            if (4 * u + j < ngroups) {
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const double x = double(v[4 * j + k]);
+                    uint32_t c = 0;
+                    if (x > tp)
+                        c = 1;
+                    else if (findneg && x < tn)
+                        c = 2;
+                    packed |= c << (8 * k);
+                }
+            }
+            if (packed) {
+                const uint32_t s = uint32_t(16 * u + 4 * j);
+                P4[4 * u + j] = make_uint4(s, s + 1, s + 2, s + 3);
+            }
+            w[j] = packed;
+        }
+        cls16[u] = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
@@ -616,26 +852,34 @@ __global__ void k_ccl_label(const uint8_t* cls, const uint32_t* P, const uint32_
     L[m] = c == 0 ? 0 : (c == 1 ? int32_t(R[P[s]]) : -int32_t(R[P[s]]));
 }
 
-// The same four keys of one column at a time (rows % 4 == 0, 16-byte aligned
-// label map): one 4-byte class load and one 16-byte store per step.
-__global__ void __launch_bounds__(SF_THREADS) k_ccl_label4(const uint8_t* cls, const uint32_t* P, const uint32_t* R,
+// The same CCL_KPT keys at a time in groups of four keys of one column
+// (rows % 4 == 0, 16-byte aligned label map): one 16-byte class load and four
+// 16-byte stores per step; the label lookups of a step are independent.
+__global__ void __launch_bounds__(SF_THREADS) k_ccl_label16(const uint8_t* cls, const uint32_t* P, const uint32_t* R,
     CclGeom g, int64_t ngroups, int32_t* L)
 {
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < ngroups; q += stride) {
-        const uint32_t c4 = reinterpret_cast<const uint32_t*>(cls)[q];
-        int v[4] = { 0, 0, 0, 0 };
-        if (c4) {
+    const int64_t nunits = (ngroups + 3) / 4;
+    for (int64_t u = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < nunits; u += stride) {
+        const uint4 c16 = reinterpret_cast<const uint4*>(cls)[u];
+        const uint32_t cw[4] = { c16.x, c16.y, c16.z, c16.w };
+        int v[16];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const uint32_t c = (c4 >> (8 * k)) & 0xffu;
-                if (c) {
-                    const int r = int(R[P[4 * q + k]]);
-                    v[k] = c == 1 ? r : -r;
-                }
+        for (int k = 0; k < 16; k++) {
+            const uint32_t c = (cw[k >> 2] >> (8 * (k & 3))) & 0xffu;
+            v[k] = 0;
+            if (c) {
+                const int r = int(R[P[16 * u + k]]);
+                v[k] = c == 1 ? r : -r;
             }
         }
-        reinterpret_cast<int4*>(L)[g.mem_of_key(4 * q) >> 2] = make_int4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t q = 4 * u + j;
+            if (q < ngroups)
+                reinterpret_cast<int4*>(L)[g.mem_of_key(4 * q) >> 2]
+                    = make_int4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        }
     }
 }
 
@@ -717,24 +961,6 @@ __global__ void k_fg_gather(const T* img, const uint8_t* cls, const uint32_t* P,
     }
 }
 
-// Packed keys -> the order keys of the extrema (double) and their indices.
-__global__ void k_extrema_unpack(const unsigned long long* pk, int np, int nl, uint32_t thr_pos, uint32_t thr_neg,
-    unsigned long long kpos, unsigned long long kneg, unsigned long long* ext, unsigned long long* eidx)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nl)
-        return;
-    const bool pos = i < np;
-    const uint32_t hi = uint32_t(pk[i] >> 32), lo = uint32_t(pk[i]);
-    if (hi != (pos ? thr_pos : thr_neg)) {
-        ext[i] = okey(double(fkey32_inv(hi)));
-        eidx[i] = pos ? (unsigned long long)(0xffffffffu - lo) : (unsigned long long)lo;
-    } else {
-        ext[i] = pos ? kpos : kneg;
-        eidx[i] = ~0ull;
-    }
-}
-
 // First memory index holding the extremum (the serial reference keeps the
 // first occurrence in memory order).
 template <typename T>
@@ -755,15 +981,24 @@ __global__ void k_fg_extrema_idx(const T* img, const uint32_t* fcode, const uint
 // Sort keys of the list: the label code of labels whose extremum passes the
 // detection threshold, `sentinel` (above every code) for the others, whose
 // pixels are zeroed in the label map L when given (generate_labelmap).
+// PACKED: ext holds the single-precision value-and-index keys, which pass
+// when their value part left the starting threshold (thr_pos / thr_neg);
+// else the order keys of the extrema, compared with the detection keys.
+template <bool PACKED>
 __global__ void k_fg_keys(const uint32_t* fcode, const uint32_t* fm, int nfg, int np, const unsigned long long* ext,
-    unsigned long long det_pos_key, unsigned long long det_neg_key, uint32_t sentinel, uint32_t* keys, uint32_t* vals,
-    int32_t* L)
+    unsigned long long det_pos_key, unsigned long long det_neg_key, uint32_t thr_pos, uint32_t thr_neg,
+    uint32_t sentinel, uint32_t* keys, uint32_t* vals, int32_t* L)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nfg)
         return;
     const uint32_t code = fcode[i], m = fm[i];
-    const bool valid = int(code) < np ? ext[code] > det_pos_key : ext[code] < det_neg_key;
+    const bool pos = int(code) < np;
+    bool valid;
+    if constexpr (PACKED)
+        valid = uint32_t(ext[code] >> 32) != (pos ? thr_pos : thr_neg);
+    else
+        valid = pos ? ext[code] > det_pos_key : ext[code] < det_neg_key;
     keys[i] = valid ? code : sentinel;
     vals[i] = m;
     if (!valid && L)
@@ -815,13 +1050,11 @@ __global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uin
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= nl)
         return;
-    const uint32_t b = seg_begin[l], e = seg_end[l], sp = seg_split[l];
+    const uint32_t b = seg_begin[l], e = seg_end[l], sp = seg_split[l], len = e - b;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
     const int vs = rows / 2, hs = cols / 2;
-    for (uint32_t j = 0; j < e - b; j++) {
-        const int64_t m = vals[seg_at(b, sp, e, j)];
-        const double val = ld(img, m);
-        const int c = int(uint32_t(m) / uint32_t(rows)), r = int(uint32_t(m) - uint32_t(c) * uint32_t(rows));
+    auto add = [&](uint32_t m, double val) {
+        const int c = int(m / uint32_t(rows)), r = int(m - uint32_t(c) * uint32_t(rows));
         const double y = r < vs ? double(r + vs) : double(r - vs);
         const double x = c < hs ? double(c + hs) : double(c - hs);
         const double xb = __dmul_rn(x, val), yb = __dmul_rn(y, val);
@@ -831,6 +1064,25 @@ __global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uin
         a3 = __dadd_rn(a3, __dmul_rn(yb, y));
         a4 = __dadd_rn(a4, __dmul_rn(xb, y));
         a5 = __dadd_rn(a5, val);
+    };
+    // four pixels' loads in flight, then their sums in order
+    uint32_t j = 0;
+    for (; j + 4 <= len; j += 4) {
+        uint32_t m[4];
+        double val[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            m[q] = vals[seg_at(b, sp, e, j + q)];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            val[q] = ld(img, m[q]);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            add(m[q], val[q]);
+    }
+    for (; j < len; j++) {
+        const uint32_t m = vals[seg_at(b, sp, e, j)];
+        add(m, ld(img, m));
     }
     double* mo = mom + 6 * size_t(l);
     mo[0] = a0;
@@ -839,7 +1091,7 @@ __global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uin
     mo[3] = a3;
     mo[4] = a4;
     mo[5] = a5;
-    ns[l] = int(e - b);
+    ns[l] = int(len);
 }
 
 
@@ -851,51 +1103,48 @@ struct IslandRaw {
     double mom[6];
 };
 
-// flags for island compaction: positives [0, np), negatives [np, np+nn)
-__global__ void k_island_flags(int np, int nn, const unsigned long long* ext_pos, const unsigned long long* ext_neg,
-    unsigned long long det_pos_key, unsigned long long det_neg_key, const int* ns_pos, const int* ns_neg,
-    int min_area, uint32_t* flags, uint32_t* nvalid)
+// One thread per label (positives [0, np), negatives [np, np + nn)): the
+// extremum and its first index (PACKED: unpacked from the single-precision
+// keys), the valid-label count (extremum beyond the detection threshold,
+// sourcefind.cpp:380-456) and, for valid labels of at least min_area
+// pixels, the island record appended at an atomic cursor (the host orders
+// the records by label).
+template <bool PACKED>
+__global__ void k_islands(int np, int nn, const unsigned long long* ext, const unsigned long long* eidx,
+    uint32_t thr_pos, uint32_t thr_neg, unsigned long long det_pos_key, unsigned long long det_neg_key, const int* ns,
+    const double* mom, int min_area, uint32_t* nvalid, uint32_t* nisl, IslandRaw* out)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= np + nn)
         return;
-    bool valid, keep;
-    if (t < np) {
-        valid = ext_pos[t] > det_pos_key;
-        keep = valid && ns_pos[t] >= min_area;
+    const bool pos = t < np;
+    unsigned long long key, idx;
+    bool valid;
+    if constexpr (PACKED) {
+        const uint32_t hi = uint32_t(ext[t] >> 32), lo = uint32_t(ext[t]);
+        valid = hi != (pos ? thr_pos : thr_neg);
+        key = okey(double(fkey32_inv(hi)));
+        idx = pos ? (unsigned long long)(0xffffffffu - lo) : (unsigned long long)lo;
     } else {
-        valid = ext_neg[t - np] < det_neg_key;
-        keep = valid && ns_neg[t - np] >= min_area;
+        key = ext[t];
+        idx = eidx[t];
+        valid = pos ? key > det_pos_key : key < det_neg_key;
     }
-    flags[t] = keep ? 1u : 0u;
-    if (valid)
-        atomicAdd(nvalid, 1u);
-}
-
-__global__ void k_island_scatter(int np, int nn, const uint32_t* flags, const uint32_t* off,
-    const unsigned long long* ext_pos, const unsigned long long* ext_neg, const unsigned long long* idx_pos,
-    const unsigned long long* idx_neg, const int* ns_pos, const int* ns_neg, const double* mom_pos,
-    const double* mom_neg, IslandRaw* out)
-{
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= np + nn || !flags[t])
+    if (!valid)
+        return;
+    atomicAdd(nvalid, 1u);
+    if (ns[t] < min_area)
         return;
     IslandRaw r;
-    const bool pos = t < np;
     const int i = pos ? t : t - np;
     r.label = pos ? (i + 1) : -(i + 1);
-    r.num_samples = pos ? ns_pos[i] : ns_neg[i];
-    r.extremum_val = okey_inv(pos ? ext_pos[i] : ext_neg[i]);
-    r.extremum_idx = (long long)(pos ? idx_pos[i] : idx_neg[i]);
-    const double* mo = (pos ? mom_pos : mom_neg) + 6 * size_t(i);
+    r.num_samples = ns[t];
+    r.extremum_val = okey_inv(key);
+    r.extremum_idx = (long long)idx;
     for (int q = 0; q < 6; q++)
-        r.mom[q] = mo[q];
-    out[off[t]] = r;
+        r.mom[q] = mom[6 * size_t(t) + q];
+    out[atomicAdd(nisl, 1u)] = r;
 }
-
-} // namespace stpgpu
-
-namespace stpgpu {
 
 // ---------------------------------------------------------------- 2-D Gaussian fit
 //
