@@ -1869,17 +1869,8 @@ void enqueue_stats(stpgpu_context* c, const T* x, int64_t n, const stpgpu_sf_par
     if (est) {
         k_clip_init<<<1, 1, 0, st>>>(&s->cs, &s->st, double(n), 3.0);
         STPGPU_CHECK_LAUNCH();
-        // candidate regions of the second pass: per warp of the grid, its
-        // share of the image's 4-sample groups plus the tail
-        const bool cands = p.sigma_clip_iters > 2 && (reinterpret_cast<uintptr_t>(x) & 15) == 0;
-        const int64_t nwarps = int64_t(nb) * (SF_THREADS / 32);
-        const int64_t cap_w = (ceil_div(n / 4, int64_t(nb) * SF_THREADS) + 1) * 128;
-        T* cand = cands ? c->buf<T>("sf_cand", size_t(nwarps * cap_w)) : nullptr;
-        uint32_t* cand_cnt = cands ? c->buf<uint32_t>("sf_cand_cnt", size_t(nwarps)) : nullptr;
         for (int it = 0; it < p.sigma_clip_iters; it++) {
-            const int mode = !cands || it == 0 ? 0 : (it == 1 ? 1 : 2);
-            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0, mode, cand,
-                cand_cnt, cap_w);
+            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0);
             STPGPU_CHECK_LAUNCH();
         }
     }
@@ -2555,9 +2546,8 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += int64_t(s.nplanes) * (cs * cs * K * K * 2 * rb + lh * lh * 16 + 64 * 64 * 16);
     }
     b += rows * N * 2 * rb + N * N * rb + int64_t(image_size) * image_size * rb;
-    if (find_sources) // classes, parents, ranks, labels, foreground list, clipping candidates; list arrays for
-                      // every pixel at worst
-        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 24 + 9);
+    if (find_sources) // classes, parents, ranks, labels, foreground list; list arrays for every pixel at worst
+        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 24);
     return b + (int64_t(8) << 20);
 }
 

@@ -41,8 +41,9 @@ __device__ __forceinline__ void load4(const T* x, int64_t g, T (&v)[4])
 
 // Grid-stride visit of x[0..n) in 16-byte loads (four floats or two pairs of
 // doubles per step, when x is 16-byte aligned), then the tail; f(value) is
-// called once per element.  The wide loads keep enough bytes in flight per
-// thread for the streaming passes over an image.
+// called once per element (with the element's own type).  The wide loads
+// keep enough bytes in flight per thread for the streaming passes over an
+// image.
 template <typename T, typename F>
 __device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
 {
@@ -56,12 +57,12 @@ __device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
             load4(x, g, a);
 #pragma unroll
             for (int k = 0; k < 4; k++)
-                f(double(a[k]));
+                f(a[k]);
         }
         done = n4 * 4;
     }
     for (int64_t i = done + tid; i < n; i += stride)
-        f(double(x[i]));
+        f(x[i]);
 }
 
 // order-preserving 64-bit key of a double (non-NaN)
@@ -376,15 +377,8 @@ __global__ void k_radix_pick(const unsigned int* hist, int shift, unsigned long 
 // partials in a fixed order and updates the state exactly as the
 // reference's loop (sourcefind.cpp:82-134), with explicitly rounded
 // operations; once nothing is removed the remaining passes return at once.
-//
-// Later passes only need the samples between the shrinking bounds: the
-// second pass (mode 1) also keeps every sample with
-// 0.5 * upper < |x - median| <= upper in per-warp candidate regions (in
-// visiting order), and the passes after it (mode 2) read those regions
-// instead of the image while their band stays inside the candidates' (else
-// they read the image again).
 struct ClipState {
-    double s, d1, d2, valid, prev_upper, upper, cand_lo, cand_hi;
+    double s, d1, d2, valid, prev_upper, upper;
     int done;
 };
 
@@ -399,27 +393,32 @@ __global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double n
     c.valid = n;
     c.prev_upper = 1.7976931348623157e308;
     c.upper = __dmul_rn(num_sigma, sigma);
-    c.cand_lo = 1.7976931348623157e308;
-    c.cand_hi = 0.0;
     c.done = 0;
     *cs = c;
 }
 
-// mode 0: read the image; 1: read it and keep the candidates (x 16-byte
-// aligned; cand holds cap_w samples per warp of the grid, cand_cnt one count
-// per warp); 2: read the candidates when they cover the band.
 template <typename T>
 __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(const T* x, int64_t n, const SfStats* st,
-    ClipState* cs, double* part, unsigned int* ticket, double num_sigma, int mode, T* cand, uint32_t* cand_cnt,
-    int64_t cap_w)
+    ClipState* cs, double* part, unsigned int* ticket, double num_sigma)
 {
     if (cs->done)
         return;
     const double median = st->median;
     const double upper = cs->upper, prev_upper = cs->prev_upper;
-    const double lo = __dmul_rn(0.5, upper);
+    // Single-precision screen: samples with |x - median| certainly not above
+    // upper skip the double-precision tests.  With xf = float(x), mf =
+    // float(median), |x - median| <= |xf - mf| (1 + 2^-23) + |xf| 2^-23 +
+    // |median| 2^-24, so |xf - mf| + |xf| 2^-21 < skip, skip <= upper
+    // (1 - 2^-12) - |median| 2^-12, implies |x - median| < upper.  NaN and
+    // infinite samples fail the screen and take the exact tests.
+    const float mf = float(median);
+    const float skip = __double2float_rd(upper * (1.0 - 0x1p-12) - fabs(median) * 0x1p-12);
+    auto screened = [&](T xr) {
+        const float xf = float(xr);
+        return fabsf(xf - mf) + fabsf(xf) * 0x1p-21f < skip;
+    };
     double v[3] = { 0.0, 0.0, 0.0 };
-    auto band = [&](double xv) {
+    auto band_exact = [&](double xv) {
         const double d = xv - median;
         const double a = fabs(d);
         if (a > upper && !(a > prev_upper)) {
@@ -428,75 +427,11 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
             v[2] += 1.0;
         }
     };
-    const int lane = threadIdx.x & 31;
-    const int64_t wid = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    if (mode == 2 && !(upper < cs->cand_lo) && !(prev_upper > cs->cand_hi)) {
-        const uint32_t cnt = cand_cnt[wid];
-        const T* r = cand + wid * cap_w;
-        for (uint32_t i = lane; i < cnt; i += 32)
-            band(double(r[i]));
-    } else if (mode == 1) {
-        T* r = cand + wid * cap_w;
-        uint32_t pos = 0;
-        // one warp-wide step: this lane's k values (k <= 4), band sums, and
-        // the candidates appended in lane order
-        auto step = [&](const T (&a)[4], int k) {
-            uint32_t m = 0;
-            for (int q = 0; q < k; q++) {
-                const double xv = double(a[q]);
-                band(xv);
-                const double ad = fabs(xv - median);
-                if (ad > lo && !(ad > upper))
-                    m |= 1u << q;
-            }
-            const int c = __popc(m);
-            int incl = c;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o)
-                    incl += y;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            uint32_t p = pos + uint32_t(incl - c);
-            while (m) {
-                const int q = __ffs(m) - 1;
-                m &= m - 1;
-                r[p++] = a[q];
-            }
-            pos += uint32_t(total);
-        };
-        const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-        const int64_t n4 = n / 4;
-        // the next step's load is issued before this step's scan and stores
-        T nxt[4];
-        if ((wid << 5) + lane < n4)
-            load4(x, (wid << 5) + lane, nxt);
-        for (int64_t g0 = wid << 5; g0 < n4; g0 += stride) {
-            T a[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++)
-                a[q] = nxt[q];
-            const int k = g0 + lane < n4 ? 4 : 0;
-            if (g0 + stride + lane < n4)
-                load4(x, g0 + stride + lane, nxt);
-            step(a, k);
-        }
-        if (wid == 0) { // the last n % 4 samples
-            const int64_t i = n4 * 4 + lane;
-            T a[4];
-            int k = 0;
-            if (i < n) {
-                a[0] = x[i];
-                k = 1;
-            }
-            step(a, k);
-        }
-        if (lane == 0)
-            cand_cnt[wid] = pos;
-    } else {
-        for_each_elem(x, n, band);
-    }
+    auto band = [&](T xr) {
+        if (!screened(xr))
+            band_exact(double(xr));
+    };
+    for_each_elem(x, n, band);
     block_sums<3>(v, part + 3 * blockIdx.x);
     if (!last_block(ticket))
         return;
@@ -505,10 +440,6 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
     if (threadIdx.x != 0)
         return;
     ClipState c = *cs;
-    if (mode == 1) {
-        c.cand_lo = lo;
-        c.cand_hi = upper;
-    }
     const unsigned long long rem = (unsigned long long)(sm[2] + 0.5);
     if (rem == 0) {
         c.done = 1;
