@@ -912,26 +912,15 @@ struct ScalarsBack {
 
 ScalarsBack read_back(stpgpu_context* c, const GridOut& g)
 {
-    std::vector<int> sup(g.nplanes);
-    struct Stage {
-        double total;
-        unsigned long long ngood;
-        uint32_t nitems;
-        unsigned int err;
-    };
-    Stage* h = c->host_stage<Stage>(1);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&h->total, g.d_total, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    STPGPU_CUDA_TRY(
-        cudaMemcpyAsync(&h->ngood, g.d_ngood, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&h->nitems, g.d_nitems, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(&h->err, g.d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
-    if (g.nplanes > 0)
-        STPGPU_CUDA_TRY(
-            cudaMemcpyAsync(sup.data(), g.d_plane_support, sizeof(int) * g.nplanes, cudaMemcpyDeviceToHost, c->stream));
+    // one copy of the packed scalars instead of one per scalar
+    ScalarPack* d = c->buf<ScalarPack>("scalar_pack", 1);
+    k_pack_scalars<<<1, 32, 0, c->stream>>>(g.d_total, g.d_ngood, g.d_nitems, g.d_err, g.d_plane_support,
+        g.nplanes > 0 ? g.nplanes : 0, d);
+    STPGPU_CHECK_LAUNCH();
+    ScalarPack* h = c->host_stage<ScalarPack>(1);
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(ScalarPack), cudaMemcpyDeviceToHost, c->stream));
     STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    ScalarsBack r { h->total, h->ngood, h->nitems, h->err, 0 };
-    for (int v : sup)
-        r.max_support = std::max(r.max_support, v);
+    ScalarsBack r { h->total, h->ngood, h->nitems, h->err, h->max_support };
     // bit 4: the 32-bit |w| sort met a long run of distinct |w| (the caller
     // repeats the gridding with the 64-bit sort); other bits are errors
     if (r.err & ~4u)

@@ -2154,4 +2154,34 @@ __global__ void k_wk_expand(const double2* convd, const double* invd, const int*
     }
 }
 
+// The scalars a call reads back, gathered for one copy: sampling-grid
+// total, good visibilities, tile-list entries, error flags and the largest
+// plane support (one warp).
+struct ScalarPack {
+    double total;
+    unsigned long long ngood;
+    uint32_t nitems;
+    unsigned int err;
+    int max_support;
+    int pad;
+};
+
+__global__ void k_pack_scalars(const double* total, const unsigned long long* ngood, const uint32_t* nitems,
+    const unsigned int* err, const int* sup, int nsup, ScalarPack* out)
+{
+    int m = 0;
+    for (int i = threadIdx.x; i < nsup; i += 32)
+        m = max(m, sup[i]);
+    for (int o = 16; o > 0; o >>= 1)
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) {
+        out->total = *total;
+        out->ngood = *ngood;
+        out->nitems = *nitems;
+        out->err = *err;
+        out->max_support = m;
+        out->pad = 0;
+    }
+}
+
 } // namespace stpgpu
