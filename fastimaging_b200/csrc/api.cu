@@ -1912,7 +1912,7 @@ cudaError_t ccl_enqueue(cudaStream_t st, const T* img, const CclGeom& g, const d
     if (b.L) {
         if (g.rows % 4 == 0 && (reinterpret_cast<uintptr_t>(b.L) & 15) == 0) {
             const int64_t ng = n / 4;
-            k_ccl_label16<<<unsigned(std::min<int64_t>(ceil_div(ceil_div(ng, 4), SF_THREADS), 148 * 4)), SF_THREADS,
+            k_ccl_label16<<<unsigned(std::min<int64_t>(ceil_div(ceil_div(ng, 4), SF_THREADS), 148 * 8)), SF_THREADS,
                 0, st>>>(b.cls, b.P, b.R, g, ng, b.L);
         } else {
             k_ccl_label<<<grid1d(n, 256), 256, 0, st>>>(b.cls, b.P, b.R, g, b.L);
