@@ -8,6 +8,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -1802,6 +1803,21 @@ void moments_fit(int sign, double extremum, const double* mb, double rms, double
     constrain(g);
 }
 
+// k_sort_small uses SORT_SMALL keys of dynamic shared memory (more than the
+// default 48 KB): raise its limit once per device.
+void set_sort_small_smem()
+{
+    static std::atomic<uint64_t> done { 0 };
+    int dev = 0;
+    STPGPU_CUDA_TRY(cudaGetDevice(&dev));
+    const uint64_t bit = uint64_t(1) << (dev & 63);
+    if (done.load() & bit)
+        return;
+    STPGPU_CUDA_TRY(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        int(SORT_SMALL * sizeof(unsigned long long))));
+    done.fetch_or(bit);
+}
+
 // Device state of one source-finder call: labeller counters, pass tickets,
 // statistics and the clipping state, cleared by one memset per call.
 struct SfState {
@@ -1993,16 +2009,13 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     const int64_t nfk = std::max(nfg, 1);
     uint32_t* fcode = c->buf<uint32_t>("fg_code", nfk);
     uint32_t* fm = c->buf<uint32_t>("fg_m", nfk);
-    uint32_t* k0 = c->buf<uint32_t>("fg_k0", nfk);
-    uint32_t* v0 = c->buf<uint32_t>("fg_v0", nfk);
-    uint32_t* k1 = c->buf<uint32_t>("fg_k1", nfk);
-    uint32_t* v1 = c->buf<uint32_t>("fg_v1", nfk);
+    unsigned long long* vkeys = c->buf<unsigned long long>("fg_vkeys", nfk); // valid entries, then sorted
+    uint32_t* v1 = c->buf<uint32_t>("fg_v1", nfk); // memory index of each sorted valid entry
+    uint32_t* nvk = cb.misc + 6; // valid entries
+    uint32_t* sort_overflow = cb.misc + 7;
     IslandRaw* raw = c->buf<IslandRaw>("sf_raw", nl);
     const unsigned gl = unsigned(ceil_div(std::max(nfg, 1), 256));
-    int end_bit = 1;
-    while (end_bit < 32 && (uint64_t(1) << end_bit) <= uint64_t(nl))
-        end_bit++;
-    const uint32_t sentinel = uint32_t((uint64_t(1) << end_bit) - 1);
+    const uint32_t split_m = uint32_t(cols / 2) * uint32_t(rows);
     int32_t* zero_map = p.generate_labelmap ? cb.L : nullptr;
     constexpr bool packed = sizeof(T) == 4;
     uint32_t fpos = 0, fneg = 0;
@@ -2023,8 +2036,7 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         STPGPU_CHECK_LAUNCH();
         k_fg_gather<T, true><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, ext);
         STPGPU_CHECK_LAUNCH();
-        k_fg_keys<true><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, fpos, fneg, sentinel, k0, v0,
-            zero_map);
+        k_fg_keys<true><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, fpos, fneg, vkeys, nvk, zero_map);
         STPGPU_CHECK_LAUNCH();
     } else {
         k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(ext, eidx, np, nl, kpos, kneg, sb, se, sp, nvalid);
@@ -2033,38 +2045,58 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         STPGPU_CHECK_LAUNCH();
         k_fg_extrema_idx<T><<<gl, 256, 0, st>>>(d_img, fcode, fm, nfg, np, ext, kpos, kneg, eidx);
         STPGPU_CHECK_LAUNCH();
-        k_fg_keys<false><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, 0u, 0u, sentinel, k0, v0, zero_map);
+        k_fg_keys<false><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, 0u, 0u, vkeys, nvk, zero_map);
         STPGPU_CHECK_LAUNCH();
     }
-    // ordered (deterministic) moments: stable sort of the list by label
-    // (invalid labels last), segments, per-label sums in memory order
-    const uint32_t* fit_pix = nullptr;
+    // ordered (deterministic) moments: the valid entries sorted by (label,
+    // list position) in one block (up to SORT_SMALL entries), segments,
+    // per-label sums in memory order; island records appended in any order
+    auto moments_and_islands = [&] {
+        k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, sp, mom, ns);
+        STPGPU_CHECK_LAUNCH();
+        k_islands<packed><<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext, eidx, fpos, fneg, kpos, kneg, ns, mom,
+            p.source_min_area, nvalid, nisl, raw);
+        STPGPU_CHECK_LAUNCH();
+    };
     if (nfg > 0) {
-        size_t tb = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, nfg, 0, end_bit, st);
-        void* tmp = c->buf<unsigned char>("cubtmp_sf", tb);
-        if (cub::DeviceRadixSort::SortPairs(tmp, tb, k0, k1, v0, v1, nfg, 0, end_bit, st) != cudaSuccess)
-            fail(STPGPU_ERR_CUDA, "label sort failed");
-        k_seg_bounds<<<gl, 256, 0, st>>>(k1, v1, nfg, uint32_t(np + nneg), uint32_t(cols / 2) * uint32_t(rows), sb, se,
-            sp);
+        set_sort_small_smem();
+        k_sort_small<<<1, 1024, SORT_SMALL * sizeof(unsigned long long), st>>>(vkeys, nvk, fm, split_m, v1, sb, se, sp,
+            sort_overflow);
         STPGPU_CHECK_LAUNCH();
-        fit_pix = v1;
     }
-    k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, sp, mom, ns);
-    STPGPU_CHECK_LAUNCH();
-    // islands appended in any order; the valid-label and island counts and
-    // the first records come back in one read (a second only for more)
-    k_islands<packed><<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext, eidx, fpos, fneg, kpos, kneg, ns, mom,
-        p.source_min_area, nvalid, nisl, raw);
-    STPGPU_CHECK_LAUNCH();
+    moments_and_islands();
+    // the valid-label, island and valid-entry counts, the sort-overflow flag
+    // and the first records come back in one read (a second only for more)
     constexpr int kFirst = 512;
     const int first = std::min(nl, kFirst);
     unsigned char* hb = c->host_stage<unsigned char>(64 + sizeof(IslandRaw) * size_t(kFirst));
     uint32_t* hcnt = reinterpret_cast<uint32_t*>(hb);
     IslandRaw* hfirst = reinterpret_cast<IslandRaw*>(hb + 64);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * first, cudaMemcpyDeviceToHost, st));
     STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hcnt[3]) {
+        // more valid entries than the one-block sort holds: sort them with
+        // the multi-block sort, then sums and islands again
+        const uint32_t nv = hcnt[2];
+        int end_bit = 33;
+        while (end_bit < 64 && (uint64_t(1) << (end_bit - 32)) <= uint64_t(nl))
+            end_bit++;
+        unsigned long long* vk2 = c->buf<unsigned long long>("fg_vkeys2", nv);
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, tb, vkeys, vk2, int(nv), 0, end_bit, st);
+        void* tmp = c->buf<unsigned char>("cubtmp_sf", tb);
+        if (cub::DeviceRadixSort::SortKeys(tmp, tb, vkeys, vk2, int(nv), 0, end_bit, st) != cudaSuccess)
+            fail(STPGPU_ERR_CUDA, "label sort failed");
+        k_seg_mark<<<grid1d(nv, 256), 256, 0, st>>>(vk2, nv, fm, split_m, v1, sb, se, sp);
+        STPGPU_CHECK_LAUNCH();
+        STPGPU_CUDA_TRY(cudaMemsetAsync(cb.misc + 4, 0, 2 * sizeof(uint32_t), st));
+        moments_and_islands();
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * first, cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    const uint32_t* fit_pix = hcnt[2] > 0 ? v1 : nullptr;
     const int nis = int(hcnt[1]);
     info.n_valid_labels = int(hcnt[0]);
     info.n_islands = nis;

@@ -909,59 +909,126 @@ __global__ void k_fg_extrema_idx(const T* img, const uint32_t* fcode, const uint
         atomicMin(&eidx[code], (unsigned long long)m);
 }
 
-// Sort keys of the list: the label code of labels whose extremum passes the
-// detection threshold, `sentinel` (above every code) for the others, whose
-// pixels are zeroed in the label map L when given (generate_labelmap).
-// PACKED: ext holds the single-precision value-and-index keys, which pass
-// when their value part left the starting threshold (thr_pos / thr_neg);
-// else the order keys of the extrema, compared with the detection keys.
+// Entries of labels whose extremum passes the detection threshold, as 64-bit
+// keys (label code above the list position) appended at an atomic cursor;
+// pixels of the other labels are zeroed in the label map L when given
+// (generate_labelmap).  PACKED: ext holds the single-precision
+// value-and-index keys, which pass when their value part left the starting
+// threshold (thr_pos / thr_neg); else the order keys of the extrema,
+// compared with the detection keys.
 template <bool PACKED>
 __global__ void k_fg_keys(const uint32_t* fcode, const uint32_t* fm, int nfg, int np, const unsigned long long* ext,
     unsigned long long det_pos_key, unsigned long long det_neg_key, uint32_t thr_pos, uint32_t thr_neg,
-    uint32_t sentinel, uint32_t* keys, uint32_t* vals, int32_t* L)
+    unsigned long long* keys, uint32_t* count, int32_t* L)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nfg)
         return;
-    const uint32_t code = fcode[i], m = fm[i];
+    const uint32_t code = fcode[i];
     const bool pos = int(code) < np;
     bool valid;
     if constexpr (PACKED)
         valid = uint32_t(ext[code] >> 32) != (pos ? thr_pos : thr_neg);
     else
         valid = pos ? ext[code] > det_pos_key : ext[code] < det_neg_key;
-    keys[i] = valid ? code : sentinel;
-    vals[i] = m;
-    if (!valid && L)
-        L[m] = 0;
+    if (valid)
+        keys[atomicAdd(count, 1u)] = (unsigned long long)code << 32 | uint32_t(i);
+    else if (L)
+        L[fm[i]] = 0;
 }
 
-// Deterministic moments (sourcefind.cpp:457-569).  After a stable sort of
-// the list by key, each valid label's pixels form one segment in scan order.
-// Scan order visits the memory columns from cols/2 first, so a segment is
-// memory order rotated: its pixels in memory columns < cols/2 (memory index
-// < split_m) start at seg_split.  Memory order is [split, end) then
-// [begin, split) -- the order of the reference's single-range loop.
-__global__ void k_seg_bounds(const uint32_t* keys, const uint32_t* vals, int64_t nk, uint32_t nl, uint32_t split_m,
-    uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split)
+// Deterministic moments (sourcefind.cpp:457-569).  Sorted by key, the valid
+// entries form one segment per label in list (scan) order.  Scan order visits
+// the memory columns from cols/2 first, so a segment is memory order rotated:
+// its pixels in memory columns < cols/2 (memory index < split_m) start at
+// seg_split.  Memory order is [split, end) then [begin, split) -- the order
+// of the reference's single-range loop.  seg_mark records, for sorted entry
+// t of cnt, its memory index and the segment bounds it opens or closes.
+__device__ __forceinline__ void seg_mark(const unsigned long long* k, uint32_t t, uint32_t cnt, const uint32_t* fm,
+    uint32_t split_m, uint32_t* vals, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split)
 {
-    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= nk)
-        return;
-    const uint32_t k = keys[t];
-    if (k >= nl)
-        return;
-    const bool first = t == 0 || keys[t - 1] != k;
-    const bool last = t == nk - 1 || keys[t + 1] != k;
+    const unsigned long long key = k[t];
+    const uint32_t code = uint32_t(key >> 32), m = fm[uint32_t(key)];
+    vals[t] = m;
+    const bool first = t == 0 || uint32_t(k[t - 1] >> 32) != code;
+    const bool last = t == cnt - 1 || uint32_t(k[t + 1] >> 32) != code;
     if (first)
-        seg_begin[k] = uint32_t(t);
+        seg_begin[code] = t;
     if (last)
-        seg_end[k] = uint32_t(t + 1);
-    const bool low = vals[t] < split_m;
-    if (low && (first || vals[t - 1] >= split_m))
-        seg_split[k] = uint32_t(t);
+        seg_end[code] = t + 1;
+    const bool low = m < split_m;
+    if (low && (first || fm[uint32_t(k[t - 1])] >= split_m))
+        seg_split[code] = t;
     if (!low && last)
-        seg_split[k] = uint32_t(t + 1);
+        seg_split[code] = t + 1;
+}
+
+// Up to SORT_SMALL valid entries: one block sorts the keys in shared memory
+// (bitonic network over the next power of two, padded with the largest key;
+// steps whose partners lie in one warp's chunk take only a warp barrier) and
+// marks the segments; more entries set *overflow and leave the work to the
+// multi-block sort.  (Keeping the keys in registers and exchanging them by
+// shuffles measured slower.)
+constexpr int SORT_SMALL = 8192;
+__global__ void __launch_bounds__(1024) k_sort_small(const unsigned long long* keys, const uint32_t* count,
+    const uint32_t* fm, uint32_t split_m, uint32_t* vals, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split,
+    uint32_t* overflow)
+{
+    extern __shared__ unsigned long long sk[]; // SORT_SMALL keys
+    const uint32_t cnt = *count;
+    if (cnt > uint32_t(SORT_SMALL)) {
+        if (threadIdx.x == 0)
+            *overflow = 1u;
+        return;
+    }
+    if (cnt == 0)
+        return;
+    uint32_t len = 1;
+    while (len < cnt)
+        len <<= 1;
+    for (uint32_t t = threadIdx.x; t < len; t += blockDim.x)
+        sk[t] = t < cnt ? keys[t] : ~0ull;
+    __syncthreads();
+    // compare-exchange steps with partner distance j below the chunk size C
+    // stay inside one warp's chunk of C keys and need only a warp barrier
+    const uint32_t C = len >= 2048 ? len / 32 : (len >= 64 ? 64 : len);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto cx = [&](uint32_t t, uint32_t j, uint32_t k) {
+        const uint32_t u = t ^ j;
+        if (u > t) {
+            const unsigned long long a = sk[t], b = sk[u];
+            if ((a > b) == ((t & k) == 0)) {
+                sk[t] = b;
+                sk[u] = a;
+            }
+        }
+    };
+    for (uint32_t k = 2; k <= len; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            if (j >= C) {
+                __syncthreads();
+                for (uint32_t t = threadIdx.x; t < len; t += blockDim.x)
+                    cx(t, j, k);
+                __syncthreads();
+            } else {
+                if (warp * C < len)
+                    for (uint32_t t = warp * C + lane; t < warp * C + C; t += 32)
+                        cx(t, j, k);
+                __syncwarp();
+            }
+        }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x)
+        seg_mark(sk, t, cnt, fm, split_m, vals, seg_begin, seg_end, seg_split);
+}
+
+// The same marking over keys sorted by the multi-block sort.
+__global__ void k_seg_mark(const unsigned long long* keys, uint32_t cnt, const uint32_t* fm, uint32_t split_m,
+    uint32_t* vals, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < cnt)
+        seg_mark(keys, t, cnt, fm, split_m, vals, seg_begin, seg_end, seg_split);
 }
 
 // List position of the j-th pixel (memory order) of segment [b, e) split at sp.

@@ -116,6 +116,24 @@ def test_source_find_no_labelmap_cleanup(ctx):
     _compare(isl, ref, lab, ref.label_map)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_crowded_field(ctx, dtype):
+    """About a thousand bright islands (tens of thousands of valid pixels): the label sort takes the
+    multi-block path and the island records come back in two reads; labels and islands as the oracle's."""
+    rng = np.random.default_rng(9)
+    img = rng.normal(size=(384, 384))
+    for r in range(2, 384 - 10, 12):
+        for c in range(2, 384 - 10, 12):
+            img[r:r + 8, c:c + 8] += 6.0 + rng.uniform(0, 4)
+    img = img.astype(dtype)
+    ref = orc.source_find(img.astype(np.float64), 4.0, 2.5, 1.0, True, 5, orc.ZEROMEDIAN, False, False, True, 3, 0)
+    assert sum(i[4] for i in ref.islands) > 8192 and len(ref.islands) > 512
+    for _ in range(2):
+        isl, lab, info = ctx.source_find(img, 4.0, 2.5, 1.0, True, 5, capi.ZEROMEDIAN, False, False, True, 3, 0)
+        assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
+        _compare(isl, ref, lab, ref.label_map)
+
+
 def test_source_find_rejects(ctx):
     with pytest.raises(capi.StpGpuError):
         ctx.source_find(np.zeros((7, 8)), 5, 3)
