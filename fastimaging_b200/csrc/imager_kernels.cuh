@@ -1352,13 +1352,6 @@ __global__ void k_kernel_table(int kf, double trunc, int support, int os, double
         out[c * K + i] = out[c * K + i] / s;
 }
 
-__global__ void k_iota_u32(uint32_t* p, int64_t n)
-{
-    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n)
-        p[i] = uint32_t(i);
-}
-
 __global__ void k_d2f(const double* in, float* out, int64_t n)
 {
     int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
