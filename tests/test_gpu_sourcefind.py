@@ -134,6 +134,26 @@ def test_crowded_field(ctx, dtype):
         _compare(isl, ref, lab, ref.label_map)
 
 
+@pytest.mark.parametrize("shape", [(130, 98), (98, 130)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_rows_not_multiple_of_four(ctx, shape, dtype):
+    """Row counts of 2 mod 4 take the one-key-per-thread class and label passes; labels and islands as the
+    oracle's, with fixed and with estimated thresholds."""
+    rng = np.random.default_rng(21)
+    img = rng.normal(size=shape)
+    img[10:18, 20:27] += 9.0
+    img[0:2, :] += 4.5  # across the shifted-topology seams
+    img[:, shape[1] // 2 - 1:shape[1] // 2 + 1] -= 5.0
+    img = img.astype(dtype)
+    ref = orc.source_find(img.astype(np.float64), 4.0, 2.5, 1.0, True, 5, orc.ZEROMEDIAN, False, False, True, 3, 0)
+    isl, lab, info = ctx.source_find(img, 4.0, 2.5, 1.0, True, 5, capi.ZEROMEDIAN, False, False, True, 3, 0)
+    assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
+    _compare(isl, ref, lab, ref.label_map)
+    ref = orc.source_find(img.astype(np.float64), 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5)
+    assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
+
+
 def test_source_find_rejects(ctx):
     with pytest.raises(capi.StpGpuError):
         ctx.source_find(np.zeros((7, 8)), 5, 3)
