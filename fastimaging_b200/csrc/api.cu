@@ -115,6 +115,8 @@ struct stpgpu_context {
     cudaGraph_t single_graph = nullptr;
     cudaGraphExec_t single_exec = nullptr;
     GridOut single_g {};
+    uint32_t sf_label_cap = 0; // source finder: label-analysis capacities that sufficed so far
+    uint32_t sf_fg_cap = 0;
     int single_launches = 0; // our kernels in single_graph (counted at capture)
     int batch_launches = 0;  // our kernels in batch_graph
 
@@ -1756,13 +1758,6 @@ double median_exact(stpgpu_context* c, const T* x, int64_t n)
     return (v1 + v2) / 2;
 }
 
-unsigned long long host_okey(double v)
-{
-    unsigned long long u;
-    std::memcpy(&u, &v, sizeof(u));
-    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
-}
-
 // Gaussian2dParams::convert_to_constrained_parameters (fitting.cpp:32-57)
 void constrain(double* g)
 {
@@ -1964,121 +1959,115 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     SfState* sfs = c->buf<SfState>("sf_state", 1);
     cb.misc = sfs->misc;
     const int slice = p.ccl_slice_cols > 0 ? p.ccl_slice_cols : std::max(2, cols / 8);
-    // statistics, thresholds and labels with one read-back (label counts,
-    // foreground count, union-find flag, statistics); a second attempt only
-    // when the binned median does not apply
-    SfState h;
-    for (int attempt = 0;; attempt++) {
-        STPGPU_CUDA_TRY(cudaMemsetAsync(sfs, 0, sizeof(SfState), st));
-        enqueue_stats<T>(c, d_img, n, p, sfs, attempt > 0);
-        STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
-            p.ccl_4connectivity, slice, cb));
-        SfState* hs = c->host_stage<SfState>(1);
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hs, sfs, sizeof(SfState), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-        h = *hs;
-        if (!h.st.need_exact || attempt > 0)
-            break;
-    }
-    if (h.misc[3])
-        fail(STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)");
-    info.bg_level = h.st.median;
-    info.rms_est = h.st.rms;
-    info.mean = h.st.mean;
-    info.sigma = h.st.sigma;
-    const double d_pos = h.st.thr[2], d_neg = h.st.thr[3];
-    const double rms = h.st.rms;
-    const int np = int(h.misc[0]), nneg = int(h.misc[1]), nfg = int(h.misc[2]);
-    info.n_labels_pos = np;
-    info.n_labels_neg = nneg;
 
-    // ---- extrema, detection filter, moments (sourcefind.cpp:342-628) over the foreground list
-    const int nl = std::max(1, np + nneg);
-    // per label: extremum keys (single precision: value-and-index keys),
-    // first indices, moments, sample counts, list segments
-    unsigned long long* ext = c->buf<unsigned long long>("sf_ext", nl);
-    unsigned long long* eidx = c->buf<unsigned long long>("sf_eidx", nl);
-    double* mom = c->buf<double>("sf_mom", 6 * size_t(nl));
-    int* ns = c->buf<int>("sf_ns", nl);
-    uint32_t* sb = c->buf<uint32_t>("fg_sb", nl);
-    uint32_t* se = c->buf<uint32_t>("fg_se", nl);
-    uint32_t* sp = c->buf<uint32_t>("fg_sp", nl);
-    uint32_t* nvalid = cb.misc + 4;
-    uint32_t* nisl = cb.misc + 5;
-    const unsigned long long kpos = host_okey(d_pos), kneg = host_okey(d_neg);
-    const int64_t nfk = std::max(nfg, 1);
-    uint32_t* fcode = c->buf<uint32_t>("fg_code", nfk);
-    uint32_t* fm = c->buf<uint32_t>("fg_m", nfk);
-    unsigned long long* vkeys = c->buf<unsigned long long>("fg_vkeys", nfk); // valid entries, then sorted
-    uint32_t* v1 = c->buf<uint32_t>("fg_v1", nfk); // memory index of each sorted valid entry
-    uint32_t* nvk = cb.misc + 6; // valid entries
-    uint32_t* sort_overflow = cb.misc + 7;
-    IslandRaw* raw = c->buf<IslandRaw>("sf_raw", nl);
-    const unsigned gl = unsigned(ceil_div(std::max(nfg, 1), 256));
+    // ---- extrema, detection filter, moments (sourcefind.cpp:342-628) over
+    // the foreground list, enqueued behind the labeller before its counts are
+    // known: the buffers are sized by capacities (remembered per context),
+    // and a call whose counts exceed them runs this stage again
+    constexpr bool packed = sizeof(T) == 4;
+    constexpr int kFirst = 512; // island records read back with the counts
+    const unsigned G = 148 * 4; // grid of the label-analysis loops
     const uint32_t split_m = uint32_t(cols / 2) * uint32_t(rows);
     int32_t* zero_map = p.generate_labelmap ? cb.L : nullptr;
-    constexpr bool packed = sizeof(T) == 4;
-    uint32_t fpos = 0, fneg = 0;
-    if constexpr (packed) {
-        // extremum and first index in one pass: threshold rounded onto the
-        // float grid (largest float <= the positive threshold, smallest
-        // float >= the negative one)
-        float tf = float(d_pos);
-        if (double(tf) > d_pos)
-            tf = std::nextafter(tf, -HUGE_VALF);
-        float tc = float(d_neg);
-        if (double(tc) < d_neg)
-            tc = std::nextafter(tc, HUGE_VALF);
-        fpos = fkey32(tf);
-        fneg = fkey32(tc);
-        k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(ext, nullptr, np, nl, (unsigned long long)fpos << 32 | 0xffffffffull,
-            (unsigned long long)fneg << 32, sb, se, sp, nvalid);
+    uint32_t* nvalid = cb.misc + 4;
+    uint32_t* nisl = cb.misc + 5;
+    uint32_t* nvk = cb.misc + 6; // valid entries
+    uint32_t* sort_overflow = cb.misc + 7;
+    uint32_t lcap = uint32_t(std::min<int64_t>(n, std::max<int64_t>(c->sf_label_cap, std::max<int64_t>(65536, n / 64))));
+    uint32_t fcap = uint32_t(std::min<int64_t>(n, std::max<int64_t>(c->sf_fg_cap, std::max<int64_t>(131072, n / 16))));
+    unsigned long long *ext = nullptr, *eidx = nullptr, *vkeys = nullptr;
+    double* mom = nullptr;
+    int* ns = nullptr;
+    uint32_t *sb = nullptr, *se = nullptr, *sp = nullptr, *fcode = nullptr, *fm = nullptr, *v1 = nullptr;
+    IslandRaw* raw = nullptr;
+    auto size_buffers = [&] {
+        // per label: extremum keys (single precision: value-and-index keys),
+        // first indices, moments, sample counts, list segments; per list
+        // entry: label code, memory index, valid keys, sorted memory indices
+        ext = c->buf<unsigned long long>("sf_ext", lcap);
+        eidx = c->buf<unsigned long long>("sf_eidx", lcap);
+        mom = c->buf<double>("sf_mom", 6 * size_t(lcap));
+        ns = c->buf<int>("sf_ns", lcap);
+        sb = c->buf<uint32_t>("fg_sb", lcap);
+        se = c->buf<uint32_t>("fg_se", lcap);
+        sp = c->buf<uint32_t>("fg_sp", lcap);
+        raw = c->buf<IslandRaw>("sf_raw", std::max<uint32_t>(lcap, kFirst));
+        fcode = c->buf<uint32_t>("fg_code", fcap);
+        fm = c->buf<uint32_t>("fg_m", fcap);
+        vkeys = c->buf<unsigned long long>("fg_vkeys", fcap);
+        v1 = c->buf<uint32_t>("fg_v1", fcap);
+    };
+    auto moments_and_islands = [&](const FgSizes& z) {
+        k_label_sums<T><<<G, 128, 0, st>>>(z, d_img, rows, cols, v1, sb, se, sp, mom, ns);
         STPGPU_CHECK_LAUNCH();
-        k_fg_gather<T, true><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, ext);
-        STPGPU_CHECK_LAUNCH();
-        k_fg_keys<true><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, fpos, fneg, vkeys, nvk, zero_map);
-        STPGPU_CHECK_LAUNCH();
-    } else {
-        k_fg_init<<<grid1d(nl, 256), 256, 0, st>>>(ext, eidx, np, nl, kpos, kneg, sb, se, sp, nvalid);
-        STPGPU_CHECK_LAUNCH();
-        k_fg_gather<T, false><<<gl, 256, 0, st>>>(d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, nfg, np, fcode, fm, ext);
-        STPGPU_CHECK_LAUNCH();
-        k_fg_extrema_idx<T><<<gl, 256, 0, st>>>(d_img, fcode, fm, nfg, np, ext, kpos, kneg, eidx);
-        STPGPU_CHECK_LAUNCH();
-        k_fg_keys<false><<<gl, 256, 0, st>>>(fcode, fm, nfg, np, ext, kpos, kneg, 0u, 0u, vkeys, nvk, zero_map);
-        STPGPU_CHECK_LAUNCH();
-    }
-    // ordered (deterministic) moments: the valid entries sorted by (label,
-    // list position) in one block (up to SORT_SMALL entries), segments,
-    // per-label sums in memory order; island records appended in any order
-    auto moments_and_islands = [&] {
-        k_label_sums<T><<<grid1d(nl, 128), 128, 0, st>>>(d_img, rows, cols, np + nneg, v1, sb, se, sp, mom, ns);
-        STPGPU_CHECK_LAUNCH();
-        k_islands<packed><<<grid1d(nl, 256), 256, 0, st>>>(np, nneg, ext, eidx, fpos, fneg, kpos, kneg, ns, mom,
-            p.source_min_area, nvalid, nisl, raw);
+        k_islands<packed><<<G, 256, 0, st>>>(z, &sfs->st, ext, eidx, ns, mom, p.source_min_area, nvalid, nisl, raw);
         STPGPU_CHECK_LAUNCH();
     };
-    if (nfg > 0) {
+    auto enqueue_analysis = [&] {
+        const FgSizes z { cb.misc, lcap, fcap };
+        k_fg_init<packed><<<G, 256, 0, st>>>(z, &sfs->st, ext, packed ? nullptr : eidx, sb, se, sp);
+        STPGPU_CHECK_LAUNCH();
+        k_fg_gather<T, packed><<<G, 256, 0, st>>>(z, d_img, cb.cls, cb.P, cb.R, geom, cb.fgl, fcode, fm, ext);
+        STPGPU_CHECK_LAUNCH();
+        if constexpr (!packed) {
+            k_fg_extrema_idx<T><<<G, 256, 0, st>>>(z, &sfs->st, d_img, fcode, fm, ext, eidx);
+            STPGPU_CHECK_LAUNCH();
+        }
+        k_fg_keys<packed><<<G, 256, 0, st>>>(z, &sfs->st, fcode, fm, ext, vkeys, nvk, zero_map);
+        STPGPU_CHECK_LAUNCH();
+        // ordered (deterministic) moments: the valid entries sorted by
+        // (label, list position) in one block (up to SORT_SMALL entries),
+        // segments, per-label sums in memory order; island records appended
+        // in any order
         set_sort_small_smem();
         k_sort_small<<<1, 1024, SORT_SMALL * sizeof(unsigned long long), st>>>(vkeys, nvk, fm, split_m, v1, sb, se, sp,
             sort_overflow);
         STPGPU_CHECK_LAUNCH();
+        moments_and_islands(z);
+    };
+    // everything, then one read-back: state (statistics, counts, flags) and
+    // the first island records
+    unsigned char* hb = c->host_stage<unsigned char>(sizeof(SfState) + 64 + sizeof(IslandRaw) * size_t(kFirst));
+    SfState* hstate = reinterpret_cast<SfState*>(hb);
+    IslandRaw* hfirst = reinterpret_cast<IslandRaw*>(hb + ((sizeof(SfState) + 63) / 64) * 64);
+    auto read_back_state = [&] {
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hstate, sfs, sizeof(SfState), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * kFirst, cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+    };
+    size_buffers();
+    for (int attempt = 0;; attempt++) {
+        // a second attempt only when the binned median does not apply
+        STPGPU_CUDA_TRY(cudaMemsetAsync(sfs, 0, sizeof(SfState), st));
+        enqueue_stats<T>(c, d_img, n, p, sfs, attempt > 0);
+        STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
+            p.ccl_4connectivity, slice, cb));
+        enqueue_analysis();
+        read_back_state();
+        if (!hstate->st.need_exact || attempt > 0)
+            break;
     }
-    moments_and_islands();
-    // the valid-label, island and valid-entry counts, the sort-overflow flag
-    // and the first records come back in one read (a second only for more)
-    constexpr int kFirst = 512;
-    const int first = std::min(nl, kFirst);
-    unsigned char* hb = c->host_stage<unsigned char>(64 + sizeof(IslandRaw) * size_t(kFirst));
-    uint32_t* hcnt = reinterpret_cast<uint32_t*>(hb);
-    IslandRaw* hfirst = reinterpret_cast<IslandRaw*>(hb + 64);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * first, cudaMemcpyDeviceToHost, st));
-    STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-    if (hcnt[3]) {
+    if (hstate->misc[3])
+        fail(STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)");
+    const int np = int(hstate->misc[0]), nneg = int(hstate->misc[1]), nfg = int(hstate->misc[2]);
+    const int nl = std::max(1, np + nneg);
+    if (uint32_t(np + nneg) > lcap || uint32_t(nfg) > fcap) {
+        // counts beyond the capacities: larger buffers, the stage again
+        lcap = uint32_t(std::max<int64_t>(lcap, np + nneg + (np + nneg) / 4));
+        fcap = uint32_t(std::max<int64_t>(fcap, nfg + nfg / 4));
+        lcap = uint32_t(std::min<int64_t>(lcap, n));
+        fcap = uint32_t(std::min<int64_t>(fcap, n));
+        size_buffers();
+        STPGPU_CUDA_TRY(cudaMemsetAsync(cb.misc + 4, 0, 4 * sizeof(uint32_t), st));
+        enqueue_analysis();
+        read_back_state();
+    }
+    c->sf_label_cap = std::max<uint32_t>(c->sf_label_cap, lcap);
+    c->sf_fg_cap = std::max<uint32_t>(c->sf_fg_cap, fcap);
+    if (hstate->misc[7]) {
         // more valid entries than the one-block sort holds: sort them with
         // the multi-block sort, then sums and islands again
-        const uint32_t nv = hcnt[2];
+        const uint32_t nv = hstate->misc[6];
         int end_bit = 33;
         while (end_bit < 64 && (uint64_t(1) << (end_bit - 32)) <= uint64_t(nl))
             end_bit++;
@@ -2091,14 +2080,21 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         k_seg_mark<<<grid1d(nv, 256), 256, 0, st>>>(vk2, nv, fm, split_m, v1, sb, se, sp);
         STPGPU_CHECK_LAUNCH();
         STPGPU_CUDA_TRY(cudaMemsetAsync(cb.misc + 4, 0, 2 * sizeof(uint32_t), st));
-        moments_and_islands();
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hcnt, cb.misc + 4, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * first, cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+        moments_and_islands(FgSizes { cb.misc, lcap, fcap });
+        read_back_state();
     }
-    const uint32_t* fit_pix = hcnt[2] > 0 ? v1 : nullptr;
-    const int nis = int(hcnt[1]);
-    info.n_valid_labels = int(hcnt[0]);
+    const SfState h = *hstate;
+    info.bg_level = h.st.median;
+    info.rms_est = h.st.rms;
+    info.mean = h.st.mean;
+    info.sigma = h.st.sigma;
+    const double rms = h.st.rms;
+    info.n_labels_pos = np;
+    info.n_labels_neg = nneg;
+    const int first = std::min(nl, kFirst);
+    const uint32_t* fit_pix = h.misc[6] > 0 ? v1 : nullptr;
+    const int nis = int(h.misc[5]);
+    info.n_valid_labels = int(h.misc[4]);
     info.n_islands = nis;
     std::vector<IslandRaw> hr(nis);
     std::copy(hfirst, hfirst + std::min(nis, first), hr.begin());

@@ -152,6 +152,8 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
 struct SfStats {
     double mean, sigma, median, rms;
     double thr[4]; // analysis +, analysis -, detection +, detection -
+    unsigned long long kpos, kneg; // order keys of the detection thresholds
+    unsigned int fpos, fneg; // single-precision keys of the detection thresholds rounded onto the float grid
     unsigned int need_exact; // the binned median does not apply: the exact path must run
     unsigned int pad;
 };
@@ -455,16 +457,32 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
     *cs = c;
 }
 
+__device__ __host__ inline uint32_t fkey32(float v);
+
 // rms (the clipped sigma, or the caller's estimate when cs is null) and the
-// thresholds bg +- n_sigma * rms with bg = the median (sourcefind.cpp:298-301).
+// thresholds bg +- n_sigma * rms with bg = the median (sourcefind.cpp:298-301),
+// with the detection thresholds' keys for the label analysis: order keys,
+// and for single-precision images the largest float <= the positive
+// threshold and the smallest float >= the negative one.
 __global__ void k_sf_thresholds(SfStats* st, const ClipState* cs, double rms_fixed, double ana, double det)
 {
     const double rms = cs ? cs->s : rms_fixed, bg = st->median;
     st->rms = rms;
     st->thr[0] = __dadd_rn(bg, __dmul_rn(ana, rms));
     st->thr[1] = __dsub_rn(bg, __dmul_rn(ana, rms));
-    st->thr[2] = __dadd_rn(bg, __dmul_rn(det, rms));
-    st->thr[3] = __dsub_rn(bg, __dmul_rn(det, rms));
+    const double dp = __dadd_rn(bg, __dmul_rn(det, rms)), dn = __dsub_rn(bg, __dmul_rn(det, rms));
+    st->thr[2] = dp;
+    st->thr[3] = dn;
+    st->kpos = okey(dp);
+    st->kneg = okey(dn);
+    float tf = __double2float_rn(dp);
+    if (double(tf) > dp)
+        tf = nextafterf(tf, -INFINITY);
+    float tc = __double2float_rn(dn);
+    if (double(tc) < dn)
+        tc = nextafterf(tc, INFINITY);
+    st->fpos = fkey32(tf);
+    st->fneg = fkey32(tc);
 }
 
 // -------------------------------------------------- connected components
@@ -816,10 +834,27 @@ __global__ void __launch_bounds__(SF_THREADS) k_ccl_label16(const uint8_t* cls, 
 
 // -------------------------------------------------- label analysis
 //
+// The stage is enqueued before the host knows its sizes: FgSizes reads the
+// label counts and the foreground-list length from the labeller's counters
+// and caps them at the capacities the buffers were sized for (the host runs
+// the stage again with larger buffers when a cap was hit).  The kernels loop
+// over their entries with a fixed grid.
+//
 // Everything after the labelling works on the list of foreground keys in
 // scan order (k_ccl_rank's fgl), not on the image: entry i has the label
 // code (positives 0..np-1, negatives np..np+nn-1) and the memory index of
 // its pixel.
+
+struct FgSizes {
+    const uint32_t* misc; // [0] positive labels, [1] negative labels, [2] foreground entries
+    uint32_t label_cap, fg_cap;
+    __device__ __forceinline__ int np() const { return int(misc[0]); }
+    __device__ __forceinline__ uint32_t nl() const { return min(misc[0] + misc[1], label_cap); }
+    __device__ __forceinline__ uint32_t nfg() const { return min(misc[2], fg_cap); }
+};
+
+#define FG_LOOP(i, count)                                                                                            \
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, i##_n = (count); i < i##_n; i += gridDim.x * blockDim.x)
 
 // Single-precision images keep the extremum and its first memory index as
 // one 64-bit key per label (the value's order key above the index;
@@ -841,22 +876,25 @@ __device__ inline float fkey32_inv(uint32_t k)
 }
 
 // Per-label starting state: extremum keys at the detection threshold
-// (sourcefind.cpp:342-378 starts from it and compares strictly), first
-// indices unset (eidx, when given), empty segments.
-__global__ void k_fg_init(unsigned long long* ext, unsigned long long* eidx, int np, int nl, unsigned long long vpos,
-    unsigned long long vneg, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split, uint32_t* nvalid)
+// (sourcefind.cpp:342-378 starts from it and compares strictly; PACKED: the
+// value-and-index keys), first indices unset (eidx, when given), empty
+// segments.
+template <bool PACKED>
+__global__ void k_fg_init(FgSizes z, const SfStats* st, unsigned long long* ext, unsigned long long* eidx,
+    uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i == 0)
-        *nvalid = 0;
-    if (i >= nl)
-        return;
-    ext[i] = i < np ? vpos : vneg;
-    if (eidx)
-        eidx[i] = ~0ull;
-    seg_begin[i] = 0;
-    seg_end[i] = 0;
-    seg_split[i] = 0;
+    const int np = z.np();
+    const unsigned long long vpos = PACKED ? (unsigned long long)st->fpos << 32 | 0xffffffffull : st->kpos;
+    const unsigned long long vneg = PACKED ? (unsigned long long)st->fneg << 32 : st->kneg;
+    FG_LOOP(i, z.nl())
+    {
+        ext[i] = int(i) < np ? vpos : vneg;
+        if (eidx)
+            eidx[i] = ~0ull;
+        seg_begin[i] = 0;
+        seg_end[i] = 0;
+        seg_split[i] = 0;
+    }
 }
 
 // Label code and memory index of each foreground key, and the extremum of
@@ -864,49 +902,55 @@ __global__ void k_fg_init(unsigned long long* ext, unsigned long long* eidx, int
 // above, else the order key of the value (its first index follows in
 // k_fg_extrema_idx).
 template <typename T, bool PACKED>
-__global__ void k_fg_gather(const T* img, const uint8_t* cls, const uint32_t* P, const uint32_t* R, CclGeom g,
-    const uint32_t* fgl, int nfg, int np, uint32_t* fcode, uint32_t* fm, unsigned long long* ext)
+__global__ void k_fg_gather(FgSizes z, const T* img, const uint8_t* cls, const uint32_t* P, const uint32_t* R,
+    CclGeom g, const uint32_t* fgl, uint32_t* fcode, uint32_t* fm, unsigned long long* ext)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nfg)
-        return;
-    const uint32_t s = fgl[i];
-    const bool pos = cls[s] == 1;
-    const uint32_t r = R[P[s]] - 1;
-    const uint32_t code = pos ? r : uint32_t(np) + r;
-    const uint32_t m = uint32_t(g.mem_of_key(s));
-    fcode[i] = code;
-    fm[i] = m;
-    if constexpr (PACKED) {
-        const unsigned long long k = (unsigned long long)fkey32(float(img[m])) << 32;
-        if (pos)
-            atomicMax(&ext[code], k | (0xffffffffu - m));
-        else
-            atomicMin(&ext[code], k | m);
-    } else {
-        const unsigned long long k = okey(ld(img, m));
-        if (pos)
-            atomicMax(&ext[code], k);
-        else
-            atomicMin(&ext[code], k);
+    const uint32_t np = uint32_t(z.np());
+    FG_LOOP(i, z.nfg())
+    {
+        const uint32_t s = fgl[i];
+        const bool pos = cls[s] == 1;
+        const uint32_t r = R[P[s]] - 1;
+        const uint32_t code = pos ? r : np + r;
+        const uint32_t m = uint32_t(g.mem_of_key(s));
+        fcode[i] = code;
+        fm[i] = m;
+        if (code >= z.label_cap)
+            continue; // over capacity: the host runs the stage again
+        if constexpr (PACKED) {
+            const unsigned long long k = (unsigned long long)fkey32(float(img[m])) << 32;
+            if (pos)
+                atomicMax(&ext[code], k | (0xffffffffu - m));
+            else
+                atomicMin(&ext[code], k | m);
+        } else {
+            const unsigned long long k = okey(ld(img, m));
+            if (pos)
+                atomicMax(&ext[code], k);
+            else
+                atomicMin(&ext[code], k);
+        }
     }
 }
 
 // First memory index holding the extremum (the serial reference keeps the
 // first occurrence in memory order).
 template <typename T>
-__global__ void k_fg_extrema_idx(const T* img, const uint32_t* fcode, const uint32_t* fm, int nfg, int np,
-    const unsigned long long* ext, unsigned long long det_pos_key, unsigned long long det_neg_key,
-    unsigned long long* eidx)
+__global__ void k_fg_extrema_idx(FgSizes z, const SfStats* st, const T* img, const uint32_t* fcode, const uint32_t* fm,
+    const unsigned long long* ext, unsigned long long* eidx)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nfg)
-        return;
-    const uint32_t code = fcode[i], m = fm[i];
-    const unsigned long long k = okey(ld(img, m));
-    const bool hit = int(code) < np ? k > det_pos_key : k < det_neg_key;
-    if (hit && k == ext[code])
-        atomicMin(&eidx[code], (unsigned long long)m);
+    const int np = z.np();
+    const unsigned long long kpos = st->kpos, kneg = st->kneg;
+    FG_LOOP(i, z.nfg())
+    {
+        const uint32_t code = fcode[i], m = fm[i];
+        if (code >= z.label_cap)
+            continue;
+        const unsigned long long k = okey(ld(img, m));
+        const bool hit = int(code) < np ? k > kpos : k < kneg;
+        if (hit && k == ext[code])
+            atomicMin(&eidx[code], (unsigned long long)m);
+    }
 }
 
 // Entries of labels whose extremum passes the detection threshold, as 64-bit
@@ -917,24 +961,26 @@ __global__ void k_fg_extrema_idx(const T* img, const uint32_t* fcode, const uint
 // threshold (thr_pos / thr_neg); else the order keys of the extrema,
 // compared with the detection keys.
 template <bool PACKED>
-__global__ void k_fg_keys(const uint32_t* fcode, const uint32_t* fm, int nfg, int np, const unsigned long long* ext,
-    unsigned long long det_pos_key, unsigned long long det_neg_key, uint32_t thr_pos, uint32_t thr_neg,
-    unsigned long long* keys, uint32_t* count, int32_t* L)
+__global__ void k_fg_keys(FgSizes z, const SfStats* st, const uint32_t* fcode, const uint32_t* fm,
+    const unsigned long long* ext, unsigned long long* keys, uint32_t* count, int32_t* L)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nfg)
-        return;
-    const uint32_t code = fcode[i];
-    const bool pos = int(code) < np;
-    bool valid;
-    if constexpr (PACKED)
-        valid = uint32_t(ext[code] >> 32) != (pos ? thr_pos : thr_neg);
-    else
-        valid = pos ? ext[code] > det_pos_key : ext[code] < det_neg_key;
-    if (valid)
-        keys[atomicAdd(count, 1u)] = (unsigned long long)code << 32 | uint32_t(i);
-    else if (L)
-        L[fm[i]] = 0;
+    const int np = z.np();
+    FG_LOOP(i, z.nfg())
+    {
+        const uint32_t code = fcode[i];
+        if (code >= z.label_cap)
+            continue;
+        const bool pos = int(code) < np;
+        bool valid;
+        if constexpr (PACKED)
+            valid = uint32_t(ext[code] >> 32) != (pos ? st->fpos : st->fneg);
+        else
+            valid = pos ? ext[code] > st->kpos : ext[code] < st->kneg;
+        if (valid)
+            keys[atomicAdd(count, 1u)] = (unsigned long long)code << 32 | i;
+        else if (L)
+            L[fm[i]] = 0;
+    }
 }
 
 // Deterministic moments (sourcefind.cpp:457-569).  Sorted by key, the valid
@@ -1042,54 +1088,54 @@ __device__ __forceinline__ uint32_t seg_at(uint32_t b, uint32_t sp, uint32_t e, 
 // the reference's.  mom: 6 doubles per label code: sum x v, y v, x^2 v,
 // y^2 v, x y v, v (display coordinates).
 template <typename T>
-__global__ void k_label_sums(const T* img, int rows, int cols, int nl, const uint32_t* vals,
+__global__ void k_label_sums(FgSizes z, const T* img, int rows, int cols, const uint32_t* vals,
     const uint32_t* seg_begin, const uint32_t* seg_end, const uint32_t* seg_split, double* mom, int* ns)
 {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    if (l >= nl)
-        return;
-    const uint32_t b = seg_begin[l], e = seg_end[l], sp = seg_split[l], len = e - b;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
-    const int vs = rows / 2, hs = cols / 2;
-    auto add = [&](uint32_t m, double val) {
-        const int c = int(m / uint32_t(rows)), r = int(m - uint32_t(c) * uint32_t(rows));
-        const double y = r < vs ? double(r + vs) : double(r - vs);
-        const double x = c < hs ? double(c + hs) : double(c - hs);
-        const double xb = __dmul_rn(x, val), yb = __dmul_rn(y, val);
-        a0 = __dadd_rn(a0, xb);
-        a1 = __dadd_rn(a1, yb);
-        a2 = __dadd_rn(a2, __dmul_rn(xb, x));
-        a3 = __dadd_rn(a3, __dmul_rn(yb, y));
-        a4 = __dadd_rn(a4, __dmul_rn(xb, y));
-        a5 = __dadd_rn(a5, val);
-    };
-    // four pixels' loads in flight, then their sums in order
-    uint32_t j = 0;
-    for (; j + 4 <= len; j += 4) {
-        uint32_t m[4];
-        double val[4];
+    FG_LOOP(l, z.nl())
+    {
+        const uint32_t b = seg_begin[l], e = seg_end[l], sp = seg_split[l], len = e - b;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0, a5 = 0.0;
+        const int vs = rows / 2, hs = cols / 2;
+        auto add = [&](uint32_t m, double val) {
+            const int c = int(m / uint32_t(rows)), r = int(m - uint32_t(c) * uint32_t(rows));
+            const double y = r < vs ? double(r + vs) : double(r - vs);
+            const double x = c < hs ? double(c + hs) : double(c - hs);
+            const double xb = __dmul_rn(x, val), yb = __dmul_rn(y, val);
+            a0 = __dadd_rn(a0, xb);
+            a1 = __dadd_rn(a1, yb);
+            a2 = __dadd_rn(a2, __dmul_rn(xb, x));
+            a3 = __dadd_rn(a3, __dmul_rn(yb, y));
+            a4 = __dadd_rn(a4, __dmul_rn(xb, y));
+            a5 = __dadd_rn(a5, val);
+        };
+        // four pixels' loads in flight, then their sums in order
+        uint32_t j = 0;
+        for (; j + 4 <= len; j += 4) {
+            uint32_t m[4];
+            double val[4];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-            m[q] = vals[seg_at(b, sp, e, j + q)];
+            for (int q = 0; q < 4; q++)
+                m[q] = vals[seg_at(b, sp, e, j + q)];
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-            val[q] = ld(img, m[q]);
+            for (int q = 0; q < 4; q++)
+                val[q] = ld(img, m[q]);
 #pragma unroll
-        for (int q = 0; q < 4; q++)
-            add(m[q], val[q]);
+            for (int q = 0; q < 4; q++)
+                add(m[q], val[q]);
+        }
+        for (; j < len; j++) {
+            const uint32_t m = vals[seg_at(b, sp, e, j)];
+            add(m, ld(img, m));
+        }
+        double* mo = mom + 6 * size_t(l);
+        mo[0] = a0;
+        mo[1] = a1;
+        mo[2] = a2;
+        mo[3] = a3;
+        mo[4] = a4;
+        mo[5] = a5;
+        ns[l] = int(len);
     }
-    for (; j < len; j++) {
-        const uint32_t m = vals[seg_at(b, sp, e, j)];
-        add(m, ld(img, m));
-    }
-    double* mo = mom + 6 * size_t(l);
-    mo[0] = a0;
-    mo[1] = a1;
-    mo[2] = a2;
-    mo[3] = a3;
-    mo[4] = a4;
-    mo[5] = a5;
-    ns[l] = int(len);
 }
 
 
@@ -1108,40 +1154,42 @@ struct IslandRaw {
 // pixels, the island record appended at an atomic cursor (the host orders
 // the records by label).
 template <bool PACKED>
-__global__ void k_islands(int np, int nn, const unsigned long long* ext, const unsigned long long* eidx,
-    uint32_t thr_pos, uint32_t thr_neg, unsigned long long det_pos_key, unsigned long long det_neg_key, const int* ns,
-    const double* mom, int min_area, uint32_t* nvalid, uint32_t* nisl, IslandRaw* out)
+__global__ void k_islands(FgSizes z, const SfStats* st, const unsigned long long* ext,
+    const unsigned long long* eidx, const int* ns, const double* mom, int min_area, uint32_t* nvalid, uint32_t* nisl,
+    IslandRaw* out)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= np + nn)
-        return;
-    const bool pos = t < np;
-    unsigned long long key, idx;
-    bool valid;
-    if constexpr (PACKED) {
-        const uint32_t hi = uint32_t(ext[t] >> 32), lo = uint32_t(ext[t]);
-        valid = hi != (pos ? thr_pos : thr_neg);
-        key = okey(double(fkey32_inv(hi)));
-        idx = pos ? (unsigned long long)(0xffffffffu - lo) : (unsigned long long)lo;
-    } else {
-        key = ext[t];
-        idx = eidx[t];
-        valid = pos ? key > det_pos_key : key < det_neg_key;
+    const int np = z.np();
+    FG_LOOP(ut, z.nl())
+    {
+        const int t = int(ut);
+        const bool pos = t < np;
+        unsigned long long key, idx;
+        bool valid;
+        if constexpr (PACKED) {
+            const uint32_t hi = uint32_t(ext[t] >> 32), lo = uint32_t(ext[t]);
+            valid = hi != (pos ? st->fpos : st->fneg);
+            key = okey(double(fkey32_inv(hi)));
+            idx = pos ? (unsigned long long)(0xffffffffu - lo) : (unsigned long long)lo;
+        } else {
+            key = ext[t];
+            idx = eidx[t];
+            valid = pos ? key > st->kpos : key < st->kneg;
+        }
+        if (!valid)
+            continue;
+        atomicAdd(nvalid, 1u);
+        if (ns[t] < min_area)
+            continue;
+        IslandRaw r;
+        const int i = pos ? t : t - np;
+        r.label = pos ? (i + 1) : -(i + 1);
+        r.num_samples = ns[t];
+        r.extremum_val = okey_inv(key);
+        r.extremum_idx = (long long)idx;
+        for (int q = 0; q < 6; q++)
+            r.mom[q] = mom[6 * size_t(t) + q];
+        out[atomicAdd(nisl, 1u)] = r;
     }
-    if (!valid)
-        return;
-    atomicAdd(nvalid, 1u);
-    if (ns[t] < min_area)
-        return;
-    IslandRaw r;
-    const int i = pos ? t : t - np;
-    r.label = pos ? (i + 1) : -(i + 1);
-    r.num_samples = ns[t];
-    r.extremum_val = okey_inv(key);
-    r.extremum_idx = (long long)idx;
-    for (int q = 0; q < 6; q++)
-        r.mom[q] = mom[6 * size_t(t) + q];
-    out[atomicAdd(nisl, 1u)] = r;
 }
 
 // ---------------------------------------------------------------- 2-D Gaussian fit

@@ -159,8 +159,8 @@ def test_binned_median_falls_back_to_exact(ctx, dtype):
     """sigma * 2 < 1e-4: the binned median is not defined and the exact median is taken (the device flags
     it and the call runs the exact path); labels, islands and statistics as the oracle's."""
     rng = np.random.default_rng(4)
-    img = (1.0 + 1e-6 * rng.normal(size=(128, 96))).astype(dtype)
-    img[40:44, 50:53] = dtype(1.0 + 2e-5)
+    img = (1e-6 * rng.normal(size=(128, 96))).astype(dtype)  # zero mean: no cancellation in sum x^2 / n - mean^2
+    img[40:44, 50:53] = dtype(2e-5)
     ref = orc.source_find(img.astype(np.float64), 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True, 5)
     isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5)
     assert info.sigma * 2 < 1e-4
