@@ -851,6 +851,7 @@ struct FgSizes {
     __device__ __forceinline__ int np() const { return int(misc[0]); }
     __device__ __forceinline__ uint32_t nl() const { return min(misc[0] + misc[1], label_cap); }
     __device__ __forceinline__ uint32_t nfg() const { return min(misc[2], fg_cap); }
+    __device__ __forceinline__ bool capped() const { return misc[0] + misc[1] > label_cap || misc[2] > fg_cap; }
 };
 
 #define FG_LOOP(i, count)                                                                                            \
@@ -965,6 +966,10 @@ __global__ void k_fg_keys(FgSizes z, const SfStats* st, const uint32_t* fcode, c
     const unsigned long long* ext, unsigned long long* keys, uint32_t* count, int32_t* L)
 {
     const int np = z.np();
+    // over capacity the validity is not final (the host runs the stage
+    // again): the label map is left untouched until then
+    if (z.capped())
+        L = nullptr;
     FG_LOOP(i, z.nfg())
     {
         const uint32_t code = fcode[i];

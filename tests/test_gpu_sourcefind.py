@@ -169,6 +169,24 @@ def test_binned_median_falls_back_to_exact(ctx, dtype):
     assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
 
 
+def test_foreground_beyond_first_capacity():
+    """A 512^2 image with a low analysis threshold has about 200 k foreground pixels, beyond the
+    label-analysis capacity a fresh context starts with (n / 16 entries, at least 131072): the first call runs
+    that stage again with larger buffers, the second uses the remembered capacity; both match the oracle."""
+    fresh = capi.Context(0)
+    rng = np.random.default_rng(17)
+    img = rng.normal(size=(512, 512))
+    ref = orc.source_find(img, 3.0, 0.3, 1.0, True, 5, orc.ZEROMEDIAN, False, False, True, 3, 0)
+    try:
+        for _ in range(2):
+            isl, lab, info = fresh.source_find(img, 3.0, 0.3, 1.0, True, 5, capi.ZEROMEDIAN, False, False, True, 3,
+                                               0)
+            assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
+            _compare(isl, ref, lab, ref.label_map)
+    finally:
+        fresh.close()
+
+
 def test_source_find_rejects(ctx):
     with pytest.raises(capi.StpGpuError):
         ctx.source_find(np.zeros((7, 8)), 5, 3)
