@@ -2563,8 +2563,9 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += int64_t(s.nplanes) * (cs * cs * K * K * 2 * rb + lh * lh * 16 + 64 * 64 * 16);
     }
     b += rows * N * 2 * rb + N * N * rb + int64_t(image_size) * image_size * rb;
-    if (find_sources) // classes, parents, ranks, labels, foreground list; list arrays for every pixel at worst
-        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 24);
+    if (find_sources) // classes, parents, ranks, labels, foreground list; at worst list arrays (20 B) for every
+                      // pixel and per-label arrays (160 B) for every second pixel
+        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 20 + 80);
     return b + (int64_t(8) << 20);
 }
 
