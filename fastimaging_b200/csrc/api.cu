@@ -2551,12 +2551,12 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
     const int64_t rb = precision == STPGPU_FP64 ? 8 : 4;
     const int64_t N = s.N, rows = N / 2 + 1;
     const int conv = s.nplanes > 0 ? s.max_support : s.support;
-    int64_t b = n * ((vis_c64 ? 8 : 16) + 8 + 24) + n * (rb == 8 ? 40 : 28);
+    int64_t b = n * ((vis_c64 ? 8 : 16) + 8 + 24) + n * (rb == 8 ? 48 : 32); // items: 48 / 32 B records
     const int64_t per_dim = ceil_div(2 * conv, 16) + 2;
     b += std::max<int64_t>(n, 1) * 2 * per_dim * per_dim * 4; // tile-list capacity
     b += std::max<int64_t>(n, 1) * 2 * kRankSlots * 4;         // list slots kept by the count pass
     if (s.nplanes > 0) {
-        b += n * (rb == 8 ? 40 : 28); // items in |w| order
+        b += n * (rb == 8 ? 48 : 32); // items in |w| order
         const int64_t os = std::max(1, (s.os >> 1) << 1), cs = (os / 2) * 2 + 1, K = 2 * conv + 1;
         const int64_t lh = conv * os + os / 2 + 1;
         b += n * 41;                                                  // |w| sort, planes

@@ -28,15 +28,18 @@ enum KMode { KM_SEP = 0, KM_EXACT = 1, KM_WPROJ = 2 };
 // Per-visibility record written by the prepass.  flags: bit0 conj(kernel)
 // for the original item (w < 0), bit1 conj(kernel) for the mirrored item
 // (-w < 0).  The visibility is stored conjugated when the half-plane
-// conversion flipped it.
+// conversion flipped it.  16-byte aligned (32 B single, 48 B double
+// precision): a record never straddles a 32-byte sector more than it must,
+// and the gridder's random fetch of a record is two or three 16-byte loads.
 template <typename R>
-struct Item {
+struct alignas(16) Item {
     R vr, vi, w;
     int32_t gcx, gcy;
     int16_t cpx, cpy;
     uint16_t plane;
     uint8_t good, flags;
 };
+static_assert(sizeof(Item<float>) == 32 && sizeof(Item<double>) == 48, "item record sizes");
 
 struct PrepassParams {
     int64_t n;
