@@ -1044,27 +1044,27 @@ __global__ void __launch_bounds__(1024) k_sort_small(const unsigned long long* k
     // stay inside one warp's chunk of C keys and need only a warp barrier
     const uint32_t C = len >= 2048 ? len / 32 : (len >= 64 ? 64 : len);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    auto cx = [&](uint32_t t, uint32_t j, uint32_t k) {
-        const uint32_t u = t ^ j;
-        if (u > t) {
-            const unsigned long long a = sk[t], b = sk[u];
-            if ((a > b) == ((t & k) == 0)) {
-                sk[t] = b;
-                sk[u] = a;
-            }
+    // one thread per compare-exchange pair: pair q of distance j joins
+    // t = (q / j) * 2j + q % j and t + j
+    auto cx = [&](uint32_t q, uint32_t j, uint32_t k) {
+        const uint32_t t = ((q & ~(j - 1)) << 1) | (q & (j - 1)), u = t + j;
+        const unsigned long long a = sk[t], b = sk[u];
+        if ((a > b) == ((t & k) == 0)) {
+            sk[t] = b;
+            sk[u] = a;
         }
     };
     for (uint32_t k = 2; k <= len; k <<= 1)
         for (uint32_t j = k >> 1; j > 0; j >>= 1) {
             if (j >= C) {
                 __syncthreads();
-                for (uint32_t t = threadIdx.x; t < len; t += blockDim.x)
-                    cx(t, j, k);
+                for (uint32_t q = threadIdx.x; q < len / 2; q += blockDim.x)
+                    cx(q, j, k);
                 __syncthreads();
             } else {
                 if (warp * C < len)
-                    for (uint32_t t = warp * C + lane; t < warp * C + C; t += 32)
-                        cx(t, j, k);
+                    for (uint32_t q = warp * (C / 2) + lane; q < (warp + 1) * (C / 2); q += 32)
+                        cx(q, j, k);
                 __syncwarp();
             }
         }
