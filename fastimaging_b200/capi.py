@@ -59,7 +59,7 @@ class ImagerInfo(ctypes.Structure):
                 ("n_grid_items", ctypes.c_int64), ("padded_image_size", ctypes.c_int32),
                 ("image_size", ctypes.c_int32), ("num_wplanes", ctypes.c_int32),
                 ("max_plane_support", ctypes.c_int32), ("device_ms", ctypes.c_double),
-                ("phase_ms", ctypes.c_double * 4), ("n_launches", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("phase_ms", ctypes.c_double * 4), ("n_launches", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
 class Island(ctypes.Structure):

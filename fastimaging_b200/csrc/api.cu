@@ -334,6 +334,9 @@ struct ImagerSetup {
     const double* lha = nullptr;
     const double* pbcoefs = nullptr;
     int npbcoefs = 0;
+    // compensated FP32 only: grid cells stored in double and the c2r done in
+    // double precision (wide_fft_needed decides)
+    int wide_fft = 0;
 };
 
 // W-projection with a maximum support above 32: the W-kernel tables and tile
@@ -797,8 +800,11 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     g.d_nitems = toff + ntiles;
 
     // ---- tile gridding
-    C2* grid = c->buf<C2>("grid", size_t(image_rows) * N);
-    C2* beam = s.beam ? c->buf<C2>("beamgrid", size_t(image_rows) * N) : nullptr;
+    // a wide grid (compensated FP32 for a double-precision c2r) holds double2 cells
+    const int wide = (COMP == 1 && s.wide_fft) ? 1 : 0;
+    const size_t cells = size_t(image_rows) * N * (wide ? 2 : 1);
+    C2* grid = c->buf<C2>("grid", cells);
+    C2* beam = s.beam ? c->buf<C2>("beamgrid", cells) : nullptr;
     GridParams<R> gp {};
     gp.N = N;
     gp.image_rows = image_rows;
@@ -823,6 +829,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     gp.wk_off = wk_off;
     gp.grid = grid;
     gp.beam = beam;
+    gp.wide = wide;
     using A = Acc<R, COMP>;
     size_t smem = size_t(TILE_R) * tile_c * sizeof(A) * (s.beam ? 2 : 1);
     if (!wproj && !kernel_exact)
@@ -831,9 +838,9 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         fail(STPGPU_ERR_UNSUPPORTED, "kernel support > 127 is outside the GPU path");
     const int kind = (wproj && n > 0) ? GK_WPROJ : (kernel_exact ? GK_EXACT : (!wproj ? GK_SEP : GK_NONE));
     if (kind == GK_NONE) {
-        STPGPU_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(C2) * size_t(image_rows) * N, st));
+        STPGPU_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(C2) * cells, st));
         if (beam)
-            STPGPU_CUDA_TRY(cudaMemsetAsync(beam, 0, sizeof(C2) * size_t(image_rows) * N, st));
+            STPGPU_CUDA_TRY(cudaMemsetAsync(beam, 0, sizeof(C2) * cells, st));
     }
     if (defer) {
         defer->kind = kind;
@@ -966,6 +973,12 @@ template <typename R>
 void finish_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const GridOut& g,
     void* d_image, void* d_beam, int out_f32)
 {
+    if constexpr (sizeof(R) == 4) {
+        if (s.wide_fft) { // the gridder wrote double2 cells: Z2D + double normalisation
+            finish_imager<double>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+            return;
+        }
+    }
     cudaStream_t st = c->stream;
     const int N = s.N;
     R* img = c->buf<R>("fftimg", size_t(N) * N);
@@ -1017,17 +1030,80 @@ void finish_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int 
     }
 }
 
+// Compensated FP32 keeps the grid in double and runs the c2r in double
+// precision when the grid correction would amplify the single-precision
+// transform's rounding past the 1e-5 peak-relative bound.  Normalisation
+// divides pixel (i, j) by gcf[i] gcf[j] (imager.h:97-150), so an error that
+// the FP32 c2r leaves at about 4e-10 of the peak (measured on an 8192^2
+// PSWF image with analytic correction: 2.3e-5 of the peak at
+// 1/gcf_min^2 = 6.2e4, against 2.2e-6 for an FP32 grid transformed in
+// double) is multiplied by up to 1/gcf_min^2 over the output field.  Rule:
+// wide when 1/gcf_min^2 > 4096, i.e. an expected FP32-c2r error above about
+// 1.5e-6 of the peak.  GaussianSinc S=3 with the DFT correction (1/gcf_min^2
+// = 890) keeps the FP32 transform; PSWF (1.5e4 with the DFT correction at
+// S=3, 6.2e4 analytic) takes the wide one.  The gcf values are those of
+// k_imgdom_kernel (ImgDomKernel, conv_func.h:351-412) over the kept field.
+constexpr double kWideFftAmplification = 4096.0;
+
+bool wide_fft_rule(const ImagerSetup& s, int image_size, int correction)
+{
+    if (!correction)
+        return false;
+    const int N = s.N, centre = N / 2, hs = image_size / 2;
+    double gmin = 1e300;
+    if (s.analytic) {
+        for (int m = -hs; m < hs; m++)
+            gmin = std::min(gmin, std::fabs(gcf_value(s.kf, double(m) / centre)));
+    } else {
+        const int dmax = int(std::floor(s.trunc)) + 1;
+        const int dlo = -std::min(dmax, centre), dhi = std::min(dmax, N - centre - 1);
+        double ssum = 0.0;
+        for (int d = dlo; d <= dhi; d++)
+            ssum += kernel_value(s.kf, s.trunc, double(d));
+        const double kinv = ssum > 0.0 ? 1.0 / ssum : 1.0;
+        for (int m = 0; m <= hs; m++) {
+            double r = 0.0;
+            for (int d = dlo; d <= dhi; d++) {
+                const long long jm = (long long)(d < 0 ? d + N : d) * m % N;
+                r += kernel_value(s.kf, s.trunc, double(d)) * kinv * std::cos(2.0 * M_PI * double(jm) / double(N));
+            }
+            gmin = std::min(gmin, std::fabs(r));
+        }
+    }
+    return !(gmin > 0.0) || 1.0 / (gmin * gmin) > kWideFftAmplification;
+}
+
+// wide_fft_rule memoised for the process (the DFT form costs a few thousand
+// cosines per evaluation); used by the imaging calls and the server's
+// admission estimate
+bool wide_fft_needed(const ImagerSetup& s, int image_size, int correction)
+{
+    static std::mutex mu;
+    static std::map<std::string, bool> memo;
+    const std::string key = std::to_string(s.kf) + "/" + fkey(s.trunc) + "/" + std::to_string(s.N) + "/"
+        + std::to_string(s.analytic) + "/" + std::to_string(image_size) + "/" + std::to_string(correction);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = memo.find(key);
+    if (it != memo.end())
+        return it->second;
+    const bool wide = wide_fft_rule(s, image_size, correction);
+    memo[key] = wide;
+    return wide;
+}
+
 // stp::image_visibilities (imager.h:233-376) on device buffers.  The whole
 // pipeline is enqueued without a host round trip; the normalisation reads
 // the sampling total on the device, and the scalars are read back once at
 // the end (an empty result, imager.h:355, is reported then).
 template <typename R, int COMP>
-void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int correction, const void* d_vis,
+void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int correction, const void* d_vis,
     int vis_c64, const double* d_wts, const double* d_uvw, int64_t n, void* d_image, void* d_beam, int out_f32,
     stpgpu_imager_info* info, bool graphable = false)
 {
-    if (image_size <= 0 || image_size > s.N || (image_size % 2) != 0)
+    if (image_size <= 0 || image_size > s_in.N || (image_size % 2) != 0)
         fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
+    ImagerSetup s = s_in;
+    s.wide_fft = (COMP == 1 && wide_fft_needed(s, image_size, correction)) ? 1 : 0;
     // tile width: the autotuned choice of this size class; the first call of
     // a class grids with both widths, times them, keeps the faster for later
     // calls (every pass produces the complete grid; the last one is used)
@@ -1161,6 +1237,7 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int cor
         info->padded_image_size = N;
         info->num_wplanes = s.nplanes;
         info->max_plane_support = sb.max_support;
+        info->flags = s.wide_fft ? 1 : 0;
         info->image_size = sb.total > 0.0 ? image_size : 0;
         if (c->timing) {
             float ms[4] = { 0, 0, 0, 0 };
@@ -1528,6 +1605,8 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         if (x.vis_dtype != STPGPU_C128 && x.vis_dtype != STPGPU_C64)
             fail(STPGPU_ERR_INVALID_ARG, "snapshot " + std::to_string(i) + ": vis_dtype");
         b.correction = x.pars.gridding_correction;
+        if (precision == STPGPU_FP32C)
+            b.s.wide_fft = wide_fft_needed(b.s, b.image_size, b.correction) ? 1 : 0;
         b.vis = x.vis;
         b.c64 = x.vis_dtype == STPGPU_C64;
         b.wts = x.weights;
@@ -1700,6 +1779,7 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             f.num_wplanes = B[i].s.nplanes;
             f.max_plane_support = scal[i].max_support;
             f.image_size = scal[i].total > 0.0 ? B[i].image_size : 0;
+            f.flags = B[i].s.wide_fft ? 1 : 0;
         }
     }
     if (bi) {
@@ -2546,7 +2626,8 @@ struct ServerJob {
 
 // Device working set of one request (inputs, items, tile lists, W-planes and
 // W-kernel tables, grid, FFT output, image, source-finder arrays), bytes.
-int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c64, int precision, int find_sources)
+int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c64, int precision, int find_sources,
+    int correction)
 {
     const int64_t rb = precision == STPGPU_FP64 ? 8 : 4;
     const int64_t N = s.N, rows = N / 2 + 1;
@@ -2563,6 +2644,8 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += int64_t(s.nplanes) * (cs * cs * K * K * 2 * rb + lh * lh * 16 + 64 * 64 * 16);
     }
     b += rows * N * 2 * rb + N * N * rb + int64_t(image_size) * image_size * rb;
+    if (precision == STPGPU_FP32C && wide_fft_needed(s, image_size, correction))
+        b += rows * N * 2 * rb + N * N * rb; // double-precision grid and c2r output
     if (find_sources) // classes, parents, ranks, labels, foreground list; at worst list arrays (20 B) for every
                       // pixel and per-label arrays (160 B) for every second pixel
         b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 20 + 80);
@@ -2778,7 +2861,8 @@ stpgpu_status check_request(const stpgpu_server* sv, const stpgpu_request* r, in
             return STPGPU_ERR_INVALID_ARG;
         if (r->find_sources && (r->island_capacity < 0 || (r->island_capacity > 0 && !r->islands)))
             return STPGPU_ERR_INVALID_ARG;
-        est = request_bytes(s, image_size, r->n_vis, r->vis_dtype == STPGPU_C64, sv->pars.precision, r->find_sources);
+        est = request_bytes(s, image_size, r->n_vis, r->vis_dtype == STPGPU_C64, sv->pars.precision, r->find_sources,
+            r->pars.gridding_correction);
     } catch (const Error& e) {
         return e.status;
     }

@@ -134,6 +134,39 @@ __host__ __device__ inline double gcf_value(int kf, double r)
     }
 }
 
+// Bessel function of the first kind, order 1, as the reference evaluates it
+// for its discrete Hankel transform (besselj1, src/stp/gridder/aw_projection.cpp:490-508):
+// the published rational approximation (Hart's coefficients, as tabulated in
+// Numerical Recipes' bessj1; about 1e-8 absolute accuracy) for x < 8, and
+// the asymptotic form sqrt(2/(pi x)) (P cos(x - 3pi/4) - z Q sin(x - 3pi/4)),
+// z = 8/x, above.  The coefficients must be the reference's for identical
+// W-kernels.  Arguments are >= 0 on this path.
+__host__ __device__ inline double besselj1_ref(double x)
+{
+    if (x < 8.0) {
+        const double num[6] = { 72362614232.0, -7895059235.0, 242396853.1, -2972611.439, 15704.48260, -30.16036606 };
+        const double den[6] = { 144725228442.0, 2300535178.0, 18583304.74, 99447.43394, 376.9991397, 1.0 };
+        const double xx = x * x;
+        double p = num[5], q = den[5];
+        for (int k = 4; k >= 0; k--) {
+            p = num[k] + xx * p;
+            q = den[k] + xx * q;
+        }
+        return (x * p) / q;
+    }
+    const double a[5] = { 1.0, 0.183105e-2, -0.3516396496e-4, 0.2457520174e-5, -0.240337019e-6 };
+    const double b[5] = { 0.04687499995, -0.2002690873e-3, 0.8449199096e-5, -0.88228987e-6, 0.105787412e-6 };
+    const double z = 8.0 / x;
+    const double zz = z * z;
+    const double y = x - 2.356194491;
+    double p = a[4], q = b[4];
+    for (int k = 3; k >= 0; k--) {
+        p = a[k] + zz * p;
+        q = b[k] + zz * q;
+    }
+    return sqrt(0.636619772 / x) * (cos(y) * p - z * sin(y) * q);
+}
+
 // Maximum radius (in pixels) beyond which every functor is exactly zero.
 __host__ __device__ inline double kernel_zero_beyond(int kf, double trunc) { return trunc; }
 

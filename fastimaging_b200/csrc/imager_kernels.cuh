@@ -597,6 +597,21 @@ struct Cplx<float> {
     using T = float2;
 };
 
+// Store of one finished cell: the accumulator's value in the grid's
+// precision, or (compensated FP32 into a wide grid) sum + error in double.
+template <typename R, int COMP>
+__device__ __forceinline__ void cell_store(typename Cplx<R>::T* g, size_t i, const Acc<R, COMP>& a, int wide)
+{
+    if constexpr (COMP == 1) {
+        if (wide) {
+            reinterpret_cast<double2*>(g)[i]
+                = make_double2(double(a.s.x) + double(a.c.x), double(a.s.y) + double(a.c.y));
+            return;
+        }
+    }
+    g[i] = acc_value(a);
+}
+
 // ---------------------------------------------------------------- gridder
 
 template <typename R>
@@ -627,6 +642,9 @@ struct GridParams {
     const uint32_t* wk_off;
     typename Cplx<R>::T* grid; // image_rows x N column-major
     typename Cplx<R>::T* beam; // nullable
+    // compensated FP32 only: grid and beam hold double2 cells (sum + error
+    // term carried into double) for a double-precision c2r transform
+    int wide;
 };
 
 // One warp per 32x32 tile of the (half-plane) grid.  Lanes take 32 items of
@@ -894,9 +912,9 @@ __device__ __forceinline__ void grid_tile(const GridParams<R>& p, int tile, unsi
         const int rl = q % TILE_R, cl = q / TILE_R;
         if (rl < nr && cl < nc) {
             const size_t g = size_t(c0 + cl) * grows + (r0 + rl);
-            p.grid[g] = acc_value(acc[q]);
+            cell_store<R, COMP>(p.grid, g, acc[q], p.wide);
             if (BEAM)
-                p.beam[g] = acc_value(bacc[q]);
+                cell_store<R, COMP>(p.beam, g, bacc[q], p.wide);
         }
     }
 }
@@ -1087,9 +1105,9 @@ __device__ __forceinline__ void grid_tile_cols(const GridParams<R>& p, int tile,
         const int rl = q % TILE_R, cl = q / TILE_R;
         if (rl < nr && cl < nc) {
             const size_t g = size_t(c0 + cl) * grows + (r0 + rl);
-            p.grid[g] = acc_value(acc[q]);
+            cell_store<R, COMP>(p.grid, g, acc[q], p.wide);
             if (BEAM)
-                p.beam[g] = acc_value(bacc[q]);
+                cell_store<R, COMP>(p.beam, g, bacc[q], p.wide);
         }
     }
 }
@@ -1239,9 +1257,9 @@ __device__ __forceinline__ void grid_tile_taps(const GridParams<R>& p, int tile,
         const int rl = q % TILE_R, cl = q / TILE_R;
         if (rl < nr && cl < nc) {
             const size_t g = size_t(c0 + cl) * grows + (r0 + rl);
-            p.grid[g] = acc_value(acc[q]);
+            cell_store<R, COMP>(p.grid, g, acc[q], p.wide);
             if (BEAM)
-                p.beam[g] = acc_value(bacc[q]);
+                cell_store<R, COMP>(p.beam, g, bacc[q], p.wide);
         }
     }
 }
@@ -2003,7 +2021,7 @@ __global__ void __launch_bounds__(1024) k_hankel_plane(WkParams q, HankelParams 
             double prev = 0.0;
             for (int j = 0; j < jmax; j++) {
                 const double rn = j == n - 1 ? double(n - 1) : double(j) + 0.5;
-                const double F = k == 0 ? kPi * rn * rn : kn * rn * j1(kk * rn);
+                const double F = k == 0 ? kPi * rn * rn : kn * rn * besselj1_ref(kk * rn);
                 const double d = j == 0 ? F : F - prev;
                 prev = F;
                 re += d * R[j].x;

@@ -51,8 +51,11 @@ typedef enum { STPGPU_ZEROMEDIAN = 0, STPGPU_BINMEDIAN, STPGPU_BINAPPROX, STPGPU
 /* Arithmetic of the imager.  FP64 is the plain form matched to the
  * reference's double build; FP32 uses single-precision visibilities, kernel
  * weights, grid and FFT; FP32C adds two-sum compensated accumulation of the
- * grid cells.  uvw -> pixel scaling, W-kernel generation and the final
- * normalisation stay FP64 in all modes. */
+ * grid cells, and stores the grid in double with a double-precision c2r
+ * when the grid correction amplifies the FFT's rounding by more than 4096
+ * (1/gcf_min^2 over the output field; e.g. PSWF kernels).  uvw -> pixel
+ * scaling, W-kernel generation and the final normalisation stay FP64 in all
+ * modes. */
 typedef enum { STPGPU_FP64 = 0, STPGPU_FP32 = 1, STPGPU_FP32C = 2 } stpgpu_precision;
 
 typedef enum { STPGPU_C128 = 0, STPGPU_C64 = 1 } stpgpu_vis_dtype;
@@ -128,7 +131,11 @@ typedef struct {
      * [1] grid loop (the tile gridder kernel), [2] FFT, [3] normalise. */
     double phase_ms[4];
     int32_t n_launches; /* kernels of this library the call ran, graph replays included (cuFFT's excluded) */
-    int32_t reserved;
+    /* bit 0: the compensated-FP32 call kept its grid in double and ran the
+     * c2r in double precision, because the grid correction amplifies the
+     * single-precision transform's rounding by 1/gcf_min^2 > 4096 over the
+     * output field */
+    int32_t flags;
 } stpgpu_imager_info;
 
 /* One island, stp::IslandParams (src/stp/sourcefind/sourcefind.h:63-133).
@@ -390,10 +397,18 @@ STPGPU_API stpgpu_status stpgpu_server_stats_get(stpgpu_server* server, stpgpu_s
  * ccl_slice_cols <= 0 selects max(2, cols / 8).  The call returns after the
  * labels are written.  The scratch array is shared by all calls on a device
  * and keeps the previous call's contents (each call clears what must start at
- * zero): calls whose work overlaps on the GPU race on it.  The first call on
- * a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.
- * err_msg (nullable) receives a message on failure. */
+ * zero): calls whose work overlaps on the GPU race on it.  The array
+ * (about 9 MiB) is committed on a device when this library's device code is
+ * loaded there: with CUDA's lazy loading that is the first launch of any of
+ * the library's kernels on that device, otherwise the first CUDA call of the
+ * process.  A caller that hands the rest of HBM to another allocator should
+ * make one small call first, so the array is in place.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current and keeps it for the life of the process; make that
+ * first call before any stream capture.  A cudaDeviceReset (or a reset of
+ * the primary context) unloads the module and leaves the kept address
+ * stale: a process that resets a device must not call this entry point on
+ * it afterwards.  err_msg (nullable) receives a message on failure. */
 #define STPGPU_NOALLOC_MAX_PIXELS (1024 * 1024)
 STPGPU_API stpgpu_status stpgpu_label_noalloc(int device, void* stream, const void* image, int image_dtype, int32_t rows,
     int32_t cols, double analysis_thresh_pos, double analysis_thresh_neg, int find_negative_sources, int ccl_4connectivity,

@@ -232,16 +232,51 @@ def wkernel_plane(w_value, aa, workarea, oversampling, cell_size_arcsec, scaling
     return support, cache
 
 
-def dht_matrix(n):
+def besselj1(x):
+    """The reference's order-1 Bessel function (besselj1,
+    aw_projection.cpp:490-508): a rational approximation for x < 8 and the
+    asymptotic form with z = 8/x above (the published Hart coefficients of
+    Numerical Recipes' bessj1, about 1e-8 absolute accuracy), Horner-evaluated
+    in the reference's order.  x >= 0."""
+    x = np.asarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    lo = x < 8.0
+    xl = x[lo]
+    xx = xl * xl
+    num = (72362614232.0, -7895059235.0, 242396853.1, -2972611.439, 15704.48260, -30.16036606)
+    den = (144725228442.0, 2300535178.0, 18583304.74, 99447.43394, 376.9991397, 1.0)
+    p = np.full_like(xl, num[5])
+    q = np.full_like(xl, den[5])
+    for k in range(4, -1, -1):
+        p = num[k] + xx * p
+        q = den[k] + xx * q
+    out[lo] = (xl * p) / q
+    xh = x[~lo]
+    a = (1.0, 0.183105e-2, -0.3516396496e-4, 0.2457520174e-5, -0.240337019e-6)
+    b = (0.04687499995, -0.2002690873e-3, 0.8449199096e-5, -0.88228987e-6, 0.105787412e-6)
+    z = 8.0 / xh
+    zz = z * z
+    y = xh - 2.356194491
+    p = np.full_like(xh, a[4])
+    q = np.full_like(xh, b[4])
+    for k in range(3, -1, -1):
+        p = a[k] + zz * p
+        q = b[k] + zz * q
+    out[~lo] = np.sqrt(0.636619772 / xh) * (np.cos(y) * p - z * np.sin(y) * q)
+    return out
+
+
+def dht_matrix(n, j1=None):
     """Discrete Hankel transform matrix, stored transposed: D[j, i] is the
     weight of radial sample j in output i (WideFieldImaging::dht,
     aw_projection.cpp:532-596).  Sample j covers the annulus [rn_{j-1}, rn_j]
     with rn_j = j + 1/2 (rn_{n-1} = n - 1); output i is the order-0 Hankel
     transform at k_i = pi i / n of the piecewise-constant profile:
     D[j, 0] = pi (rn_j^2 - rn_{j-1}^2), D[j, i] = F_i(j) - F_i(j-1) with
-    F_i(j) = (2 pi / k_i) rn_j J1(k_i rn_j).  J1 is scipy's Bessel function
-    (the reference evaluates a rational approximation good to about 1e-8)."""
-    from scipy.special import j1
+    F_i(j) = (2 pi / k_i) rn_j J1(k_i rn_j).  J1 is the reference's rational
+    approximation (besselj1 above) unless another function is given."""
+    if j1 is None:
+        j1 = besselj1
 
     idx = np.arange(n, dtype=np.float64)
     k = (np.pi / n) * idx

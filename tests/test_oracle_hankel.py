@@ -13,9 +13,19 @@ from scipy.special import j1
 from oracle import stp_oracle as orc
 
 
+def test_besselj1_approximation():
+    """The reference's rational J1 (aw_projection.cpp:490-508) stays within its
+    published accuracy of the exact Bessel function on both branches, and is
+    continuous enough at the branch point x = 8."""
+    x = np.concatenate([np.linspace(0.0, 8.0, 2001)[:-1], np.linspace(8.0, 400.0, 4001)])
+    assert np.max(np.abs(orc.besselj1(x) - j1(x))) < 2e-8
+    assert abs(orc.besselj1(np.array([8.0 - 1e-12]))[0] - orc.besselj1(np.array([8.0]))[0]) < 2e-8
+    assert orc.besselj1(np.array([0.0]))[0] == 0.0
+
+
 def test_dht_is_exact_for_a_disc():
     n = 64
-    D = orc.dht_matrix(n)
+    D = orc.dht_matrix(n, j1=j1)
     m = 10
     f = np.zeros(n)
     f[:m + 1] = 1.0  # 1 on the annuli j <= m, i.e. a disc of radius m + 1/2
