@@ -143,6 +143,9 @@ struct stpgpu_context {
     void* pinned = nullptr;
     size_t pinned_cap = 0;
     std::map<std::string, std::string> memo_keys; // buffer name -> key of its current contents
+    // record capacity of the staged gridder per namespace and tile width
+    // (0: size from the counted total at the next call)
+    std::map<std::string, uint64_t> rec_caps;
 
     // True when buffer `name` already holds the data described by `key`
     // (static tables: gcf, kernel tables, cos tables); records `key`.
@@ -392,16 +395,21 @@ struct GridLaunch {
 constexpr int kLayoutPersist = 1 << 8; // batch: persistent work queue
 constexpr int kLayoutCols = 1 << 9;    // column-packed tile gridder (grid_tile_cols)
 constexpr int kLayoutTaps = 1 << 10;   // lane-per-tap tile gridder (grid_tile_taps)
+constexpr int kLayoutRecs = 1 << 11;   // staged tile gridder over decoded records (grid_tile_recs)
 // gridder form of a layout: 0 lanes-per-item, 1 column-packed, 2 lane-per-tap
-inline int form_of(int lay) { return (lay & kLayoutCols) ? 1 : ((lay & kLayoutTaps) ? 2 : 0); }
+// (3: staged records)
+inline int form_of(int lay)
+{
+    return (lay & kLayoutRecs) ? 3 : ((lay & kLayoutCols) ? 1 : ((lay & kLayoutTaps) ? 2 : 0));
+}
 
 template <typename R, int COMP>
 GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, int vis_c64, const double* d_wts,
     const double* d_uv, int uv_is_pixels, int64_t n, int tile_c = TILE_C_DEFAULT, GridLaunch<R>* defer = nullptr,
     int form = 0)
 {
-    if (tile_c != 32 && tile_c != 16 && !(tile_c == 8 && form == 2))
-        fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32 (8 with the lane-per-tap gridder)");
+    if (tile_c != 32 && tile_c != 16 && !(tile_c == 8 && (form == 2 || form == 3)))
+        fail(STPGPU_ERR_INVALID_ARG, "tile width must be 16 or 32 (8 with the lane-per-tap or staged gridder)");
     using C2 = typename Cplx<R>::T;
     check_pars(s);
     cudaStream_t st = c->stream;
@@ -729,6 +737,21 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         g.nplanes = PT;
     }
 
+    const int kind = (wproj && n > 0) ? GK_WPROJ : (kernel_exact ? GK_EXACT : (!wproj ? GK_SEP : GK_NONE));
+    // the clipped forms need one footprint segment per axis and tile
+    const bool clip_ok = kind != GK_EXACT && N >= 2 * (2 * conv_support + 1 + 32) + 2;
+    // staged records: tabulated kernels, no beam (else the lane-per-tap form)
+    // and four warps' shared memory within the 227 KB of a block
+    const size_t rec_wb = sizeof(Acc<R, COMP>) * TILE_R * size_t(tile_c) + 2 * kRecChunk * sizeof(TapRec<R>) + 16
+        + (kind == GK_SEP ? sizeof(R) * size_t(cs) * size_t(2 * s.support + 1) : 0);
+    const bool use_recs = form == 3 && clip_ok && !s.beam && (kind == GK_WPROJ || kind == GK_SEP)
+        && 4 * (rec_wb + 15) <= 227 * 1024;
+    if (form == 3 && !use_recs)
+        form = 2;
+    // 8-column tiles exist for the clipped lane-per-tap and staged forms only
+    if (tile_c == 8 && !(clip_ok && (form == 2 || form == 3)))
+        tile_c = 16;
+
     // ---- binning into 32x32 uv tiles
     const int tiles_r = int(ceil_div(image_rows, TILE_R));
     const int tiles_c = int(ceil_div(N, tile_c));
@@ -741,7 +764,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     uint64_t cap = std::max<uint64_t>(1, uint64_t(nn) * 2 * per_dim * per_dim);
     if (!large_support(s) && cap > 0xffffffffull)
         fail(STPGPU_ERR_INVALID_ARG, "too many visibilities for one snapshot");
-    uint32_t* list = large_support(s) ? nullptr : c->buf<uint32_t>("tlist", cap);
+    uint32_t* list = (large_support(s) || use_recs) ? nullptr : c->buf<uint32_t>("tlist", cap);
     Item<R>* bin_items = items_sorted ? items_sorted : items;
     BinParams bp {};
     bp.N = N;
@@ -784,18 +807,46 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
             fail(STPGPU_ERR_CUDA, "tile offset scan failed");
         g_launches += 2;
     }
-    if (large_support(s)) { // size the list from the counted entries
-        uint32_t total = 0;
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(&total, toff + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-        cap = std::max<uint64_t>(total, 1);
-        list = c->buf<uint32_t>("tlist", cap);
-        bp.list = list;
-        bp.list_capacity = cap;
-    }
-    if (n > 0) {
-        k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first, nplanes);
-        STPGPU_CHECK_LAUNCH();
+    TapRec<R>* recs = nullptr;
+    uint64_t rec_cap = 0;
+    if (use_recs) {
+        // records sized from the counted total on the first call of this
+        // namespace and tile width (one host round trip), then from the
+        // remembered capacity; a call that exceeds it sets bit 8 and the
+        // caller grids again after a fresh count
+        uint64_t& rc = c->rec_caps[c->ns + "/" + std::to_string(tile_c)];
+        if (rc == 0 || large_support(s)) {
+            uint32_t total = 0;
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(&total, toff + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+            rc = std::max<uint64_t>(rc, uint64_t(total) + total / 4 + 1024);
+        }
+        rec_cap = rc;
+        recs = c->buf<TapRec<R>>("trecs", rc);
+        if (n > 0) {
+            RecFill<R> rf { recs, rc, wk_off, cs, os };
+            if (kind == GK_WPROJ)
+                k_fill_recs<R, KM_WPROJ><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first,
+                    nplanes, rf);
+            else
+                k_fill_recs<R, KM_SEP><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first,
+                    nplanes, rf);
+            STPGPU_CHECK_LAUNCH();
+        }
+    } else {
+        if (large_support(s)) { // size the list from the counted entries
+            uint32_t total = 0;
+            STPGPU_CUDA_TRY(cudaMemcpyAsync(&total, toff + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
+            cap = std::max<uint64_t>(total, 1);
+            list = c->buf<uint32_t>("tlist", cap);
+            bp.list = list;
+            bp.list_capacity = cap;
+        }
+        if (n > 0) {
+            k_fill_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first, nplanes);
+            STPGPU_CHECK_LAUNCH();
+        }
     }
     g.d_nitems = toff + ntiles;
 
@@ -827,6 +878,8 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     gp.plane_support = plane_support;
     gp.wk = wk;
     gp.wk_off = wk_off;
+    gp.recs = recs;
+    gp.rec_cap = rec_cap;
     gp.grid = grid;
     gp.beam = beam;
     gp.wide = wide;
@@ -836,7 +889,6 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         smem += sizeof(R) * size_t(cs) * (2 * s.support + 1);
     if (2 * conv_support + 1 > 255)
         fail(STPGPU_ERR_UNSUPPORTED, "kernel support > 127 is outside the GPU path");
-    const int kind = (wproj && n > 0) ? GK_WPROJ : (kernel_exact ? GK_EXACT : (!wproj ? GK_SEP : GK_NONE));
     if (kind == GK_NONE) {
         STPGPU_CUDA_TRY(cudaMemsetAsync(grid, 0, sizeof(C2) * cells, st));
         if (beam)
@@ -860,11 +912,35 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         };
         const bool b = s.beam != 0;
         const bool t32 = tile_c == 32;
-        // the column-packed and lane-per-tap gridders need one footprint
-        // segment per axis and tile
-        const bool clip_ok = kind != GK_EXACT && N >= 2 * (2 * conv_support + 1 + 32) + 2;
         const bool use_cols = form == 1 && clip_ok, use_taps = form == 2 && clip_ok;
-        if (use_cols && kind == GK_WPROJ)
+        if (use_recs) {
+            // four warps per block, each on its own tile
+            const int sep_len = kind == GK_SEP ? cs * (2 * s.support + 1) : 0;
+            auto launch_recs = [&](auto kern, size_t wb) {
+                const size_t bs = 4 * wb;
+                if (bs > 48 * 1024)
+                    STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bs)));
+                c->mark(1);
+                kern<<<unsigned((ntiles + 3) / 4), 128, bs, st>>>(gp, ntiles, int(wb), g.d_err);
+                STPGPU_CHECK_LAUNCH();
+                c->mark(2);
+            };
+            if (kind == GK_WPROJ) {
+                if (tile_c == 8)
+                    launch_recs(k_grid_tiles_recs<R, COMP, KM_WPROJ, 8, 4>, rec_warp_bytes<R, COMP, 8>(0));
+                else if (tile_c == 16)
+                    launch_recs(k_grid_tiles_recs<R, COMP, KM_WPROJ, 16, 4>, rec_warp_bytes<R, COMP, 16>(0));
+                else
+                    launch_recs(k_grid_tiles_recs<R, COMP, KM_WPROJ, 32, 4>, rec_warp_bytes<R, COMP, 32>(0));
+            } else {
+                if (tile_c == 8)
+                    launch_recs(k_grid_tiles_recs<R, COMP, KM_SEP, 8, 4>, rec_warp_bytes<R, COMP, 8>(sep_len));
+                else if (tile_c == 16)
+                    launch_recs(k_grid_tiles_recs<R, COMP, KM_SEP, 16, 4>, rec_warp_bytes<R, COMP, 16>(sep_len));
+                else
+                    launch_recs(k_grid_tiles_recs<R, COMP, KM_SEP, 32, 4>, rec_warp_bytes<R, COMP, 32>(sep_len));
+            }
+        } else if (use_cols && kind == GK_WPROJ)
             b ? (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, true, 16, 1>))
               : (t32 ? launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 32, 1>) : launch(k_grid_tiles<R, COMP, KM_WPROJ, false, 16, 1>));
         else if (use_cols)
@@ -932,8 +1008,10 @@ ScalarsBack read_back(stpgpu_context* c, const GridOut& g)
     STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
     ScalarsBack r { h->total, h->ngood, h->nitems, h->err, h->max_support };
     // bit 4: the 32-bit |w| sort met a long run of distinct |w| (the caller
-    // repeats the gridding with the 64-bit sort); other bits are errors
-    if (r.err & ~4u)
+    // repeats the gridding with the 64-bit sort); bit 8: the staged
+    // gridder's records exceeded their capacity (the caller grids again with
+    // the buffer sized from the count); other bits are errors
+    if (r.err & ~(4u | 8u))
         fail(STPGPU_ERR_DEVICE, "gridder reported internal error flags " + std::to_string(r.err));
     return r;
 }
@@ -1110,14 +1188,15 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
     const int precision = sizeof(R) == 8 ? STPGPU_FP64 : (COMP ? STPGPU_FP32C : STPGPU_FP32);
     const std::string cls = size_class(s, precision);
     GridOut g;
-    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c|32t|16t|8t pins the tile width and
-    // gridder form (c: column-packed, t: lane-per-tap) instead of the
-    // autotuner's choice
+    // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c|32t|16t|8t|32r|16r|8r pins the tile
+    // width and gridder form (c: column-packed, t: lane-per-tap, r: staged
+    // records) instead of the autotuner's choice
     if (const char* pin = std::getenv("STPGPU_GRIDDER_LAYOUT")) {
         const int w = std::atoi(pin);
-        if (w == 16 || w == 32 || (w == 8 && std::strchr(pin, 't')))
+        if (w == 16 || w == 32 || (w == 8 && (std::strchr(pin, 't') || std::strchr(pin, 'r'))))
             c->tune_set(cls,
-                w | (std::strchr(pin, 'c') ? kLayoutCols : 0) | (std::strchr(pin, 't') ? kLayoutTaps : 0));
+                w | (std::strchr(pin, 'c') ? kLayoutCols : 0) | (std::strchr(pin, 't') ? kLayoutTaps : 0)
+                    | (std::strchr(pin, 'r') ? kLayoutRecs : 0));
     }
     int tuned_lay = 0;
     const bool have_tune = c->tune_get(cls, tuned_lay);
@@ -1177,16 +1256,25 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
         // tiles) and fills the cached tables, so no timed pass pays that
         // the column-packed form is a candidate for large kernels only (with
         // K <= 17 the lane-per-item form is faster on every measured workload)
-        const int lays[7] = { 32, 16, 32 | kLayoutTaps, 16 | kLayoutTaps, 8 | kLayoutTaps, 32 | kLayoutCols,
-            16 | kLayoutCols };
-        float ms[7] = { 0.f, 0.f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f };
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, 16);
         // the widest kernel the data actually uses (W-planes are truncated
         // below the maximum support), read back from the untimed pass
         const int used_support = s.nplanes > 0 ? std::max(read_back(c, g).max_support, 0) : s.support;
         // the clipped forms need one footprint segment per axis and tile
         const bool clip_ok = !s.kernel_exact && s.N >= 2 * (2 * (s.nplanes > 0 ? s.max_support : s.support) + 33) + 2;
-        const int ncand = !clip_ok ? 2 : ((2 * used_support + 1) > 17 ? 7 : 5);
+        std::vector<int> lays = { 32, 16 };
+        if (clip_ok) {
+            for (int w : { 32 | kLayoutTaps, 16 | kLayoutTaps, 8 | kLayoutTaps })
+                lays.push_back(w);
+            if (2 * used_support + 1 > 17)
+                for (int w : { 32 | kLayoutCols, 16 | kLayoutCols })
+                    lays.push_back(w);
+            if (!s.beam)
+                for (int w : { 32 | kLayoutRecs, 16 | kLayoutRecs, 8 | kLayoutRecs })
+                    lays.push_back(w);
+        }
+        const int ncand = int(lays.size());
+        std::vector<float> ms(size_t(ncand), 1e30f);
         // each candidate timed twice, the faster pass kept (single passes
         // of close candidates swap order from run to run)
         for (int rep = 0; rep < 2; rep++)
@@ -1198,20 +1286,23 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
                 STPGPU_CUDA_TRY(cudaEventSynchronize(c->tev[1]));
                 float t = 0.f;
                 STPGPU_CUDA_TRY(cudaEventElapsedTime(&t, c->tev[0], c->tev[1]));
-                ms[k] = rep == 0 ? t : std::min(ms[k], t);
+                ms[k] = std::min(ms[k], t);
             }
         int best = 0;
         for (int k = 1; k < ncand; k++)
             if (ms[k] < ms[best])
                 best = k;
         c->tune_set(cls, lays[best]);
-        if (std::getenv("STPGPU_LOG_TUNING"))
-            std::fprintf(stderr,
-                "stpgpu gridder tuner: %s  lanes-per-item 32/16 cols %.3f/%.3f ms, lane-per-tap 32/16/8 %.3f/%.3f/%.3f"
-                " ms, column-packed 32/16 %.3f/%.3f ms -> %d%s (single call)\n",
-                cls.c_str(), double(ms[0]), double(ms[1]), double(ms[2]), double(ms[3]), double(ms[4]),
-                double(ms[5]), double(ms[6]), lays[best] & 0xff,
-                (lays[best] & kLayoutCols) ? " column-packed" : ((lays[best] & kLayoutTaps) ? " lane-per-tap" : ""));
+        if (std::getenv("STPGPU_LOG_TUNING")) {
+            std::string line;
+            for (int k = 0; k < ncand; k++) {
+                const int f = form_of(lays[k]);
+                line += " " + std::to_string(lays[k] & 0xff)
+                    + (f == 1 ? "c" : (f == 2 ? "t" : (f == 3 ? "r" : ""))) + " " + std::to_string(ms[k]);
+            }
+            std::fprintf(stderr, "stpgpu gridder tuner: %s (layout ms):%s -> candidate %d (single call)\n", cls.c_str(),
+                line.c_str(), best);
+        }
     }
     if (!(repeat && c->single_exec))
         finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
@@ -1219,6 +1310,19 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
         c->single_sig = sig;
     const int N = s.N;
     ScalarsBack sb = read_back(c, g);
+    if (sb.err & 8u) {
+        // records outgrew the remembered capacity: size them from a fresh
+        // count (the next run_gridder reads the total) and grid again
+        for (auto& kv : c->rec_caps)
+            if (kv.first.compare(0, c->ns.size() + 1, c->ns + "/") == 0)
+                kv.second = 0;
+        c->drop_single();
+        int lay = TILE_C_DEFAULT;
+        c->tune_get(cls, lay);
+        g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr, form_of(lay));
+        finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+        sb = read_back(c, g);
+    }
     if ((sb.err & 4u) && !s.full_wsort) {
         // rare data (many distinct |w| within one single-precision step): redo with the 64-bit |w| sort
         ImagerSetup s64 = s;

@@ -235,6 +235,31 @@ __device__ __forceinline__ int map_row(int raw, int N, int rows, bool wrap_neg)
 
 constexpr int kRankSlots = 4; // tiles per (item, mirror) whose list slots the count pass keeps
 
+// One (entry, tile) pair of the binning, decoded for the staged gridder
+// (grid_tile_recs): the entry's footprint clipped to the tile, the weighted
+// visibility and the kernel-table offset of the window's first tap.  The
+// fill pass writes these records contiguously in tile order, so a tile's
+// entries are one contiguous byte range that the gridder copies into shared
+// memory with bulk (TMA) copies.  16 B in single precision, 32 B in double.
+//   geom: row0 (5 bits, local row of the window's first tap), col0 (5 bits),
+//         nrows (6 bits, 1..32), ncols (6 bits), conj (1 bit, W-kernel
+//         conjugated), K (8 bits, kernel width; the row stride of W-kernels)
+//   koff: W-projection: index of tap (ilo, jlo) in the expanded kernel
+//         tables; separable: (cpy*K + ilo) << 16 | (cpx*K + jlo)
+template <typename R>
+struct alignas(16) TapRec {
+    R vr, vi;
+    uint32_t koff;
+    uint32_t geom;
+};
+static_assert(sizeof(TapRec<float>) == 16 && sizeof(TapRec<double>) == 32, "tile record sizes");
+
+__host__ __device__ __forceinline__ uint32_t rec_geom(int row0, int col0, int nrows, int ncols, int conj, int K)
+{
+    return uint32_t(row0) | (uint32_t(col0) << 5) | (uint32_t(nrows) << 10) | (uint32_t(ncols) << 16)
+        | (uint32_t(conj & 1) << 22) | (uint32_t(K) << 23);
+}
+
 struct BinParams {
     int N, image_rows, tiles_r, tiles_c;
     int tile_c;              // tile width in grid columns (TILE_R rows per tile)
@@ -640,6 +665,10 @@ struct GridParams {
     // cached kernel (conv * inv, tap i*K + j) at wk + wk_off[plane] + (cpy*cs + cpx)*K*K
     const typename Cplx<R>::T* wk;
     const uint32_t* wk_off;
+    // staged form (grid_tile_recs): the decoded entries in tile order, and
+    // how many the buffer holds
+    const TapRec<R>* recs;
+    uint64_t rec_cap;
     typename Cplx<R>::T* grid; // image_rows x N column-major
     typename Cplx<R>::T* beam; // nullable
     // compensated FP32 only: grid and beam hold double2 cells (sum + error
@@ -1262,6 +1291,296 @@ __device__ __forceinline__ void grid_tile_taps(const GridParams<R>& p, int tile,
                 cell_store<R, COMP>(p.beam, g, bacc[q], p.wide);
         }
     }
+}
+
+// ---------------------------------------------------------------- staged gridder
+
+// Record fill: like k_fill_tiles, but each (entry, tile) pair is written as a
+// decoded TapRec at its slot of the tile's range (tile order), the footprint
+// already clipped to the tile (tile_span, as grid_tile_taps clips it).  Slots
+// beyond `cap` are not written and set bit 8 of *err (the caller grows the
+// buffer to the counted total and grids again).
+template <typename R>
+struct RecFill {
+    TapRec<R>* rec;
+    uint64_t cap;
+    const uint32_t* wk_off; // W-projection: table offset per plane (x time step)
+    int cs, os;
+};
+
+template <typename R, int KMODE>
+__global__ void k_fill_recs(BinParams p, Item<R>* items, const uint32_t* order, const int64_t* first, int P,
+    RecFill<R> q)
+{
+    const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= p.n)
+        return;
+    const Item<R> it = items[k];
+    if (!it.good)
+        return;
+    int S = p.support, plane = 0;
+    if (order) {
+        plane = plane_of(first, P, k);
+        if (p.ts_of)
+            plane = plane * p.ntimesteps + p.ts_of[order[k]];
+        S = p.plane_support[plane];
+        items[k].plane = uint16_t(plane);
+    }
+    const int K = 2 * S + 1;
+    const bool ranked = p.ranks && *p.rank_overflow == 0u;
+    for (int mir = 0; mir < int(it.good); mir++) {
+        int cx, cy;
+        item_centre(it, mir, p.N, cx, cy);
+        int cpx = it.cpx, cpy = it.cpy;
+        if (mir && q.os > 1) {
+            cpx = q.os - cpx;
+            cpy = q.os - cpy;
+        }
+        TapRec<R> r;
+        r.vr = it.vr * it.w;
+        r.vi = (mir ? -it.vi : it.vi) * it.w;
+        const int conj = KMODE == KM_WPROJ ? int((it.flags >> (mir ? 1 : 0)) & 1u) : 0;
+        const uint32_t kbase = KMODE == KM_WPROJ ? q.wk_off[plane] + uint32_t((cpy * q.cs + cpx) * K * K) : 0u;
+        const int rb = cy - S, cb = cx - S;
+        int qn = 0;
+        for_item_tiles(it, mir, S, p, [&](uint32_t t) {
+            const uint32_t slot = ranked ? p.ranks[size_t(qn * 2 + mir) * size_t(p.n) + size_t(k)]
+                                         : atomicAdd(&p.tile_cursor[t], 1u);
+            qn++;
+            const int r0 = int(t % uint32_t(p.tiles_r)) * TILE_R, c0 = int(t / uint32_t(p.tiles_r)) * p.tile_c;
+            int ilo, ihi, rsh, jlo, jhi, csh;
+            tile_span(rb, K, p.N, r0, TILE_R, p.image_rows, false, ilo, ihi, rsh);
+            tile_span(cb, K, p.N, c0, p.tile_c, p.N, true, jlo, jhi, csh);
+            int nrows = max(ihi - ilo, 0), ncols = max(jhi - jlo, 0);
+            if (nrows == 0 || ncols == 0)
+                nrows = ncols = 0;
+            const int row0 = nrows ? rb + rsh - r0 + ilo : 0;
+            const int col0 = ncols ? cb + csh - c0 + jlo : 0;
+            r.koff = KMODE == KM_WPROJ ? kbase + uint32_t(ilo * K + jlo)
+                                       : (uint32_t(cpy * K + ilo) << 16) | uint32_t(cpx * K + jlo);
+            r.geom = rec_geom(row0, col0, nrows, ncols, conj, K);
+            const uint64_t pos = uint64_t(p.tile_off[t]) + slot;
+            if (pos < q.cap)
+                q.rec[pos] = r;
+            else
+                atomicOr(p.err, 8u);
+        });
+    }
+}
+
+// Bulk (TMA) copies into shared memory completing on an mbarrier, and a
+// bounded wait for a barrier phase.
+constexpr int kRecChunk = 64;              // records per staged chunk (two chunks in flight per warp)
+constexpr uint32_t kWaitLimit = 1u << 22; // try_wait rounds before a wait gives up
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(1u) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// one arrival that expects `bytes`, then the copy that delivers them
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+{
+    const uint32_t a = smem_addr(bar);
+    for (uint32_t it = 0; it < kWaitLimit; it++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+// ceil(65536 / n), n = 1..32: (t * m) >> 16 == t / n for t < 1024
+__constant__ uint32_t c_div_magic[33] = { 0, 65536, 32768, 21846, 16384, 13108, 10923, 9363, 8192, 7282, 6554, 5958,
+    5462, 5042, 4682, 4370, 4096, 3856, 3641, 3450, 3277, 3121, 2979, 2850, 2731, 2622, 2521, 2428, 2341, 2260, 2185,
+    2115, 2048 };
+
+// Shared memory of one warp of the staged gridder: accumulators, two record
+// buffers, two barriers and the separable kernel table.
+template <typename R, int COMP, int TILE_C>
+__host__ __device__ constexpr size_t rec_warp_bytes(int sep_table_len)
+{
+    return ((sizeof(Acc<R, COMP>) * TILE_R * TILE_C + 2 * kRecChunk * sizeof(TapRec<R>) + 16
+                + sizeof(R) * size_t(sep_table_len))
+               + 15)
+        / 16 * 16;
+}
+
+// Staged tile gridder: one warp per tile.  The tile's records (k_fill_recs)
+// arrive in chunks of kRecChunk by bulk copies into two shared-memory
+// buffers (the next chunk is in flight while one is processed); the warp
+// takes the entries one at a time, each lane one tap of the entry's clipped
+// window (column-major, so consecutive lanes update consecutive cells: the
+// taps of one entry are distinct cells, entries are ordered by __syncwarp),
+// the record read from shared memory by all lanes at once.  Accumulation,
+// zeroing and the single coalesced store are those of grid_tile_taps.  A
+// barrier wait that gives up (never expected) sets bit 16 of *err, waits for
+// the copies still in flight and leaves the tile unwritten.
+template <typename R, int COMP, int KMODE, int TILE_C>
+__device__ __forceinline__ void grid_tile_recs(const GridParams<R>& p, int tile, unsigned char* smem_raw,
+    unsigned int* err)
+{
+    using A = Acc<R, COMP>;
+    using C2 = typename Cplx<R>::T;
+    A* acc = reinterpret_cast<A*>(smem_raw);
+    TapRec<R>* rbuf = reinterpret_cast<TapRec<R>*>(acc + TILE_R * TILE_C);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(rbuf + 2 * kRecChunk);
+    R* tab = reinterpret_cast<R*>(bar + 2);
+    const int lane = threadIdx.x & 31;
+    const int gN = p.N, grows = p.image_rows;
+    const int tr = tile % p.tiles_r, tc = tile / p.tiles_r;
+    const int r0 = tr * TILE_R, c0 = tc * TILE_C;
+    const uint32_t beg = p.tile_off[tile];
+    uint32_t cnt = p.tile_off[tile + 1] - beg;
+    if (uint64_t(beg) + cnt > p.rec_cap) { // the fill overflowed (bit 8 is set): copy nothing
+        cnt = 0;
+        if (lane == 0)
+            atomicOr(err, 8u);
+    }
+    const int nch = int((cnt + kRecChunk - 1) / kRecChunk);
+    auto issue = [&](int c) {
+        const uint32_t n = min(uint32_t(kRecChunk), cnt - uint32_t(c) * kRecChunk);
+        bulk_copy_g2s(rbuf + (c & 1) * kRecChunk, p.recs + beg + uint32_t(c) * kRecChunk,
+            n * uint32_t(sizeof(TapRec<R>)), &bar[c & 1]);
+    };
+    if (lane == 0) {
+        mbar_init(&bar[0]);
+        mbar_init(&bar[1]);
+        mbar_init_fence();
+        if (nch > 0)
+            issue(0);
+        if (nch > 1)
+            issue(1);
+    }
+    for (int t = lane; t < TILE_R * TILE_C; t += 32)
+        acc_zero(&acc[t]);
+    if (KMODE == KM_SEP) {
+        const int K = 2 * p.support + 1;
+        for (int t = lane; t < p.cs * K; t += 32)
+            tab[t] = p.k1d[t];
+    }
+    __syncwarp();
+    for (int c = 0; c < nch; c++) {
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar[c & 1], uint32_t(c >> 1) & 1u));
+        if (!ok) {
+            if (lane == 0) {
+                // record the failure, then wait (bounded again) for this
+                // chunk's copy and the other buffer's before leaving
+                atomicOr(err, 16u);
+                mbar_wait(&bar[c & 1], uint32_t(c >> 1) & 1u);
+                if (c + 1 < nch)
+                    mbar_wait(&bar[(c + 1) & 1], uint32_t((c + 1) >> 1) & 1u);
+            }
+            __syncwarp();
+            return;
+        }
+        const TapRec<R>* rb = rbuf + (c & 1) * kRecChunk;
+        const int ne = min(kRecChunk, int(cnt) - c * kRecChunk);
+        // tap t of an entry: its accumulator cell and weighted value
+        auto tap = [&](const TapRec<R>& r, int t, int& cell, R& re, R& im) {
+            const uint32_t g = r.geom;
+            const int nrows = int((g >> 10) & 63u);
+            const int dj = int((uint32_t(t) * c_div_magic[nrows]) >> 16);
+            const int di = t - dj * nrows;
+            R kr, ki;
+            if (KMODE == KM_WPROJ) {
+                const C2 v = __ldg(&p.wk[r.koff + uint32_t(di * int(g >> 23) + dj)]);
+                kr = v.x;
+                ki = ((g >> 22) & 1u) ? -v.y : v.y;
+            } else {
+                kr = tab[(r.koff >> 16) + uint32_t(di)] * tab[(r.koff & 0xffffu) + uint32_t(dj)];
+                ki = R(0);
+            }
+            re = r.vr * kr - r.vi * ki;
+            im = r.vr * ki + r.vi * kr;
+            cell = (int((g >> 5) & 31u) + dj) * TILE_R + int(g & 31u) + di;
+        };
+        auto ntaps = [](const TapRec<R>& r) { return int((r.geom >> 10) & 63u) * int((r.geom >> 16) & 63u); };
+        // two single-pass entries at a time where possible: both kernel
+        // loads in flight before either entry's cells are updated
+        for (int e = 0; e < ne;) {
+            const TapRec<R> ra = rb[e];
+            const int na = ntaps(ra);
+            if (na <= 32 && e + 1 < ne) {
+                const TapRec<R> rb2 = rb[e + 1];
+                const int nb = ntaps(rb2);
+                if (nb <= 32) {
+                    int ca = 0, cb = 0;
+                    R xa = R(0), ya = R(0), xb = R(0), yb = R(0);
+                    if (lane < na)
+                        tap(ra, lane, ca, xa, ya);
+                    if (lane < nb)
+                        tap(rb2, lane, cb, xb, yb);
+                    if (lane < na)
+                        acc_rmw(&acc[ca], xa, ya);
+                    __syncwarp();
+                    if (lane < nb)
+                        acc_rmw(&acc[cb], xb, yb);
+                    __syncwarp();
+                    e += 2;
+                    continue;
+                }
+            }
+            for (int t = lane; t < na; t += 32) {
+                int cell;
+                R re, im;
+                tap(ra, t, cell, re, im);
+                acc_rmw(&acc[cell], re, im);
+            }
+            __syncwarp();
+            e++;
+        }
+        if (lane == 0 && c + 2 < nch) {
+            // the buffer's records were read by every lane (ordered by the
+            // __syncwarp above) before the async proxy overwrites it
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            issue(c + 2);
+        }
+        __syncwarp();
+    }
+    const int nr = min(TILE_R, grows - r0);
+    const int nc = min(TILE_C, gN - c0);
+    for (int q = lane; q < TILE_R * TILE_C; q += 32) {
+        const int rl = q % TILE_R, cl = q / TILE_R;
+        if (rl < nr && cl < nc) {
+            cell_store<R, COMP>(p.grid, size_t(c0 + cl) * grows + (r0 + rl), acc[q], p.wide);
+        }
+    }
+}
+
+// Staged gridder with WPB warps per block, each on its own tile (tile
+// blockIdx.x * WPB + warp; its shared memory at warp * warp_bytes).
+template <typename R, int COMP, int KMODE, int TILE_C, int WPB>
+__global__ void __launch_bounds__(32 * WPB) k_grid_tiles_recs(GridParams<R> p, int ntiles, int warp_bytes,
+    unsigned int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5;
+    const int tile = int(blockIdx.x) * WPB + warp;
+    if (tile < ntiles)
+        grid_tile_recs<R, COMP, KMODE, TILE_C>(p, tile, smem_raw + size_t(warp) * size_t(warp_bytes), err);
 }
 
 // Lane-per-tap gridder with WPB warps per block, each on its own tile (tile

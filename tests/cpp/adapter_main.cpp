@@ -70,10 +70,10 @@ int main(int argc, char** argv)
         write_file(out + "_image.bin", iv_result.vis_grid.memptr(), iv_result.vis_grid.n_elem);
         write_file(out + "_beam.bin", iv_result.sampling_grid.memptr(), iv_result.sampling_grid.n_elem);
 
-        // the template path with a functor object, default W/A parameters
+        // the template path with a functor object (A-projection parameters defaulted)
         stp::ImagerPars ip2 = ip;
         ip2.generate_beam = false;
-        auto r = stp::image_visibilities(stp::GaussianSinc(double(iv[2])), vis, weights, uvw, ip2);
+        auto r = stp::image_visibilities(stp::GaussianSinc(double(iv[2])), vis, weights, uvw, ip2, wp);
         write_file(out + "_image_gs.bin", r.first.memptr(), r.first.n_elem);
         if (!r.second.is_empty())
             throw std::runtime_error("beam returned without generate_beam");

@@ -4,7 +4,7 @@ Reads the reference gtest sources as text (never compiles or runs them) and
 records the literal expected matrices/values with the parameters of each test.
 Run in a container that has the reference tree:
 
-    python tests/golden/make_reference_pins.py /root/reference
+    python tests/golden/make_reference_pins.py <path of the FastImaging source tree>
 
 The JSON is committed; nothing on the GPU side reads the reference tree.
 """
@@ -201,4 +201,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_reference_pins.py <path of the FastImaging source tree>")
+    main(sys.argv[1])

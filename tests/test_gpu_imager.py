@@ -219,14 +219,15 @@ def test_imager_aproj_device_pointers_and_fp32c(ctx):
     assert peak_rel(img32.astype(np.float64), ri) < 1e-5
 
 
-@pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal"])
+@pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal", "oversized_bucket"])
 def test_imager_wproj_near_tied_w(ctx, pattern):
     """|w| values that are equal in single precision but distinct in double
     (or exactly equal): the W-plane boundaries must follow the exact stable
     double order of the reference's sort.  Short runs are re-sorted after the
-    32-bit key sort; a long run of distinct values takes the 64-bit sort;
-    exactly equal values keep index order."""
-    s = _imager_case(35, 256, 4000, w_range=(-600.0, 600.0))
+    32-bit key sort; long runs of distinct values (200 of them, or 5000 within
+    one part in 1e6) take the 64-bit sort; exactly equal values keep index
+    order."""
+    s = _imager_case(35, 256, 6000 if pattern == "oversized_bucket" else 4000, w_range=(-600.0, 600.0))
     uvw = np.array(s.uvw, order="F")
     w = uvw[:, 2]
     rng = np.random.default_rng(7)
@@ -234,6 +235,10 @@ def test_imager_wproj_near_tied_w(ctx, pattern):
     if pattern == "short_runs":
         for k in range(0, w.size - 1, 2):  # |w| of the pair one double step apart
             w[k + 1] = np.copysign(np.nextafter(abs(w[k]), np.inf), w[k + 1])
+    elif pattern == "oversized_bucket":
+        # 5000 distinct |w| within one part in 1e6: runs of hundreds per single-precision key
+        mags = 300.0 * (1.0 + rng.permutation(5000) * 1e-10)
+        w[:5000] = np.where(rng.random(5000) < 0.5, mags, -mags)
     else:
         # a cluster placed across the first plane boundary
         aw = np.sort(np.abs(w))
@@ -333,7 +338,7 @@ def test_repeated_device_calls_replay_graph_with_new_data(ctx):
         c2.close()
 
 
-@pytest.mark.parametrize("layout", ["32", "16", "32c", "16c", "32t", "16t", "8t"])
+@pytest.mark.parametrize("layout", ["32", "16", "32c", "16c", "32t", "16t", "8t", "32r", "16r", "8r"])
 @pytest.mark.parametrize("wproj", [False, True])
 def test_imager_every_gridder_layout_vs_oracle(layout, wproj, monkeypatch):
     """Each tile width and gridder form the autotuner may pick gives the oracle's image (FP64 1e-10,

@@ -134,6 +134,25 @@ def test_crowded_field(ctx, dtype):
         _compare(isl, ref, lab, ref.label_map)
 
 
+@pytest.mark.parametrize("step", [44, 36])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_medium_field_one_block_sort(ctx, step, dtype):
+    """Between 2048 and 8192 valid island pixels (about 5.2k and 7.8k here): the one-block label sort in
+    the regime where each warp handles len/32 > 64 entries of the bitonic network; labels and islands as
+    the oracle's."""
+    rng = np.random.default_rng(10)
+    img = rng.normal(size=(384, 384))
+    for r in range(2, 384 - 10, step):
+        for c in range(2, 384 - 10, step):
+            img[r:r + 8, c:c + 8] += 6.0 + rng.uniform(0, 4)
+    img = img.astype(dtype)
+    ref = orc.source_find(img.astype(np.float64), 4.0, 2.5, 1.0, True, 5, orc.ZEROMEDIAN, False, False, True, 3, 0)
+    assert 2048 < sum(i[4] for i in ref.islands) <= 8192
+    isl, lab, info = ctx.source_find(img, 4.0, 2.5, 1.0, True, 5, capi.ZEROMEDIAN, False, False, True, 3, 0)
+    assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
+    _compare(isl, ref, lab, ref.label_map)
+
+
 @pytest.mark.parametrize("shape", [(130, 98), (98, 130)])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_rows_not_multiple_of_four(ctx, shape, dtype):
