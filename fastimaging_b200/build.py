@@ -5,6 +5,8 @@
                       cuFFT from the CUDA toolkit.
     stp_python*.so    pybind11 module mirroring the reference's stp_python
                       binding, calling the C ABI.
+    libstpgpu_peaks.so  FP32/FP64 FMA-throughput probe (the roofline's
+                      compute roof, used by bench.py).
 
 Run ``python -m fastimaging_b200.build`` (or ``__graft_entry__.build()``).
 Cross-compiles without a GPU.
@@ -73,9 +75,26 @@ def build_python(verbose=False, force=False):
     return out
 
 
+PEAKS = os.path.join(PKG, "libstpgpu_peaks.so")
+
+
+def build_peaks(verbose=False, force=False):
+    """FMA-throughput probe for the roofline's compute roof (bench.py)."""
+    src = os.path.join(CSRC, "peaks.cu")
+    if not force and not _newer(PEAKS, [src]):
+        return PEAKS
+    cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared",
+           "-cudart", "static", "-o", PEAKS, src]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return PEAKS
+
+
 def build(verbose=False, force=False):
     build_lib(verbose, force)
     build_python(verbose, force)
+    build_peaks(verbose, force)
 
 
 if __name__ == "__main__":

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <iterator>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -143,9 +144,9 @@ struct stpgpu_context {
     void* pinned = nullptr;
     size_t pinned_cap = 0;
     std::map<std::string, std::string> memo_keys; // buffer name -> key of its current contents
-    // record capacity of the staged gridder per namespace and tile width
-    // (0: size from the counted total at the next call)
-    std::map<std::string, uint64_t> rec_caps;
+    // staged gridder: records per visibility last counted, per namespace,
+    // tile width, support and truncation (absent: count at the next call)
+    std::map<std::string, double> rec_ratio;
 
     // True when buffer `name` already holds the data described by `key`
     // (static tables: gcf, kernel tables, cos tables); records `key`.
@@ -370,8 +371,10 @@ void check_pars(const ImagerSetup& s)
 std::string size_class(const ImagerSetup& s, int precision)
 {
     const int conv = s.nplanes > 0 ? s.max_support : s.support;
+    // W-projection: the truncation percentage decides the plane supports, so it is part of the class
     return "p" + std::to_string(precision) + "/k" + std::to_string(s.nplanes > 0 ? 2 : (s.kernel_exact ? 1 : 0))
-        + "/N" + std::to_string(s.N) + "/S" + std::to_string(conv) + "/os" + std::to_string(s.os);
+        + "/N" + std::to_string(s.N) + "/S" + std::to_string(conv) + "/os" + std::to_string(s.os)
+        + (s.nplanes > 0 ? "/t" + fkey(s.trunc_perc) : std::string());
 }
 
 // Gridder launch prepared by run_gridder when the caller launches it itself
@@ -810,21 +813,25 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     TapRec<R>* recs = nullptr;
     uint64_t rec_cap = 0;
     if (use_recs) {
-        // records sized from the counted total on the first call of this
-        // namespace and tile width (one host round trip), then from the
-        // remembered capacity; a call that exceeds it sets bit 8 and the
-        // caller grids again after a fresh count
-        uint64_t& rc = c->rec_caps[c->ns + "/" + std::to_string(tile_c)];
-        if (rc == 0 || large_support(s)) {
+        // records sized from the records per visibility counted on the first
+        // call of this namespace and class (one host round trip), scaled by
+        // the call's visibilities with a quarter spare; a call that exceeds
+        // the capacity sets bit 8 and the caller grids again after a fresh
+        // count
+        const std::string rkey = c->ns + "/" + std::to_string(tile_c) + "/S" + std::to_string(conv_support) + "/t"
+            + fkey(s.trunc_perc) + "/os" + std::to_string(os);
+        auto it = c->rec_ratio.find(rkey);
+        if (it == c->rec_ratio.end() || large_support(s)) {
             uint32_t total = 0;
             STPGPU_CUDA_TRY(cudaMemcpyAsync(&total, toff + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
-            rc = std::max<uint64_t>(rc, uint64_t(total) + total / 4 + 1024);
+            const double r = double(total) / double(nn);
+            it = c->rec_ratio.insert_or_assign(rkey, it == c->rec_ratio.end() ? r : std::max(r, it->second)).first;
         }
-        rec_cap = rc;
-        recs = c->buf<TapRec<R>>("trecs", rc);
+        rec_cap = uint64_t(std::ceil(double(nn) * it->second * 1.25)) + 1024;
+        recs = c->buf<TapRec<R>>("trecs", rec_cap);
         if (n > 0) {
-            RecFill<R> rf { recs, rc, wk_off, cs, os };
+            RecFill<R> rf { recs, rec_cap, wk_off, cs, os };
             if (kind == GK_WPROJ)
                 k_fill_recs<R, KM_WPROJ><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first,
                     nplanes, rf);
@@ -1313,9 +1320,8 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
     if (sb.err & 8u) {
         // records outgrew the remembered capacity: size them from a fresh
         // count (the next run_gridder reads the total) and grid again
-        for (auto& kv : c->rec_caps)
-            if (kv.first.compare(0, c->ns.size() + 1, c->ns + "/") == 0)
-                kv.second = 0;
+        for (auto it = c->rec_ratio.begin(); it != c->rec_ratio.end();)
+            it = it->first.compare(0, c->ns.size() + 1, c->ns + "/") == 0 ? c->rec_ratio.erase(it) : std::next(it);
         c->drop_single();
         int lay = TILE_C_DEFAULT;
         c->tune_get(cls, lay);

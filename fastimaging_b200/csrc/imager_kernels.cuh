@@ -1543,11 +1543,20 @@ __device__ __forceinline__ void grid_tile_recs(const GridParams<R>& p, int tile,
                     continue;
                 }
             }
-            for (int t = lane; t < na; t += 32) {
-                int cell;
-                R re, im;
-                tap(ra, t, cell, re, im);
-                acc_rmw(&acc[cell], re, im);
+            // an entry's taps are distinct cells: up to four passes' kernel
+            // loads are issued before their updates, with no ordering
+            // between the passes
+            for (int t0 = 0; t0 < na; t0 += 128) {
+                int cell[4];
+                R xr[4], yi[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (t0 + q * 32 + lane < na)
+                        tap(ra, t0 + q * 32 + lane, cell[q], xr[q], yi[q]);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (t0 + q * 32 + lane < na)
+                        acc_rmw(&acc[cell[q]], xr[q], yi[q]);
             }
             __syncwarp();
             e++;

@@ -8,8 +8,9 @@ namespace stpgpu {
 
 constexpr int SF_THREADS = 256;
 // Resident blocks per SM that the streaming statistics passes are built for
-// (<= 32 registers a thread) and launched with: one wave of 148 * 8 blocks.
-constexpr int SF_STREAM_BLOCKS = 8;
+// (<= 64 registers a thread: room for several wide loads in flight per
+// thread) and launched with: one wave of 148 * 4 blocks.
+constexpr int SF_STREAM_BLOCKS = 4;
 constexpr int BINS_N = 1000; // binapprox / binmedian bin count (matrix_math.cpp:54,339)
 constexpr uint32_t UF_MAX_STEPS = 1u << 26; // bound on union-find loops
 
@@ -52,7 +53,22 @@ __device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
     int64_t done = 0;
     if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
         const int64_t n4 = n / 4;
-        for (int64_t g = tid; g < n4; g += stride) {
+        // UNR groups of four loaded before any is used: several 16-byte
+        // loads in flight per thread (64 bytes single, 64 bytes double)
+        constexpr int UNR = sizeof(T) == 4 ? 4 : 2;
+        int64_t g = tid;
+        for (; g + (UNR - 1) * stride < n4; g += UNR * stride) {
+            T a[UNR][4];
+#pragma unroll
+            for (int u = 0; u < UNR; u++)
+                load4(x, g + u * stride, a[u]);
+#pragma unroll
+            for (int u = 0; u < UNR; u++)
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    f(a[u][k]);
+        }
+        for (; g < n4; g += stride) {
             T a[4];
             load4(x, g, a);
 #pragma unroll
