@@ -384,6 +384,7 @@ template <typename R>
 struct GridLaunch {
     int kind = GK_NONE;
     int beam = 0;
+    int form = 0; // gridder form the binning was built for (0 lanes-per-item, 2 lane-per-tap, 3 staged)
     int tile_c = TILE_C_DEFAULT;
     int ntiles = 0;
     size_t smem = 0;
@@ -887,6 +888,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     gp.wk_off = wk_off;
     gp.recs = recs;
     gp.rec_cap = rec_cap;
+    gp.err = g.d_err;
     gp.grid = grid;
     gp.beam = beam;
     gp.wide = wide;
@@ -904,9 +906,10 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     if (defer) {
         defer->kind = kind;
         defer->beam = s.beam ? 1 : 0;
+        defer->form = use_recs ? 3 : (form == 2 && clip_ok && kind != GK_EXACT ? 2 : 0);
         defer->tile_c = tile_c;
         defer->ntiles = kind == GK_NONE ? 0 : ntiles;
-        defer->smem = smem;
+        defer->smem = use_recs ? (rec_wb + 15) / 16 * 16 : smem;
         defer->gp = gp;
     } else if (kind != GK_NONE) {
         auto launch = [&](auto kern) {
@@ -928,7 +931,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
                 if (bs > 48 * 1024)
                     STPGPU_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bs)));
                 c->mark(1);
-                kern<<<unsigned((ntiles + 3) / 4), 128, bs, st>>>(gp, ntiles, int(wb), g.d_err);
+                kern<<<unsigned((ntiles + 3) / 4), 128, bs, st>>>(gp, ntiles, int(wb));
                 STPGPU_CHECK_LAUNCH();
                 c->mark(2);
             };
@@ -1461,7 +1464,9 @@ void apply_layout(BatchSnap& b, int lay)
     b.persist = (lay & kLayoutPersist) ? 1 : 0;
     const int conv = b.s.nplanes > 0 ? b.s.max_support : b.s.support;
     const bool clip_ok = !b.s.kernel_exact && b.s.N >= 2 * (2 * conv + 1 + 32) + 2;
-    b.form = ((lay & kLayoutTaps) && clip_ok) ? 2 : 0;
+    // the staged form: run_gridder falls back to the lane-per-tap form where
+    // it does not apply and reports the form it built in GridLaunch::form
+    b.form = ((lay & kLayoutRecs) && clip_ok) ? 3 : (((lay & kLayoutTaps) && clip_ok) ? 2 : 0);
 }
 
 void batch_streams(stpgpu_context* c)
@@ -1534,7 +1539,9 @@ void launch_mode_form(cudaStream_t st, int layout, size_t smem, const BatchGridP
 template <typename R, int COMP, int KMODE>
 void launch_mode(cudaStream_t st, int layout, size_t smem, const BatchGridParams<R>& P, uint32_t total, bool cap)
 {
-    if (KMODE != KM_EXACT && (layout & kLayoutTaps))
+    if (KMODE != KM_EXACT && (layout & kLayoutRecs))
+        launch_mode_form<R, COMP, KMODE, 3>(st, layout, smem, P, total, cap);
+    else if (KMODE != KM_EXACT && (layout & kLayoutTaps))
         launch_mode_form<R, COMP, KMODE, 2>(st, layout, smem, P, total, cap);
     else
         launch_mode_form<R, COMP, KMODE, 0>(st, layout, smem, P, total, cap);
@@ -1582,7 +1589,7 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
             const double* duvw = to_device<double>(c, "in_uvw", b.uvw, 3 * size_t(b.n));
             const size_t ob = (out_f32 ? 4 : 8) * size_t(b.image_size) * b.image_size;
             void* di = c->buf<unsigned char>("out_img", ob);
-            GridOut g = run_gridder<R, COMP>(c, b.s, dv, b.c64, dw, duvw, 0, b.n, b.tile_c);
+            GridOut g = run_gridder<R, COMP>(c, b.s, dv, b.c64, dw, duvw, 0, b.n, b.tile_c, nullptr, b.form);
             finish_imager<R>(c, b.s, b.image_size, b.correction, g, di, nullptr, out_f32);
             BatchScalars* ds = c->buf<BatchScalars>("scal", 1);
             k_collect_scalars<<<1, 1, 0, c->stream>>>(g.d_total, g.d_ngood, g.d_nitems, g.d_err,
@@ -1613,7 +1620,7 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
             duvw = to_device<double>(c, "in_uvw", b.uvw, 3 * size_t(b.n));
             dimg[i] = c->buf<unsigned char>("out_img", (out_f32 ? 4 : 8) * size_t(b.image_size) * b.image_size);
         }
-        G[i] = run_gridder<R, COMP>(c, b.s, dv, b.c64, dw, duvw, 0, b.n, b.tile_c, &L[i]);
+        G[i] = run_gridder<R, COMP>(c, b.s, dv, b.c64, dw, duvw, 0, b.n, b.tile_c, &L[i], b.form);
     }
     c->stream = main;
     c->ns = "batch/";
@@ -1625,7 +1632,7 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
         if (L[i].kind == GK_NONE || L[i].ntiles == 0)
             continue;
         std::string key = std::to_string(L[i].kind) + "/" + std::to_string(L[i].tile_c) + "/"
-            + std::to_string(B[i].persist) + "/" + std::to_string(B[i].form);
+            + std::to_string(B[i].persist) + "/" + std::to_string(L[i].form);
         if (class_ms)
             key += "|" + B[i].cls;
         groups[key].push_back(i);
@@ -1653,7 +1660,8 @@ int batch_enqueue(stpgpu_context* c, std::vector<BatchSnap>& B, int out_f32, int
                 STPGPU_CUDA_TRY(cudaEventRecord(c->pev[0], main));
             const GridLaunch<R>& l0 = L[all[c0]];
             launch_group<R, COMP>(main, l0.kind,
-                l0.tile_c | (B[all[c0]].persist ? kLayoutPersist : 0) | (B[all[c0]].form == 2 ? kLayoutTaps : 0),
+                l0.tile_c | (B[all[c0]].persist ? kLayoutPersist : 0) | (l0.form == 2 ? kLayoutTaps : 0)
+                    | (l0.form == 3 ? kLayoutRecs : 0),
                 smem, *P, tot, capturing);
             nlaunch++;
             if (class_ms) {
@@ -1790,9 +1798,10 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
             if (int v; !c->tune_get(b.cls, v) && std::find(fresh.begin(), fresh.end(), b.cls) == fresh.end())
                 fresh.push_back(b.cls);
         if (!fresh.empty()) {
-            constexpr int NC = 8;
+            constexpr int NC = 12;
             const int layouts[NC] = { 32, 16, 32 | kLayoutPersist, 16 | kLayoutPersist, 32 | kLayoutTaps,
-                16 | kLayoutTaps, 32 | kLayoutPersist | kLayoutTaps, 16 | kLayoutPersist | kLayoutTaps };
+                16 | kLayoutTaps, 32 | kLayoutPersist | kLayoutTaps, 16 | kLayoutPersist | kLayoutTaps, 32 | kLayoutRecs,
+                16 | kLayoutRecs, 32 | kLayoutPersist | kLayoutRecs, 16 | kLayoutPersist | kLayoutRecs };
             std::map<std::string, float> t[NC];
             for (int k = 0; k < 5; k++)
                 if (!c->pev[k])
@@ -1816,11 +1825,13 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
                 if (log_tuning)
                     std::fprintf(stderr,
                         "stpgpu gridder tuner: %s  32/16 cols %.3f/%.3f ms, persistent %.3f/%.3f ms, lane-per-tap"
-                        " %.3f/%.3f ms, lane-per-tap persistent %.3f/%.3f ms -> %d%s%s\n",
+                        " %.3f/%.3f ms, lane-per-tap persistent %.3f/%.3f ms, staged %.3f/%.3f ms, staged"
+                        " persistent %.3f/%.3f ms -> %d%s%s\n",
                         cls.c_str(), double(t[0][cls]), double(t[1][cls]), double(t[2][cls]), double(t[3][cls]),
                         double(t[4][cls]), double(t[5][cls]), double(t[6][cls]), double(t[7][cls]),
+                        double(t[8][cls]), double(t[9][cls]), double(t[10][cls]), double(t[11][cls]),
                         layouts[best] & 0xff, (layouts[best] & kLayoutPersist) ? " persistent" : "",
-                        (layouts[best] & kLayoutTaps) ? " lane-per-tap" : "");
+                        (layouts[best] & kLayoutRecs) ? " staged" : ((layouts[best] & kLayoutTaps) ? " lane-per-tap" : ""));
             }
             tuned = int(fresh.size());
         }

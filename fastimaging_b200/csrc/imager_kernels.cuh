@@ -669,6 +669,7 @@ struct GridParams {
     // how many the buffer holds
     const TapRec<R>* recs;
     uint64_t rec_cap;
+    unsigned int* err; // error flags of the call (staged form: bits 8 and 16)
     typename Cplx<R>::T* grid; // image_rows x N column-major
     typename Cplx<R>::T* beam; // nullable
     // compensated FP32 only: grid and beam hold double2 cells (sum + error
@@ -1439,9 +1440,9 @@ __host__ __device__ constexpr size_t rec_warp_bytes(int sep_table_len)
 // barrier wait that gives up (never expected) sets bit 16 of *err, waits for
 // the copies still in flight and leaves the tile unwritten.
 template <typename R, int COMP, int KMODE, int TILE_C>
-__device__ __forceinline__ void grid_tile_recs(const GridParams<R>& p, int tile, unsigned char* smem_raw,
-    unsigned int* err)
+__device__ __forceinline__ bool grid_tile_recs(const GridParams<R>& p, int tile, unsigned char* smem_raw)
 {
+    unsigned int* err = p.err;
     using A = Acc<R, COMP>;
     using C2 = typename Cplx<R>::T;
     A* acc = reinterpret_cast<A*>(smem_raw);
@@ -1494,7 +1495,7 @@ __device__ __forceinline__ void grid_tile_recs(const GridParams<R>& p, int tile,
                     mbar_wait(&bar[(c + 1) & 1], uint32_t((c + 1) >> 1) & 1u);
             }
             __syncwarp();
-            return;
+            return false;
         }
         const TapRec<R>* rb = rbuf + (c & 1) * kRecChunk;
         const int ne = min(kRecChunk, int(cnt) - c * kRecChunk);
@@ -1577,19 +1578,26 @@ __device__ __forceinline__ void grid_tile_recs(const GridParams<R>& p, int tile,
             cell_store<R, COMP>(p.grid, size_t(c0 + cl) * grows + (r0 + rl), acc[q], p.wide);
         }
     }
+    // every copy has completed: the barriers can be initialised again for
+    // the warp's next tile (persistent batch gridder)
+    if (lane == 0) {
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[0])) : "memory");
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&bar[1])) : "memory");
+    }
+    __syncwarp();
+    return true;
 }
 
 // Staged gridder with WPB warps per block, each on its own tile (tile
 // blockIdx.x * WPB + warp; its shared memory at warp * warp_bytes).
 template <typename R, int COMP, int KMODE, int TILE_C, int WPB>
-__global__ void __launch_bounds__(32 * WPB) k_grid_tiles_recs(GridParams<R> p, int ntiles, int warp_bytes,
-    unsigned int* err)
+__global__ void __launch_bounds__(32 * WPB) k_grid_tiles_recs(GridParams<R> p, int ntiles, int warp_bytes)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5;
     const int tile = int(blockIdx.x) * WPB + warp;
     if (tile < ntiles)
-        grid_tile_recs<R, COMP, KMODE, TILE_C>(p, tile, smem_raw + size_t(warp) * size_t(warp_bytes), err);
+        grid_tile_recs<R, COMP, KMODE, TILE_C>(p, tile, smem_raw + size_t(warp) * size_t(warp_bytes));
 }
 
 // Lane-per-tap gridder with WPB warps per block, each on its own tile (tile
@@ -1665,7 +1673,10 @@ __global__ void __launch_bounds__(32, TILE_C == 16 ? (sizeof(R) == 8 ? 24 : 28) 
                 hi = mid - 1;
         }
         __syncwarp();
-        if constexpr (FORM == 2 && KMODE != KM_EXACT)
+        if constexpr (FORM == 3 && KMODE != KM_EXACT && !BEAM) {
+            if (!grid_tile_recs<R, COMP, KMODE, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw))
+                break; // a staged copy's wait gave up (flagged): this warp stops
+        } else if constexpr (FORM == 2 && KMODE != KM_EXACT)
             grid_tile_taps<R, COMP, KMODE, BEAM, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw);
         else
             grid_tile<R, COMP, KMODE, BEAM, TILE_C>(P.ps[lo], int(w - P.tile_base[lo]), smem_raw);
