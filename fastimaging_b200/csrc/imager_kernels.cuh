@@ -1499,45 +1499,65 @@ __device__ __forceinline__ bool grid_tile_recs(const GridParams<R>& p, int tile,
         }
         const TapRec<R>* rb = rbuf + (c & 1) * kRecChunk;
         const int ne = min(kRecChunk, int(cnt) - c * kRecChunk);
-        // tap t of an entry: its accumulator cell and weighted value
-        auto tap = [&](const TapRec<R>& r, int t, int& cell, R& re, R& im) {
+        // an entry decoded once: window shape, divisor magic, first cell,
+        // kernel offsets and the weighted visibility
+        struct Ent {
+            int nrows, nt, sbase, K;
+            uint32_t m, koff, ky, kx;
+            bool conj;
+            R vr, vi;
+        };
+        auto decode = [&](const TapRec<R>& r) {
+            Ent x;
             const uint32_t g = r.geom;
-            const int nrows = int((g >> 10) & 63u);
-            const int dj = int((uint32_t(t) * c_div_magic[nrows]) >> 16);
-            const int di = t - dj * nrows;
+            x.nrows = int((g >> 10) & 63u);
+            x.nt = x.nrows * int((g >> 16) & 63u);
+            x.m = c_div_magic[x.nrows];
+            x.sbase = int((g >> 5) & 31u) * TILE_R + int(g & 31u);
+            x.K = int(g >> 23);
+            x.conj = (g >> 22) & 1u;
+            x.koff = r.koff;
+            x.ky = r.koff >> 16;
+            x.kx = r.koff & 0xffffu;
+            x.vr = r.vr;
+            x.vi = r.vi;
+            return x;
+        };
+        // tap t of an entry: its accumulator cell and weighted value
+        auto tap = [&](const Ent& x, int t, int& cell, R& re, R& im) {
+            const int dj = int((uint32_t(t) * x.m) >> 16);
+            const int di = t - dj * x.nrows;
             R kr, ki;
             if (KMODE == KM_WPROJ) {
-                const C2 v = __ldg(&p.wk[r.koff + uint32_t(di * int(g >> 23) + dj)]);
+                const C2 v = __ldg(&p.wk[x.koff + uint32_t(di * x.K + dj)]);
                 kr = v.x;
-                ki = ((g >> 22) & 1u) ? -v.y : v.y;
+                ki = x.conj ? -v.y : v.y;
             } else {
-                kr = tab[(r.koff >> 16) + uint32_t(di)] * tab[(r.koff & 0xffffu) + uint32_t(dj)];
+                kr = tab[x.ky + uint32_t(di)] * tab[x.kx + uint32_t(dj)];
                 ki = R(0);
             }
-            re = r.vr * kr - r.vi * ki;
-            im = r.vr * ki + r.vi * kr;
-            cell = (int((g >> 5) & 31u) + dj) * TILE_R + int(g & 31u) + di;
+            re = x.vr * kr - x.vi * ki;
+            im = x.vr * ki + x.vi * kr;
+            cell = x.sbase + dj * TILE_R + di;
         };
-        auto ntaps = [](const TapRec<R>& r) { return int((r.geom >> 10) & 63u) * int((r.geom >> 16) & 63u); };
         // two single-pass entries at a time where possible: both kernel
         // loads in flight before either entry's cells are updated
         for (int e = 0; e < ne;) {
-            const TapRec<R> ra = rb[e];
-            const int na = ntaps(ra);
-            if (na <= 32 && e + 1 < ne) {
-                const TapRec<R> rb2 = rb[e + 1];
-                const int nb = ntaps(rb2);
-                if (nb <= 32) {
+            const Ent ea = decode(rb[e]);
+            if (ea.nt <= 32 && e + 1 < ne) {
+                const Ent eb = decode(rb[e + 1]);
+                if (eb.nt <= 32) {
                     int ca = 0, cb = 0;
                     R xa = R(0), ya = R(0), xb = R(0), yb = R(0);
-                    if (lane < na)
-                        tap(ra, lane, ca, xa, ya);
-                    if (lane < nb)
-                        tap(rb2, lane, cb, xb, yb);
-                    if (lane < na)
+                    const bool ia = lane < ea.nt, ib = lane < eb.nt;
+                    if (ia)
+                        tap(ea, lane, ca, xa, ya);
+                    if (ib)
+                        tap(eb, lane, cb, xb, yb);
+                    if (ia)
                         acc_rmw(&acc[ca], xa, ya);
                     __syncwarp();
-                    if (lane < nb)
+                    if (ib)
                         acc_rmw(&acc[cb], xb, yb);
                     __syncwarp();
                     e += 2;
@@ -1547,16 +1567,19 @@ __device__ __forceinline__ bool grid_tile_recs(const GridParams<R>& p, int tile,
             // an entry's taps are distinct cells: up to four passes' kernel
             // loads are issued before their updates, with no ordering
             // between the passes
-            for (int t0 = 0; t0 < na; t0 += 128) {
+            for (int t0 = lane; t0 < ea.nt; t0 += 128) {
                 int cell[4];
                 R xr[4], yi[4];
+                bool in[4];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    in[q] = t0 + q * 32 < ea.nt;
+                    if (in[q])
+                        tap(ea, t0 + q * 32, cell[q], xr[q], yi[q]);
+                }
 #pragma unroll
                 for (int q = 0; q < 4; q++)
-                    if (t0 + q * 32 + lane < na)
-                        tap(ra, t0 + q * 32 + lane, cell[q], xr[q], yi[q]);
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (t0 + q * 32 + lane < na)
+                    if (in[q])
                         acc_rmw(&acc[cell[q]], xr[q], yi[q]);
             }
             __syncwarp();
