@@ -297,7 +297,8 @@ def run_gpu(args):
             traffic = json.load(open(tfile)).get(dom_name)
         except Exception:
             traffic = None
-    roofline = {"bound": "hbm", "kernel": "k_grid_tiles (grid_loop phase)", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+    roofline = {"bound": "hbm", "kernel": "tile gridder, autotuned form (grid_loop phase)", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "peak_source": peak_kind, "traffic": traffic,
                 "phase_ms": {k: round(float(v), 4) for k, v in zip(names, mean_ph)},
                 "algorithmic_bytes": alg[dom_name],
@@ -730,6 +731,51 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_calls(args):
+    """A few library calls and nothing else, for ncu captures: imaging calls of one workload, or
+    source-finder calls on the headline image (device pointers, no timing)."""
+    import numpy as np
+    import torch
+
+    from fastimaging_b200 import capi
+    from fastimaging_b200 import synthetic as syn
+
+    ctx = capi.Context(0)
+    try:
+        if args.section == "imager_call":
+            s = {1: syn.config1, 2: syn.config2, 3: syn.config3}[args.cfg]()
+            kw = dict({1: syn.CONFIG1_IMAGER, 2: syn.CONFIG2_IMAGER, 3: syn.CONFIG3_IMAGER}[args.cfg])
+            if args.trunc is not None:
+                kw["kernel_trunc_perc"] = args.trunc
+            prec = {"fp64": capi.FP64, "fp32": capi.FP32, "fp32c": capi.FP32C}[args.prec]
+            N = s.image_size
+            out = torch.empty(N * N, dtype=torch.float64 if prec == capi.FP64 else torch.float32, device="cuda")
+            dv = torch.from_numpy(s.vis).cuda()
+            dw = torch.from_numpy(s.weights).cuda()
+            duvw = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+            for _ in range(args.calls):
+                _, _, info = ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=prec,
+                                                    out_dtype=capi.F64 if prec == capi.FP64 else capi.F32,
+                                                    device_ptrs=True, image_out=out, **kw)
+            torch.cuda.synchronize()
+            print(json.dumps({"section": "imager_call", "cfg": args.cfg, "prec": args.prec,
+                              "n_grid_items": int(info.n_grid_items), "max_plane_support": int(info.max_plane_support),
+                              "flags": int(info.flags)}))
+        else:
+            s = syn.config2()
+            img, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 4096, s.cell_size, precision=capi.FP32C,
+                                               out_dtype=capi.F32, **syn.CONFIG2_IMAGER)
+            dimg = torch.from_numpy(np.asfortranarray(img).reshape(-1, order="F").copy()).cuda()
+            lab = torch.empty(4096 * 4096, dtype=torch.int32, device="cuda")
+            for _ in range(args.calls):
+                isl, _, info = ctx.source_find(dimg, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5,
+                                               device_ptrs=True, rows=4096, cols=4096, label_out=lab)
+            torch.cuda.synchronize()
+            print(json.dumps({"section": "sf_call", "islands": len(isl)}))
+    finally:
+        ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -739,10 +785,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
                     help="skip the batched, precision-study and serving sections")
-    ap.add_argument("--section", choices=["config1_sf"], default=None,
-                    help="run one section alone and print its JSON (config1_sf: the plain 2048^2 imager and the "
-                         "source finder), for profiling")
+    ap.add_argument("--section", choices=["config1_sf", "imager_call", "sf_call"], default=None,
+                    help="run one section alone, for profiling: config1_sf (the plain 2048^2 imager and the "
+                         "source finder, JSON), imager_call (--calls imaging calls of --cfg in --prec, device "
+                         "pointers), sf_call (--calls source-finder calls on the 4096^2 FP32 headline image)")
+    ap.add_argument("--cfg", type=int, choices=[1, 2, 3], default=2, help="imager_call: workload 1, 2 or 3")
+    ap.add_argument("--prec", choices=["fp64", "fp32", "fp32c"], default="fp32c", help="imager_call: precision")
+    ap.add_argument("--trunc", type=float, default=None, help="imager_call: W-kernel truncation percentage")
+    ap.add_argument("--calls", type=int, default=2, help="imager_call / sf_call: number of calls")
     args = ap.parse_args()
+    if args.section in ("imager_call", "sf_call"):
+        run_profile_calls(args)
+        return
     if args.section == "config1_sf":
         from fastimaging_b200 import capi
 
