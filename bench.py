@@ -687,6 +687,49 @@ def _cpu_one(snap, threads, fast=True):
     return time.perf_counter() - t0
 
 
+def _cpu_host():
+    """The host the CPU figures ran on: model name, logical CPUs, the affinity set used."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    aff = sorted(os.sched_getaffinity(0))
+    return {"cpu_model": model, "nproc": os.cpu_count(), "affinity_count": len(aff),
+            "affinity": f"{aff[0]}-{aff[-1]}" if aff and aff[-1] - aff[0] + 1 == len(aff) else ",".join(map(str, aff))}
+
+
+def _cpu_extra(threads):
+    """Further CPU-port figures on the same host: the plain 2048^2 imager (config 1) and the source finder
+    on serving-size images (the oracle port's labelling is serial, as the reference's merge step)."""
+    from fastimaging_b200 import synthetic as syn
+    from oracle import stp_oracle as orc
+
+    out = {}
+    s = syn.config1()
+    t0 = time.perf_counter()
+    img, _ = orc.image_visibilities(s.vis, s.weights, s.uvw, s.image_size, s.cell_size, threads=threads, fast=True,
+                                    **syn.CONFIG1_IMAGER)
+    dt = time.perf_counter() - t0
+    out["config1_plain_2048"] = {"Mvis_per_s": round(s.vis.size / dt / 1e6, 3), "s": round(dt, 3)}
+    for size, seed in ((2048, 51), (4096, 52)):
+        snap = syn.make_snapshot(seed, 300_000, size, 1.0, n_src=50, flux=(0.5, 10.0), noise_sigma=0.05,
+                                 w_range=(-500.0, 500.0), n_extended=5)
+        kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, gridding_correction=True,
+                  analytic_gcf=False, num_wplanes=16, max_wpconv_support=16, undersampling_opt=1,
+                  kernel_trunc_perc=1.0)
+        im, _ = orc.image_visibilities(snap.vis, snap.weights, snap.uvw, size, 1.0, threads=threads, fast=True, **kw)
+        t0 = time.perf_counter()
+        orc.source_find(im, 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True, 5)
+        dt = time.perf_counter() - t0
+        out[f"source_finder_{size}"] = {"Mpix_per_s": round(size * size / dt / 1e6, 2), "ms": round(dt * 1e3, 1)}
+    return out
+
+
 def cpu_baseline(args, snap, budget_s=20.0):
     threads = len(os.sched_getaffinity(0))
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
@@ -700,7 +743,8 @@ def cpu_baseline(args, snap, budget_s=20.0):
     v = n * len(times) / sum(times) / 1e6
     return {"value": round(v, 3), "unit": "Mvis/s", "cores": threads, "kind": "port",
             "sample": f"{len(times)} full config-2 snapshot(s) ({n} vis, 4096^2) through the CPU oracle port "
-                      f"(-O3 -ffast-math, OpenMP residue-partitioned gridder, scipy FFT workers={threads})"}
+                      f"(-O3 -ffast-math, OpenMP residue-partitioned gridder, scipy FFT workers={threads})",
+            "host": _cpu_host(), "other_workloads": _cpu_extra(threads)}
 
 
 def run_reference(args):
@@ -725,7 +769,8 @@ def run_reference(args):
         "impl": "reference",
         "cpu_baseline": {"value": round(v, 3), "unit": "Mvis/s", "cores": threads, "kind": "port",
                          "sample": f"{len(times)} full config-2 snapshot(s) through the CPU oracle port of the "
-                                   f"reference algorithm (reference C++ needs Armadillo/TBB, absent)"},
+                                   f"reference algorithm (reference C++ needs Armadillo/TBB, absent)",
+                         "host": _cpu_host()},
         "e2e": {"value": round(v, 3), "unit": "Mvis/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -1999,9 +1999,9 @@ void moments_fit(int sign, double extremum, const double* mb, double rms, double
     constrain(g);
 }
 
-// k_sort_small uses SORT_SMALL keys of dynamic shared memory (more than the
+// k_seg_sort_big uses SEG_BIG indices of dynamic shared memory (more than the
 // default 48 KB): raise its limit once per device.
-void set_sort_small_smem()
+void set_seg_sort_smem()
 {
     static std::atomic<uint64_t> done { 0 };
     int dev = 0;
@@ -2009,8 +2009,8 @@ void set_sort_small_smem()
     const uint64_t bit = uint64_t(1) << (dev & 63);
     if (done.load() & bit)
         return;
-    STPGPU_CUDA_TRY(cudaFuncSetAttribute(k_sort_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-        int(SORT_SMALL * sizeof(unsigned long long))));
+    STPGPU_CUDA_TRY(cudaFuncSetAttribute(k_seg_sort_big, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        int(SEG_BIG * sizeof(uint32_t))));
     done.fetch_or(bit);
 }
 
@@ -2019,6 +2019,7 @@ void set_sort_small_smem()
 struct SfState {
     uint32_t misc[8]; // CclBufs::misc, then the valid-label count [4] and the island count [5]
     unsigned int tickets[4];
+    uint32_t seg[3]; // label analysis: segment allocation cursor, labels with entries, labels for the one-block sort
     SfStats st;
     ClipState cs;
 };
@@ -2180,6 +2181,7 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     double* mom = nullptr;
     int* ns = nullptr;
     uint32_t *sb = nullptr, *se = nullptr, *sp = nullptr, *fcode = nullptr, *fm = nullptr, *v1 = nullptr;
+    uint32_t *cursor = nullptr, *slots = nullptr, *bigl = nullptr, *listed = nullptr;
     IslandRaw* raw = nullptr;
     auto size_buffers = [&] {
         // per label: extremum keys (single precision: value-and-index keys),
@@ -2197,6 +2199,10 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         fm = c->buf<uint32_t>("fg_m", fcap);
         vkeys = c->buf<unsigned long long>("fg_vkeys", fcap);
         v1 = c->buf<uint32_t>("fg_v1", fcap);
+        cursor = c->buf<uint32_t>("fg_cur", lcap);
+        slots = c->buf<uint32_t>("fg_slots", fcap);
+        bigl = c->buf<uint32_t>("fg_big", lcap);
+        listed = c->buf<uint32_t>("fg_listed", lcap);
     };
     auto moments_and_islands = [&](const FgSizes& z) {
         k_label_sums<T><<<G, 128, 0, st>>>(z, d_img, rows, cols, v1, sb, se, sp, mom, ns);
@@ -2214,15 +2220,21 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
             k_fg_extrema_idx<T><<<G, 256, 0, st>>>(z, &sfs->st, d_img, fcode, fm, ext, eidx);
             STPGPU_CHECK_LAUNCH();
         }
-        k_fg_keys<packed><<<G, 256, 0, st>>>(z, &sfs->st, fcode, fm, ext, vkeys, nvk, zero_map);
+        k_fg_keys<packed><<<G, 256, 0, st>>>(z, &sfs->st, fcode, fm, ext, vkeys, nvk, zero_map, se);
         STPGPU_CHECK_LAUNCH();
-        // ordered (deterministic) moments: the valid entries sorted by
-        // (label, list position) in one block (up to SORT_SMALL entries),
-        // segments, per-label sums in memory order; island records appended
-        // in any order
-        set_sort_small_smem();
-        k_sort_small<<<1, 1024, SORT_SMALL * sizeof(unsigned long long), st>>>(vkeys, nvk, fm, split_m, v1, sb, se, sp,
-            sort_overflow);
+        // ordered (deterministic) moments: each valid label's entries in a
+        // range of their own, ordered by list position (one warp per label,
+        // one block for the large ones), per-label sums in memory order;
+        // island records appended in any order
+        k_seg_alloc<<<G, 256, 0, st>>>(z, sb, se, cursor, &sfs->seg[0], listed);
+        STPGPU_CHECK_LAUNCH();
+        k_seg_scatter<<<G, 256, 0, st>>>(vkeys, nvk, cursor, slots);
+        STPGPU_CHECK_LAUNCH();
+        k_seg_sort<<<G, 256, 0, st>>>(listed, &sfs->seg[1], sb, se, slots, fm, split_m, v1, sp, bigl, &sfs->seg[2]);
+        STPGPU_CHECK_LAUNCH();
+        set_seg_sort_smem();
+        k_seg_sort_big<<<64, 1024, SEG_BIG * sizeof(uint32_t), st>>>(sb, se, slots, fm, split_m, v1, sp, bigl,
+            &sfs->seg[2], sort_overflow);
         STPGPU_CHECK_LAUNCH();
         moments_and_islands(z);
     };
@@ -2260,14 +2272,16 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         fcap = uint32_t(std::min<int64_t>(fcap, n));
         size_buffers();
         STPGPU_CUDA_TRY(cudaMemsetAsync(cb.misc + 4, 0, 4 * sizeof(uint32_t), st));
+        STPGPU_CUDA_TRY(cudaMemsetAsync(sfs->seg, 0, sizeof(sfs->seg), st));
         enqueue_analysis();
         read_back_state();
     }
     c->sf_label_cap = std::max<uint32_t>(c->sf_label_cap, lcap);
     c->sf_fg_cap = std::max<uint32_t>(c->sf_fg_cap, fcap);
     if (hstate->misc[7]) {
-        // more valid entries than the one-block sort holds: sort them with
-        // the multi-block sort, then sums and islands again
+        // a label with more valid entries than the one-block sort holds:
+        // sort all entries with the multi-block sort, then sums and islands
+        // again
         const uint32_t nv = hstate->misc[6];
         int end_bit = 33;
         while (end_bit < 64 && (uint64_t(1) << (end_bit - 32)) <= uint64_t(nl))

@@ -979,7 +979,7 @@ __global__ void k_fg_extrema_idx(FgSizes z, const SfStats* st, const T* img, con
 // compared with the detection keys.
 template <bool PACKED>
 __global__ void k_fg_keys(FgSizes z, const SfStats* st, const uint32_t* fcode, const uint32_t* fm,
-    const unsigned long long* ext, unsigned long long* keys, uint32_t* count, int32_t* L)
+    const unsigned long long* ext, unsigned long long* keys, uint32_t* count, int32_t* L, uint32_t* seg_count)
 {
     const int np = z.np();
     // over capacity the validity is not final (the host runs the stage
@@ -997,10 +997,12 @@ __global__ void k_fg_keys(FgSizes z, const SfStats* st, const uint32_t* fcode, c
             valid = uint32_t(ext[code] >> 32) != (pos ? st->fpos : st->fneg);
         else
             valid = pos ? ext[code] > st->kpos : ext[code] < st->kneg;
-        if (valid)
+        if (valid) {
             keys[atomicAdd(count, 1u)] = (unsigned long long)code << 32 | i;
-        else if (L)
+            atomicAdd(&seg_count[code], 1u); // the label's valid entries (k_seg_alloc)
+        } else if (L) {
             L[fm[i]] = 0;
+        }
     }
 }
 
@@ -1030,72 +1032,187 @@ __device__ __forceinline__ void seg_mark(const unsigned long long* k, uint32_t t
         seg_split[code] = t + 1;
 }
 
-// Up to SORT_SMALL valid entries: one block sorts the keys in shared memory
-// (bitonic network over the next power of two, padded with the largest key;
-// steps whose partners lie in one warp's chunk take only a warp barrier) and
-// marks the segments; more entries set *overflow and leave the work to the
-// multi-block sort.  (Keeping the keys in registers and exchanging them by
-// shuffles measured slower.)
-constexpr int SORT_SMALL = 8192;
-__global__ void __launch_bounds__(1024) k_sort_small(const unsigned long long* keys, const uint32_t* count,
-    const uint32_t* fm, uint32_t split_m, uint32_t* vals, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split,
-    uint32_t* overflow)
-{
-    extern __shared__ unsigned long long sk[]; // SORT_SMALL keys
-    const uint32_t cnt = *count;
-    if (cnt > uint32_t(SORT_SMALL)) {
-        if (threadIdx.x == 0)
-            *overflow = 1u;
-        return;
-    }
-    if (cnt == 0)
-        return;
-    uint32_t len = 1;
-    while (len < cnt)
-        len <<= 1;
-    for (uint32_t t = threadIdx.x; t < len; t += blockDim.x)
-        sk[t] = t < cnt ? keys[t] : ~0ull;
-    __syncthreads();
-    // compare-exchange steps with partner distance j below the chunk size C
-    // stay inside one warp's chunk of C keys and need only a warp barrier
-    const uint32_t C = len >= 2048 ? len / 32 : (len >= 64 ? 64 : len);
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // one thread per compare-exchange pair: pair q of distance j joins
-    // t = (q / j) * 2j + q % j and t + j
-    auto cx = [&](uint32_t q, uint32_t j, uint32_t k) {
-        const uint32_t t = ((q & ~(j - 1)) << 1) | (q & (j - 1)), u = t + j;
-        const unsigned long long a = sk[t], b = sk[u];
-        if ((a > b) == ((t & k) == 0)) {
-            sk[t] = b;
-            sk[u] = a;
-        }
-    };
-    for (uint32_t k = 2; k <= len; k <<= 1)
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            if (j >= C) {
-                __syncthreads();
-                for (uint32_t q = threadIdx.x; q < len / 2; q += blockDim.x)
-                    cx(q, j, k);
-                __syncthreads();
-            } else {
-                if (warp * C < len)
-                    for (uint32_t q = warp * (C / 2) + lane; q < (warp + 1) * (C / 2); q += 32)
-                        cx(q, j, k);
-                __syncwarp();
-            }
-        }
-    __syncthreads();
-    for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x)
-        seg_mark(sk, t, cnt, fm, split_m, vals, seg_begin, seg_end, seg_split);
-}
-
-// The same marking over keys sorted by the multi-block sort.
+// seg_mark over keys sorted by the multi-block sort (the fall-back for a
+// label above SEG_BIG valid entries).
 __global__ void k_seg_mark(const unsigned long long* keys, uint32_t cnt, const uint32_t* fm, uint32_t split_m,
     uint32_t* vals, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* seg_split)
 {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < cnt)
         seg_mark(keys, t, cnt, fm, split_m, vals, seg_begin, seg_end, seg_split);
+}
+
+// Segments without a global sort.  The segments of the valid labels need
+// not lie in label order (k_label_sums reads each label's own range), only
+// each segment's entries in list (scan) order.  k_seg_alloc turns the
+// per-label counts (in seg_end, from k_fg_keys) into ranges taken from an
+// atomic cursor; k_seg_scatter drops every valid entry into its label's
+// range; k_seg_sort orders each range by list position -- one warp per
+// label (shuffles up to 32 entries, the warp's shared memory up to
+// SEG_WARP), larger ranges queued for k_seg_sort_big (one block, up to
+// SEG_BIG), above that the flag for the host's multi-block sort -- and writes
+// the memory indices and the split point (the layout seg_mark gives the
+// multi-block sort's result).
+constexpr int SEG_WARP = 256;
+constexpr int SEG_BIG = 16384;
+
+// (the labels with entries are also listed, for k_seg_sort: alloc[1] of them)
+__global__ void k_seg_alloc(FgSizes z, uint32_t* seg_begin, uint32_t* seg_end, uint32_t* cursor, uint32_t* alloc,
+    uint32_t* listed)
+{
+    FG_LOOP(l, z.nl())
+    {
+        const uint32_t c = seg_end[l];
+        if (c == 0)
+            continue;
+        const uint32_t b = atomicAdd(&alloc[0], c);
+        seg_begin[l] = b;
+        seg_end[l] = b + c;
+        cursor[l] = b;
+        listed[atomicAdd(&alloc[1], 1u)] = l;
+    }
+}
+
+__global__ void k_seg_scatter(const unsigned long long* keys, const uint32_t* count, uint32_t* cursor, uint32_t* slots)
+{
+    FG_LOOP(t, *count)
+    {
+        const unsigned long long k = keys[t];
+        slots[atomicAdd(&cursor[uint32_t(k >> 32)], 1u)] = uint32_t(k);
+    }
+}
+
+// After the entries of range [b, e) are sorted in slots: memory indices and
+// the split (scan order visits memory columns >= cols/2 first: the range is
+// [high ..., low ...], split at the first low entry).
+__device__ __forceinline__ void seg_finish_warp(const uint32_t* slots, uint32_t b, uint32_t e, const uint32_t* fm,
+    uint32_t split_m, uint32_t* vals, uint32_t* split_out)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t high = 0;
+    for (uint32_t t = b + lane; t < e; t += 32) {
+        const uint32_t m = fm[slots[t]];
+        vals[t] = m;
+        high += m >= split_m ? 1u : 0u;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        high += __shfl_xor_sync(0xffffffffu, high, o);
+    if (lane == 0)
+        *split_out = b + high;
+}
+
+__global__ void __launch_bounds__(256) k_seg_sort(const uint32_t* listed, const uint32_t* nlisted,
+    const uint32_t* seg_begin, const uint32_t* seg_end, uint32_t* slots, const uint32_t* fm, uint32_t split_m,
+    uint32_t* vals, uint32_t* seg_split, uint32_t* big, uint32_t* nbig)
+{
+    __shared__ uint32_t buf[8][SEG_WARP];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    uint32_t* wb = buf[warp];
+    for (uint32_t q = blockIdx.x * (blockDim.x >> 5) + warp, nq = *nlisted; q < nq; q += nwarps) {
+        const uint32_t l = listed[q];
+        const uint32_t b = seg_begin[l], e = seg_end[l], c = e - b;
+        if (c == 0)
+            continue;
+        if (c > uint32_t(SEG_WARP)) {
+            if (lane == 0)
+                big[atomicAdd(nbig, 1u)] = l;
+            continue;
+        }
+        if (c <= 32) {
+            uint32_t v = uint32_t(lane) < c ? slots[b + lane] : 0xffffffffu;
+            for (int k = 2; k <= 32; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+                    const bool up = (lane & k) == 0, lower = (lane & j) == 0;
+                    v = (lower == up) ? min(v, o) : max(v, o);
+                }
+            if (uint32_t(lane) < c)
+                slots[b + lane] = v;
+        } else {
+            uint32_t p2 = 64;
+            while (p2 < c)
+                p2 <<= 1;
+            for (uint32_t t = lane; t < p2; t += 32)
+                wb[t] = t < c ? slots[b + t] : 0xffffffffu;
+            __syncwarp();
+            for (uint32_t k = 2; k <= p2; k <<= 1)
+                for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                    for (uint32_t q = lane; q < (p2 >> 1); q += 32) {
+                        const uint32_t lo = 2 * q - (q & (j - 1)), hi = lo + j;
+                        const uint32_t x = wb[lo], y = wb[hi];
+                        if ((x > y) == ((lo & k) == 0)) {
+                            wb[lo] = y;
+                            wb[hi] = x;
+                        }
+                    }
+                    __syncwarp();
+                }
+            for (uint32_t t = lane; t < c; t += 32)
+                slots[b + t] = wb[t];
+            __syncwarp();
+        }
+        seg_finish_warp(slots, b, e, fm, split_m, vals, &seg_split[l]);
+    }
+}
+
+// The ranges above SEG_WARP entries: one block each, up to SEG_BIG entries in
+// dynamic shared memory; larger ones set *overflow (the host sorts all the
+// entries with the multi-block sort instead).
+__global__ void __launch_bounds__(1024) k_seg_sort_big(const uint32_t* seg_begin, const uint32_t* seg_end,
+    uint32_t* slots, const uint32_t* fm, uint32_t split_m, uint32_t* vals, uint32_t* seg_split, const uint32_t* big,
+    const uint32_t* nbig, uint32_t* overflow)
+{
+    extern __shared__ uint32_t sb[]; // SEG_BIG
+    __shared__ uint32_t whigh[32];
+    const uint32_t n = *nbig;
+    for (uint32_t q = blockIdx.x; q < n; q += gridDim.x) {
+        const uint32_t l = big[q];
+        const uint32_t b = seg_begin[l], e = seg_end[l], c = e - b;
+        if (c > uint32_t(SEG_BIG)) {
+            if (threadIdx.x == 0)
+                *overflow = 1u;
+            continue;
+        }
+        uint32_t p2 = 2 * SEG_WARP;
+        while (p2 < c)
+            p2 <<= 1;
+        for (uint32_t t = threadIdx.x; t < p2; t += blockDim.x)
+            sb[t] = t < c ? slots[b + t] : 0xffffffffu;
+        __syncthreads();
+        for (uint32_t k = 2; k <= p2; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t r = threadIdx.x; r < (p2 >> 1); r += blockDim.x) {
+                    const uint32_t lo = 2 * r - (r & (j - 1)), hi = lo + j;
+                    const uint32_t x = sb[lo], y = sb[hi];
+                    if ((x > y) == ((lo & k) == 0)) {
+                        sb[lo] = y;
+                        sb[hi] = x;
+                    }
+                }
+                __syncthreads();
+            }
+        uint32_t high = 0;
+        for (uint32_t t = threadIdx.x; t < c; t += blockDim.x) {
+            const uint32_t i = sb[t];
+            slots[b + t] = i;
+            const uint32_t m = fm[i];
+            vals[b + t] = m;
+            high += m >= split_m ? 1u : 0u;
+        }
+        for (int o = 16; o > 0; o >>= 1)
+            high += __shfl_xor_sync(0xffffffffu, high, o);
+        if ((threadIdx.x & 31) == 0)
+            whigh[threadIdx.x >> 5] = high;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t h = 0;
+            for (int w = 0; w < int(blockDim.x >> 5); w++)
+                h += whigh[w];
+            seg_split[l] = b + h;
+        }
+        __syncthreads();
+    }
 }
 
 // List position of the j-th pixel (memory order) of segment [b, e) split at sp.

@@ -118,8 +118,9 @@ def test_source_find_no_labelmap_cleanup(ctx):
 
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_crowded_field(ctx, dtype):
-    """About a thousand bright islands (tens of thousands of valid pixels): the label sort takes the
-    multi-block path and the island records come back in two reads; labels and islands as the oracle's."""
+    """About a thousand bright islands (tens of thousands of valid pixels): each island's entries are
+    ordered by one warp, and the island records come back in two reads; labels and islands as the
+    oracle's."""
     rng = np.random.default_rng(9)
     img = rng.normal(size=(384, 384))
     for r in range(2, 384 - 10, 12):
@@ -137,9 +138,8 @@ def test_crowded_field(ctx, dtype):
 @pytest.mark.parametrize("step", [44, 36])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
 def test_medium_field_one_block_sort(ctx, step, dtype):
-    """Between 2048 and 8192 valid island pixels (about 5.2k and 7.8k here): the one-block label sort in
-    the regime where each warp handles len/32 > 64 entries of the bitonic network; labels and islands as
-    the oracle's."""
+    """Between 2048 and 8192 valid island pixels (about 5.2k and 7.8k here) in 64-pixel islands; labels
+    and islands as the oracle's."""
     rng = np.random.default_rng(10)
     img = rng.normal(size=(384, 384))
     for r in range(2, 384 - 10, step):
@@ -148,6 +148,24 @@ def test_medium_field_one_block_sort(ctx, step, dtype):
     img = img.astype(dtype)
     ref = orc.source_find(img.astype(np.float64), 4.0, 2.5, 1.0, True, 5, orc.ZEROMEDIAN, False, False, True, 3, 0)
     assert 2048 < sum(i[4] for i in ref.islands) <= 8192
+    isl, lab, info = ctx.source_find(img, 4.0, 2.5, 1.0, True, 5, capi.ZEROMEDIAN, False, False, True, 3, 0)
+    assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
+    _compare(isl, ref, lab, ref.label_map)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_large_islands(ctx, dtype):
+    """One island of 1600 pixels (ordered by one block) and one of 22500 (beyond the one-block
+    limit of 16384: the multi-block sort of every entry), beside small ones; labels and islands as
+    the oracle's."""
+    rng = np.random.default_rng(12)
+    img = rng.normal(size=(384, 384))
+    img[20:60, 20:60] += 9.0
+    img[200:350, 180:330] += 9.0
+    img[100:104, 300:304] -= 9.0
+    img = img.astype(dtype)
+    ref = orc.source_find(img.astype(np.float64), 4.0, 2.5, 1.0, True, 5, orc.ZEROMEDIAN, False, False, True, 3, 0)
+    assert max(i[4] for i in ref.islands) > 16384
     isl, lab, info = ctx.source_find(img, 4.0, 2.5, 1.0, True, 5, capi.ZEROMEDIAN, False, False, True, 3, 0)
     assert info.n_labels_pos == ref.n_pos and info.n_labels_neg == ref.n_neg
     _compare(isl, ref, lab, ref.label_map)
