@@ -2071,8 +2071,14 @@ void enqueue_stats(stpgpu_context* c, const T* x, int64_t n, const stpgpu_sf_par
     if (est) {
         k_clip_init<<<1, 1, 0, st>>>(&s->cs, &s->st, double(n), 3.0);
         STPGPU_CHECK_LAUNCH();
+        // with three passes or more: the first clears the band mask, the
+        // second fills it, the later ones visit its samples while their
+        // threshold stays in the band
+        const bool banded = p.sigma_clip_iters >= 3;
+        uint32_t* mask = banded ? c->buf<uint32_t>("sf_clip_mask", size_t((n + 31) / 32)) : nullptr;
         for (int it = 0; it < p.sigma_clip_iters; it++) {
-            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0);
+            const int mode = !banded ? 0 : std::min(it, 2);
+            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0, mask, mode);
             STPGPU_CHECK_LAUNCH();
         }
     }
@@ -2783,7 +2789,7 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += rows * N * 2 * rb + N * N * rb; // double-precision grid and c2r output
     if (find_sources) // classes, parents, ranks, labels, foreground list; at worst list arrays (20 B) for every
                       // pixel and per-label arrays (160 B) for every second pixel
-        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 20 + 80);
+        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 20 + 80) + int64_t(image_size) * image_size / 8;
     return b + (int64_t(8) << 20);
 }
 

@@ -81,6 +81,41 @@ __device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
         f(x[i]);
 }
 
+// The same visit with each element's index: f(value, index).
+template <typename T, typename F>
+__device__ __forceinline__ void for_each_elem_idx(const T* x, int64_t n, F f)
+{
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    int64_t done = 0;
+    if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
+        const int64_t n4 = n / 4;
+        constexpr int UNR = sizeof(T) == 4 ? 4 : 2;
+        int64_t g = tid;
+        for (; g + (UNR - 1) * stride < n4; g += UNR * stride) {
+            T a[UNR][4];
+#pragma unroll
+            for (int u = 0; u < UNR; u++)
+                load4(x, g + u * stride, a[u]);
+#pragma unroll
+            for (int u = 0; u < UNR; u++)
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    f(a[u][k], 4 * (g + u * stride) + k);
+        }
+        for (; g < n4; g += stride) {
+            T a[4];
+            load4(x, g, a);
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                f(a[k], 4 * g + k);
+        }
+        done = n4 * 4;
+    }
+    for (int64_t i = done + tid; i < n; i += stride)
+        f(x[i], i);
+}
+
 // order-preserving 64-bit key of a double (non-NaN)
 __device__ __forceinline__ unsigned long long okey(double v)
 {
@@ -398,7 +433,15 @@ __global__ void k_radix_pick(const unsigned int* hist, int shift, unsigned long 
 struct ClipState {
     double s, d1, d2, valid, prev_upper, upper;
     int done;
+    // band: the band mask holds the samples with band_lo < |x - median| <=
+    // the upper threshold of the pass that wrote it (k_clip_pass mode 1)
+    int band;
+    double band_lo;
 };
+
+// Fraction of the second pass's threshold below which the band mask starts:
+// later passes whose threshold stays above it visit the mask's samples only.
+constexpr double kClipBand = 0.9;
 
 // Starting state from the mean, sigma and median in st (m = mean - median).
 __global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double num_sigma)
@@ -412,25 +455,42 @@ __global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double n
     c.prev_upper = 1.7976931348623157e308;
     c.upper = __dmul_rn(num_sigma, sigma);
     c.done = 0;
+    c.band = 0;
+    c.band_lo = 0.0;
     *cs = c;
 }
 
+// mode 0: a full pass.  mode 1 (the second pass): a full pass that also
+// sets, in `mask`, the bit of every sample with kClipBand * upper < |x -
+// median| <= upper (the samples any later pass can still remove while its
+// threshold stays above kClipBand * upper), and records that band in cs;
+// mode 0 with a mask clears it for the mode-1 pass that follows.  mode 2
+// (later passes): when the threshold is still within the band, only the
+// mask's samples are visited, else a full pass.  A later pass removes the
+// samples with upper < |x - median| <= prev_upper, and prev_upper <= the
+// second pass's threshold (thresholds fall while passes remove samples), so
+// they are all in the band.  The removed samples are those of a full pass in
+// every mode; the sums differ only in the order of addition (fixed, so the
+// result is the same on every run).
 template <typename T>
 __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(const T* x, int64_t n, const SfStats* st,
-    ClipState* cs, double* part, unsigned int* ticket, double num_sigma)
+    ClipState* cs, double* part, unsigned int* ticket, double num_sigma, uint32_t* mask, int mode)
 {
     if (cs->done)
         return;
     const double median = st->median;
     const double upper = cs->upper, prev_upper = cs->prev_upper;
     // Single-precision screen: samples with |x - median| certainly not above
-    // upper skip the double-precision tests.  With xf = float(x), mf =
+    // `bound` skip the double-precision tests.  With xf = float(x), mf =
     // float(median), |x - median| <= |xf - mf| (1 + 2^-23) + |xf| 2^-23 +
-    // |median| 2^-24, so |xf - mf| + |xf| 2^-21 < skip, skip <= upper
-    // (1 - 2^-12) - |median| 2^-12, implies |x - median| < upper.  NaN and
-    // infinite samples fail the screen and take the exact tests.
+    // |median| 2^-24, so |xf - mf| + |xf| 2^-21 < skip, skip <= bound
+    // (1 - 2^-12) - |median| 2^-12, implies |x - median| < bound.  NaN and
+    // infinite samples fail the screen and take the exact tests.  The bound
+    // is the threshold, or in mode 1 the band's lower edge.
+    const double lo_band = kClipBand * upper;
+    const double bound = mode == 1 ? lo_band : upper;
     const float mf = float(median);
-    const float skip = __double2float_rd(upper * (1.0 - 0x1p-12) - fabs(median) * 0x1p-12);
+    const float skip = __double2float_rd(bound * (1.0 - 0x1p-12) - fabs(median) * 0x1p-12);
     auto screened = [&](T xr) {
         const float xf = float(xr);
         return fabsf(xf - mf) + fabsf(xf) * 0x1p-21f < skip;
@@ -445,11 +505,37 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
             v[2] += 1.0;
         }
     };
-    auto band = [&](T xr) {
-        if (!screened(xr))
-            band_exact(double(xr));
-    };
-    for_each_elem(x, n, band);
+    if (mode == 2 && cs->band && upper >= cs->band_lo) {
+        const int64_t words = (n + 31) / 32;
+        for (int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
+             w += int64_t(gridDim.x) * blockDim.x) {
+            uint32_t m = mask[w];
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                band_exact(double(x[w * 32 + b]));
+            }
+        }
+    } else if (mode == 1) {
+        for_each_elem_idx(x, n, [&](T xr, int64_t i) {
+            if (screened(xr))
+                return;
+            const double xv = double(xr);
+            const double a = fabs(xv - median);
+            band_exact(xv);
+            if (a > lo_band && !(a > upper))
+                atomicOr(&mask[i >> 5], 1u << (i & 31));
+        });
+    } else {
+        if (mask)
+            for (int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < (n + 31) / 32;
+                 w += int64_t(gridDim.x) * blockDim.x)
+                mask[w] = 0;
+        for_each_elem(x, n, [&](T xr) {
+            if (!screened(xr))
+                band_exact(double(xr));
+        });
+    }
     block_sums<3>(v, part + 3 * blockIdx.x);
     if (!last_block(ticket))
         return;
@@ -458,6 +544,10 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
     if (threadIdx.x != 0)
         return;
     ClipState c = *cs;
+    if (mode == 1) {
+        c.band = 1;
+        c.band_lo = lo_band;
+    }
     const unsigned long long rem = (unsigned long long)(sm[2] + 0.5);
     if (rem == 0) {
         c.done = 1;

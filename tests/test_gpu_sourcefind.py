@@ -206,6 +206,35 @@ def test_binned_median_falls_back_to_exact(ctx, dtype):
     assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
 
 
+def _clip_image(kind, dtype):
+    rng = np.random.default_rng(23)
+    shape = (516, 388)  # 200208 pixels: not a multiple of 32 (the band mask's partial last word)
+    if kind == "gauss":  # thresholds settle in the band, the clip ends early
+        x = rng.normal(size=shape)
+    elif kind == "laplace":  # thresholds stay in the band for eight passes
+        x = rng.laplace(size=shape)
+    elif kind == "skew":  # the third threshold falls below the band: full passes again
+        x = np.where(rng.random(shape) < 0.3, rng.exponential(4.0, size=shape), rng.normal(size=shape))
+    else:  # uniform: nothing beyond three sigma, the first pass ends the clip
+        x = rng.uniform(-1.0, 1.0, size=shape)
+    return np.asfortranarray(x.astype(dtype))
+
+
+@pytest.mark.parametrize("kind", ["gauss", "laplace", "skew", "uniform"])
+@pytest.mark.parametrize("iters", [1, 2, 3, 5, 8])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_sigma_clip_iterations(ctx, kind, iters, dtype):
+    """The estimated RMS after 1-8 sigma-clip passes (sourcefind.cpp:280-301), exact median, within 1e-10 of
+    the oracle's: from the third pass on, the device visits only the samples of the band mask written by the
+    second pass while the threshold stays in the band, else the whole image."""
+    img = _clip_image(kind, dtype)
+    x = img.astype(np.float64)
+    ref = orc.source_find(x, 5.0, 3.0, 0.0, True, iters, orc.NTHELEMENT, False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, iters, capi.NTHELEMENT, False, False, True, 5)
+    assert abs(info.rms_est - ref.rms_est) <= 1e-10 * abs(ref.rms_est)
+    assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
+
+
 def test_foreground_beyond_first_capacity():
     """A 512^2 image with a low analysis threshold has about 200 k foreground pixels, beyond the
     label-analysis capacity a fresh context starts with (n / 16 entries, at least 131072): the first call runs
