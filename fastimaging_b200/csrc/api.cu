@@ -2024,17 +2024,93 @@ struct SfState {
     ClipState cs;
 };
 
+// Blocks of the fused statistics kernel for T on the context's device (the
+// cooperative grid: one block per SM); 0 when it cannot be launched
+// cooperatively.
+template <typename T>
+int sf_stats_grid(stpgpu_context* c)
+{
+    static std::mutex mu;
+    static std::map<int, int> grid;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = grid.find(c->device);
+    if (it != grid.end())
+        return it->second;
+    int coop = 0, sms = 0, per_sm = 0;
+    STPGPU_CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+    STPGPU_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    STPGPU_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sf_stats<T>, SF_STATS_THREADS, 0));
+    const int g = coop ? std::min(per_sm, 1) * sms : 0;
+    grid[c->device] = g;
+    return g;
+}
+
+// Images of at least this many samples take the fused statistics kernel;
+// smaller ones the pass kernels.
+constexpr int64_t kSfFusedMin = int64_t(1) << 16;
+
+// The pass kernels for every image when STPGPU_SF_STATS=passes.
+bool sf_passes_forced()
+{
+    const char* e = std::getenv("STPGPU_SF_STATS");
+    return e && std::strcmp(e, "passes") == 0;
+}
+
 // Statistics and thresholds (sourcefind.cpp:280-301) enqueued into s->st;
 // only the exact median (NTHELEMENT, BINMEDIAN, or exact = the binned
-// median's fallback) waits on the host.
+// median's fallback) waits on the host.  With `fused` (16-byte aligned
+// images of at least kSfFusedMin samples) one cooperative launch of
+// k_sf_stats does the passes; otherwise one kernel per pass.
 template <typename T>
-void enqueue_stats(stpgpu_context* c, const T* x, int64_t n, const stpgpu_sf_pars& p, SfState* s, bool exact)
+void enqueue_stats(stpgpu_context* c, const T* x, int64_t n, const stpgpu_sf_pars& p, SfState* s, bool exact,
+    bool fused)
 {
     cudaStream_t st = c->stream;
+    const bool est = !(std::fabs(p.rms_est) > 0.0);
+    const int grid = fused ? sf_stats_grid<T>(c) : 0;
+    if (grid > 0 && n >= kSfFusedMin && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && !sf_passes_forced()) {
+        int do_sum = est, do_hist = 0;
+        switch (p.median_method) {
+        case STPGPU_ZEROMEDIAN:
+            break;
+        case STPGPU_BINAPPROX:
+            if (!exact) {
+                do_sum = 1;
+                do_hist = 1;
+                break;
+            }
+            [[fallthrough]];
+        case STPGPU_BINMEDIAN:
+            do_sum = 1;
+            [[fallthrough]];
+        case STPGPU_NTHELEMENT:
+            k_sf_set_median<<<1, 1, 0, st>>>(&s->st, median_exact(c, x, n));
+            STPGPU_CHECK_LAUNCH();
+            break;
+        default:
+            fail(STPGPU_ERR_INVALID_ARG, "unknown median method");
+        }
+        const int64_t G = int64_t(grid) * SF_STATS_THREADS;
+        int cap = est ? sf_band_cap(n, G) : 0;
+        double* part = c->buf<double>("sf_part_fused", 8 * size_t(grid));
+        unsigned long long* bins = c->buf<unsigned long long>("sf_bins", BINS_N + 2);
+        T* cand = est ? c->buf<T>("sf_clip_lists", size_t(cap) * size_t(G)) : nullptr;
+        int iters = est ? p.sigma_clip_iters : 0;
+        double rms = p.rms_est, ana = p.analysis_n_sigma, det = p.detection_n_sigma;
+        const T* xa = x;
+        SfStats* sta = &s->st;
+        ClipState* csa = &s->cs;
+        unsigned int* bar = &s->tickets[3];
+        void* args[] = { (void*)&xa, (void*)&n, (void*)&sta, (void*)&csa, (void*)&part, (void*)&bins, (void*)&cand,
+            (void*)&cap, (void*)&bar, (void*)&do_sum, (void*)&do_hist, (void*)&iters, (void*)&rms, (void*)&ana,
+            (void*)&det };
+        STPGPU_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_sf_stats<T>, dim3(grid), dim3(SF_STATS_THREADS), args,
+            0, st));
+        return;
+    }
     const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * SF_STREAM_BLOCKS);
     double* part = c->buf<double>("sf_part", 3 * size_t(nb));
     unsigned long long* bins = c->buf<unsigned long long>("sf_bins", BINS_N + 2);
-    const bool est = !(std::fabs(p.rms_est) > 0.0);
     auto sum_sq = [&](bool with_bins) {
         k_sum_sq<T><<<nb, SF_THREADS, 0, st>>>(x, n, part, &s->tickets[0], &s->st, with_bins ? bins : nullptr);
         STPGPU_CHECK_LAUNCH();
@@ -2071,14 +2147,8 @@ void enqueue_stats(stpgpu_context* c, const T* x, int64_t n, const stpgpu_sf_par
     if (est) {
         k_clip_init<<<1, 1, 0, st>>>(&s->cs, &s->st, double(n), 3.0);
         STPGPU_CHECK_LAUNCH();
-        // with three passes or more: the first clears the band mask, the
-        // second fills it, the later ones visit its samples while their
-        // threshold stays in the band
-        const bool banded = p.sigma_clip_iters >= 3;
-        uint32_t* mask = banded ? c->buf<uint32_t>("sf_clip_mask", size_t((n + 31) / 32)) : nullptr;
         for (int it = 0; it < p.sigma_clip_iters; it++) {
-            const int mode = !banded ? 0 : std::min(it, 2);
-            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0, mask, mode);
+            k_clip_pass<T><<<nb, SF_THREADS, 0, st>>>(x, n, &s->st, &s->cs, part, &s->tickets[2], 3.0);
             STPGPU_CHECK_LAUNCH();
         }
     }
@@ -2255,17 +2325,29 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
     };
     size_buffers();
-    for (int attempt = 0;; attempt++) {
-        // a second attempt only when the binned median does not apply
+    bool exact = false, fused = true;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        // again when the binned median does not apply (the exact median), or
+        // when the fused statistics kernel gave up at a barrier (the pass
+        // kernels)
         STPGPU_CUDA_TRY(cudaMemsetAsync(sfs, 0, sizeof(SfState), st));
-        enqueue_stats<T>(c, d_img, n, p, sfs, attempt > 0);
+        enqueue_stats<T>(c, d_img, n, p, sfs, exact, fused);
         STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
             p.ccl_4connectivity, slice, cb));
         enqueue_analysis();
         read_back_state();
-        if (!hstate->st.need_exact || attempt > 0)
-            break;
+        if (hstate->st.stats_err && fused) {
+            fused = false;
+            continue;
+        }
+        if (hstate->st.need_exact && !exact) {
+            exact = true;
+            continue;
+        }
+        break;
     }
+    if (hstate->st.stats_err)
+        fail(STPGPU_ERR_DEVICE, "source-finder statistics failed");
     if (hstate->misc[3])
         fail(STPGPU_ERR_DEVICE, "labeler gave up (union-find step bound)");
     const int np = int(hstate->misc[0]), nneg = int(hstate->misc[1]), nfg = int(hstate->misc[2]);
@@ -2789,7 +2871,7 @@ int64_t request_bytes(const ImagerSetup& s, int image_size, int64_t n, int vis_c
         b += rows * N * 2 * rb + N * N * rb; // double-precision grid and c2r output
     if (find_sources) // classes, parents, ranks, labels, foreground list; at worst list arrays (20 B) for every
                       // pixel and per-label arrays (160 B) for every second pixel
-        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 20 + 80) + int64_t(image_size) * image_size / 8;
+        b += int64_t(image_size) * image_size * (1 + 4 + 4 + 4 + 4 + 20 + 80 + 2) + (int64_t(8) << 20); // + clip lists
     return b + (int64_t(8) << 20);
 }
 

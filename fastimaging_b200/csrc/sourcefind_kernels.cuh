@@ -81,41 +81,6 @@ __device__ __forceinline__ void for_each_elem(const T* x, int64_t n, F f)
         f(x[i]);
 }
 
-// The same visit with each element's index: f(value, index).
-template <typename T, typename F>
-__device__ __forceinline__ void for_each_elem_idx(const T* x, int64_t n, F f)
-{
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    int64_t done = 0;
-    if ((reinterpret_cast<uintptr_t>(x) & 15) == 0) {
-        const int64_t n4 = n / 4;
-        constexpr int UNR = sizeof(T) == 4 ? 4 : 2;
-        int64_t g = tid;
-        for (; g + (UNR - 1) * stride < n4; g += UNR * stride) {
-            T a[UNR][4];
-#pragma unroll
-            for (int u = 0; u < UNR; u++)
-                load4(x, g + u * stride, a[u]);
-#pragma unroll
-            for (int u = 0; u < UNR; u++)
-#pragma unroll
-                for (int k = 0; k < 4; k++)
-                    f(a[u][k], 4 * (g + u * stride) + k);
-        }
-        for (; g < n4; g += stride) {
-            T a[4];
-            load4(x, g, a);
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-                f(a[k], 4 * g + k);
-        }
-        done = n4 * 4;
-    }
-    for (int64_t i = done + tid; i < n; i += stride)
-        f(x[i], i);
-}
-
 // order-preserving 64-bit key of a double (non-NaN)
 __device__ __forceinline__ unsigned long long okey(double v)
 {
@@ -145,10 +110,10 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
-template <int NV>
+template <int NV, int BT = SF_THREADS>
 __device__ __forceinline__ void block_sums(double (&v)[NV], double* out_part)
 {
-    __shared__ double s[NV][SF_THREADS / 32];
+    __shared__ double s[NV][BT / 32];
     for (int q = 0; q < NV; q++) {
         double w = warp_sum(v[q]);
         if ((threadIdx.x & 31) == 0)
@@ -157,17 +122,18 @@ __device__ __forceinline__ void block_sums(double (&v)[NV], double* out_part)
     __syncthreads();
     if (threadIdx.x < NV) {
         double t = 0.0;
-        for (int k = 0; k < SF_THREADS / 32; k++)
+        for (int k = 0; k < BT / 32; k++)
             t += s[threadIdx.x][k];
         out_part[threadIdx.x] = t;
     }
 }
 
-// Exclusive scan of v over the block (SF_THREADS threads); *total = the sum.
+// Exclusive scan of v over the block (BT threads); *total = the sum.
 // Callers pack up to three 16-bit counts into v.
+template <int BT = SF_THREADS>
 __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long v, unsigned long long* total)
 {
-    __shared__ unsigned long long ws[SF_THREADS / 32];
+    __shared__ unsigned long long ws[BT / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned long long x = v;
 #pragma unroll
@@ -181,7 +147,7 @@ __device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long
     __syncthreads();
     unsigned long long before = 0, all = 0;
 #pragma unroll
-    for (int w = 0; w < SF_THREADS / 32; w++) {
+    for (int w = 0; w < BT / 32; w++) {
         const unsigned long long t = ws[w];
         if (w < warp)
             before += t;
@@ -206,7 +172,7 @@ struct SfStats {
     unsigned long long kpos, kneg; // order keys of the detection thresholds
     unsigned int fpos, fneg; // single-precision keys of the detection thresholds rounded onto the float grid
     unsigned int need_exact; // the binned median does not apply: the exact path must run
-    unsigned int pad;
+    unsigned int stats_err; // the fused statistics kernel gave up at a grid barrier: the pass kernels must run
 };
 
 // True in exactly one block, the last to finish the pass; every other
@@ -230,28 +196,40 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket)
     return last;
 }
 
-// Sum NV-wide partials of nb blocks in a fixed order (one block of
-// SF_THREADS threads: strided sums, warp trees, warps in order); the result
-// is valid in thread 0.
-template <int NV>
+// Sum NV-wide partials of nb blocks in a fixed order (one block of BT
+// threads: strided sums, warp trees, warps in order); the result is valid in
+// every thread.
+template <int NV, int BT = SF_THREADS>
 __device__ __forceinline__ void reduce_parts(const double* part, int nb, double (&out)[NV])
 {
-    __shared__ double s[NV][SF_THREADS / 32];
+    __shared__ double s[NV][BT / 32];
+    double t[NV];
+    for (int q = 0; q < NV; q++)
+        t[q] = 0.0;
+    // all of a thread's loads in flight together (one L2 round trip per BT
+    // blocks), the same order of addition per quantity
+#pragma unroll 4
+    for (int k = threadIdx.x; k < nb; k += BT)
+        for (int q = 0; q < NV; q++)
+            t[q] += __ldcg(part + NV * k + q);
     for (int q = 0; q < NV; q++) {
-        double t = 0.0;
-        for (int k = threadIdx.x; k < nb; k += SF_THREADS)
-            t += __ldcg(part + NV * k + q);
-        t = warp_sum(t);
+        const double w = warp_sum(t[q]);
         if ((threadIdx.x & 31) == 0)
-            s[q][threadIdx.x >> 5] = t;
+            s[q][threadIdx.x >> 5] = w;
     }
     __syncthreads();
-    for (int q = 0; q < NV; q++) {
-        double t = 0.0;
-        for (int w = 0; w < SF_THREADS / 32; w++)
-            t += s[q][w];
-        out[q] = t;
+    // thread q sums quantity q over the warps in order; every thread reads
+    // the NV results
+    __shared__ double r[NV];
+    if (threadIdx.x < NV) {
+        double u = 0.0;
+        for (int w = 0; w < BT / 32; w++)
+            u += s[threadIdx.x][w];
+        r[threadIdx.x] = u;
     }
+    __syncthreads();
+    for (int q = 0; q < NV; q++)
+        out[q] = r[q];
 }
 
 // mean and sigma (mat_mean_and_stddev, matrix_math.cpp:457-499):
@@ -281,6 +259,65 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_sum_sq(const T
         st->mean = mean;
         st->sigma = __dsqrt_rn(__dsub_rn(__ddiv_rn(s[1], dn), __dmul_rn(mean, mean)));
     }
+}
+
+// The binned median from the merged bins (every thread of a block of BT
+// threads calls it; the result is valid in every thread): the cumulative
+// counts, consecutive bins per thread, locate the bin holding rank
+// k = ceil(n / 2); for even n the walk continues over the bins whose
+// cumulative count equals k, as the reference's loop does.  False when no
+// bin reaches the rank.
+template <int BT = SF_THREADS>
+__device__ __forceinline__ bool hist_median(const unsigned long long* bins, int64_t n, double scale, double leftend,
+    double* median)
+{
+    constexpr int BPT = (BINS_N + 1 + BT - 1) / BT; // bins per thread
+    __shared__ unsigned long long cum[BPT * BT];
+    __shared__ int hit;
+    __shared__ double res;
+    unsigned long long b4[BPT], loc = 0;
+    for (int q = 0; q < BPT; q++) {
+        const int i = BPT * threadIdx.x + q;
+        b4[q] = i <= BINS_N ? __ldcg(bins + i) : 0ull;
+        loc += b4[q];
+    }
+    if (threadIdx.x == 0)
+        hit = -1;
+    unsigned long long tot = 0;
+    unsigned long long c = __ldcg(bins + BINS_N + 1) + block_excl_scan<BT>(loc, &tot);
+    const unsigned long long k = (n & 1) ? (unsigned long long)(n + 1) / 2 : (unsigned long long)n / 2;
+    for (int q = 0; q < BPT; q++) {
+        const unsigned long long prev = c;
+        c += b4[q];
+        cum[BPT * threadIdx.x + q] = c;
+        const int i = BPT * threadIdx.x + q;
+        if (i <= BINS_N && c >= k && prev < k)
+            hit = i; // exactly one bin crosses the rank
+        if (i == 0 && prev >= k)
+            hit = 0; // the count below the range already reaches it
+    }
+    __syncthreads();
+    const int i = hit;
+    if (threadIdx.x == 0 && i >= 0) {
+        if (n & 1) {
+            res = __dadd_rn(__ddiv_rn(double(i) + 0.5, scale), leftend);
+        } else {
+            unsigned long long count = cum[i];
+            int j = i;
+            while (count == k) {
+                j++;
+                count += __ldcg(bins + j);
+                if (j == BINS_N)
+                    break;
+            }
+            res = __dadd_rn(__ddiv_rn(double(i + j + 1), __dmul_rn(2.0, scale)), leftend);
+        }
+    }
+    __syncthreads();
+    *median = res;
+    const bool ok = i >= 0;
+    __syncthreads();
+    return ok;
 }
 
 // mat_median_binapprox (matrix_math.cpp:334-455): N+1 bins over
@@ -317,51 +354,13 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_hist(const T* 
             atomicAdd(&bins[k], (unsigned long long)h[k]);
     if (!last_block(ticket))
         return;
-    // cumulative counts: 4 consecutive bins per thread (1024 >= N + 1)
-    static_assert(4 * SF_THREADS >= BINS_N + 1, "bins per thread");
-    __shared__ unsigned long long cum[4 * SF_THREADS];
-    __shared__ int hit;
-    unsigned long long b4[4], loc = 0;
-    for (int q = 0; q < 4; q++) {
-        const int i = 4 * threadIdx.x + q;
-        b4[q] = i <= BINS_N ? __ldcg(bins + i) : 0ull;
-        loc += b4[q];
-    }
-    if (threadIdx.x == 0)
-        hit = -1;
-    unsigned long long tot = 0;
-    unsigned long long c = __ldcg(bins + BINS_N + 1) + block_excl_scan(loc, &tot);
-    const unsigned long long k = (n & 1) ? (unsigned long long)(n + 1) / 2 : (unsigned long long)n / 2;
-    for (int q = 0; q < 4; q++) {
-        const unsigned long long prev = c;
-        c += b4[q];
-        cum[4 * threadIdx.x + q] = c;
-        const int i = 4 * threadIdx.x + q;
-        if (i <= BINS_N && c >= k && prev < k)
-            hit = i; // exactly one bin crosses the rank
-        if (i == 0 && prev >= k)
-            hit = 0; // the count below the range already reaches it
-    }
-    __syncthreads();
-    if (threadIdx.x != 0)
-        return;
-    const int i = hit;
-    if (i < 0) {
-        st->need_exact = 1;
-        return;
-    }
-    if (n & 1) {
-        st->median = __dadd_rn(__ddiv_rn(double(i) + 0.5, scale), leftend);
-    } else {
-        unsigned long long count = cum[i];
-        int j = i;
-        while (count == k) {
-            j++;
-            count += __ldcg(bins + j);
-            if (j == BINS_N)
-                break;
-        }
-        st->median = __dadd_rn(__ddiv_rn(double(i + j + 1), __dmul_rn(2.0, scale)), leftend);
+    double median;
+    const bool ok = hist_median(bins, n, scale, leftend, &median);
+    if (threadIdx.x == 0) {
+        if (ok)
+            st->median = median;
+        else
+            st->need_exact = 1;
     }
 }
 
@@ -433,20 +432,12 @@ __global__ void k_radix_pick(const unsigned int* hist, int shift, unsigned long 
 struct ClipState {
     double s, d1, d2, valid, prev_upper, upper;
     int done;
-    // band: the band mask holds the samples with band_lo < |x - median| <=
-    // the upper threshold of the pass that wrote it (k_clip_pass mode 1)
-    int band;
-    double band_lo;
 };
 
-// Fraction of the second pass's threshold below which the band mask starts:
-// later passes whose threshold stays above it visit the mask's samples only.
-constexpr double kClipBand = 0.9;
-
-// Starting state from the mean, sigma and median in st (m = mean - median).
-__global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double num_sigma)
+// Starting state from the mean, sigma and median (m = mean - median).
+__device__ __forceinline__ ClipState clip_start(double mean, double sigma, double median, double n, double num_sigma)
 {
-    const double sigma = st->sigma, m = __dsub_rn(st->mean, st->median);
+    const double m = __dsub_rn(mean, median);
     ClipState c;
     c.s = sigma;
     c.d1 = __dmul_rn(m, n);
@@ -455,42 +446,48 @@ __global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double n
     c.prev_upper = 1.7976931348623157e308;
     c.upper = __dmul_rn(num_sigma, sigma);
     c.done = 0;
-    c.band = 0;
-    c.band_lo = 0.0;
-    *cs = c;
+    return c;
 }
 
-// mode 0: a full pass.  mode 1 (the second pass): a full pass that also
-// sets, in `mask`, the bit of every sample with kClipBand * upper < |x -
-// median| <= upper (the samples any later pass can still remove while its
-// threshold stays above kClipBand * upper), and records that band in cs;
-// mode 0 with a mask clears it for the mode-1 pass that follows.  mode 2
-// (later passes): when the threshold is still within the band, only the
-// mask's samples are visited, else a full pass.  A later pass removes the
-// samples with upper < |x - median| <= prev_upper, and prev_upper <= the
-// second pass's threshold (thresholds fall while passes remove samples), so
-// they are all in the band.  The removed samples are those of a full pass in
-// every mode; the sums differ only in the order of addition (fixed, so the
-// result is the same on every run).
+// One pass's update from the sums of the removed samples (sm: v, v^2,
+// count), sourcefind.cpp:82-134.
+__device__ __forceinline__ void clip_update(ClipState& c, const double* sm, double num_sigma)
+{
+    const unsigned long long rem = (unsigned long long)(sm[2] + 0.5);
+    if (rem == 0) {
+        c.done = 1;
+        return;
+    }
+    c.valid = __dsub_rn(c.valid, double(rem));
+    c.d1 = __dsub_rn(c.d1, sm[0]);
+    c.d2 = __dsub_rn(c.d2, sm[1]);
+    const double a = __ddiv_rn(c.d2, c.valid), b = __ddiv_rn(c.d1, c.valid);
+    c.s = __dsqrt_rn(__dsub_rn(a, __dmul_rn(b, b)));
+    c.prev_upper = c.upper;
+    c.upper = __dmul_rn(num_sigma, c.s);
+}
+
+__global__ void k_clip_init(ClipState* cs, const SfStats* st, double n, double num_sigma)
+{
+    *cs = clip_start(st->mean, st->sigma, st->median, n, num_sigma);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(const T* x, int64_t n, const SfStats* st,
-    ClipState* cs, double* part, unsigned int* ticket, double num_sigma, uint32_t* mask, int mode)
+    ClipState* cs, double* part, unsigned int* ticket, double num_sigma)
 {
     if (cs->done)
         return;
     const double median = st->median;
     const double upper = cs->upper, prev_upper = cs->prev_upper;
     // Single-precision screen: samples with |x - median| certainly not above
-    // `bound` skip the double-precision tests.  With xf = float(x), mf =
+    // upper skip the double-precision tests.  With xf = float(x), mf =
     // float(median), |x - median| <= |xf - mf| (1 + 2^-23) + |xf| 2^-23 +
-    // |median| 2^-24, so |xf - mf| + |xf| 2^-21 < skip, skip <= bound
-    // (1 - 2^-12) - |median| 2^-12, implies |x - median| < bound.  NaN and
-    // infinite samples fail the screen and take the exact tests.  The bound
-    // is the threshold, or in mode 1 the band's lower edge.
-    const double lo_band = kClipBand * upper;
-    const double bound = mode == 1 ? lo_band : upper;
+    // |median| 2^-24, so |xf - mf| + |xf| 2^-21 < skip, skip <= upper
+    // (1 - 2^-12) - |median| 2^-12, implies |x - median| < upper.  NaN and
+    // infinite samples fail the screen and take the exact tests.
     const float mf = float(median);
-    const float skip = __double2float_rd(bound * (1.0 - 0x1p-12) - fabs(median) * 0x1p-12);
+    const float skip = __double2float_rd(upper * (1.0 - 0x1p-12) - fabs(median) * 0x1p-12);
     auto screened = [&](T xr) {
         const float xf = float(xr);
         return fabsf(xf - mf) + fabsf(xf) * 0x1p-21f < skip;
@@ -505,37 +502,11 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
             v[2] += 1.0;
         }
     };
-    if (mode == 2 && cs->band && upper >= cs->band_lo) {
-        const int64_t words = (n + 31) / 32;
-        for (int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < words;
-             w += int64_t(gridDim.x) * blockDim.x) {
-            uint32_t m = mask[w];
-            while (m) {
-                const int b = __ffs(m) - 1;
-                m &= m - 1;
-                band_exact(double(x[w * 32 + b]));
-            }
-        }
-    } else if (mode == 1) {
-        for_each_elem_idx(x, n, [&](T xr, int64_t i) {
-            if (screened(xr))
-                return;
-            const double xv = double(xr);
-            const double a = fabs(xv - median);
-            band_exact(xv);
-            if (a > lo_band && !(a > upper))
-                atomicOr(&mask[i >> 5], 1u << (i & 31));
-        });
-    } else {
-        if (mask)
-            for (int64_t w = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; w < (n + 31) / 32;
-                 w += int64_t(gridDim.x) * blockDim.x)
-                mask[w] = 0;
-        for_each_elem(x, n, [&](T xr) {
-            if (!screened(xr))
-                band_exact(double(xr));
-        });
-    }
+    auto band = [&](T xr) {
+        if (!screened(xr))
+            band_exact(double(xr));
+    };
+    for_each_elem(x, n, band);
     block_sums<3>(v, part + 3 * blockIdx.x);
     if (!last_block(ticket))
         return;
@@ -544,22 +515,7 @@ __global__ void __launch_bounds__(SF_THREADS, SF_STREAM_BLOCKS) k_clip_pass(cons
     if (threadIdx.x != 0)
         return;
     ClipState c = *cs;
-    if (mode == 1) {
-        c.band = 1;
-        c.band_lo = lo_band;
-    }
-    const unsigned long long rem = (unsigned long long)(sm[2] + 0.5);
-    if (rem == 0) {
-        c.done = 1;
-    } else {
-        c.valid = __dsub_rn(c.valid, double(rem));
-        c.d1 = __dsub_rn(c.d1, sm[0]);
-        c.d2 = __dsub_rn(c.d2, sm[1]);
-        const double a = __ddiv_rn(c.d2, c.valid), b = __ddiv_rn(c.d1, c.valid);
-        c.s = __dsqrt_rn(__dsub_rn(a, __dmul_rn(b, b)));
-        c.prev_upper = c.upper;
-        c.upper = __dmul_rn(num_sigma, c.s);
-    }
+    clip_update(c, sm, num_sigma);
     *cs = c;
 }
 
@@ -570,9 +526,9 @@ __device__ __host__ inline uint32_t fkey32(float v);
 // with the detection thresholds' keys for the label analysis: order keys,
 // and for single-precision images the largest float <= the positive
 // threshold and the smallest float >= the negative one.
-__global__ void k_sf_thresholds(SfStats* st, const ClipState* cs, double rms_fixed, double ana, double det)
+__device__ __forceinline__ void sf_set_thresholds(SfStats* st, double rms, double ana, double det)
 {
-    const double rms = cs ? cs->s : rms_fixed, bg = st->median;
+    const double bg = st->median;
     st->rms = rms;
     st->thr[0] = __dadd_rn(bg, __dmul_rn(ana, rms));
     st->thr[1] = __dsub_rn(bg, __dmul_rn(ana, rms));
@@ -589,6 +545,307 @@ __global__ void k_sf_thresholds(SfStats* st, const ClipState* cs, double rms_fix
         tc = nextafterf(tc, INFINITY);
     st->fpos = fkey32(tf);
     st->fneg = fkey32(tc);
+}
+
+__global__ void k_sf_thresholds(SfStats* st, const ClipState* cs, double rms_fixed, double ana, double det)
+{
+    sf_set_thresholds(st, cs ? cs->s : rms_fixed, ana, det);
+}
+
+// -------------------------------------------------- fused statistics (one cooperative launch)
+
+// Polls of a grid barrier before it gives up (each poll sleeps ~32 ns; a
+// legitimate wait is one pass over the image, tens of microseconds).
+constexpr uint32_t kGridWaitLimit = 1u << 20;
+
+// Grid-wide barrier of a cooperative launch (every block resident): the
+// k-th arrival of each block adds one to *count and waits until it reaches
+// k * gridDim.x.  Writes before the barrier are visible after it (fence,
+// then acquire loads; readers use L2 loads).  A wait that runs out records
+// the failure in *err and returns false in the whole block; the caller's
+// kernel then ends, and so does every other block's at its next wait.
+__device__ __forceinline__ bool grid_barrier(unsigned int* count, unsigned int target, unsigned int* err)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(count, 1u);
+        int good = 0;
+        for (uint32_t it = 0; it < kGridWaitLimit; it++) {
+            unsigned int v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if (v >= target) {
+                good = 1;
+                break;
+            }
+            __nanosleep(32);
+        }
+        if (!good)
+            atomicExch(err, 1u);
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+// Lower edge of a full clip pass's band, as a fraction of its threshold:
+// the samples with kClipBand * upper < |x - median| <= upper are kept for
+// the passes that follow.
+constexpr double kClipBand = 0.8;
+
+// Capacity of a thread's band list in k_sf_stats for n samples over G
+// threads (a quarter of the thread's samples, plus slack).
+__host__ __device__ inline int sf_band_cap(int64_t n, int64_t G)
+{
+    const int64_t per_thread = 4 * ((n / 4 + G - 1) / G) + 1;
+    return int(per_thread / 4 + 4);
+}
+
+// Threads of a k_sf_stats block; one block per SM.
+constexpr int SF_STATS_THREADS = 1024;
+
+// Histogram slot of a single-precision sample for the binned median without
+// double-precision arithmetic where that is safe; the slot is that of
+// int_trunc_x86((double(x) - leftend) * scale) in double precision (bins 0..N,
+// N + 1 = below the range).  With lf = float(leftend), sf = float(scale), tf =
+// (x - lf) * sf in single precision differs from the exact t = (x - leftend)
+// * scale by at most 2^-22 (|tf| + |leftend| scale) (three roundings of 2^-24
+// each on the terms, one of 2^-24 |leftend| from lf); e = 2^-20 |tf| + els,
+// els >= 2^-20 |leftend| scale, covers that and the roundings of tf -+ e.
+// When [tf - e, tf + e] holds no bin edge the slot follows from it: below
+// (t < -1), bin 0 (-1 < t < 1: truncation), the bin of floor (through the
+// 1.5 * 2^23 rounding constant), or none (N + 1 <= t < 2^30; beyond 2^31 the
+// truncation's integer-indefinite value counts as below, so large t are not
+// decided here).  Returns the slot, -2 for none, -3 when undecided (an edge
+// in the interval, NaN or infinite samples): the caller then takes the
+// double-precision path.  Straight-line code: the rare -3 is the only branch
+// a warp may split on.
+__device__ __forceinline__ int fast_bin(float x, float lf, float sf, float els)
+{
+    const float tf = __fmul_rn(__fsub_rn(x, lf), sf);
+    const float e = __fmaf_rn(fabsf(tf), 0x1p-20f, els);
+    const float lo = __fsub_rn(tf, e), hi = __fadd_rn(tf, e);
+    constexpr float M = 12582912.0f; // 1.5 * 2^23: adding it rounds to an integer
+    const float hm = __fadd_rn(hi, M);
+    const float rf = __fsub_rn(hm, M);
+    const bool up = rf > hi;
+    const float fl = up ? __fsub_rn(rf, 1.0f) : rf;
+    const int fi = __float_as_int(hm) - 0x4B400000 - (up ? 1 : 0);
+    const bool below = hi < -1.0f;
+    const bool none = lo >= float(BINS_N + 1) && hi < 0x1p30f;
+    const bool in = lo > -1.0f && hi < float(BINS_N + 1) && (hi < 1.0f || fmaxf(lo, 0.0f) >= fl);
+    return below ? BINS_N + 1 : in ? max(fi, 0) : none ? -2 : -3;
+}
+
+// Statistics and thresholds of the source finder in one cooperative launch
+// of one SF_STATS_THREADS block per SM (sourcefind.cpp:280-301): sum x and
+// x^2 (mean, sigma; do_sum), the binned median (do_hist; otherwise the
+// median already in st), clip_iters sigma-clip passes (estimate_rms; none
+// when the caller gives the rms), the thresholds.  Grid barriers separate
+// the steps, and after each every block reduces all blocks' partials in the
+// same fixed order, so every block holds the same statistics and takes the
+// same branches; the arithmetic of each step is that of the pass kernels
+// above (the histogram of single-precision images through fast_bin, which
+// gives the same bins).  A full clip pass keeps, per thread, its samples
+// with kClipBand * upper < |x - median| <= upper in a private list
+// (cand[k * G + thread], k < cap), and a later pass whose threshold is still
+// above the band's lower edge visits only those lists: it removes the
+// samples with upper' < |x - median| <= prev_upper, and prev_upper <= the
+// full pass's upper (thresholds fall while passes remove samples), so all
+// of them are listed.  A list that would overflow is counted in a fourth
+// partial and the next pass reads the image again.  Failures: the binned
+// median not applying sets need_exact (and thresholds that label nothing); a
+// barrier that gives up sets stats_err.
+template <typename T>
+__global__ void __launch_bounds__(SF_STATS_THREADS, 1) k_sf_stats(const T* x, int64_t n, SfStats* st,
+    ClipState* cs, double* part /* 2 * 4 * gridDim.x */, unsigned long long* bins /* BINS_N + 2 */, T* cand, int cap,
+    unsigned int* bar, int do_sum, int do_hist, int clip_iters, double rms_fixed, double ana, double det)
+{
+    constexpr int BT = SF_STATS_THREADS;
+    const int nb = gridDim.x;
+    const int64_t G = int64_t(nb) * BT, gt = int64_t(blockIdx.x) * BT + threadIdx.x;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    const double dn = double(n);
+    unsigned int arrivals = 0;
+    auto sync = [&]() {
+        arrivals++;
+        return grid_barrier(bar, arrivals * unsigned(nb), &st->stats_err);
+    };
+    int step = 0;
+    auto next_part = [&]() { return part + 4 * int64_t(nb) * (step++ & 1); };
+    auto label_nothing = [&]() {
+        if (lead) {
+            st->need_exact = 1;
+            sf_set_thresholds(st, INFINITY, ana, det);
+        }
+    };
+    double mean = st->mean, sigma = st->sigma, median = st->median;
+    if (do_sum) {
+        double v[2] = { 0.0, 0.0 };
+        for_each_elem(x, n, [&](double a) {
+            v[0] += a;
+            v[1] += a * a;
+        });
+        double* pp = next_part();
+        block_sums<2, BT>(v, pp + 2 * blockIdx.x);
+        if (do_hist && blockIdx.x == 0)
+            for (int k = threadIdx.x; k < BINS_N + 2; k += BT)
+                bins[k] = 0;
+        if (!sync())
+            return;
+        double s2[2];
+        reduce_parts<2, BT>(pp, nb, s2);
+        mean = __ddiv_rn(s2[0], dn);
+        sigma = __dsqrt_rn(__dsub_rn(__ddiv_rn(s2[1], dn), __dmul_rn(mean, mean)));
+        if (lead) {
+            st->mean = mean;
+            st->sigma = sigma;
+        }
+    }
+    if (do_hist) {
+        if (__dmul_rn(sigma, 2.0) < 0.0001) {
+            label_nothing();
+            return;
+        }
+        const double scale = __ddiv_rn(double(BINS_N), __dmul_rn(2.0, sigma));
+        const double leftend = __dsub_rn(mean, sigma);
+        // four copies of the bins (warp w adds to copy w % 4), summed at the end
+        constexpr int HB = BINS_N + 2;
+        __shared__ unsigned int h[4 * HB];
+        for (int k = threadIdx.x; k < 4 * HB; k += BT)
+            h[k] = 0;
+        __syncthreads();
+        unsigned int* hw = h + HB * ((threadIdx.x >> 5) & 3);
+        auto exact_bin = [&](double a) {
+            const int b = int_trunc_x86(__dmul_rn(__dsub_rn(a, leftend), scale));
+            if (b <= BINS_N)
+                atomicAdd(&hw[b < 0 ? BINS_N + 1 : b], 1u);
+        };
+        if constexpr (sizeof(T) == 4) {
+            const float lf = __double2float_rn(leftend), sf = __double2float_rn(scale);
+            const float els = __double2float_ru(fabs(leftend) * scale * 0x1p-20);
+            for_each_elem(x, n, [&](T xr) {
+                const int b = fast_bin(xr, lf, sf, els);
+                if (b >= 0)
+                    atomicAdd(&hw[b], 1u);
+                else if (b == -3)
+                    exact_bin(double(xr));
+            });
+        } else {
+            for_each_elem(x, n, [&](double a) { exact_bin(a); });
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < HB; k += BT) {
+            const unsigned int c = h[k] + h[HB + k] + h[2 * HB + k] + h[3 * HB + k];
+            if (c)
+                atomicAdd(&bins[k], (unsigned long long)c);
+        }
+        if (!sync())
+            return;
+        if (!hist_median<BT>(bins, n, scale, leftend, &median)) {
+            label_nothing();
+            return;
+        }
+        if (lead)
+            st->median = median;
+    }
+    double rms = rms_fixed;
+    if (clip_iters > 0) {
+        ClipState c = clip_start(mean, sigma, median, dn, 3.0);
+        const float mf = float(median);
+        int cnt = 0; // this thread's listed samples
+        double list_lo = INFINITY; // lower edge of the lists' band (none yet)
+        for (int it = 0; it < clip_iters && !c.done; it++) {
+            const double upper = c.upper, prev_upper = c.prev_upper;
+            double v[4] = { 0.0, 0.0, 0.0, 0.0 };
+            auto band_exact = [&](double xv) {
+                const double d = xv - median;
+                const double a = fabs(d);
+                if (a > upper && !(a > prev_upper)) {
+                    v[0] += d;
+                    v[1] += d * d;
+                    v[2] += 1.0;
+                }
+            };
+            if (upper >= list_lo) {
+                for (int k = 0; k < cnt; k++)
+                    band_exact(double(cand[int64_t(k) * G + gt]));
+            } else {
+                // full pass; the single-precision screen of k_clip_pass at
+                // the band's lower edge
+                const double lo = kClipBand * upper;
+                const float skip = __double2float_rd(lo * (1.0 - 0x1p-12) - fabs(median) * 0x1p-12);
+                int m = 0;
+                auto visit = [&](T xr) {
+                    const double xv = double(xr);
+                    band_exact(xv);
+                    const double a = fabs(xv - median);
+                    if (a > lo && !(a > upper)) {
+                        if (m < cap)
+                            cand[int64_t(m) * G + gt] = xr;
+                        m++;
+                    }
+                };
+                auto fails = [&](T xr) {
+                    const float xf = float(xr);
+                    return !(fabsf(xf - mf) + fabsf(xf) * 0x1p-21f < skip);
+                };
+                // the screen over a step's samples first, then the samples
+                // that fail it (re-read), so that a warp splits once a step
+                // rather than once a sample
+                constexpr int UNR = sizeof(T) == 4 ? 4 : 2;
+                const int64_t n4 = n / 4;
+                int64_t g = gt;
+                for (; g + (UNR - 1) * G < n4; g += UNR * G) {
+                    T a[UNR][4];
+#pragma unroll
+                    for (int u = 0; u < UNR; u++)
+                        load4(x, g + u * G, a[u]);
+                    unsigned int fm = 0;
+#pragma unroll
+                    for (int u = 0; u < UNR; u++)
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            fm |= (fails(a[u][k]) ? 1u : 0u) << (4 * u + k);
+                    while (fm) {
+                        const int slot = __ffs(fm) - 1;
+                        fm &= fm - 1;
+                        visit(x[4 * (g + (slot >> 2) * G) + (slot & 3)]);
+                    }
+                }
+                for (; g < n4; g += G) {
+                    T a[4];
+                    load4(x, g, a);
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (fails(a[k]))
+                            visit(a[k]);
+                }
+                for (int64_t i = n4 * 4 + gt; i < n; i += G)
+                    if (fails(x[i]))
+                        visit(x[i]);
+                cnt = m < cap ? m : cap;
+                v[3] = m > cap ? 1.0 : 0.0;
+                list_lo = lo;
+            }
+            double* pp = next_part();
+            block_sums<4, BT>(v, pp + 4 * blockIdx.x);
+            if (!sync())
+                return;
+            double sm[4];
+            reduce_parts<4, BT>(pp, nb, sm);
+            if (sm[3] > 0.0)
+                list_lo = INFINITY; // a list overflowed: the next pass reads the image
+            clip_update(c, sm, 3.0);
+        }
+        rms = c.s;
+        if (lead)
+            *cs = c;
+    }
+    if (lead)
+        sf_set_thresholds(st, rms, ana, det);
 }
 
 // -------------------------------------------------- connected components

@@ -223,16 +223,40 @@ def _clip_image(kind, dtype):
 @pytest.mark.parametrize("kind", ["gauss", "laplace", "skew", "uniform"])
 @pytest.mark.parametrize("iters", [1, 2, 3, 5, 8])
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_sigma_clip_iterations(ctx, kind, iters, dtype):
-    """The estimated RMS after 1-8 sigma-clip passes (sourcefind.cpp:280-301), exact median, within 1e-10 of
-    the oracle's: from the third pass on, the device visits only the samples of the band mask written by the
-    second pass while the threshold stays in the band, else the whole image."""
+@pytest.mark.parametrize("method", ["NTHELEMENT", "BINAPPROX"])
+def test_sigma_clip_iterations(ctx, kind, iters, dtype, method):
+    """The estimated RMS after 1-8 sigma-clip passes (sourcefind.cpp:280-301) within 1e-10 of the oracle's,
+    labels bit-exact, through the fused statistics kernel: after a full pass, the passes whose threshold stays
+    above the band's lower edge visit only the listed band samples; the skewed image's thresholds leave the
+    band, so full passes come again."""
     img = _clip_image(kind, dtype)
     x = img.astype(np.float64)
-    ref = orc.source_find(x, 5.0, 3.0, 0.0, True, iters, orc.NTHELEMENT, False, False, True, 5)
-    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, iters, capi.NTHELEMENT, False, False, True, 5)
+    ref = orc.source_find(x, 5.0, 3.0, 0.0, True, iters, getattr(orc, method), False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, iters, getattr(capi, method), False, False, True, 5)
     assert abs(info.rms_est - ref.rms_est) <= 1e-10 * abs(ref.rms_est)
+    assert abs(info.bg_level - ref.bg_level) <= 1e-12 * max(1.0, abs(ref.bg_level))
     assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
+
+
+@pytest.mark.parametrize("method", ["ZEROMEDIAN", "BINAPPROX", "BINMEDIAN", "NTHELEMENT"])
+@pytest.mark.parametrize("rms_est", [0.0, 1.5])
+def test_stats_fused_and_pass_kernels_agree(ctx, monkeypatch, method, rms_est):
+    """Each median method, with the rms estimated or given: the fused statistics kernel and the pass kernels
+    (STPGPU_SF_STATS=passes) give the oracle's labels and islands and the same statistics."""
+    img = _clip_image("laplace", np.float64)
+    img[100:104, 200:203] += 30.0
+    ref = orc.source_find(img, 5.0, 3.0, rms_est, True, 5, getattr(orc, method), False, False, True, 5)
+    got = []
+    for mode in ("fused", "passes"):
+        if mode == "passes":
+            monkeypatch.setenv("STPGPU_SF_STATS", "passes")
+        isl, lab, info = ctx.source_find(img, 5.0, 3.0, rms_est, True, 5, getattr(capi, method), False, False, True,
+                                         5)
+        monkeypatch.delenv("STPGPU_SF_STATS", raising=False)
+        assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands), mode
+        assert abs(info.rms_est - ref.rms_est) <= 1e-10 * abs(ref.rms_est), mode
+        got.append((info.bg_level, info.rms_est))
+    assert np.allclose(got[0], got[1], rtol=1e-12, atol=0)
 
 
 def test_foreground_beyond_first_capacity():
