@@ -10,7 +10,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <initializer_list>
 #include <iterator>
+#include <utility>
 #include <cstdlib>
 #include <cstring>
 #include <functional>
@@ -34,6 +36,25 @@
 #include "aproj_kernels.cuh"
 
 using namespace stpgpu;
+
+namespace {
+// Zeroes ranges of 32-bit words (at most four) with one kernel launch.
+void zero_words(cudaStream_t st, std::initializer_list<std::pair<void*, int64_t>> ranges)
+{
+    ZeroRanges z {};
+    int64_t most = 0;
+    int r = 0;
+    for (const auto& q : ranges) {
+        z.p[r] = static_cast<uint32_t*>(q.first);
+        z.n[r] = q.second;
+        most = std::max(most, q.second);
+        r++;
+    }
+    const unsigned blocks = unsigned(std::min<int64_t>(std::max<int64_t>((most + 255) / 256, 1), 148 * 4));
+    k_zero_ranges<<<blocks, 256, 0, st>>>(z);
+    STPGPU_CHECK_LAUNCH();
+}
+} // namespace
 
 namespace {
 struct DevBuf {
@@ -444,7 +465,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     g.d_total = c->buf<double>("total", 2);
     g.d_ngood = c->buf<unsigned long long>("ngood", 2);
     g.d_err = c->buf<unsigned int>("err", 2);
-    STPGPU_CUDA_TRY(cudaMemsetAsync(g.d_err, 0, sizeof(unsigned int), st));
+    zero_words(st, { { g.d_err, 1 } });
     PrepassParams pp {};
     pp.n = n;
     pp.vis = d_vis;
@@ -464,14 +485,14 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     pp.wsum_part = wpart;
     pp.ngood_part = npart;
     pp.absw_key = wproj ? c->buf<double>("absw", nn) : nullptr;
-    pp.absw_key32 = (wproj && !s.full_wsort) ? c->buf<uint32_t>("absw32", nn) : nullptr;
+    pp.wmax_part = (wproj && !s.full_wsort) ? c->buf<double>("wmaxpart", nb_pre) : nullptr;
     pp.iota = wproj ? c->buf<uint32_t>("perm_in", nn) : nullptr;
     pp.w_out = nullptr;
     if (n > 0) {
         k_prepass<R><<<nb_pre, GRID_THREADS, 0, st>>>(pp, items);
         STPGPU_CHECK_LAUNCH();
     }
-    k_finish_wsum<<<1, 1024, 0, st>>>(wpart, npart, n > 0 ? int(nb_pre) : 0, g.d_total, g.d_ngood);
+    k_finish_wsum<<<1, 1024, 0, st>>>(wpart, npart, pp.wmax_part, n > 0 ? int(nb_pre) : 0, g.d_total, g.d_ngood);
     STPGPU_CHECK_LAUNCH();
 
     // ---- kernels
@@ -510,9 +531,9 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     }
     if (wproj && n > 0) {
         const int P = s.nplanes;
-        // |w| order (gridder.h:311-367): stable radix sort of float(|w|)
-        // rounded down (32-bit keys, half the passes of the 64-bit sort), then
-        // runs of equal 32-bit keys re-sorted by the full |w| bits; with
+        // |w| order (gridder.h:311-367): stable radix sort of 24-bit keys of
+        // |w| (k_wkey24; three digit passes instead of the eight of the 64-bit
+        // sort), then runs of equal keys re-sorted by the full |w| bits; with
         // full_wsort the IEEE bits of |w| themselves are sorted (64-bit keys;
         // non-negative doubles order as their bit patterns).
         const unsigned long long* keys64 = reinterpret_cast<const unsigned long long*>(pp.absw_key);
@@ -527,10 +548,13 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
                 != cudaSuccess)
                 fail(STPGPU_ERR_CUDA, "radix sort failed");
         } else {
-            uint32_t* k32out = c->buf<uint32_t>("absw32_sorted", nn);
-            cub::DeviceRadixSort::SortPairs(nullptr, tb, pp.absw_key32, k32out, perm_in, perm, int(n), 0, 32, st);
+            uint32_t* key24 = c->buf<uint32_t>("absw24", nn);
+            k_wkey24<<<std::min<unsigned>(grid1d(n, 256), 148 * 8), 256, 0, st>>>(pp.absw_key, n, g.d_total, key24);
+            STPGPU_CHECK_LAUNCH();
+            uint32_t* k32out = c->buf<uint32_t>("absw24_sorted", nn);
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, key24, k32out, perm_in, perm, int(n), 0, 24, st);
             void* tmp = c->buf<unsigned char>("cubtmp", tb);
-            if (cub::DeviceRadixSort::SortPairs(tmp, tb, pp.absw_key32, k32out, perm_in, perm, int(n), 0, 32, st)
+            if (cub::DeviceRadixSort::SortPairs(tmp, tb, key24, k32out, perm_in, perm, int(n), 0, 24, st)
                 != cudaSuccess)
                 fail(STPGPU_ERR_CUDA, "radix sort failed");
             k_fix_runs<<<grid1d(n, 256), 256, 0, st>>>(k32out, perm, keys64, n, g.d_err);
@@ -546,7 +570,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         k_gather_good<R><<<grid1d(n, 256), 256, 0, st>>>(perm, items, pp.absw_key, n, good_sorted, gflag, absw_sorted,
             items_sorted);
         STPGPU_CHECK_LAUNCH();
-        STPGPU_CUDA_TRY(cudaMemsetAsync(gflag + n, 0, sizeof(uint32_t), st));
+        zero_words(st, { { gflag + n, 1 } });
         size_t tb2 = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tb2, gflag, cgood, int(n + 1), st);
         void* tmp2 = c->buf<unsigned char>("cubtmp2", tb2);
@@ -561,7 +585,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
             k_wplane_values<<<P, 256, 0, st>>>(cgood, absw_sorted, good_sorted, first, last, n, P, 1, w_avg);
             STPGPU_CHECK_LAUNCH();
         } else {
-            const int nblk = int(std::min<int64_t>(1024, ceil_div(n, 2048)));
+            const int nblk = int(std::min<int64_t>(2048, ceil_div(n, 512)));
             const int64_t chunk = ceil_div(n, nblk);
             double* partial = c->buf<double>("wpartial", size_t(P) * nblk);
             k_wplane_partial<<<nblk, 256, 0, st>>>(absw_sorted, good_sorted, first, last, n, P, chunk, nblk, partial);
@@ -791,9 +815,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     bp.list = list;
     bp.list_capacity = cap;
     bp.err = g.d_err;
-    STPGPU_CUDA_TRY(cudaMemsetAsync(tcount, 0, sizeof(uint32_t) * (ntiles + 1), st));
-    STPGPU_CUDA_TRY(cudaMemsetAsync(tcur, 0, sizeof(uint32_t) * (ntiles + 1), st));
-    STPGPU_CUDA_TRY(cudaMemsetAsync(bp.rank_overflow, 0, sizeof(uint32_t), st));
+    zero_words(st, { { tcount, ntiles + 1 }, { tcur, ntiles + 1 }, { bp.rank_overflow, 1 } });
     if (n > 0) {
         k_count_tiles<R><<<grid1d(n, 256), 256, 0, st>>>(bp, bin_items, sorted_perm, plane_first, nplanes);
         STPGPU_CHECK_LAUNCH();
@@ -2330,7 +2352,8 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         // again when the binned median does not apply (the exact median), or
         // when the fused statistics kernel gave up at a barrier (the pass
         // kernels)
-        STPGPU_CUDA_TRY(cudaMemsetAsync(sfs, 0, sizeof(SfState), st));
+        static_assert(sizeof(SfState) % 4 == 0, "SfState in 32-bit words");
+        zero_words(st, { { sfs, int64_t(sizeof(SfState) / 4) } });
         enqueue_stats<T>(c, d_img, n, p, sfs, exact, fused);
         STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
             p.ccl_4connectivity, slice, cb));

@@ -56,8 +56,8 @@ struct PrepassParams {
     unsigned long long* ngood_part;
     double* absw_key; // n |w| (W-proj only), may be null
     double* w_out;    // n half-plane-converted w (W-proj), may be null
-    uint32_t* absw_key32; // n float(|w|) rounded down, as bits (W-proj), may be null
-    uint32_t* iota;       // n identity permutation (W-proj), may be null
+    double* wmax_part; // per-block maximum of |w| over samples with finite |w| (W-proj), may be null
+    uint32_t* iota;    // n identity permutation (W-proj), may be null
 };
 
 template <typename R>
@@ -65,8 +65,9 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
 {
     __shared__ double s_w[GRID_THREADS / 32];
     __shared__ unsigned long long s_n[GRID_THREADS / 32];
+    __shared__ double s_m[GRID_THREADS / 32];
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    double wgood = 0.0;
+    double wgood = 0.0, wmax = 0.0;
     unsigned long long ngood = 0;
     if (i < p.n) {
         double u, v, w = 0.0;
@@ -135,8 +136,8 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
         }
         if (p.absw_key)
             p.absw_key[i] = fabs(w);
-        if (p.absw_key32) // monotone: |a| <= |b| implies key32(a) <= key32(b)
-            p.absw_key32[i] = __float_as_uint(__double2float_rd(fabs(w)));
+        if (fabs(w) <= 1.7976931348623157e308) // finite
+            wmax = fabs(w);
         if (p.iota)
             p.iota[i] = uint32_t(i);
         if (p.w_out)
@@ -162,51 +163,101 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
     for (int o = 16; o > 0; o >>= 1) {
         wgood += __shfl_down_sync(0xffffffffu, wgood, o);
         ngood += __shfl_down_sync(0xffffffffu, ngood, o);
+        wmax = fmax(wmax, __shfl_down_sync(0xffffffffu, wmax, o));
     }
     if ((threadIdx.x & 31) == 0) {
         s_w[threadIdx.x >> 5] = wgood;
         s_n[threadIdx.x >> 5] = ngood;
+        s_m[threadIdx.x >> 5] = wmax;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0;
+        double t = 0.0, m = 0.0;
         unsigned long long c = 0;
         for (int k = 0; k < int(blockDim.x >> 5); k++) {
             t += s_w[k];
             c += s_n[k];
+            m = fmax(m, s_m[k]);
         }
         p.wsum_part[blockIdx.x] = t;
         p.ngood_part[blockIdx.x] = c;
+        if (p.wmax_part)
+            p.wmax_part[blockIdx.x] = m;
     }
 }
 
 // Sum of block partials in a fixed order (one block).  out[0] = 2 * sum
-// (the half-plane doubling of gridder.h:423), out_n[0] = count.
-__global__ void k_finish_wsum(const double* part, const unsigned long long* npart, int nb, double* out,
-    unsigned long long* out_n)
+// (the half-plane doubling of gridder.h:423), out_n[0] = count; with mpart,
+// out[1] = the largest per-block |w| maximum.
+__global__ void k_finish_wsum(const double* part, const unsigned long long* npart, const double* mpart, int nb,
+    double* out, unsigned long long* out_n)
 {
     __shared__ double s[1024];
     __shared__ unsigned long long sn[1024];
-    double t = 0.0;
+    __shared__ double sm[1024];
+    double t = 0.0, m = 0.0;
     unsigned long long c = 0;
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
         t += part[k];
         c += npart[k];
+        if (mpart)
+            m = fmax(m, mpart[k]);
     }
     s[threadIdx.x] = t;
     sn[threadIdx.x] = c;
+    sm[threadIdx.x] = m;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) {
             s[threadIdx.x] += s[threadIdx.x + o];
             sn[threadIdx.x] += sn[threadIdx.x + o];
+            sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         out[0] = s[0] * 2.0;
         out_n[0] = sn[0];
+        if (mpart)
+            out[1] = sm[0];
     }
+}
+
+// Sort keys of |w| for the W-plane order, 24 bits: x = |w| / wmax (wmax =
+// total[1], the largest finite |w|) rounded down to single precision and
+// raised to at least 2^-31; key = (bits(x) - bits(2^-31)) >> 4, which keeps
+// the 32 exponents from 2^-31 to 1 and 19 mantissa bits (largest finite key
+// 0xF80000); non-finite |w| (NaN included) take 2^24 - 1, above every finite
+// key.  Monotone: |a| <= |b| implies key(a) <= key(b), so a stable sort of
+// the keys followed by k_fix_runs (runs of equal keys re-sorted by the full
+// |w| bits, NaN after every number) gives the order of the IEEE bits of |w|.
+// The relative resolution 2^-19 keeps runs short wherever the |w| lie below
+// wmax; only |w| below 2^-31 wmax share key 0.
+__global__ void k_wkey24(const double* __restrict__ absw, int64_t n, const double* total, uint32_t* __restrict__ key)
+{
+    const double wmax = total[1];
+    const double r = wmax > 0.0 ? 1.0 / wmax : 0.0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const double a = absw[i];
+        const float x = fmaxf(__double2float_rd(a * r), 0x1p-31f);
+        key[i] = a <= wmax ? ((__float_as_uint(x) - 0x30000000u) >> 4) : 0xFFFFFFu;
+    }
+}
+
+// Zeroes up to four ranges of 32-bit words (one launch instead of several
+// memset nodes in a captured call).
+struct ZeroRanges {
+    uint32_t* p[4];
+    int64_t n[4];
+};
+__global__ void k_zero_ranges(ZeroRanges z)
+{
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, st = int64_t(gridDim.x) * blockDim.x;
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+        if (z.p[r])
+            for (int64_t i = t; i < z.n[r]; i += st)
+                z.p[r][i] = 0;
 }
 
 // ---------------------------------------------------------------- footprint segments
@@ -1988,6 +2039,7 @@ __global__ void __launch_bounds__(256) k_wplane_partial(const double* __restrict
     for (; p < P && first[p] < b; p++) {
         const int64_t s0 = max(a, first[p]), s1 = min(b, last[p]);
         double t = 0.0;
+#pragma unroll 2
         for (int64_t k = s0 + threadIdx.x; k < s1; k += blockDim.x)
             if (good_sorted[k])
                 t += absw_sorted[k];

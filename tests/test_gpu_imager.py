@@ -219,14 +219,15 @@ def test_imager_aproj_device_pointers_and_fp32c(ctx):
     assert peak_rel(img32.astype(np.float64), ri) < 1e-5
 
 
-@pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal", "oversized_bucket"])
+@pytest.mark.parametrize("pattern", ["short_runs", "long_run", "all_equal", "oversized_bucket", "outlier"])
 def test_imager_wproj_near_tied_w(ctx, pattern):
-    """|w| values that are equal in single precision but distinct in double
+    """|w| values that are equal in the 24-bit sort key but distinct in double
     (or exactly equal): the W-plane boundaries must follow the exact stable
     double order of the reference's sort.  Short runs are re-sorted after the
-    32-bit key sort; long runs of distinct values (200 of them, or 5000 within
+    24-bit key sort; long runs of distinct values (200 of them, or 5000 within
     one part in 1e6) take the 64-bit sort; exactly equal values keep index
-    order."""
+    order; one |w| 10^4 times the others (the key's scale) leaves the rest
+    resolved to 2^-19 of their own size."""
     s = _imager_case(35, 256, 6000 if pattern == "oversized_bucket" else 4000, w_range=(-600.0, 600.0))
     uvw = np.array(s.uvw, order="F")
     w = uvw[:, 2]
@@ -235,6 +236,8 @@ def test_imager_wproj_near_tied_w(ctx, pattern):
     if pattern == "short_runs":
         for k in range(0, w.size - 1, 2):  # |w| of the pair one double step apart
             w[k + 1] = np.copysign(np.nextafter(abs(w[k]), np.inf), w[k + 1])
+    elif pattern == "outlier":
+        w[17] = 6.0e6
     elif pattern == "oversized_bucket":
         # 5000 distinct |w| within one part in 1e6: runs of hundreds per single-precision key
         mags = 300.0 * (1.0 + rng.permutation(5000) * 1e-10)
