@@ -2099,9 +2099,8 @@ __global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, const 
         items_sorted[k] = it; // binning and gridding read the items in |w| order
 }
 
-// The |w| order from a stable sort on 32-bit keys (float(|w|) rounded down)
-// is exact except inside runs of equal keys, whose members are in index
-// order.  Each run is re-sorted by the full 64-bit key (the bits of |w|),
+// The |w| order from a stable sort on the 24-bit keys of k_wkey24 is exact
+// except inside runs of equal keys, whose members are in index order.  Each run is re-sorted by the full 64-bit key (the bits of |w|),
 // keeping index order among equal |w|: the result is the stable order of the
 // 64-bit sort.  Runs longer than kFixRun whose |w| are not all equal set
 // bit 4 of *err (the caller then repeats the step with the 64-bit sort).
@@ -2119,6 +2118,14 @@ __global__ void k_fix_runs(const uint32_t* __restrict__ key32, uint32_t* perm, c
     while (e < n && e - k <= kFixRun && key32[e] == kk)
         e++;
     const int len = int(e - k);
+    if (len == 2) { // the common run: one compare, no per-thread arrays
+        const uint32_t p0 = perm[k], p1 = perm[k + 1];
+        if (key64[p1] < key64[p0]) {
+            perm[k] = p1;
+            perm[k + 1] = p0;
+        }
+        return;
+    }
     if (len > kFixRun) {
         const unsigned long long first = key64[perm[k]];
         for (int64_t j = k + 1; j < n && key32[j] == kk; j++)
