@@ -238,6 +238,40 @@ def test_sigma_clip_iterations(ctx, kind, iters, dtype, method):
     assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+@pytest.mark.parametrize("case", ["two_level", "offset"])
+def test_binned_median_cases(ctx, case, dtype):
+    """The binned median (matrix_math.cpp:334-455) through the fused statistics kernel: a two-level image
+    whose cumulative count equals the rank at the lower level's bin, so the even-count walk crosses empty bins
+    to the upper level's bin; a large offset (mean 3e4 sigma), where the single-precision bin screen defers
+    most samples to double precision.  Labels and islands as the oracle's; bg_level exact for the two-level
+    image.  With the offset, sigma = sqrt(sum x^2 / n - mean^2) cancels 9e8 against 9e8 (the reference's
+    formula, matrix_math.cpp:457-499), and the clip's d^2 sums inherit it, so the oracle's sequential sums and
+    the device's tree sums agree only to that conditioning: bg_level within 1e-10 relative, rms within 1e-4
+    (measured 1e-5 and 2e-6)."""
+    rng = np.random.default_rng(31)
+    if case == "two_level":
+        img = np.empty((512, 384))
+        img[: img.shape[0] // 2] = -1.0
+        img[img.shape[0] // 2:] = 1.0
+        img[300:303, 100:103] = 40.0  # in the upper half: the lower half's count is exactly the rank
+        img[301, 101] = 41.0
+    else:
+        img = 3.0e4 + rng.normal(size=(512, 384))
+        img[300:304, 60:63] += 15.0
+    img = np.asfortranarray(img.astype(dtype))
+    x = img.astype(np.float64)
+    ref = orc.source_find(x, 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True, 5)
+    isl, lab, info = ctx.source_find(img, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5)
+    if case == "two_level":
+        assert info.bg_level == ref.bg_level
+        assert abs(info.rms_est - ref.rms_est) <= 1e-10 * abs(ref.rms_est)
+    else:
+        assert abs(info.bg_level - ref.bg_level) <= 1e-10 * abs(ref.bg_level)
+        assert abs(info.rms_est - ref.rms_est) <= 1e-4 * abs(ref.rms_est)
+    assert np.array_equal(lab, ref.label_map) and len(isl) == len(ref.islands)
+
+
 @pytest.mark.parametrize("method", ["ZEROMEDIAN", "BINAPPROX", "BINMEDIAN", "NTHELEMENT"])
 @pytest.mark.parametrize("rms_est", [0.0, 1.5])
 def test_stats_fused_and_pass_kernels_agree(ctx, monkeypatch, method, rms_est):
