@@ -2100,9 +2100,9 @@ __global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, const 
 }
 
 // The |w| order from a stable sort on the 24-bit keys of k_wkey24 is exact
-// except inside runs of equal keys, whose members are in index order.  Each run is re-sorted by the full 64-bit key (the bits of |w|),
-// keeping index order among equal |w|: the result is the stable order of the
-// 64-bit sort.  Runs longer than kFixRun whose |w| are not all equal set
+// except inside runs of equal keys, whose members are in index order.  Each
+// run is re-sorted by the full 64-bit key (the bits of |w|), keeping index
+// order among equal |w|: the result is the stable order of the 64-bit sort.  Runs longer than kFixRun whose |w| are not all equal set
 // bit 4 of *err (the caller then repeats the step with the 64-bit sort).
 constexpr int kFixRun = 32;
 __global__ void k_fix_runs(const uint32_t* __restrict__ key32, uint32_t* perm, const unsigned long long* __restrict__ key64,
