@@ -141,6 +141,28 @@ struct stpgpu_context {
     uint32_t sf_fg_cap = 0;
     int single_launches = 0; // our kernels in single_graph (counted at capture)
     int batch_launches = 0;  // our kernels in batch_graph
+    // source finder: graph of the first attempt of the last call (see
+    // run_source_find); sf_graph_off after a capture that failed
+    std::string sf_sig;
+    cudaGraph_t sf_graph = nullptr;
+    cudaGraphExec_t sf_exec = nullptr;
+    int sf_launches = 0;
+    bool sf_graph_off = false;
+    // bumped whenever a device buffer or the page-locked stage is
+    // reallocated: a captured graph whose signature holds an older value
+    // may point at freed memory
+    uint64_t buf_gen = 0;
+
+    void drop_sf_graph()
+    {
+        if (sf_exec)
+            cudaGraphExecDestroy(sf_exec);
+        if (sf_graph)
+            cudaGraphDestroy(sf_graph);
+        sf_exec = nullptr;
+        sf_graph = nullptr;
+        sf_sig.clear();
+    }
 
     void drop_single()
     {
@@ -207,6 +229,7 @@ struct stpgpu_context {
             }
             const size_t want = bytes + bytes / 8;
             const auto t0 = std::chrono::steady_clock::now();
+            buf_gen++;
             STPGPU_CUDA_TRY(cudaMalloc(&b.p, want));
             log_alloc("device buffer", ns + name, want, t0);
             b.cap = want;
@@ -227,6 +250,7 @@ struct stpgpu_context {
             pinned = nullptr;
             pinned_cap = 0;
             const auto t0 = std::chrono::steady_clock::now();
+            buf_gen++;
             STPGPU_CUDA_TRY(cudaMallocHost(&pinned, bytes));
             log_alloc("page-locked stage", ns, bytes, t0);
             pinned_cap = bytes;
@@ -284,6 +308,7 @@ struct stpgpu_context {
             cudaStreamSynchronize(w);
         drop_graph();
         drop_single();
+        drop_sf_graph();
         batch_sig.clear();
         batch_calls = 0;
         for (auto& kv : plans)
@@ -2078,6 +2103,24 @@ bool sf_passes_forced()
     return e && std::strcmp(e, "passes") == 0;
 }
 
+// The statistics' working buffers at the sizes enqueue_stats asks for, so
+// that a call sizes them before it looks at its graph signature.
+template <typename T>
+void size_stats_buffers(stpgpu_context* c, int64_t n, const stpgpu_sf_pars& p)
+{
+    const bool est = !(std::fabs(p.rms_est) > 0.0);
+    const int grid = sf_stats_grid<T>(c);
+    if (grid > 0) {
+        const int64_t G = int64_t(grid) * SF_STATS_THREADS;
+        c->buf<double>("sf_part_fused", 8 * size_t(grid));
+        if (est)
+            c->buf<T>("sf_clip_lists", size_t(sf_band_cap(n, G)) * size_t(G));
+    }
+    const unsigned nb = std::min<unsigned>(grid1d(n, SF_THREADS), 148 * SF_STREAM_BLOCKS);
+    c->buf<double>("sf_part", 3 * size_t(nb));
+    c->buf<unsigned long long>("sf_bins", BINS_N + 2);
+}
+
 // Statistics and thresholds (sourcefind.cpp:280-301) enqueued into s->st;
 // only the exact median (NTHELEMENT, BINMEDIAN, or exact = the binned
 // median's fallback) waits on the host.  With `fused` (16-byte aligned
@@ -2347,18 +2390,83 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
     };
     size_buffers();
+    auto enqueue_attempt = [&](bool exact_median, bool fused_stats) {
+        static_assert(sizeof(SfState) % 4 == 0, "SfState in 32-bit words");
+        zero_words(st, { { sfs, int64_t(sizeof(SfState) / 4) } });
+        enqueue_stats<T>(c, d_img, n, p, sfs, exact_median, fused_stats);
+        STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
+            p.ccl_4connectivity, slice, cb));
+        enqueue_analysis();
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hstate, sfs, sizeof(SfState), cudaMemcpyDeviceToHost, st));
+        STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * kFirst, cudaMemcpyDeviceToHost, st));
+    };
+    // The first attempt of a call identical to the previous one (same
+    // buffers, sizes, parameters and capacities, no reallocation since)
+    // replays a CUDA graph of it; the second such call captures it.  Calls
+    // whose median needs the host (NTHELEMENT, BINMEDIAN) run eagerly, as does
+    // every call after a capture that the runtime refused.
+    size_stats_buffers<T>(c, n, p);
+    std::string sig;
+    if (!c->timing && !c->sf_graph_off
+        && (p.median_method == STPGPU_ZEROMEDIAN || p.median_method == STPGPU_BINAPPROX)) {
+        auto put = [&](const void* q, size_t nb) { sig.append(reinterpret_cast<const char*>(q), nb); };
+        const int tsize = int(sizeof(T));
+        const int forced = sf_passes_forced() ? 1 : 0;
+        const int wl = write_labels ? 1 : 0;
+        put(&tsize, sizeof(tsize));
+        put(&rows, sizeof(rows));
+        put(&cols, sizeof(cols));
+        put(&p, sizeof(p));
+        put(&wl, sizeof(wl));
+        put(&forced, sizeof(forced));
+        put(&lcap, sizeof(lcap));
+        put(&fcap, sizeof(fcap));
+        put(&c->buf_gen, sizeof(c->buf_gen));
+        const void* ptrs[4] = { d_img, d_labels, hb, reinterpret_cast<const void*>(st) };
+        put(ptrs, sizeof(ptrs));
+    }
+    const bool repeat = !sig.empty() && sig == c->sf_sig;
+    if (!repeat) {
+        c->drop_sf_graph();
+        c->sf_sig = sig;
+    }
     bool exact = false, fused = true;
     for (int attempt = 0; attempt < 3; attempt++) {
         // again when the binned median does not apply (the exact median), or
         // when the fused statistics kernel gave up at a barrier (the pass
         // kernels)
-        static_assert(sizeof(SfState) % 4 == 0, "SfState in 32-bit words");
-        zero_words(st, { { sfs, int64_t(sizeof(SfState) / 4) } });
-        enqueue_stats<T>(c, d_img, n, p, sfs, exact, fused);
-        STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
-            p.ccl_4connectivity, slice, cb));
-        enqueue_analysis();
-        read_back_state();
+        if (attempt == 0 && repeat && c->sf_exec) {
+            STPGPU_CUDA_TRY(cudaGraphLaunch(c->sf_exec, st));
+            g_launches += c->sf_launches;
+        } else if (attempt == 0 && repeat) {
+            const int before = g_launches;
+            bool captured = false;
+            STPGPU_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_attempt(false, true);
+                STPGPU_CUDA_TRY(cudaStreamEndCapture(st, &c->sf_graph));
+                STPGPU_CUDA_TRY(cudaGraphInstantiate(&c->sf_exec, c->sf_graph, 0));
+                captured = true;
+            } catch (const Error&) {
+                cudaGraph_t dead = nullptr;
+                cudaStreamEndCapture(st, &dead); // ends a capture still open; fails harmlessly otherwise
+                if (dead)
+                    cudaGraphDestroy(dead);
+                (void)cudaGetLastError();
+                c->drop_sf_graph();
+                c->sf_graph_off = true;
+            }
+            if (captured) {
+                c->sf_launches = g_launches - before;
+                STPGPU_CUDA_TRY(cudaGraphLaunch(c->sf_exec, st));
+            } else {
+                g_launches = before;
+                enqueue_attempt(false, true);
+            }
+        } else {
+            enqueue_attempt(exact, fused);
+        }
+        STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
         if (hstate->st.stats_err && fused) {
             fused = false;
             continue;

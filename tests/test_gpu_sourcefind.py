@@ -293,6 +293,40 @@ def test_stats_fused_and_pass_kernels_agree(ctx, monkeypatch, method, rms_est):
     assert np.allclose(got[0], got[1], rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_repeated_device_calls_replay_graph_with_new_data(dtype):
+    """Identical device-pointer calls: the second captures the first attempt into a CUDA graph, later ones
+    replay it.  New pixel values written into the same device buffer between calls must be what the replay
+    reads: every call's labels and islands equal the oracle's for that call's image."""
+    import torch
+
+    fresh = capi.Context(0)
+    rng = np.random.default_rng(41)
+    rows, cols = 512, 384
+    dimg = torch.empty(rows * cols, dtype=torch.float64 if dtype == np.float64 else torch.float32, device="cuda")
+    lab = torch.empty(rows * cols, dtype=torch.int32, device="cuda")
+    try:
+        for call in range(5):
+            img = rng.normal(size=(rows, cols))
+            for _ in range(4 + call):
+                r, c = rng.integers(0, rows - 6), rng.integers(0, cols - 6)
+                img[r:r + 4, c:c + 3] += rng.choice([-9.0, 9.0])
+            img = np.asfortranarray(img.astype(dtype))
+            dimg.copy_(torch.from_numpy(img.reshape(-1, order="F").copy()))
+            torch.cuda.synchronize()
+            isl, _, info = fresh.source_find(dimg, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5,
+                                             device_ptrs=True, rows=rows, cols=cols, label_out=lab)
+            torch.cuda.synchronize()
+            got = lab.cpu().numpy().reshape((rows, cols), order="F")
+            ref = orc.source_find(img.astype(np.float64), 5.0, 3.0, 0.0, True, 5, orc.BINAPPROX, False, False, True,
+                                  5)
+            assert np.array_equal(got, ref.label_map), f"call {call}"
+            assert abs(info.rms_est - ref.rms_est) <= 1e-10 * abs(ref.rms_est)
+            _compare(isl, ref, got, ref.label_map)
+    finally:
+        fresh.close()
+
+
 def test_foreground_beyond_first_capacity():
     """A 512^2 image with a low analysis threshold has about 200 k foreground pixels, beyond the
     label-analysis capacity a fresh context starts with (n / 16 entries, at least 131072): the first call runs
