@@ -1135,7 +1135,7 @@ void finish_imager(stpgpu_context* c, const ImagerSetup& s, int image_size, int 
     // 16-byte path: every 4-row group inside one crop segment and aligned
     const bool vec4 = (image_size % 8) == 0 && (N % 4) == 0
         && (reinterpret_cast<uintptr_t>(d_image) % 16) == 0 && (!d_beam || (reinterpret_cast<uintptr_t>(d_beam) % 16) == 0);
-    const dim3 ngrid4(grid1d(image_size / 4, 256), image_size);
+    const dim3 ngrid4(grid1d(image_size / 4, 256), (image_size + kNormCols - 1) / kNormCols);
     auto normalise = [&](void* out) {
         if (vec4) {
             if (out_f32)

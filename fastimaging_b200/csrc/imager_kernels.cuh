@@ -1854,51 +1854,71 @@ __global__ void __launch_bounds__(256) k_normalise(const RI* __restrict__ img, i
 
 // Same pass, four rows per thread with 16-byte loads and stores, for
 // image_size % 8 == 0 and padded % 4 == 0 (each group of four rows then lies
-// inside one crop segment and is 16-byte aligned).  blockIdx.y = column.
+// inside one crop segment and is 16-byte aligned).  blockIdx.y = a group of
+// kNormCols output columns: a thread keeps its rows' 1/gcf for all of them
+// and has their loads in flight together (one short block per column spent
+// more time in block scheduling than in the copy).
+constexpr int kNormCols = 8;
 template <typename RI, typename RO>
 __global__ void __launch_bounds__(256) k_normalise4(const RI* __restrict__ img, int padded, int image_size,
     const double* total, const double* __restrict__ ginv, int corr, RO* __restrict__ out)
 {
-    const int j = blockIdx.y;
     const double tot = total[0];
     const double nf = tot > 0.0 ? 1.0 / tot : 0.0;
     const int hp = padded / 2, hs = image_size / 2;
-    const int oj = j < hs ? j : padded + j - image_size;
-    const int jj = j < hs ? j + hp : hp + j - image_size;
-    const double fj = corr ? nf * ginv[jj] : nf;
-    const RI* src = img + size_t(oj) * padded;
-    RO* dst = out + size_t(j) * image_size;
     const int groups = image_size / 4;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x) {
         const int i = g * 4;
         const int oi = i < hs ? i : padded - hs + (i - hs);
         const int ii = i < hs ? hp + i : hp - hs + (i - hs);
-        double v[4];
-        if constexpr (sizeof(RI) == 4) {
-            const float4 x = *reinterpret_cast<const float4*>(src + oi);
-            v[0] = x.x;
-            v[1] = x.y;
-            v[2] = x.z;
-            v[3] = x.w;
-        } else {
-            const double2 a = *reinterpret_cast<const double2*>(src + oi);
-            const double2 b = *reinterpret_cast<const double2*>(src + oi + 2);
-            v[0] = a.x;
-            v[1] = a.y;
-            v[2] = b.x;
-            v[3] = b.y;
+        double gi[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            gi[k] = corr ? ginv[ii + k] : 1.0;
+        RI x[kNormCols][4];
+#pragma unroll
+        for (int c = 0; c < kNormCols; c++) {
+            const int j = blockIdx.y * kNormCols + c;
+            if (j >= image_size)
+                break;
+            const int oj = j < hs ? j : padded + j - image_size;
+            const RI* src = img + size_t(oj) * padded + oi;
+            if constexpr (sizeof(RI) == 4) {
+                const float4 q = *reinterpret_cast<const float4*>(src);
+                x[c][0] = q.x;
+                x[c][1] = q.y;
+                x[c][2] = q.z;
+                x[c][3] = q.w;
+            } else {
+                const double2 a = *reinterpret_cast<const double2*>(src);
+                const double2 b = *reinterpret_cast<const double2*>(src + 2);
+                x[c][0] = a.x;
+                x[c][1] = a.y;
+                x[c][2] = b.x;
+                x[c][3] = b.y;
+            }
         }
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            v[k] *= fj;
-            if (corr)
-                v[k] *= ginv[ii + k];
-        }
-        if constexpr (sizeof(RO) == 4) {
-            *reinterpret_cast<float4*>(dst + i) = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
-        } else {
-            *reinterpret_cast<double2*>(dst + i) = make_double2(v[0], v[1]);
-            *reinterpret_cast<double2*>(dst + i + 2) = make_double2(v[2], v[3]);
+        for (int c = 0; c < kNormCols; c++) {
+            const int j = blockIdx.y * kNormCols + c;
+            if (j >= image_size)
+                break;
+            const int jj = j < hs ? j + hp : hp + j - image_size;
+            const double fj = corr ? nf * ginv[jj] : nf;
+            double v[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                v[k] = double(x[c][k]) * fj;
+                if (corr)
+                    v[k] *= gi[k];
+            }
+            RO* dst = out + size_t(j) * image_size + i;
+            if constexpr (sizeof(RO) == 4) {
+                *reinterpret_cast<float4*>(dst) = make_float4(float(v[0]), float(v[1]), float(v[2]), float(v[3]));
+            } else {
+                *reinterpret_cast<double2*>(dst) = make_double2(v[0], v[1]);
+                *reinterpret_cast<double2*>(dst + 2) = make_double2(v[2], v[3]);
+            }
         }
     }
 }
