@@ -487,7 +487,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     const unsigned nb_pre = grid1d(n, GRID_THREADS);
     double* wpart = c->buf<double>("wpart", nb_pre);
     unsigned long long* npart = c->buf<unsigned long long>("npart", nb_pre);
-    g.d_total = c->buf<double>("total", 2);
+    g.d_total = c->buf<double>("total", 4);
     g.d_ngood = c->buf<unsigned long long>("ngood", 2);
     g.d_err = c->buf<unsigned int>("err", 2);
     zero_words(st, { { g.d_err, 1 } });
@@ -510,7 +510,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     pp.wsum_part = wpart;
     pp.ngood_part = npart;
     pp.absw_key = wproj ? c->buf<double>("absw", nn) : nullptr;
-    pp.wmax_part = (wproj && !s.full_wsort) ? c->buf<double>("wmaxpart", nb_pre) : nullptr;
+    pp.wmax_part = (wproj && !s.full_wsort) ? c->buf<double>("wmaxpart", 2 * size_t(nb_pre)) : nullptr;
     pp.iota = wproj ? c->buf<uint32_t>("perm_in", nn) : nullptr;
     pp.w_out = nullptr;
     if (n > 0) {

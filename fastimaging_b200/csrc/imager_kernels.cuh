@@ -56,7 +56,7 @@ struct PrepassParams {
     unsigned long long* ngood_part;
     double* absw_key; // n |w| (W-proj only), may be null
     double* w_out;    // n half-plane-converted w (W-proj), may be null
-    double* wmax_part; // per-block maximum of |w| over samples with finite |w| (W-proj), may be null
+    double* wmax_part; // per block: the maximum and the sum of the finite |w| (W-proj), may be null
     uint32_t* iota;    // n identity permutation (W-proj), may be null
 };
 
@@ -65,9 +65,9 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
 {
     __shared__ double s_w[GRID_THREADS / 32];
     __shared__ unsigned long long s_n[GRID_THREADS / 32];
-    __shared__ double s_m[GRID_THREADS / 32];
+    __shared__ double s_m[GRID_THREADS / 32], s_a[GRID_THREADS / 32];
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    double wgood = 0.0, wmax = 0.0;
+    double wgood = 0.0, wmax = 0.0, wabs = 0.0;
     unsigned long long ngood = 0;
     if (i < p.n) {
         double u, v, w = 0.0;
@@ -136,8 +136,10 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
         }
         if (p.absw_key)
             p.absw_key[i] = fabs(w);
-        if (fabs(w) <= 1.7976931348623157e308) // finite
+        if (fabs(w) <= 1.7976931348623157e308) { // finite
             wmax = fabs(w);
+            wabs = fabs(w);
+        }
         if (p.iota)
             p.iota[i] = uint32_t(i);
         if (p.w_out)
@@ -164,83 +166,108 @@ __global__ void k_prepass(PrepassParams p, Item<R>* items)
         wgood += __shfl_down_sync(0xffffffffu, wgood, o);
         ngood += __shfl_down_sync(0xffffffffu, ngood, o);
         wmax = fmax(wmax, __shfl_down_sync(0xffffffffu, wmax, o));
+        wabs += __shfl_down_sync(0xffffffffu, wabs, o);
     }
     if ((threadIdx.x & 31) == 0) {
         s_w[threadIdx.x >> 5] = wgood;
         s_n[threadIdx.x >> 5] = ngood;
         s_m[threadIdx.x >> 5] = wmax;
+        s_a[threadIdx.x >> 5] = wabs;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t = 0.0, m = 0.0;
+        double t = 0.0, m = 0.0, a = 0.0;
         unsigned long long c = 0;
         for (int k = 0; k < int(blockDim.x >> 5); k++) {
             t += s_w[k];
             c += s_n[k];
             m = fmax(m, s_m[k]);
+            a += s_a[k];
         }
         p.wsum_part[blockIdx.x] = t;
         p.ngood_part[blockIdx.x] = c;
-        if (p.wmax_part)
-            p.wmax_part[blockIdx.x] = m;
+        if (p.wmax_part) {
+            p.wmax_part[2 * blockIdx.x] = m;
+            p.wmax_part[2 * blockIdx.x + 1] = a;
+        }
     }
 }
 
 // Sum of block partials in a fixed order (one block).  out[0] = 2 * sum
 // (the half-plane doubling of gridder.h:423), out_n[0] = count; with mpart,
-// out[1] = the largest per-block |w| maximum.
+// out[1] = the largest finite |w| and out[2] = the sum of the finite |w|.
 __global__ void k_finish_wsum(const double* part, const unsigned long long* npart, const double* mpart, int nb,
     double* out, unsigned long long* out_n)
 {
     __shared__ double s[1024];
     __shared__ unsigned long long sn[1024];
-    __shared__ double sm[1024];
-    double t = 0.0, m = 0.0;
+    __shared__ double sm[1024], sa[1024];
+    double t = 0.0, m = 0.0, a = 0.0;
     unsigned long long c = 0;
     for (int k = threadIdx.x; k < nb; k += blockDim.x) {
         t += part[k];
         c += npart[k];
-        if (mpart)
-            m = fmax(m, mpart[k]);
+        if (mpart) {
+            m = fmax(m, mpart[2 * k]);
+            a += mpart[2 * k + 1];
+        }
     }
     s[threadIdx.x] = t;
     sn[threadIdx.x] = c;
     sm[threadIdx.x] = m;
+    sa[threadIdx.x] = a;
     __syncthreads();
     for (int o = blockDim.x / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) {
             s[threadIdx.x] += s[threadIdx.x + o];
             sn[threadIdx.x] += sn[threadIdx.x + o];
             sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + o]);
+            sa[threadIdx.x] += sa[threadIdx.x + o];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
         out[0] = s[0] * 2.0;
         out_n[0] = sn[0];
-        if (mpart)
+        if (mpart) {
             out[1] = sm[0];
+            out[2] = sa[0];
+        }
     }
 }
 
-// Sort keys of |w| for the W-plane order, 24 bits: x = |w| / wmax (wmax =
-// total[1], the largest finite |w|) rounded down to single precision and
-// raised to at least 2^-31; key = (bits(x) - bits(2^-31)) >> 4, which keeps
-// the 32 exponents from 2^-31 to 1 and 19 mantissa bits (largest finite key
-// 0xF80000); non-finite |w| (NaN included) take 2^24 - 1, above every finite
-// key.  Monotone: |a| <= |b| implies key(a) <= key(b), so a stable sort of
-// the keys followed by k_fix_runs (runs of equal keys re-sorted by the full
-// |w| bits, NaN after every number) gives the order of the IEEE bits of |w|.
-// The relative resolution 2^-19 keeps runs short wherever the |w| lie below
-// wmax; only |w| below 2^-31 wmax share key 0.
+// Sort keys of |w| for the W-plane order, 24 bits, monotone in |w| (|a| <=
+// |b| implies key(a) <= key(b)), so that a stable sort of the keys followed
+// by k_fix_runs (runs of equal keys re-sorted by the full |w| bits, NaN after
+// every number) gives the order of the IEEE bits of |w|.  With x = |w| /
+// wmax (wmax = total[1], the largest finite |w|), two encodings, chosen by
+// how far the mean |w| (total[2] / n) sits below wmax so that runs of equal
+// keys stay short:
+//  * spread |w| (mean >= wmax / 16): floor(sqrt(x) (2^24 - 2)), resolution
+//    2^-24 in sqrt(x) (about 8 % of the headline snapshot's keys in runs);
+//  * |w| concentrated far below wmax: x rounded down to single precision and
+//    raised to at least 2^-31, key = (bits(x) - bits(2^-31)) >> 4 (the 32
+//    exponents from 2^-31 to 1 and 19 mantissa bits: relative resolution
+//    2^-19 at every scale).
+// Non-finite |w| (NaN included) take 2^24 - 1, above every finite key.
 __global__ void k_wkey24(const double* __restrict__ absw, int64_t n, const double* total, uint32_t* __restrict__ key)
 {
     const double wmax = total[1];
     const double r = wmax > 0.0 ? 1.0 / wmax : 0.0;
+    const bool spread = wmax > 0.0 && total[2] >= wmax * 0.0625 * double(n);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         const double a = absw[i];
-        const float x = fmaxf(__double2float_rd(a * r), 0x1p-31f);
-        key[i] = a <= wmax ? ((__float_as_uint(x) - 0x30000000u) >> 4) : 0xFFFFFFu;
+        uint32_t k = 0xFFFFFFu;
+        if (a <= wmax) {
+            if (spread) {
+                const double q = __dsqrt_rn(a * r) * 16777214.0;
+                k = q < 16777214.0 ? uint32_t(q) : 16777214u;
+            } else {
+                const float x = fmaxf(__double2float_rd(a * r), 0x1p-31f);
+                k = (__float_as_uint(x) - 0x30000000u) >> 4;
+            }
+        }
+        key[i] = k;
     }
 }
 
