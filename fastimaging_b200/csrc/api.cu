@@ -17,6 +17,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <set>
 #include <unordered_map>
 #include <chrono>
 #include <thread>
@@ -216,6 +217,9 @@ struct stpgpu_context {
     cudaGraphExec_t sf_exec = nullptr;
     int sf_launches = 0;
     bool sf_graph_off = false;
+    // size classes whose last single call could not take the W-planes
+    // without the |w| sort (their calls sort)
+    std::set<std::string> wsel_off;
     // bumped whenever a device buffer or the page-locked stage is
     // reallocated: a captured graph whose signature holds an older value
     // may point at freed memory
@@ -443,6 +447,7 @@ struct ImagerSetup {
     int nplanes = 0, max_support = 0, undersampling = 1, wmedian = 0;
     double trunc_perc = 0.0;
     int full_wsort = 0; // |w| order from the 64-bit sort (fallback of the 32-bit sort + run fix-up)
+    int wsel = 0;       // W-planes without the |w| sort (k_wsel_*; single calls, falls back through error bit 16)
     int hankel = 0, proj_slice = 0, cubic = 0; // Hankel-transform W-kernels (hankel_opt)
     // A-projection: time steps, rotated-kernel option, pointing (radians),
     // per-visibility hour angles (device pointer once the call has staged
@@ -622,7 +627,42 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
             k1d = reinterpret_cast<const R*>(t32);
         }
     }
-    if (wproj && n > 0) {
+    const uint16_t* plane16 = nullptr;
+    if (wproj && n > 0 && s.wsel) {
+        // the planes without sorting (k_wsel_*, see imager_kernels.cuh); a
+        // condition it cannot meet sets error bit 16 and the caller grids
+        // again on the sorting path
+        const int P = s.nplanes;
+        uint32_t* key24 = c->buf<uint32_t>("absw24", nn);
+        const unsigned g2 = std::min<unsigned>(grid1d(n, 256), 148 * 8);
+        k_wkey24<<<g2, 256, 0, st>>>(pp.absw_key, n, g.d_total, key24);
+        STPGPU_CHECK_LAUNCH();
+        WselState* ws = c->buf<WselState>("wsel", 1);
+        zero_words(st, { { ws, int64_t(kWselZeroWords) } });
+        k_wsel_hist<<<std::min<unsigned>(grid1d(n, 256), 148 * 4), 256, 0, st>>>(key24, n, ws);
+        STPGPU_CHECK_LAUNCH();
+        k_wsel_plan<<<1, 1024, 0, st>>>(ws, n, P, g.d_ngood, g.d_err);
+        STPGPU_CHECK_LAUNCH();
+        // members of the start bins: at most P - 1 bins of WSEL_CAP
+        unsigned long long* mbits = c->buf<unsigned long long>("wsel_mb", size_t(std::max(P - 1, 1)) * WSEL_CAP);
+        uint32_t* midx = c->buf<uint32_t>("wsel_mi", size_t(std::max(P - 1, 1)) * WSEL_CAP);
+        k_wsel_collect<<<g2, 256, 0, st>>>(key24, pp.absw_key, n, ws, mbits, midx);
+        STPGPU_CHECK_LAUNCH();
+        if (P > 1) {
+            k_wsel_resolve<<<P - 1, 256, 0, st>>>(ws, mbits, midx);
+            STPGPU_CHECK_LAUNCH();
+        }
+        uint16_t* pl = c->buf<uint16_t>("wsel_plane", nn);
+        k_wsel_classify<<<g2, 256, 0, st>>>(pp.absw_key, n, P, g.d_total, ws, pl, g.d_err);
+        STPGPU_CHECK_LAUNCH();
+        int64_t* first = c->buf<int64_t>("pfirst", P);
+        double* w_avg = c->buf<double>("wavg", P);
+        k_wsel_finish<<<1, 256, 0, st>>>(ws, n, P, g.d_total, w_avg, first);
+        STPGPU_CHECK_LAUNCH();
+        plane16 = pl;
+        plane_first = first;
+        nplanes = P;
+    } else if (wproj && n > 0) {
         const int P = s.nplanes;
         // |w| order (gridder.h:311-367): stable radix sort of 24-bit keys of
         // |w| (k_wkey24; three digit passes instead of the eight of the 64-bit
@@ -689,7 +729,10 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         sorted_perm = perm;
         plane_first = first;
         nplanes = P;
-
+    }
+    if (wproj && n > 0) {
+        const int P = s.nplanes;
+        double* w_avg = c->buf<double>("wavg", P); // the plane means, from either path above
         // W-kernels in FP64 (WideFieldImaging, aw_projection.cpp:19-111,173-210,366-452)
         const int K = 2 * s.max_support + 1;
         const int u = s.undersampling > 0 ? int(std::pow(2, s.undersampling - 1)) : 0;
@@ -888,6 +931,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     uint32_t* list = (large_support(s) || use_recs) ? nullptr : c->buf<uint32_t>("tlist", cap);
     Item<R>* bin_items = items_sorted ? items_sorted : items;
     BinParams bp {};
+    bp.plane16 = plane16;
     bp.N = N;
     bp.image_rows = image_rows;
     bp.tiles_r = tiles_r;
@@ -1135,8 +1179,10 @@ ScalarsBack read_back(stpgpu_context* c, const GridOut& g)
     // bit 4: the 32-bit |w| sort met a long run of distinct |w| (the caller
     // repeats the gridding with the 64-bit sort); bit 8: the staged
     // gridder's records exceeded their capacity (the caller grids again with
-    // the buffer sized from the count); other bits are errors
-    if (r.err & ~(4u | 8u))
+    // the buffer sized from the count); bit 16: the W-planes without the
+    // sort did not apply (the caller grids again on the sorting path); other
+    // bits are errors
+    if (r.err & ~(4u | 8u | 16u))
         fail(STPGPU_ERR_DEVICE, "gridder reported internal error flags " + std::to_string(r.err));
     return r;
 }
@@ -1307,11 +1353,18 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
         fail(STPGPU_ERR_INVALID_ARG, "image_size must be even, > 0 and <= padded_image_size");
     ImagerSetup s = s_in;
     s.wide_fft = (COMP == 1 && wide_fft_needed(s, image_size, correction)) ? 1 : 0;
+    // W-planes without the |w| sort where they apply (mean |w| per plane, no
+    // A-projection time steps); a size class whose data did not allow it on
+    // its last call (visibilities outside the grid, non-finite w) sorts
+    s.wsel = s.nplanes > 0 && s.nplanes <= WSEL_MAXP && !s.wmedian && s.ntimesteps == 0 && !s.full_wsort
+        && n < (int64_t(1) << 31);
     // tile width: the autotuned choice of this size class; the first call of
     // a class grids with both widths, times them, keeps the faster for later
     // calls (every pass produces the complete grid; the last one is used)
     const int precision = sizeof(R) == 8 ? STPGPU_FP64 : (COMP ? STPGPU_FP32C : STPGPU_FP32);
     const std::string cls = size_class(s, precision);
+    if (s.wsel && c->wsel_off.count(cls))
+        s.wsel = 0;
     GridOut g;
     // STPGPU_GRIDDER_LAYOUT=32|16|32c|16c|32t|16t|8t|32r|16r|8r pins the tile
     // width and gridder form (c: column-packed, t: lane-per-tap, r: staged
@@ -1444,6 +1497,18 @@ void run_imager(stpgpu_context* c, const ImagerSetup& s_in, int image_size, int 
         for (auto it = c->rec_ratio.begin(); it != c->rec_ratio.end();)
             it = it->first.compare(0, c->ns.size() + 1, c->ns + "/") == 0 ? c->rec_ratio.erase(it) : std::next(it);
         c->drop_single();
+        int lay = TILE_C_DEFAULT;
+        c->tune_get(cls, lay);
+        g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr, form_of(lay));
+        finish_imager<R>(c, s, image_size, correction, g, d_image, d_beam, out_f32);
+        sb = read_back(c, g);
+    }
+    if (sb.err & 16u) {
+        // the W-planes without the sort did not apply: the sorting path, for
+        // this call and the size class's next ones
+        c->wsel_off.insert(cls);
+        c->drop_single();
+        s.wsel = 0;
         int lay = TILE_C_DEFAULT;
         c->tune_get(cls, lay);
         g = run_gridder<R, COMP>(c, s, d_vis, vis_c64, d_wts, d_uvw, 0, n, lay & 0xff, nullptr, form_of(lay));

@@ -343,6 +343,7 @@ struct BinParams {
     int tile_c;              // tile width in grid columns (TILE_R rows per tile)
     int support;             // non-W-proj support
     const int* plane_support; // W-proj truncated support per plane (nullable)
+    const uint16_t* plane16;  // W-proj without the |w| sort: plane of each item (input order), else null
     const uint8_t* ts_of;     // A-projection: time step per visibility (nullable)
     int ntimesteps;           // planes are indexed plane * ntimesteps + step
     int exact;               // rows wrap negative (exact gridder)
@@ -498,7 +499,9 @@ __global__ void k_count_tiles(BinParams p, const Item<R>* items, const uint32_t*
     if (!it.good)
         return;
     int S = p.support;
-    if (order) {
+    if (p.plane16) {
+        S = p.plane_support[p.plane16[k]];
+    } else if (order) {
         int plane = plane_of(first, P, k);
         if (p.ts_of)
             plane = plane * p.ntimesteps + p.ts_of[order[k]];
@@ -534,7 +537,11 @@ __global__ void k_fill_tiles(BinParams p, Item<R>* items, const uint32_t* order,
     if (!it.good)
         return;
     int S = p.support;
-    if (order) {
+    if (p.plane16) {
+        const int plane = p.plane16[k];
+        S = p.plane_support[plane];
+        items[k].plane = uint16_t(plane);
+    } else if (order) {
         int plane = plane_of(first, P, k);
         if (p.ts_of)
             plane = plane * p.ntimesteps + p.ts_of[order[k]];
@@ -1398,7 +1405,11 @@ __global__ void k_fill_recs(BinParams p, Item<R>* items, const uint32_t* order, 
     if (!it.good)
         return;
     int S = p.support, plane = 0;
-    if (order) {
+    if (p.plane16) {
+        plane = p.plane16[k];
+        S = p.plane_support[plane];
+        items[k].plane = uint16_t(plane);
+    } else if (order) {
         plane = plane_of(first, P, k);
         if (p.ts_of)
             plane = plane * p.ntimesteps + p.ts_of[order[k]];
@@ -2144,6 +2155,352 @@ __global__ void k_gather_good(const uint32_t* perm, const Item<R>* items, const 
         absw_sorted[k] = absw[i];
     if (items_sorted)
         items_sorted[k] = it; // binning and gridding read the items in |w| order
+}
+
+// ---------------------------------------------------------------- W-planes without the |w| sort
+//
+// The reference's W-planes (gridder.cpp:68-146) take equal counts of the
+// |w|-sorted visibilities.  When every visibility is good, plane p holds the
+// sorted ranks [G_p, G_p+1) with G_0 = 0, G_p+1 = G_p + ceil((n - G_p) / (P -
+// p)), so an item's plane follows from how many plane-start items precede
+// it in the sort order ((|w| bits, input index), the stable order).  Those
+// P - 1 items are found without sorting: a histogram of the 24-bit keys'
+// top 12 bits (k_wsel_hist) places each start rank in a bin and at a rank
+// within it (k_wsel_plan); the members of those bins are collected
+// (k_wsel_collect) and each start item is the member of its bin with the
+// wanted rank under the exact order (k_wsel_resolve: every member counts the
+// members before it).  k_wsel_classify then gives every item its plane (a
+// binary search over the start items) and sums |w| per plane exactly, in
+// 64-bit fixed point relative to the plane's smallest |w| (so the sums do
+// not depend on the order of the additions); k_wsel_finish forms the means
+// and plane starts.  Items not all good, non-finite |w|, more than WSEL_MAXP
+// planes or a start bin of more than WSEL_CAP members set bit 16 of the
+// error word: the host then runs the sorting path.
+constexpr int WSEL_BINS_LOG = 16;
+constexpr int WSEL_BINS = 1 << WSEL_BINS_LOG; // key24 >> 8
+constexpr int WSEL_CAP = 2048;  // members of a start item's bin that k_wsel_resolve holds
+constexpr int WSEL_MAXP = 1024; // planes
+
+struct WselState {
+    // zeroed before the pass
+    uint32_t hist[WSEL_BINS];
+    uint32_t cursor[WSEL_MAXP];
+    unsigned long long sum[WSEL_MAXP];
+    // written by k_wsel_plan / k_wsel_resolve
+    int32_t binmap[WSEL_BINS];      // list of a start bin, -1 otherwise
+    uint32_t list_off[WSEL_MAXP + 1];
+    uint32_t list_cnt[WSEL_MAXP];
+    int32_t start_list[WSEL_MAXP];  // per plane p >= 1: its start item's list
+    uint32_t start_rank[WSEL_MAXP]; // and rank within the list's bin
+    uint32_t start_bin[WSEL_MAXP];
+    unsigned long long start_bits[WSEL_MAXP]; // the start item: |w| bits, input index
+    uint32_t start_idx[WSEL_MAXP];
+    int64_t G[WSEL_MAXP + 1];
+    int valid;
+};
+constexpr size_t kWselZeroWords = (sizeof(uint32_t) * (WSEL_BINS + WSEL_MAXP) + sizeof(unsigned long long) * WSEL_MAXP) / 4;
+
+__global__ void __launch_bounds__(256) k_wsel_hist(const uint32_t* __restrict__ key24, int64_t n, WselState* ws)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        atomicAdd(&ws->hist[key24[i] >> (24 - WSEL_BINS_LOG)], 1u);
+    // no start bins yet (k_wsel_plan marks them)
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < WSEL_BINS; b += gridDim.x * blockDim.x)
+        ws->binmap[b] = -1;
+}
+
+// Exclusive scan over the 1024 threads of a block of the values v; *total =
+// their sum.
+__device__ __forceinline__ uint32_t wsel_block_scan(uint32_t v, uint32_t* total)
+{
+    __shared__ uint32_t wsum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+            x += y;
+    }
+    if (lane == 31)
+        wsum[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o)
+                w += y;
+        }
+        wsum[lane] = w; // inclusive over the warps
+    }
+    __syncthreads();
+    const uint32_t r = x - v + (warp ? wsum[warp - 1] : 0u);
+    *total = wsum[31];
+    __syncthreads();
+    return r;
+}
+
+// One block of 1024 threads.  The plane starts have a closed form: with q =
+// n / P and r = n % P, ceil((n - G_p) / (P - p)) = q + [p < r], so G_p = p q +
+// min(p, r).  Thread t sums bins [64 t, 64 t + 64) (16-byte loads); a block
+// scan of those totals locates each start rank's chunk, and the plane's
+// thread walks the chunk's 64 bins to the bin and the rank within it.  The
+// start bins become lists in plane order.
+__global__ void __launch_bounds__(1024) k_wsel_plan(WselState* ws, int64_t n, int P, const unsigned long long* ngood,
+    unsigned int* err)
+{
+    constexpr int PER = WSEL_BINS / 1024;
+    __shared__ uint32_t chunk[1025]; // prefix at each thread's first bin
+    const int tid = threadIdx.x;
+    const bool ok0 = ngood[0] == (unsigned long long)n && P >= 1 && P <= WSEL_MAXP;
+    const uint4* h4 = reinterpret_cast<const uint4*>(ws->hist + PER * tid);
+    uint32_t t = 0;
+#pragma unroll
+    for (int q = 0; q < PER / 4; q++) {
+        const uint4 v = h4[q];
+        t += v.x + v.y + v.z + v.w;
+    }
+    uint32_t total = 0;
+    const uint32_t excl = wsel_block_scan(t, &total);
+    chunk[tid] = excl;
+    if (tid == 0)
+        chunk[1024] = total;
+    const int64_t qn = P >= 1 ? n / P : 0, rn = P >= 1 ? n % P : 0;
+    auto G = [&](int p) { return int64_t(p) * qn + (int64_t(p) < rn ? int64_t(p) : rn); };
+    if (ok0)
+        for (int p = tid; p <= P; p += blockDim.x)
+            ws->G[p] = G(p);
+    __syncthreads();
+    // plane p = tid: its start item's bin (the last b whose prefix is <= G_p)
+    // and rank within it, and the bin's size
+    const int p = tid;
+    const bool has = ok0 && p >= 1 && p < P && G(p) < n;
+    uint32_t bin = 0, m = 0;
+    if (has) {
+        const uint32_t gp = uint32_t(G(p));
+        int lo = 0, hi = 1023;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (chunk[mid] <= gp)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const uint4* c4 = reinterpret_cast<const uint4*>(ws->hist + PER * lo);
+        uint32_t before = chunk[lo];
+        bool found = false;
+        for (int q = 0; q < PER / 4 && !found; q++) {
+            const uint4 v = c4[q];
+            const uint32_t w[4] = { v.x, v.y, v.z, v.w };
+            for (int e = 0; e < 4; e++) {
+                if (before + w[e] > gp) { // rank gp lies in this bin
+                    bin = uint32_t(PER * lo + 4 * q + e);
+                    m = w[e];
+                    found = true;
+                    break;
+                }
+                before += w[e];
+            }
+        }
+        ws->start_bin[p] = bin;
+        ws->start_rank[p] = gp - before;
+    }
+    __shared__ uint32_t sbin[1024];
+    __shared__ int bad;
+    sbin[tid] = bin;
+    if (tid == 0)
+        bad = !ok0;
+    __syncthreads();
+    // a start bin opens a list unless the previous plane's start is in it
+    const bool opens = has && !(p >= 2 && G(p - 1) < n && sbin[p - 1] == bin);
+    if (opens && m > uint32_t(WSEL_CAP))
+        bad = 1;
+    uint32_t nlist = 0, noff = 0;
+    const uint32_t li = wsel_block_scan(opens ? 1u : 0u, &nlist);
+    const uint32_t off = wsel_block_scan(opens ? m : 0u, &noff);
+    __shared__ uint32_t slist[1024];
+    slist[tid] = opens ? li : 0u;
+    __syncthreads();
+    if (bad) {
+        if (tid == 0) {
+            ws->valid = 0;
+            atomicOr(err, 16u);
+        }
+        return;
+    }
+    if (opens) {
+        ws->binmap[bin] = int32_t(li);
+        ws->list_off[li] = off;
+        ws->list_cnt[li] = m;
+    }
+    if (p >= 1 && p < P) {
+        // the list of this plane's start: that of the last plane up to p that
+        // opened one (planes after the items run out have none)
+        int32_t l = -1;
+        if (has) {
+            int q = p;
+            while (q >= 2 && G(q - 1) < n && sbin[q - 1] == bin)
+                q--;
+            l = int32_t(slist[q]);
+        }
+        ws->start_list[p] = l;
+    }
+    if (tid == 0) {
+        ws->list_off[nlist] = noff;
+        ws->valid = 1;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_wsel_collect(const uint32_t* __restrict__ key24, const double* __restrict__ absw,
+    int64_t n, WselState* ws, unsigned long long* mbits, uint32_t* midx)
+{
+    if (!ws->valid)
+        return;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const int li = ws->binmap[key24[i] >> (24 - WSEL_BINS_LOG)];
+        if (li >= 0) {
+            const uint32_t pos = ws->list_off[li] + atomicAdd(&ws->cursor[li], 1u);
+            mbits[pos] = __double_as_longlong(absw[i]);
+            midx[pos] = uint32_t(i);
+        }
+    }
+}
+
+// One block per plane p >= 1: the member of the start item's bin whose rank
+// under (|w| bits, index) is the wanted one.
+__global__ void __launch_bounds__(256) k_wsel_resolve(WselState* ws, const unsigned long long* mbits, const uint32_t* midx)
+{
+    __shared__ unsigned long long sb[WSEL_CAP];
+    __shared__ uint32_t si[WSEL_CAP];
+    const int p = blockIdx.x + 1;
+    if (!ws->valid)
+        return;
+    const int li = ws->start_list[p];
+    if (li < 0) {
+        if (threadIdx.x == 0) {
+            ws->start_bits[p] = ~0ull; // after every item: the plane and all later ones are empty
+            ws->start_idx[p] = ~0u;
+        }
+        return;
+    }
+    const uint32_t off = ws->list_off[li], m = ws->list_cnt[li], want = ws->start_rank[p];
+    for (uint32_t e = threadIdx.x; e < m; e += blockDim.x) {
+        sb[e] = mbits[off + e];
+        si[e] = midx[off + e];
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < m; e += blockDim.x) {
+        const unsigned long long b = sb[e];
+        const uint32_t ix = si[e];
+        uint32_t r = 0;
+        for (uint32_t f = 0; f < m; f++)
+            r += (sb[f] < b || (sb[f] == b && si[f] < ix)) ? 1u : 0u;
+        if (r == want) {
+            ws->start_bits[p] = b;
+            ws->start_idx[p] = ix;
+        }
+    }
+}
+
+// Plane p's smallest |w| (its start item's; 0 for plane 0) and the fixed-point
+// scale of its sums: 2^e with (width * count) * 2^e <= 2^61, width = the
+// plane's |w| range (up to the next start item, or wmax).
+__device__ __forceinline__ void wsel_range(const WselState* ws, int p, int P, int64_t n, double wmax, double& lo,
+    double& scale)
+{
+    const int64_t cnt = ws->G[p + 1] - ws->G[p];
+    lo = p == 0 ? 0.0 : __longlong_as_double((long long)ws->start_bits[p]);
+    const double hi = (p + 1 < P && ws->G[p + 1] < n) ? __longlong_as_double((long long)ws->start_bits[p + 1]) : wmax;
+    const double span = (hi - lo) * double(cnt);
+    if (cnt <= 0 || !(span > 0.0)) {
+        scale = 1.0;
+        return;
+    }
+    int ex;
+    frexp(span, &ex); // span < 2^ex
+    scale = ldexp(1.0, 61 - ex);
+}
+
+__global__ void __launch_bounds__(256) k_wsel_classify(const double* __restrict__ absw, int64_t n, int P,
+    const double* total, WselState* ws, uint16_t* plane16, unsigned int* err)
+{
+    __shared__ unsigned long long sbits[WSEL_MAXP];
+    __shared__ uint32_t sidx[WSEL_MAXP];
+    __shared__ double slo[WSEL_MAXP], sscale[WSEL_MAXP];
+    // the sums: one copy per warp when the planes fit (less contention on
+    // the shared atomics), else one copy for the block
+    __shared__ unsigned long long acc[WSEL_MAXP];
+    constexpr int kWarpCopyP = WSEL_MAXP / 8;
+    const int copies = P <= kWarpCopyP ? 8 : 1;
+    if (!ws->valid) {
+        // plane 0 for every item: the binning that follows stays in bounds
+        // (the host grids again on the sorting path)
+        for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+            plane16[i] = 0;
+        return;
+    }
+    const double wmax = total[1];
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        sbits[p] = p == 0 ? 0ull : ws->start_bits[p];
+        sidx[p] = p == 0 ? 0u : ws->start_idx[p];
+        wsel_range(ws, p, P, n, wmax, slo[p], sscale[p]);
+    }
+    for (int q = threadIdx.x; q < copies * P; q += blockDim.x)
+        acc[q] = 0;
+    __syncthreads();
+    unsigned long long* myacc = acc + (copies > 1 ? ((threadIdx.x >> 5) & 7) * P : 0);
+    bool bad = false;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+        const double a = absw[i];
+        if (!(a <= wmax)) { // non-finite |w|
+            plane16[i] = 0;
+            bad = true;
+            continue;
+        }
+        const unsigned long long b = __double_as_longlong(a);
+        const uint32_t ix = uint32_t(i);
+        // the last plane whose start item is at or before (b, ix)
+        int lo = 0, hi = P - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (sbits[mid] < b || (sbits[mid] == b && sidx[mid] <= ix))
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        plane16[i] = uint16_t(lo);
+        const double d = a - slo[lo];
+        atomicAdd(&myacc[lo], (unsigned long long)rint(d * sscale[lo]));
+    }
+    if (bad)
+        atomicOr(err, 16u);
+    __syncthreads();
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        unsigned long long v = 0;
+        for (int c = 0; c < copies; c++)
+            v += acc[c * P + p];
+        if (v)
+            atomicAdd(&ws->sum[p], v);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_wsel_finish(const WselState* ws, int64_t n, int P, const double* total,
+    double* w_avg, int64_t* first)
+{
+    if (!ws->valid) {
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            w_avg[p] = 0.0;
+            first[p] = 0;
+        }
+        return;
+    }
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        double lo, scale;
+        wsel_range(ws, p, P, n, total[1], lo, scale);
+        const int64_t cnt = ws->G[p + 1] - ws->G[p];
+        w_avg[p] = cnt > 0 ? lo + (double(ws->sum[p]) / scale) / double(cnt) : 0.0;
+        first[p] = ws->G[p];
+    }
 }
 
 // The |w| order from a stable sort on the 24-bit keys of k_wkey24 is exact

@@ -110,6 +110,36 @@ def test_imager_wproj_fp64_vs_oracle(ctx, median):
     assert peak_rel(img, ri) < TOL64
 
 
+@pytest.mark.parametrize("case", ["out_of_grid", "planes_beyond_items", "many_planes", "outlier_then_again"])
+def test_imager_wproj_planes_without_sort(case):
+    """The W-planes found without sorting |w| (k_wsel_*) where every visibility is in the grid, and the
+    sorting path it falls back to otherwise: visibilities outside the grid (the reference's begin rule then
+    counts them), more planes than visibilities (empty planes), 300 planes over 3000 visibilities, and a
+    size class whose previous call fell back.  FP64 image within 1e-10 of the oracle, plane supports equal."""
+    fresh = capi.Context(0)
+    try:
+        n, planes = {"out_of_grid": (6000, 6), "planes_beyond_items": (40, 64), "many_planes": (3000, 300),
+                     "outlier_then_again": (6000, 8)}[case]
+        s = _imager_case(57, 256, n, w_range=(-700.0, 700.0))
+        uvw = np.array(s.uvw, order="F")
+        if case == "out_of_grid":
+            uvw[::97, 0] += 1.0e7  # about 1 % outside the grid
+        kw = dict(kernel_func=4, kernel_support=3, kernel_exact=False, oversampling=8, analytic_gcf=False,
+                  num_wplanes=planes, max_wpconv_support=8, undersampling_opt=1, kernel_trunc_perc=1.0)
+        calls = [uvw]
+        if case == "outlier_then_again":
+            bad = uvw.copy()
+            bad[::50, 0] += 1.0e7
+            calls = [uvw, bad, bad, uvw]
+        for u in calls:
+            img, _, info = fresh.image_visibilities(s.vis, s.weights, u, 256, s.cell_size, **kw)
+            ri, _, g = orc.image_visibilities(s.vis, s.weights, u, 256, s.cell_size, return_grid=True, **kw)
+            assert info.max_plane_support == max(g.plane_supports)
+            assert peak_rel(img, ri) < TOL64
+    finally:
+        fresh.close()
+
+
 def test_imager_wproj_untruncated(ctx):
     s = _imager_case(33, 128, 3000, w_range=(-3000.0, 3000.0))
     kw = dict(kernel_func=5, kernel_support=3, kernel_exact=False, oversampling=4, analytic_gcf=True,
