@@ -1915,6 +1915,10 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         b.n = x.n_vis;
         b.image = x.image;
         b.cls = size_class(b.s, precision) + "/batch";
+        // W-planes without the |w| sort where they apply (as in single calls)
+        b.s.wsel = b.s.nplanes > 0 && b.s.nplanes <= WSEL_MAXP && !b.s.wmedian && b.s.ntimesteps == 0
+            && x.n_vis < (int64_t(1) << 31) && !c->wsel_off.count(b.cls);
+        put(&b.s.wsel, sizeof(b.s.wsel));
         put(&x.pars, sizeof(x.pars));
         put(&x.wproj, sizeof(x.wproj));
         put(&x.n_vis, sizeof(x.n_vis));
@@ -2055,15 +2059,23 @@ void run_batch(stpgpu_context* c, const stpgpu_snapshot* sn, int nb, int precisi
         }
     }
     STPGPU_CUDA_TRY(cudaStreamSynchronize(main));
-    bool redo = false;
-    for (int i = 0; i < nb; i++)
-        if (scal[i].err & 4u) { // long run of distinct |w| in the 32-bit sort: redo with the 64-bit sort
-            B[i].s.full_wsort = 1;
-            redo = true;
+    for (int round = 0; round < 2; round++) {
+        bool redo = false;
+        for (int i = 0; i < nb; i++) {
+            if (scal[i].err & 16u) { // the W-planes without the sort did not apply: the sorting path
+                B[i].s.wsel = 0;
+                c->wsel_off.insert(B[i].cls);
+                redo = true;
+            } else if (scal[i].err & 4u) { // long run of distinct |w| in the 24-bit sort: the 64-bit sort
+                B[i].s.full_wsort = 1;
+                redo = true;
+            }
         }
-    if (redo) {
+        if (!redo)
+            break;
         c->drop_graph();
         c->batch_calls = 0;
+        c->batch_sig.clear();
         STPGPU_CUDA_TRY(cudaEventRecord(c->ev0, main));
         glaunch = batch_enqueue<R, COMP>(c, B, out_f32, device_ptrs, false, scal, hparams, nullptr);
         STPGPU_CUDA_TRY(cudaEventRecord(c->ev1, main));
