@@ -641,6 +641,9 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         zero_words(st, { { ws, int64_t(kWselZeroWords) } });
         k_wsel_hist<<<std::min<unsigned>(grid1d(n, 256), 148 * 4), 256, 0, st>>>(key24, n, ws);
         STPGPU_CHECK_LAUNCH();
+        static_assert(WSEL_BINS == 1024 * 64, "chunks of 64 bins, 32 a block");
+        k_wsel_chunks<<<32, 1024, 0, st>>>(ws);
+        STPGPU_CHECK_LAUNCH();
         k_wsel_plan<<<1, 1024, 0, st>>>(ws, n, P, g.d_ngood, g.d_err);
         STPGPU_CHECK_LAUNCH();
         // members of the start bins: at most P - 1 bins of WSEL_CAP

@@ -2193,6 +2193,7 @@ struct WselState {
     int32_t start_list[WSEL_MAXP];  // per plane p >= 1: its start item's list
     uint32_t start_rank[WSEL_MAXP]; // and rank within the list's bin
     uint32_t start_bin[WSEL_MAXP];
+    uint32_t chunk_tot[1024];       // bins per 64-bin chunk (k_wsel_chunks)
     unsigned long long start_bits[WSEL_MAXP]; // the start item: |w| bits, input index
     uint32_t start_idx[WSEL_MAXP];
     int64_t G[WSEL_MAXP + 1];
@@ -2240,12 +2241,23 @@ __device__ __forceinline__ uint32_t wsel_block_scan(uint32_t v, uint32_t* total)
     return r;
 }
 
+// Totals of the 1024 chunks of 64 bins, one warp a chunk (coalesced).
+__global__ void __launch_bounds__(1024) k_wsel_chunks(WselState* ws)
+{
+    const int c = blockIdx.x * 32 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    const uint2 v = reinterpret_cast<const uint2*>(ws->hist + 64 * c)[lane];
+    uint32_t t = v.x + v.y;
+    for (int o = 16; o > 0; o >>= 1)
+        t += __shfl_down_sync(0xffffffffu, t, o);
+    if (lane == 0)
+        ws->chunk_tot[c] = t;
+}
+
 // One block of 1024 threads.  The plane starts have a closed form: with q =
 // n / P and r = n % P, ceil((n - G_p) / (P - p)) = q + [p < r], so G_p = p q +
-// min(p, r).  Thread t sums bins [64 t, 64 t + 64) (16-byte loads); a block
-// scan of those totals locates each start rank's chunk, and the plane's
-// thread walks the chunk's 64 bins to the bin and the rank within it.  The
-// start bins become lists in plane order.
+// min(p, r).  A block scan of the chunk totals (k_wsel_chunks) locates each
+// start rank's chunk, and the plane's thread walks the chunk's 64 bins to the
+// bin and the rank within it.  The start bins become lists in plane order.
 __global__ void __launch_bounds__(1024) k_wsel_plan(WselState* ws, int64_t n, int P, const unsigned long long* ngood,
     unsigned int* err)
 {
@@ -2253,13 +2265,7 @@ __global__ void __launch_bounds__(1024) k_wsel_plan(WselState* ws, int64_t n, in
     __shared__ uint32_t chunk[1025]; // prefix at each thread's first bin
     const int tid = threadIdx.x;
     const bool ok0 = ngood[0] == (unsigned long long)n && P >= 1 && P <= WSEL_MAXP;
-    const uint4* h4 = reinterpret_cast<const uint4*>(ws->hist + PER * tid);
-    uint32_t t = 0;
-#pragma unroll
-    for (int q = 0; q < PER / 4; q++) {
-        const uint4 v = h4[q];
-        t += v.x + v.y + v.z + v.w;
-    }
+    const uint32_t t = ws->chunk_tot[tid];
     uint32_t total = 0;
     const uint32_t excl = wsel_block_scan(t, &total);
     chunk[tid] = excl;
