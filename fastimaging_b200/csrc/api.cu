@@ -584,7 +584,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
     pp.ngood_part = npart;
     pp.absw_key = wproj ? c->buf<double>("absw", nn) : nullptr;
     pp.wmax_part = (wproj && !s.full_wsort) ? c->buf<double>("wmaxpart", 2 * size_t(nb_pre)) : nullptr;
-    pp.iota = wproj ? c->buf<uint32_t>("perm_in", nn) : nullptr;
+    pp.iota = (wproj && !s.wsel) ? c->buf<uint32_t>("perm_in", nn) : nullptr;
     pp.w_out = nullptr;
     if (n > 0) {
         k_prepass<R><<<nb_pre, GRID_THREADS, 0, st>>>(pp, items);
@@ -633,13 +633,10 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         // condition it cannot meet sets error bit 16 and the caller grids
         // again on the sorting path
         const int P = s.nplanes;
-        uint32_t* key24 = c->buf<uint32_t>("absw24", nn);
         const unsigned g2 = std::min<unsigned>(grid1d(n, 256), 148 * 8);
-        k_wkey24<<<g2, 256, 0, st>>>(pp.absw_key, n, g.d_total, key24);
-        STPGPU_CHECK_LAUNCH();
         WselState* ws = c->buf<WselState>("wsel", 1);
         zero_words(st, { { ws, int64_t(kWselZeroWords) } });
-        k_wsel_hist<<<std::min<unsigned>(grid1d(n, 256), 148 * 4), 256, 0, st>>>(key24, n, ws);
+        k_wsel_hist<<<std::min<unsigned>(grid1d(n, 256), 148 * 4), 256, 0, st>>>(pp.absw_key, n, g.d_total, ws);
         STPGPU_CHECK_LAUNCH();
         static_assert(WSEL_BINS == 1024 * 64, "chunks of 64 bins, 32 a block");
         k_wsel_chunks<<<32, 1024, 0, st>>>(ws);
@@ -649,7 +646,7 @@ GridOut run_gridder(stpgpu_context* c, const ImagerSetup& s, const void* d_vis, 
         // members of the start bins: at most P - 1 bins of WSEL_CAP
         unsigned long long* mbits = c->buf<unsigned long long>("wsel_mb", size_t(std::max(P - 1, 1)) * WSEL_CAP);
         uint32_t* midx = c->buf<uint32_t>("wsel_mi", size_t(std::max(P - 1, 1)) * WSEL_CAP);
-        k_wsel_collect<<<g2, 256, 0, st>>>(key24, pp.absw_key, n, ws, mbits, midx);
+        k_wsel_collect<<<g2, 256, 0, st>>>(pp.absw_key, n, g.d_total, ws, mbits, midx);
         STPGPU_CHECK_LAUNCH();
         if (P > 1) {
             k_wsel_resolve<<<P - 1, 256, 0, st>>>(ws, mbits, midx);

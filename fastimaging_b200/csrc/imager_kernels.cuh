@@ -250,13 +250,17 @@ __global__ void k_finish_wsum(const double* part, const unsigned long long* npar
 //    exponents from 2^-31 to 1 and 19 mantissa bits: relative resolution
 //    2^-19 at every scale).
 // Non-finite |w| (NaN included) take 2^24 - 1, above every finite key.
-__global__ void k_wkey24(const double* __restrict__ absw, int64_t n, const double* total, uint32_t* __restrict__ key)
-{
-    const double wmax = total[1];
-    const double r = wmax > 0.0 ? 1.0 / wmax : 0.0;
-    const bool spread = wmax > 0.0 && total[2] >= wmax * 0.0625 * double(n);
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const double a = absw[i];
+struct WKey {
+    double wmax, r;
+    bool spread;
+    __device__ WKey(const double* total, int64_t n)
+    {
+        wmax = total[1];
+        r = wmax > 0.0 ? 1.0 / wmax : 0.0;
+        spread = wmax > 0.0 && total[2] >= wmax * 0.0625 * double(n);
+    }
+    __device__ __forceinline__ uint32_t operator()(double a) const
+    {
         uint32_t k = 0xFFFFFFu;
         if (a <= wmax) {
             if (spread) {
@@ -267,8 +271,15 @@ __global__ void k_wkey24(const double* __restrict__ absw, int64_t n, const doubl
                 k = (__float_as_uint(x) - 0x30000000u) >> 4;
             }
         }
-        key[i] = k;
+        return k;
     }
+};
+
+__global__ void k_wkey24(const double* __restrict__ absw, int64_t n, const double* total, uint32_t* __restrict__ key)
+{
+    const WKey kf(total, n);
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        key[i] = kf(absw[i]);
 }
 
 // Zeroes up to four ranges of 32-bit words (one launch instead of several
@@ -2201,10 +2212,13 @@ struct WselState {
 };
 constexpr size_t kWselZeroWords = (sizeof(uint32_t) * (WSEL_BINS + WSEL_MAXP) + sizeof(unsigned long long) * WSEL_MAXP) / 4;
 
-__global__ void __launch_bounds__(256) k_wsel_hist(const uint32_t* __restrict__ key24, int64_t n, WselState* ws)
+// (the keys of k_wkey24, formed here and again in k_wsel_collect from |w|)
+__global__ void __launch_bounds__(256) k_wsel_hist(const double* __restrict__ absw, int64_t n, const double* total,
+    WselState* ws)
 {
+    const WKey kf(total, n);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-        atomicAdd(&ws->hist[key24[i] >> (24 - WSEL_BINS_LOG)], 1u);
+        atomicAdd(&ws->hist[kf(absw[i]) >> (24 - WSEL_BINS_LOG)], 1u);
     // no start bins yet (k_wsel_plan marks them)
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < WSEL_BINS; b += gridDim.x * blockDim.x)
         ws->binmap[b] = -1;
@@ -2357,16 +2371,18 @@ __global__ void __launch_bounds__(1024) k_wsel_plan(WselState* ws, int64_t n, in
     }
 }
 
-__global__ void __launch_bounds__(256) k_wsel_collect(const uint32_t* __restrict__ key24, const double* __restrict__ absw,
-    int64_t n, WselState* ws, unsigned long long* mbits, uint32_t* midx)
+__global__ void __launch_bounds__(256) k_wsel_collect(const double* __restrict__ absw, int64_t n, const double* total,
+    WselState* ws, unsigned long long* mbits, uint32_t* midx)
 {
     if (!ws->valid)
         return;
+    const WKey kf(total, n);
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
-        const int li = ws->binmap[key24[i] >> (24 - WSEL_BINS_LOG)];
+        const double a = absw[i];
+        const int li = ws->binmap[kf(a) >> (24 - WSEL_BINS_LOG)];
         if (li >= 0) {
             const uint32_t pos = ws->list_off[li] + atomicAdd(&ws->cursor[li], 1u);
-            mbits[pos] = __double_as_longlong(absw[i]);
+            mbits[pos] = __double_as_longlong(a);
             midx[pos] = uint32_t(i);
         }
     }
