@@ -664,7 +664,11 @@ struct __align__(16) Acc<float, 1> {
     float2 s, c;
 };
 
-// Knuth's TwoSum error term with explicit rounding (no contraction).
+// Knuth's TwoSum error term with explicit rounding (no contraction).  It is
+// exact whatever the magnitudes: Dekker's cheaper Fast2Sum needs |s| >= |x|,
+// which fails throughout a cell whose running sum cancels, and there it
+// loses about one rounding of each term (enough to move a 256^2 PSWF image
+// by 3e-5 of its peak with the order of the updates).
 __device__ __forceinline__ float two_sum_err(float a, float b, float s)
 {
     const float bb = __fsub_rn(s, a);
@@ -1600,12 +1604,13 @@ __device__ __forceinline__ bool grid_tile_recs(const GridParams<R>& p, int tile,
         const TapRec<R>* rb = rbuf + (c & 1) * kRecChunk;
         const int ne = min(kRecChunk, int(cnt) - c * kRecChunk);
         // an entry decoded once: window shape, divisor magic, first cell,
-        // kernel offsets and the weighted visibility
+        // kernel offsets and the weighted visibility (pvr, pvi: its parts
+        // negated when the W-kernel is conjugated, so that the product
+        // needs no per-tap sign)
         struct Ent {
             int nrows, nt, sbase, K;
             uint32_t m, koff, ky, kx;
-            bool conj;
-            R vr, vi;
+            R vr, vi, pvr, pvi;
         };
         auto decode = [&](const TapRec<R>& r) {
             Ent x;
@@ -1615,29 +1620,30 @@ __device__ __forceinline__ bool grid_tile_recs(const GridParams<R>& p, int tile,
             x.m = c_div_magic[x.nrows];
             x.sbase = int((g >> 5) & 31u) * TILE_R + int(g & 31u);
             x.K = int(g >> 23);
-            x.conj = (g >> 22) & 1u;
+            const bool conj = (g >> 22) & 1u;
             x.koff = r.koff;
             x.ky = r.koff >> 16;
             x.kx = r.koff & 0xffffu;
             x.vr = r.vr;
             x.vi = r.vi;
+            x.pvr = conj ? -r.vr : r.vr;
+            x.pvi = conj ? -r.vi : r.vi;
             return x;
         };
         // tap t of an entry: its accumulator cell and weighted value
         auto tap = [&](const Ent& x, int t, int& cell, R& re, R& im) {
             const int dj = int((uint32_t(t) * x.m) >> 16);
             const int di = t - dj * x.nrows;
-            R kr, ki;
             if (KMODE == KM_WPROJ) {
+                // (vr + i vi)(kr + i ki), ki = -v.y for a conjugated kernel
                 const C2 v = __ldg(&p.wk[x.koff + uint32_t(di * x.K + dj)]);
-                kr = v.x;
-                ki = x.conj ? -v.y : v.y;
+                re = x.vr * R(v.x) - x.pvi * R(v.y);
+                im = x.pvr * R(v.y) + x.vi * R(v.x);
             } else {
-                kr = tab[x.ky + uint32_t(di)] * tab[x.kx + uint32_t(dj)];
-                ki = R(0);
+                const R kr = tab[x.ky + uint32_t(di)] * tab[x.kx + uint32_t(dj)];
+                re = x.vr * kr;
+                im = x.vi * kr;
             }
-            re = x.vr * kr - x.vi * ki;
-            im = x.vr * ki + x.vi * kr;
             cell = x.sbase + dj * TILE_R + di;
         };
         // two single-pass entries at a time where possible: both kernel
