@@ -664,17 +664,6 @@ struct __align__(16) Acc<float, 1> {
     float2 s, c;
 };
 
-// Knuth's TwoSum error term with explicit rounding (no contraction).  It is
-// exact whatever the magnitudes: Dekker's cheaper Fast2Sum needs |s| >= |x|,
-// which fails throughout a cell whose running sum cancels, and there it
-// loses about one rounding of each term (enough to move a 256^2 PSWF image
-// by 3e-5 of its peak with the order of the updates).
-__device__ __forceinline__ float two_sum_err(float a, float b, float s)
-{
-    const float bb = __fsub_rn(s, a);
-    return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
-}
-
 __device__ __forceinline__ void acc_rmw(Acc<double, 0>* a, double re, double im)
 {
     double2 v = a->s;
@@ -689,15 +678,51 @@ __device__ __forceinline__ void acc_rmw(Acc<float, 0>* a, float re, float im)
     v.y += im;
     a->s = v;
 }
+// Packed single-precision pairs (sm_100 f32x2: one instruction rounds both
+// halves, each as its scalar form would).
+__device__ __forceinline__ unsigned long long f2_pack(float x, float y)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+    return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long r)
+{
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long f2_sub(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// FP32C update: t = s + x and Knuth's TwoSum error term
+// e = (s - (t - bb)) + (x - bb), bb = t - s, added to c, with explicit
+// rounding (no contraction), the real and imaginary parts side by side in
+// seven packed adds.  TwoSum is exact whatever the magnitudes: Dekker's
+// cheaper Fast2Sum needs |s| >= |x|, which fails throughout a cell whose
+// running sum cancels, and there it loses about one rounding of each term
+// (enough to move a 256^2 PSWF image by 3e-5 of its peak with the order of
+// the updates).
 __device__ __forceinline__ void acc_rmw(Acc<float, 1>* a, float re, float im)
 {
-    Acc<float, 1> v = *a;
-    const float sx = __fadd_rn(v.s.x, re), sy = __fadd_rn(v.s.y, im);
-    v.c.x = __fadd_rn(v.c.x, two_sum_err(v.s.x, re, sx));
-    v.c.y = __fadd_rn(v.c.y, two_sum_err(v.s.y, im, sy));
-    v.s.x = sx;
-    v.s.y = sy;
-    *a = v;
+    const Acc<float, 1> v = *a;
+    const unsigned long long s = f2_pack(v.s.x, v.s.y), x = f2_pack(re, im);
+    const unsigned long long t = f2_add(s, x);
+    const unsigned long long bb = f2_sub(t, s);
+    const unsigned long long e = f2_add(f2_sub(s, f2_sub(t, bb)), f2_sub(x, bb));
+    Acc<float, 1> w;
+    w.s = f2_unpack(t);
+    w.c = f2_unpack(f2_add(f2_pack(v.c.x, v.c.y), e));
+    *a = w;
 }
 template <typename R, int COMP>
 __device__ __forceinline__ void acc_zero(Acc<R, COMP>* a)
