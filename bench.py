@@ -798,27 +798,83 @@ def run_profile_calls(args):
             dv = torch.from_numpy(s.vis).cuda()
             dw = torch.from_numpy(s.weights).cuda()
             duvw = torch.from_numpy(np.ascontiguousarray(s.uvw.T)).cuda()
+            def call():
+                return ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=prec,
+                                              out_dtype=capi.F64 if prec == capi.FP64 else capi.F32,
+                                              device_ptrs=True, image_out=out, **kw)
+
             for _ in range(args.calls):
-                _, _, info = ctx.image_visibilities(dv, dw, duvw, N, s.cell_size, precision=prec,
-                                                    out_dtype=capi.F64 if prec == capi.FP64 else capi.F32,
-                                                    device_ptrs=True, image_out=out, **kw)
+                _, _, info = call()
             torch.cuda.synchronize()
             print(json.dumps({"section": "imager_call", "cfg": args.cfg, "prec": args.prec,
                               "n_grid_items": int(info.n_grid_items), "max_plane_support": int(info.max_plane_support),
                               "flags": int(info.flags)}))
+            if args.timeline:
+                print_timeline(call)
         else:
             s = syn.config2()
             img, _, _ = ctx.image_visibilities(s.vis, s.weights, s.uvw, 4096, s.cell_size, precision=capi.FP32C,
                                                out_dtype=capi.F32, **syn.CONFIG2_IMAGER)
             dimg = torch.from_numpy(np.asfortranarray(img).reshape(-1, order="F").copy()).cuda()
             lab = torch.empty(4096 * 4096, dtype=torch.int32, device="cuda")
+            def call():
+                return ctx.source_find(dimg, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5,
+                                       device_ptrs=True, rows=4096, cols=4096, label_out=lab)
+
             for _ in range(args.calls):
-                isl, _, info = ctx.source_find(dimg, 5.0, 3.0, 0.0, True, 5, capi.BINAPPROX, False, False, True, 5,
-                                               device_ptrs=True, rows=4096, cols=4096, label_out=lab)
+                isl, _, info = call()
             torch.cuda.synchronize()
             print(json.dumps({"section": "sf_call", "islands": len(isl)}))
+            if args.timeline:
+                print_timeline(call)
     finally:
         ctx.close()
+
+
+def print_timeline(call):
+    """Device timeline of one warm call (after the calls above, so a repeated device-pointer call replays its
+    CUDA graph), recorded by the CUDA activity API through torch.profiler: the L2 is flushed (a 256 MB write)
+    before each of three calls and the last is printed, one JSON line per kernel or copy: start offset, duration
+    and the idle gap before it, in microseconds."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    marks = []
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for _ in range(3):
+            flush.zero_()
+            torch.cuda.synchronize()
+            call()
+            torch.cuda.synchronize()
+    with tempfile.TemporaryDirectory() as td:
+        fn = os.path.join(td, "trace.json")
+        prof.export_chrome_trace(fn)
+        with open(fn) as f:
+            tr = json.load(f)
+    ev = [e for e in tr["traceEvents"]
+          if e.get("ph") == "X" and e.get("cat") in ("kernel", "gpu_memcpy", "gpu_memset")]
+    ev.sort(key=lambda e: e["ts"])
+    calls, cur = [], []
+    for e in ev:  # the flush kernels separate the calls
+        if "at::native" in e["name"] or "FillFunctor" in e["name"]:
+            if cur:
+                calls.append(cur)
+            cur = []
+            continue
+        cur.append(e)
+    if cur:
+        calls.append(cur)
+    last = calls[-1]
+    t0 = last[0]["ts"]
+    prev = t0
+    for e in last:
+        marks.append({"kernel": e["name"][:100], "start_us": round(e["ts"] - t0, 1), "us": round(e["dur"], 1),
+                      "gap_us": round(e["ts"] - prev, 1)})
+        prev = max(prev, e["ts"] + e["dur"])
+    for m in marks:
+        print(json.dumps(m))
+    print(json.dumps({"span_us": round(prev - t0, 1), "launches": len(last)}))
 
 
 def main():
@@ -838,6 +894,8 @@ def main():
     ap.add_argument("--prec", choices=["fp64", "fp32", "fp32c"], default="fp32c", help="imager_call: precision")
     ap.add_argument("--trunc", type=float, default=None, help="imager_call: W-kernel truncation percentage")
     ap.add_argument("--calls", type=int, default=2, help="imager_call / sf_call: number of calls")
+    ap.add_argument("--timeline", action="store_true",
+                    help="imager_call / sf_call: then print the device timeline of one warm call")
     args = ap.parse_args()
     if args.section in ("imager_call", "sf_call"):
         run_profile_calls(args)
