@@ -257,6 +257,7 @@ struct stpgpu_context {
         batch_graph = nullptr;
     }
     void* pinned = nullptr;
+    void* pinned_dev = nullptr; // the device's address of the staging area (mapped)
     size_t pinned_cap = 0;
     std::map<std::string, std::string> memo_keys; // buffer name -> key of its current contents
     // staged gridder: records per visibility last counted, per namespace,
@@ -320,14 +321,26 @@ struct stpgpu_context {
                 cudaFreeHost(pinned);
             }
             pinned = nullptr;
+            pinned_dev = nullptr;
             pinned_cap = 0;
             const auto t0 = std::chrono::steady_clock::now();
             buf_gen++;
-            STPGPU_CUDA_TRY(cudaMallocHost(&pinned, bytes));
+            STPGPU_CUDA_TRY(cudaHostAlloc(&pinned, bytes, cudaHostAllocMapped));
+            STPGPU_CUDA_TRY(cudaHostGetDevicePointer(&pinned_dev, pinned, 0));
             log_alloc("page-locked stage", ns, bytes, t0);
             pinned_cap = bytes;
         }
         return reinterpret_cast<T*>(pinned);
+    }
+
+    // The device's address of a location in the staging area: kernels write
+    // a call's results there directly (a kernel node in place of a copy node
+    // in the captured graphs).
+    template <typename T>
+    T* host_stage_dev(T* h) const
+    {
+        return reinterpret_cast<T*>(static_cast<unsigned char*>(pinned_dev)
+            + (reinterpret_cast<unsigned char*>(h) - static_cast<unsigned char*>(pinned)));
     }
 
     // One plan per (size, type, stream): a plan's work area must not be
@@ -1167,13 +1180,11 @@ struct ScalarsBack {
 
 ScalarsBack read_back(stpgpu_context* c, const GridOut& g)
 {
-    // one copy of the packed scalars instead of one per scalar
-    ScalarPack* d = c->buf<ScalarPack>("scalar_pack", 1);
-    k_pack_scalars<<<1, 32, 0, c->stream>>>(g.d_total, g.d_ngood, g.d_nitems, g.d_err, g.d_plane_support,
-        g.nplanes > 0 ? g.nplanes : 0, d);
-    STPGPU_CHECK_LAUNCH();
+    // the scalars packed by one kernel straight into the page-locked stage
     ScalarPack* h = c->host_stage<ScalarPack>(1);
-    STPGPU_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(ScalarPack), cudaMemcpyDeviceToHost, c->stream));
+    k_pack_scalars<<<1, 32, 0, c->stream>>>(g.d_total, g.d_ngood, g.d_nitems, g.d_err, g.d_plane_support,
+        g.nplanes > 0 ? g.nplanes : 0, c->host_stage_dev(h));
+    STPGPU_CHECK_LAUNCH();
     STPGPU_CUDA_TRY(cudaStreamSynchronize(c->stream));
     ScalarsBack r { h->total, h->ngood, h->nitems, h->err, h->max_support };
     // bit 4: the 32-bit |w| sort met a long run of distinct |w| (the caller
@@ -2535,9 +2546,19 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
     unsigned char* hb = c->host_stage<unsigned char>(sizeof(SfState) + 64 + sizeof(IslandRaw) * size_t(kFirst));
     SfState* hstate = reinterpret_cast<SfState*>(hb);
     IslandRaw* hfirst = reinterpret_cast<IslandRaw*>(hb + ((sizeof(SfState) + 63) / 64) * 64);
+    // the state and the first island records (as many as the call found, up
+    // to kFirst) written by one kernel straight into the page-locked stage
+    static_assert(sizeof(SfState) % 4 == 0 && (sizeof(IslandRaw) * kFirst) % 16 == 0, "copy-out units");
+    auto enqueue_copy_out = [&] {
+        k_copy_out<<<unsigned((sizeof(IslandRaw) * kFirst / 16 + 255) / 256), 256, 0, st>>>(
+            reinterpret_cast<const uint32_t*>(sfs), c->host_stage_dev(reinterpret_cast<uint32_t*>(hstate)),
+            int(sizeof(SfState) / 4), reinterpret_cast<const uint4*>(raw),
+            c->host_stage_dev(reinterpret_cast<uint4*>(hfirst)), int(sizeof(IslandRaw) * kFirst / 16),
+            int(offsetof(SfState, misc) / 4) + 5, int(sizeof(IslandRaw)));
+        STPGPU_CHECK_LAUNCH();
+    };
     auto read_back_state = [&] {
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hstate, sfs, sizeof(SfState), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * kFirst, cudaMemcpyDeviceToHost, st));
+        enqueue_copy_out();
         STPGPU_CUDA_TRY(cudaStreamSynchronize(st));
     };
     size_buffers();
@@ -2548,8 +2569,7 @@ void run_source_find(stpgpu_context* c, const T* d_img, int rows, int cols, cons
         STPGPU_CUDA_TRY(ccl_enqueue<T>(st, d_img, geom, sfs->st.thr, 0.0, 0.0, p.find_negative_sources,
             p.ccl_4connectivity, slice, cb));
         enqueue_analysis();
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hstate, sfs, sizeof(SfState), cudaMemcpyDeviceToHost, st));
-        STPGPU_CUDA_TRY(cudaMemcpyAsync(hfirst, raw, sizeof(IslandRaw) * kFirst, cudaMemcpyDeviceToHost, st));
+        enqueue_copy_out();
     };
     // The first attempt of a call identical to the previous one (same
     // buffers, sizes, parameters and capacities, no reallocation since)

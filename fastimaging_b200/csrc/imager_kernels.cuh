@@ -3058,6 +3058,23 @@ struct ScalarPack {
     int pad;
 };
 
+// Copies of a call's results into page-locked host memory through its device
+// address: the na words of a, then the 16-byte units of b that hold the
+// first a[count_word] records of rec_bytes each (all nb units when
+// count_word < 0), at most nb.
+__global__ void k_copy_out(const uint32_t* a, uint32_t* ha, int na, const uint4* b, uint4* hb, int nb,
+    int count_word, int rec_bytes)
+{
+    const int t = int(blockIdx.x * blockDim.x + threadIdx.x), stride = int(gridDim.x * blockDim.x);
+    for (int i = t; i < na; i += stride)
+        ha[i] = a[i];
+    int n = nb;
+    if (count_word >= 0)
+        n = int(min((uint64_t(a[count_word]) * uint64_t(rec_bytes) + 15) / 16, uint64_t(nb)));
+    for (int i = t; i < n; i += stride)
+        hb[i] = b[i];
+}
+
 __global__ void k_pack_scalars(const double* total, const unsigned long long* ngood, const uint32_t* nitems,
     const unsigned int* err, const int* sup, int nsup, ScalarPack* out)
 {
